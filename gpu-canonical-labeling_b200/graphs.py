@@ -1,0 +1,366 @@
+"""Graph model, DIMACS-style I/O, seeded generators and the ragged CSR arena.
+
+The in-memory graph is the reference's ``CSRGraph`` (CSRGraph.h:6-39):
+``rowptr[n+1]`` / ``col[2m]`` int32 with both directions stored, every row
+sorted ascending, no self loops, plus ``color[n]`` int32 (0 = uncoloured).
+
+``read_dimacs`` follows ``CSRGraph::fromDIMACS`` (CSRGraph.cpp:40-119)
+line for line in behaviour: ``c`` lines and empty lines are skipped, ``p``
+sets the vertex count (the edge count on that line is ignored), ``n v c``
+sets a colour (1-based, vertex 0 ignored, out-of-range ignored), ``e u v``
+is 1-based, self loops are dropped and both directions are inserted.  The
+reference keeps duplicate ``e`` lines as parallel edges, which its
+refinement does not handle (partition_refinement.cpp:296-303 assumes a
+singleton splitter yields counts in {0, 1}); this module reports them as
+``ValueError`` instead of producing undefined output.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+from typing import Iterable, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+
+@dataclass
+class Graph:
+    """Undirected, optionally vertex-coloured graph in CSR form."""
+
+    n: int
+    rowptr: np.ndarray  # int32[n+1]
+    col: np.ndarray  # int32[2m]
+    color: Optional[np.ndarray] = None  # int32[n] or None (all zero)
+
+    @property
+    def m(self) -> int:
+        return int(self.rowptr[-1]) // 2
+
+    def edges(self) -> np.ndarray:
+        """Undirected edge list (u < v), shape (m, 2), lexicographic order."""
+        src = np.repeat(np.arange(self.n, dtype=np.int32), np.diff(self.rowptr))
+        mask = src < self.col
+        return np.stack([src[mask], self.col[mask]], axis=1)
+
+    def colors(self) -> np.ndarray:
+        if self.color is None:
+            return np.zeros(self.n, dtype=np.int32)
+        return self.color
+
+    def adjacency(self) -> np.ndarray:
+        """Dense n x n uint8 adjacency matrix."""
+        a = np.zeros((self.n, self.n), dtype=np.uint8)
+        src = np.repeat(np.arange(self.n), np.diff(self.rowptr))
+        a[src, self.col] = 1
+        return a
+
+
+def from_edges(n: int, edges: Iterable[Tuple[int, int]] | np.ndarray,
+               color: Optional[Sequence[int]] = None) -> Graph:
+    """Build the CSR the way CSRGraph::fromDIMACS does (0-based edges)."""
+    e = np.asarray(list(edges) if not isinstance(edges, np.ndarray) else edges,
+                   dtype=np.int64).reshape(-1, 2)
+    if e.size and (e.min() < 0 or e.max() >= n):
+        raise ValueError("edge endpoint out of range")
+    e = e[e[:, 0] != e[:, 1]]  # self loops dropped (CSRGraph.cpp:74)
+    both = np.concatenate([e, e[:, ::-1]], axis=0)
+    order = np.lexsort((both[:, 1], both[:, 0]))
+    both = both[order]
+    if len(both) > 1:
+        dup = np.all(both[1:] == both[:-1], axis=1)
+        if dup.any():
+            raise ValueError("duplicate edge (parallel edges are not supported)")
+    deg = np.bincount(both[:, 0], minlength=n) if len(both) else np.zeros(n, np.int64)
+    rowptr = np.zeros(n + 1, dtype=np.int32)
+    np.cumsum(deg, out=rowptr[1:])
+    col = both[:, 1].astype(np.int32)
+    c = None
+    if color is not None:
+        c = np.asarray(color, dtype=np.int32).copy()
+        if c.shape != (n,):
+            raise ValueError("color must have n entries")
+        if not c.any():
+            c = None
+    return Graph(n, rowptr, col, c)
+
+
+def parse_dimacs(text: str) -> Graph:
+    """Parse DIMACS-like text with CSRGraph::fromDIMACS semantics."""
+    n = 0
+    edges: List[Tuple[int, int]] = []
+    colors: List[Tuple[int, int]] = []
+    for line in text.splitlines():
+        if not line or line[0] == "c":
+            continue
+        tok = line.split()
+        if not tok:
+            continue
+        t = tok[0][0]
+        if t == "p":
+            n = int(tok[2])
+        elif t == "n":
+            vid, col = int(tok[1]), int(tok[2])
+            if vid == 0:
+                continue
+            colors.append((vid - 1, col))
+        elif t == "e":
+            u, v = int(tok[1]), int(tok[2])
+            if u == v:
+                continue
+            edges.append((u - 1, v - 1))
+    color = np.zeros(n, dtype=np.int32)
+    for v, c in colors:
+        if v < n:
+            color[v] = c
+    return from_edges(n, edges, color)
+
+
+def read_dimacs(path: str) -> Graph:
+    with open(path, "r") as f:
+        return parse_dimacs(f.read())
+
+
+def to_dimacs(g: Graph) -> str:
+    e = g.edges()
+    out = [f"p edge {g.n} {len(e)}"]
+    if g.color is not None:
+        out += [f"n {v + 1} {int(c)}" for v, c in enumerate(g.color) if c != 0]
+    out += [f"e {u + 1} {v + 1}" for u, v in e]
+    return "\n".join(out) + "\n"
+
+
+def write_dimacs(g: Graph, path: str) -> None:
+    with open(path, "w") as f:
+        f.write(to_dimacs(g))
+
+
+def relabel(g: Graph, perm: np.ndarray) -> Graph:
+    """Graph with vertex v renamed perm[v] (colours move with vertices)."""
+    perm = np.asarray(perm, dtype=np.int64)
+    e = g.edges()
+    ne = perm[e] if len(e) else e
+    col = None
+    if g.color is not None:
+        col = np.zeros(g.n, dtype=np.int32)
+        col[perm] = g.color
+    return from_edges(g.n, ne, col)
+
+
+def random_relabel(g: Graph, rng: np.random.Generator) -> Graph:
+    return relabel(g, rng.permutation(g.n))
+
+
+# --------------------------------------------------------------------------
+# Seeded generators for the benchmark workloads.
+# --------------------------------------------------------------------------
+
+def erdos_renyi(n: int, p: float, rng: np.random.Generator) -> Graph:
+    iu, ju = np.triu_indices(n, 1)
+    keep = rng.random(len(iu)) < p
+    return from_edges(n, np.stack([iu[keep], ju[keep]], axis=1))
+
+
+def move_one_edge(g: Graph, rng: np.random.Generator) -> Graph:
+    """Copy with one random edge moved to a random non-edge."""
+    e = g.edges().tolist()
+    adj = set(map(tuple, e))
+    k = int(rng.integers(len(e)))
+    del e[k]
+    while True:
+        u, v = sorted(int(x) for x in rng.choice(g.n, 2, replace=False))
+        if (u, v) not in adj:
+            break
+    e.append((u, v))
+    return from_edges(g.n, e, g.color)
+
+
+def random_regular(n: int, d: int, rng: np.random.Generator,
+                   max_tries: int = 10000) -> Graph:
+    """Configuration model, rejected until simple."""
+    if (n * d) % 2:
+        raise ValueError("n*d must be even")
+    stubs = np.repeat(np.arange(n), d)
+    for _ in range(max_tries):
+        p = rng.permutation(stubs).reshape(-1, 2)
+        if np.any(p[:, 0] == p[:, 1]):
+            continue
+        a = np.sort(p, axis=1)
+        key = a[:, 0].astype(np.int64) * n + a[:, 1]
+        if len(np.unique(key)) != len(key):
+            continue
+        return from_edges(n, a)
+    raise RuntimeError("configuration model did not produce a simple graph")
+
+
+def torus(k1: int, k2: Optional[int] = None) -> Graph:
+    """Toroidal grid C_k1 x C_k2 (k >= 3)."""
+    k2 = k1 if k2 is None else k2
+    e = []
+    for i in range(k1):
+        for j in range(k2):
+            v = i * k2 + j
+            e.append((v, i * k2 + (j + 1) % k2))
+            e.append((v, ((i + 1) % k1) * k2 + j))
+    e = np.array([(min(a, b), max(a, b)) for a, b in e])
+    e = np.unique(e, axis=0)
+    return from_edges(k1 * k2, e)
+
+
+def disjoint_union(g: Graph, k: int) -> Graph:
+    e = g.edges()
+    parts = [e + i * g.n for i in range(k)]
+    col = None if g.color is None else np.tile(g.color, k)
+    return from_edges(g.n * k, np.concatenate(parts) if len(e) else e, col)
+
+
+def prufer_tree(n: int, rng: np.random.Generator, max_deg: int = 4) -> List[Tuple[int, int]]:
+    """Uniform labelled tree (Pruefer sequence) rejected until max degree <= max_deg."""
+    if n <= 2:
+        return [(0, 1)] if n == 2 else []
+    while True:
+        seq = rng.integers(0, n, n - 2)
+        deg = np.bincount(seq, minlength=n) + 1
+        if deg.max() <= max_deg:
+            break
+    deg = deg.tolist()
+    edges = []
+    import heapq
+    leaves = [v for v in range(n) if deg[v] == 1]
+    heapq.heapify(leaves)
+    for x in seq.tolist():
+        leaf = heapq.heappop(leaves)
+        edges.append((leaf, x))
+        deg[x] -= 1
+        if deg[x] == 1:
+            heapq.heappush(leaves, x)
+    u = heapq.heappop(leaves)
+    v = heapq.heappop(leaves)
+    edges.append((u, v))
+    return edges
+
+
+def tree_plus_edges(n: int, rng: np.random.Generator, max_deg: int = 4,
+                    max_extra: int = 6) -> Graph:
+    """Pruefer tree (max degree 4) plus U{0..max_extra} ring-closing edges
+    drawn uniformly among non-edges that keep the max degree <= max_deg."""
+    edges = [(min(a, b), max(a, b)) for a, b in prufer_tree(n, rng, max_deg)]
+    deg = np.zeros(n, dtype=np.int64)
+    adj = set(edges)
+    for a, b in edges:
+        deg[a] += 1
+        deg[b] += 1
+    extra = int(rng.integers(0, max_extra + 1))
+    for _ in range(extra):
+        free = np.nonzero(deg < max_deg)[0]
+        cand = [(int(a), int(b)) for i, a in enumerate(free) for b in free[i + 1:]
+                if (int(a), int(b)) not in adj]
+        if not cand:
+            break
+        a, b = cand[int(rng.integers(len(cand)))]
+        adj.add((a, b))
+        edges.append((a, b))
+        deg[a] += 1
+        deg[b] += 1
+    return from_edges(n, edges)
+
+
+def small_batch(count: int = 10000, seed: int = 3000, n_lo: int = 10, n_hi: int = 64,
+                relabel_frac: float = 0.2) -> List[Graph]:
+    """Batched small-graph workload: ``count`` graphs, n ~ U[n_lo, n_hi],
+    Pruefer tree (max degree 4) + 0-6 extra edges; ``relabel_frac`` of them
+    are random relabelings of earlier graphs (to exercise deduplication)."""
+    rng = np.random.default_rng(seed)
+    out: List[Graph] = []
+    for i in range(count):
+        if i > 0 and rng.random() < relabel_frac:
+            src = out[int(rng.integers(len(out)))]
+            out.append(random_relabel(src, rng))
+        else:
+            n = int(rng.integers(n_lo, n_hi + 1))
+            out.append(tree_plus_edges(n, rng))
+    return out
+
+
+def mixed_batch(count: int = 2000, seed: int = 4000, n_lo: int = 64,
+                n_hi: int = 4096) -> List[Graph]:
+    """Mixed-size workload: n log-uniform in [n_lo, n_hi], four families in
+    equal shares (ER mean degree 8, random d-regular d in {3,4,6}, toroidal
+    grids, disjoint unions of identical random regular components)."""
+    rng = np.random.default_rng(seed)
+    out: List[Graph] = []
+    for i in range(count):
+        n = int(round(math.exp(rng.uniform(math.log(n_lo), math.log(n_hi)))))
+        fam = i % 4
+        if fam == 0:
+            out.append(erdos_renyi(n, min(1.0, 8.0 / max(n - 1, 1)), rng))
+        elif fam == 1:
+            d = int(rng.choice([3, 4, 6]))
+            if (n * d) % 2:
+                n += 1
+            out.append(random_regular(n, d, rng))
+        elif fam == 2:
+            k1 = max(3, int(round(math.sqrt(n) * rng.uniform(0.7, 1.3))))
+            k2 = max(3, int(round(n / k1)))
+            out.append(torus(k1, k2))
+        else:
+            c = int(rng.choice([8, 10, 12, 16]))
+            d = 3
+            comp = random_regular(c, d, rng)
+            out.append(disjoint_union(comp, max(1, n // c)))
+    return out
+
+
+# --------------------------------------------------------------------------
+# Ragged CSR arena (the batched input format).
+# --------------------------------------------------------------------------
+
+@dataclass
+class Arena:
+    """Many graphs packed back to back.
+
+    Graph g owns vertices ``[voff[g], voff[g+1])`` and CSR entries
+    ``[eoff[g], eoff[g+1])``; its local rowptr (n_g + 1 entries, starting at
+    0) sits at ``rowptr[voff[g] + g : voff[g+1] + g + 1]``.  ``color`` is
+    vertex-indexed like ``voff`` (all zero when uncoloured).
+    """
+
+    count: int
+    voff: np.ndarray  # int64[count+1]
+    eoff: np.ndarray  # int64[count+1]
+    rowptr: np.ndarray  # int32[voff[-1] + count]
+    col: np.ndarray  # int32[eoff[-1]]
+    color: np.ndarray  # int32[voff[-1]]
+
+    def sizes(self) -> np.ndarray:
+        return np.diff(self.voff)
+
+    def graph(self, g: int) -> Graph:
+        a, b = int(self.voff[g]), int(self.voff[g + 1])
+        rp = self.rowptr[a + g: b + g + 1].copy()
+        col = self.col[int(self.eoff[g]): int(self.eoff[g + 1])].copy()
+        c = self.color[a:b].copy()
+        return Graph(b - a, rp, col, c if c.any() else None)
+
+    def out_offsets(self) -> np.ndarray:
+        """Offsets of each graph's n*n output block in a dense output arena."""
+        n = self.sizes()
+        o = np.zeros(self.count + 1, dtype=np.int64)
+        np.cumsum(n * n, out=o[1:])
+        return o
+
+
+def pack(graphs: Sequence[Graph]) -> Arena:
+    count = len(graphs)
+    ns = np.array([g.n for g in graphs], dtype=np.int64)
+    ms = np.array([len(g.col) for g in graphs], dtype=np.int64)
+    voff = np.zeros(count + 1, dtype=np.int64)
+    eoff = np.zeros(count + 1, dtype=np.int64)
+    np.cumsum(ns, out=voff[1:])
+    np.cumsum(ms, out=eoff[1:])
+    rowptr = (np.concatenate([g.rowptr for g in graphs]).astype(np.int32)
+              if count else np.zeros(0, np.int32))
+    col = (np.concatenate([g.col for g in graphs]).astype(np.int32)
+           if count else np.zeros(0, np.int32))
+    color = (np.concatenate([g.colors() for g in graphs]).astype(np.int32)
+             if count else np.zeros(0, np.int32))
+    return Arena(count, voff, eoff, rowptr, col, color)

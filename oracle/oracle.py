@@ -1,0 +1,125 @@
+"""ctypes front-end for the CPU checkers -- TEST INFRASTRUCTURE ONLY.
+
+Two checkers live here:
+
+* ``port``      -- ``libgcl_oracle.so``: the plain-C restatement of the
+                   reference's sequential labeler (canon_oracle.c).
+* ``reference`` -- ``_ref/libgcl_ref.so``: the reference's own sequential
+                   sources (src/sequential.cpp et al.) compiled unchanged by
+                   ``make -C oracle ref``, behind ref_shim.cpp.
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg use
+this module, and only as the checker / the timed CPU baseline.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional, Sequence, Tuple
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PORT_SO = os.path.join(HERE, "libgcl_oracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libgcl_ref.so")
+
+
+class _Stats(ctypes.Structure):
+    _fields_ = [("num_aut", ctypes.c_int64), ("nodes", ctypes.c_int64)]
+
+
+_P = ctypes.c_void_p
+_libs = {}
+
+
+def _load(kind: str):
+    if kind in _libs:
+        return _libs[kind]
+    path = PORT_SO if kind == "port" else REF_SO
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"oracle library missing: {path} (run make -C oracle"
+                                f"{' ref' if kind == 'reference' else ''})")
+    lib = ctypes.CDLL(path)
+    if kind == "port":
+        lib.gcl_oracle_canon.argtypes = [ctypes.c_int, _P, _P, _P, ctypes.c_uint, _P, _P, _P]
+        lib.gcl_oracle_canon.restype = ctypes.c_int
+        lib.gcl_oracle_canon_batch.argtypes = [ctypes.c_int, _P, _P, _P, _P, _P, ctypes.c_uint,
+                                               _P, _P, _P, _P]
+        lib.gcl_oracle_canon_batch.restype = ctypes.c_int
+        lib.gcl_oracle_root_refine.argtypes = [ctypes.c_int, _P, _P, _P, _P, _P]
+        lib.gcl_oracle_root_refine.restype = ctypes.c_int
+    else:
+        lib.gcl_ref_canon.argtypes = [ctypes.c_int, _P, _P, _P, ctypes.c_uint, _P, _P, _P]
+        lib.gcl_ref_canon.restype = ctypes.c_int
+        lib.gcl_ref_canon_batch.argtypes = [ctypes.c_int, _P, _P, _P, _P, _P, ctypes.c_uint,
+                                            _P, _P, _P]
+        lib.gcl_ref_canon_batch.restype = ctypes.c_int
+        lib.gcl_ref_quiet.argtypes = [ctypes.c_int]
+        lib.gcl_ref_quiet(1)
+    _libs[kind] = lib
+    return lib
+
+
+def available(kind: str) -> bool:
+    return os.path.exists(PORT_SO if kind == "port" else REF_SO)
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(_P)
+
+
+def canon(g, max_aut: int = 10000, kind: str = "port") -> Tuple[np.ndarray, np.ndarray, int, int]:
+    """(canonical n x n uint8 matrix, best label, num_aut, nodes) for one graph."""
+    lib = _load(kind)
+    n = g.n
+    rp = np.ascontiguousarray(g.rowptr, dtype=np.int32)
+    cl = np.ascontiguousarray(g.col, dtype=np.int32)
+    co = None if g.color is None else np.ascontiguousarray(g.color, dtype=np.int32)
+    out = np.zeros((n, n), dtype=np.uint8)
+    lab = np.zeros(n, dtype=np.int32)
+    st = _Stats()
+    fn = lib.gcl_oracle_canon if kind == "port" else lib.gcl_ref_canon
+    rc = fn(n, _ptr(rp), _ptr(cl if cl.size else np.zeros(1, np.int32)), _ptr(co), max_aut,
+            _ptr(out if out.size else np.zeros(1, np.uint8)), _ptr(lab if lab.size else
+                                                                   np.zeros(1, np.int32)),
+            ctypes.byref(st))
+    if rc != 0:
+        raise RuntimeError(f"oracle ({kind}) failed rc={rc}")
+    return out, lab, int(st.num_aut), int(st.nodes)
+
+
+def canon_batch(arena, max_aut: int = 10000, kind: str = "port",
+                want_matrix: bool = True):
+    """Run the checker over an Arena.  Returns (out_arena or None, ooff,
+    num_aut[count], nodes[count])."""
+    lib = _load(kind)
+    ooff = arena.out_offsets()
+    out = np.zeros(max(int(ooff[-1]), 1), dtype=np.uint8) if (want_matrix or kind != "port") else None
+    st = (_Stats * max(arena.count, 1))()
+    col = arena.col if arena.col.size else np.zeros(1, np.int32)
+    if kind == "port":
+        rc = lib.gcl_oracle_canon_batch(arena.count, _ptr(arena.voff), _ptr(arena.eoff),
+                                        _ptr(arena.rowptr), _ptr(col), _ptr(arena.color),
+                                        max_aut, _ptr(out), _ptr(ooff), None, st)
+    else:
+        rc = lib.gcl_ref_canon_batch(arena.count, _ptr(arena.voff), _ptr(arena.eoff),
+                                     _ptr(arena.rowptr), _ptr(col), _ptr(arena.color),
+                                     max_aut, _ptr(out), _ptr(ooff), st)
+    if rc != 0:
+        raise RuntimeError(f"oracle batch ({kind}) failed rc={rc}")
+    na = np.array([st[i].num_aut for i in range(arena.count)], dtype=np.int64)
+    nd = np.array([st[i].nodes for i in range(arena.count)], dtype=np.int64)
+    return out, ooff, na, nd
+
+
+def root_refine(g) -> Tuple[int, np.ndarray, np.ndarray]:
+    lib = _load("port")
+    n = g.n
+    rp = np.ascontiguousarray(g.rowptr, dtype=np.int32)
+    cl = np.ascontiguousarray(g.col, dtype=np.int32)
+    co = None if g.color is None else np.ascontiguousarray(g.color, dtype=np.int32)
+    el = np.zeros(n, np.int32)
+    cs = np.zeros(n, np.int32)
+    code = lib.gcl_oracle_root_refine(n, _ptr(rp), _ptr(cl if cl.size else np.zeros(1, np.int32)),
+                                      _ptr(co), _ptr(el), _ptr(cs))
+    return code, el, cs
