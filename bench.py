@@ -1,0 +1,453 @@
+"""Benchmark: batched canonical labeling of 10,000 small graphs on B200.
+
+Workload (one "step"): the batched small-graph workload -- 10,000 uncoloured
+graphs, n ~ U[10, 64], each a random labelled tree (Pruefer sequence, max
+degree 4) plus 0-6 extra edges that keep the max degree <= 4, 20% of them
+random relabelings of earlier graphs, packed into one int32 ragged CSR
+arena and canonized in one batched call (max_aut = 10000).
+
+Reported JSON line (rank 0):
+  value  graphs/s with the arena resident in HBM, device time (CUDA events on
+         the library's stream) summed over K steps, L2 flushed between steps
+  e2e    graphs/s through the C ABI with pinned host buffers: H2D of the arena,
+         the kernels, D2H of every canonical matrix, stats and status
+  roofline  algorithmic bytes of the batch (CSR read + n^2 canonical matrix
+         write + per search node one CSR pass and one read+write of the
+         partition) / kernel time, against the measured HBM copy bandwidth
+  cpu_baseline  the reference's own sequential path (oracle/_ref), on all
+         host cores, over the same graphs
+  plain_per_launch  the same library launched once per graph (the plain form)
+
+--impl reference: the reference's CPU implementation of the path (its own
+sequential sources compiled into oracle/_ref, else the C restatement) on all
+host cores, on the same workload, metric and unit.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import importlib
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+PKG = "gpu-canonical-labeling_b200"
+
+METRIC = "graphs canonized/sec"
+UNIT = "graphs/s"
+WORKLOAD = ("batched small graphs: 10,000 uncoloured graphs, n ~ U[10,64], Pruefer tree "
+            "(max deg 4) + U{0..6} extra edges, 20% relabelings, one ragged CSR arena, "
+            "max_aut 10000")
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--graphs", type=int, default=10000)
+    p.add_argument("--seed", type=int, default=3000)
+    p.add_argument("--max-aut", type=int, default=10000)
+    p.add_argument("--cpu-seconds", type=float, default=12.0,
+                   help="wall-clock budget of the CPU-baseline sample")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-plain", action="store_true")
+    return p.parse_args()
+
+
+def workload(args):
+    G = importlib.import_module(PKG + ".graphs")
+    return G.pack(G.small_batch(args.graphs, seed=args.seed))
+
+
+def algorithmic_bytes(arena, nodes: np.ndarray) -> int:
+    """B(g) = (4(n+1) + 8m) + n^2 + nodes(g) * (4(n+1) + 8m + 32n), summed."""
+    n = arena.sizes().astype(np.int64)
+    m = (np.diff(arena.eoff) // 2).astype(np.int64)
+    csr = 4 * (n + 1) + 8 * m
+    return int((csr + n * n + nodes.astype(np.int64) * (csr + 32 * n)).sum())
+
+
+# --------------------------------------------------------------------------
+# CPU side: the reference's sequential path on all host cores
+# --------------------------------------------------------------------------
+_W = {}
+
+
+def _cpu_init(kind, arrays):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle  # the checker / CPU baseline (test infrastructure)
+    G = importlib.import_module(PKG + ".graphs")
+    _W["oracle"] = oracle
+    _W["kind"] = kind
+    _W["arena"] = G.Arena(*arrays)
+
+
+def _cpu_run(lo_hi):
+    lo, hi = lo_hi
+    O, A, kind = _W["oracle"], _W["arena"], _W["kind"]
+    G = importlib.import_module(PKG + ".graphs")
+    sub = G.Arena(hi - lo, A.voff[lo:hi + 1] - A.voff[lo], A.eoff[lo:hi + 1] - A.eoff[lo],
+                  A.rowptr[A.voff[lo] + lo: A.voff[hi] + hi], A.col[A.eoff[lo]:A.eoff[hi]],
+                  A.color[A.voff[lo]:A.voff[hi]])
+    t = time.perf_counter()
+    O.canon_batch(sub, max_aut=10000, kind=kind, want_matrix=True)
+    return hi - lo, time.perf_counter() - t
+
+
+def cpu_kind():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    if oracle.available("reference"):
+        return "reference"
+    if not oracle.available("port"):
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
+    return "port"
+
+
+class CpuPool:
+    def __init__(self, arena, kind):
+        import multiprocessing as mp
+        self.cores = os.cpu_count() or 1
+        self.kind = kind
+        arrays = (arena.count, arena.voff, arena.eoff, arena.rowptr, arena.col, arena.color)
+        self.pool = mp.get_context("spawn").Pool(self.cores, initializer=_cpu_init,
+                                                  initargs=(kind, arrays))
+        self.count = arena.count
+        chunks = max(self.cores * 4, 1)
+        b = np.linspace(0, arena.count, chunks + 1).astype(int)
+        self.tasks = [(int(b[i]), int(b[i + 1])) for i in range(chunks) if b[i + 1] > b[i]]
+
+    def step(self):
+        t = time.perf_counter()
+        done = sum(x[0] for x in self.pool.map(self._run, self.tasks))
+        return done, time.perf_counter() - t
+
+    _run = staticmethod(_cpu_run)
+
+    def close(self):
+        self.pool.close()
+        self.pool.join()
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    kind = cpu_kind()
+    arena = workload(args)
+    pool = CpuPool(arena, kind)
+    for _ in range(max(args.warmup, 1)):
+        pool.step()
+    tot_g, tot_t, per = 0, 0.0, []
+    for _ in range(args.steps):
+        g, t = pool.step()
+        tot_g += g
+        tot_t += t
+        per.append(t)
+    pool.close()
+    v = tot_g / tot_t
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_t / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic (seeded generator, same graphs as the GPU arm)",
+        "config": {"workload": WORKLOAD, "graphs_per_step": arena.count},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": pool.cores, "kind": kind,
+                         "sample": f"the full {arena.count}-graph batch per step, split over "
+                                   f"{pool.cores} processes"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "latency_ms": {"p50": float(np.percentile(per, 50)) * 1e3,
+                       "p99": float(np.percentile(per, 99)) * 1e3},
+    }
+    print(json.dumps(line))
+
+
+# --------------------------------------------------------------------------
+# GPU side
+# --------------------------------------------------------------------------
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{device}.csv")
+
+    def start(self):
+        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
+                stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        rows = []
+        for ln in open(self.path):
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if "Active" in r[5 + i]
+                          and "Not" not in r[5 + i]})
+        load = [s for s in sm if s > 0.5 * (max(mx) if mx else 1)]
+        return {"sm_mhz": float(np.median(load or sm or [0])),
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def read_traffic():
+    """dram bytes per launch of the batch kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "w64_batch_kernel_small10k.txt")
+    if not os.path.exists(p):
+        return None
+    for ln in open(p):
+        if ln.startswith("dram_bytes_per_launch:"):
+            return float(ln.split(":")[1].split()[0])
+    return None
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def gpu_arm(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    pkg = importlib.import_module(PKG)
+    api = pkg.api
+    arena = workload(args)
+    count = arena.count
+    dev = torch.device("cuda", local)
+    ctx = api.Context(local)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    ooff = arena.out_offsets()
+    max_n = int(arena.sizes().max())
+
+    # device-resident inputs and outputs
+    def d(a, dtype):
+        return torch.from_numpy(np.ascontiguousarray(a)).to(dev, dtype=dtype)
+
+    t_voff, t_eoff = d(arena.voff, torch.int64), d(arena.eoff, torch.int64)
+    t_rp, t_col = d(arena.rowptr, torch.int32), d(arena.col, torch.int32)
+    t_ooff = d(ooff, torch.int64)
+    t_dense = torch.empty(int(ooff[-1]), dtype=torch.uint8, device=dev)
+    t_stats = torch.empty((count, 2), dtype=torch.int64, device=dev)
+    t_status = torch.empty(count, dtype=torch.int32, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    lib = ctx.lib
+    P = ctypes.c_void_p
+
+    def launch():
+        rc = lib.gcl_canon_batch_device_async(
+            ctx.handle, count, P(t_voff.data_ptr()), P(t_eoff.data_ptr()), P(t_rp.data_ptr()),
+            P(t_col.data_ptr()), None, args.max_aut, max_n, P(t_dense.data_ptr()),
+            P(t_ooff.data_ptr()), None, P(t_stats.data_ptr()), P(t_status.data_ptr()))
+        if rc != 0:
+            raise RuntimeError(f"gcl_canon_batch_device_async failed: {rc}")
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        flush.zero_()
+        with torch.cuda.stream(stream):
+            launch()
+    torch.cuda.synchronize()
+    assert int((t_status != 0).sum()) == 0, "a graph failed"
+    nodes = t_stats[:, 1].cpu().numpy()
+
+    clocks = Clocks(local)
+    clocks.start()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    barrier()
+    for i in range(args.steps):
+        flush.zero_()  # L2 flush outside the timed events
+        stream.wait_stream(torch.cuda.current_stream())
+        evs[i][0].record(stream)
+        launch()
+        evs[i][1].record(stream)
+        torch.cuda.current_stream().wait_stream(stream)
+    barrier()
+    clk = clocks.stop()
+    per = np.array([a.elapsed_time(b) for a, b in evs])  # ms
+    dev_ms = float(per.sum())
+    if world > 1:
+        t = torch.tensor([dev_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dev_ms = float(t.item())
+    value = world * count * args.steps / (dev_ms / 1e3)
+
+    # end to end through the C ABI: pinned host buffers, copies inside
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
+    h_voff, h_eoff, h_rp, h_col = pin(arena.voff), pin(arena.eoff), pin(arena.rowptr), pin(arena.col)
+    h_ooff = pin(ooff)
+    h_dense = torch.empty(int(ooff[-1]), dtype=torch.uint8).pin_memory().numpy()
+    h_stats = torch.empty((count, 2), dtype=torch.int64).pin_memory().numpy()
+    h_status = torch.empty(count, dtype=torch.int32).pin_memory().numpy()
+    pp = lambda a: a.ctypes.data_as(P)  # noqa: E731
+
+    def e2e_call():
+        rc = lib.gcl_canon_batch(ctx.handle, count, pp(h_voff), pp(h_eoff), pp(h_rp), pp(h_col),
+                                 None, args.max_aut, pp(h_dense), pp(h_ooff), None, pp(h_stats),
+                                 pp(h_status))
+        if rc != 0:
+            raise RuntimeError(f"gcl_canon_batch failed: {rc}")
+
+    for _ in range(max(2, args.warmup // 2)):
+        e2e_call()
+    barrier()
+    e2e_t = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        e2e_call()
+        e2e_t.append(time.perf_counter() - t0)
+    barrier()
+    e2e_s = float(np.sum(e2e_t))
+    if world > 1:
+        t = torch.tensor([e2e_s], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    h2d = sum(a.nbytes for a in (h_voff, h_eoff, h_rp, h_col, h_ooff))
+    d2h = h_dense.nbytes + h_stats.nbytes + h_status.nbytes
+
+    line = None
+    if rank == 0:
+        peak, peak_kind = measured_peak()
+        alg = algorithmic_bytes(arena, nodes)
+        kern_ms = float(per.mean())
+        achieved = alg / (kern_ms / 1e3) / 1e9
+        traffic = read_traffic()
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic (seeded generator)",
+            "config": {"workload": WORKLOAD, "graphs_per_step_per_gpu": count,
+                       "max_aut": args.max_aut, "seed": args.seed,
+                       "parallelism": f"graph-sharded x{world} (no collective)",
+                       "l2": "flushed between steps (256 MiB write outside the timed events)"},
+            "e2e": {"value": world * count * args.steps / e2e_s, "unit": UNIT,
+                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": 2 * args.steps,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "peak_kind": peak_kind,
+                         "algorithmic_bytes_per_launch": alg},
+            "latency_ms": {"p50": float(np.percentile(per, 50)),
+                           "p99": float(np.percentile(per, 99))},
+            "clocks": clk,
+        }
+
+    # the plain form: one graph per launch (device-resident, same kernels)
+    if rank == 0 and not args.no_plain:
+        k = min(1000, count)
+        one_v = torch.zeros(2, dtype=torch.int64, device=dev)
+        one_o = torch.zeros(2, dtype=torch.int64, device=dev)
+        hv, hee = arena.voff, arena.eoff
+        starts = []
+        for g in range(k):
+            n, m = int(hv[g + 1] - hv[g]), int(hee[g + 1] - hee[g])
+            starts.append((g, n, m))
+        vo_all = torch.tensor([[0, n] for _, n, _ in starts], dtype=torch.int64, device=dev)
+        eo_all = torch.tensor([[0, m] for _, _, m in starts], dtype=torch.int64, device=dev)
+        oo_all = torch.tensor([[0, n * n] for _, n, _ in starts], dtype=torch.int64, device=dev)
+
+        def one(i):
+            g, n, m = starts[i]
+            rc = lib.gcl_canon_batch_device_async(
+                ctx.handle, 1, P(vo_all[i].data_ptr()), P(eo_all[i].data_ptr()),
+                P(t_rp.data_ptr() + 4 * int(hv[g] + g)), P(t_col.data_ptr() + 4 * int(hee[g])),
+                None, args.max_aut, n, P(t_dense.data_ptr() + int(ooff[g])),
+                P(oo_all[i].data_ptr()), None, P(t_stats.data_ptr() + 16 * g),
+                P(t_status.data_ptr() + 4 * g))
+            if rc != 0:
+                raise RuntimeError("plain launch failed")
+
+        for i in range(min(50, k)):
+            one(i)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for i in range(k):
+            one(i)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        pl = k / (e0.elapsed_time(e1) / 1e3)
+        line["plain_per_launch"] = {"value": pl, "unit": UNIT, "graphs": k,
+                                    "batched_over_plain": value / world / pl}
+        del one_v, one_o
+
+    if rank == 0 and not args.no_cpu_baseline:
+        kind = cpu_kind()
+        pool = CpuPool(arena, kind)
+        pool.step()  # warm-up (imports, page-in)
+        g_done, t_done = 0, 0.0
+        while t_done < args.cpu_seconds:
+            g, t = pool.step()
+            g_done += g
+            t_done += t
+        pool.close()
+        line["cpu_baseline"] = {"value": g_done / t_done, "unit": UNIT, "cores": pool.cores,
+                                "kind": kind,
+                                "sample": f"{g_done} graphs (the {count}-graph batch repeated) "
+                                          f"in {t_done:.1f} s on {pool.cores} processes"}
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    ctx.close()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        gpu_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,213 @@
+"""Python binding of the C ABI (include/gcl.h) over ctypes.
+
+Names mirror the reference's entry points: ``Nauty_Parallel`` returns the
+n*n canonical adjacency bytes like src/nauty_parallel.h:9-13, ``canon`` adds
+the search statistics, ``canon_batch`` is the batched arena form and
+``is_isomorphic`` is the two-graph check of main.cpp:172-197.
+
+The library is the CUDA build in this directory; there is no CPU fallback:
+importing a function that needs it raises if ``libgcl_b200.so`` is missing or
+no GPU is visible.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+from typing import List, Optional, Sequence, Union
+
+import numpy as np
+
+from .graphs import Arena, Graph, pack
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libgcl_b200.so")
+
+GCL_OK = 0
+ERRORS = {
+    -1: "invalid argument",
+    -2: "CUDA error",
+    -3: "out of memory",
+    -4: "bad input graph",
+    -5: "graph too large",
+    -6: "bounded device wait timed out",
+    -7: "internal error",
+}
+
+# Every symbol include/gcl.h declares.
+EXPORTS = [
+    "gcl_status_string", "gcl_version", "gcl_create", "gcl_destroy", "gcl_stream",
+    "gcl_canon_one", "gcl_canon_batch", "gcl_canon_batch_device_async", "gcl_sync", "gcl_iso",
+]
+
+
+class GclError(RuntimeError):
+    def __init__(self, rc: int, what: str = ""):
+        super().__init__(f"{what}: {ERRORS.get(rc, 'error')} (status {rc})")
+        self.rc = rc
+
+
+_P = ctypes.c_void_p
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load libgcl_b200.so and declare its signatures (no GPU needed)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(
+            f"{path} is missing: build it with python gpu-canonical-labeling_b200/build.py")
+    lib = ctypes.CDLL(path)
+    lib.gcl_status_string.restype = ctypes.c_char_p
+    lib.gcl_status_string.argtypes = [ctypes.c_int]
+    lib.gcl_version.restype = ctypes.c_int
+    lib.gcl_create.argtypes = [ctypes.c_int, ctypes.POINTER(_P)]
+    lib.gcl_destroy.argtypes = [_P]
+    lib.gcl_stream.argtypes = [_P]
+    lib.gcl_stream.restype = _P
+    lib.gcl_sync.argtypes = [_P]
+    lib.gcl_canon_one.argtypes = [_P, _P, _P, _P, ctypes.c_int, ctypes.c_int, _P, _P, _P]
+    lib.gcl_canon_batch.argtypes = [_P, ctypes.c_int, _P, _P, _P, _P, _P, ctypes.c_int, _P, _P,
+                                    _P, _P, _P]
+    lib.gcl_canon_batch_device_async.argtypes = [_P, ctypes.c_int, _P, _P, _P, _P, _P,
+                                                 ctypes.c_int, ctypes.c_int, _P, _P, _P, _P, _P]
+    lib.gcl_iso.argtypes = [_P, _P, _P, _P, ctypes.c_int, _P, _P, _P, ctypes.c_int,
+                            ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+    for name in ("gcl_create", "gcl_destroy", "gcl_sync", "gcl_canon_one", "gcl_canon_batch",
+                 "gcl_canon_batch_device_async", "gcl_iso"):
+        getattr(lib, name).restype = ctypes.c_int
+    _lib = lib
+    return lib
+
+
+def _check(rc: int, what: str):
+    if rc != GCL_OK:
+        raise GclError(rc, what)
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(_P)
+
+
+class Context:
+    """A device context (workspace, stream, staging buffers) on one GPU."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load_library()
+        h = _P()
+        _check(self.lib.gcl_create(device, ctypes.byref(h)), "gcl_create")
+        self.handle = h
+        self.device = device
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.gcl_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def stream(self) -> int:
+        return int(self.lib.gcl_stream(self.handle) or 0)
+
+    def sync(self):
+        _check(self.lib.gcl_sync(self.handle), "gcl_sync")
+
+
+_default: Optional[Context] = None
+
+
+def default_context() -> Context:
+    global _default
+    if _default is None:
+        _default = Context(0)
+    return _default
+
+
+@dataclass
+class CanonResult:
+    matrix: np.ndarray  # n x n uint8
+    nodes: int
+    num_aut: int
+
+
+def _csr(g: Graph):
+    rp = np.ascontiguousarray(g.rowptr, dtype=np.int32)
+    cl = np.ascontiguousarray(g.col, dtype=np.int32)
+    if cl.size == 0:
+        cl = np.zeros(1, np.int32)
+    co = None if g.color is None else np.ascontiguousarray(g.color, dtype=np.int32)
+    return rp, cl, co
+
+
+def canon(g: Graph, max_aut: int = 10000, ctx: Optional[Context] = None) -> CanonResult:
+    """Canonical form of one graph (one launch)."""
+    ctx = ctx or default_context()
+    rp, cl, co = _csr(g)
+    out = np.zeros((g.n, g.n), dtype=np.uint8)
+    nodes = ctypes.c_int64()
+    naut = ctypes.c_int64()
+    rc = ctx.lib.gcl_canon_one(ctx.handle, _ptr(rp), _ptr(cl), _ptr(co), g.n, max_aut,
+                               _ptr(out if out.size else np.zeros(1, np.uint8)),
+                               ctypes.byref(nodes), ctypes.byref(naut))
+    _check(rc, "gcl_canon_one")
+    return CanonResult(out, int(nodes.value), int(naut.value))
+
+
+def Nauty_Parallel(g: Graph, max_aut: int = 10000) -> bytes:  # noqa: N802 (reference name)
+    """The n*n canonical adjacency bytes, as src/nauty_parallel.h:9-13 returns."""
+    return canon(g, max_aut).matrix.tobytes()
+
+
+@dataclass
+class BatchResult:
+    dense: Optional[np.ndarray]  # concatenated n_g*n_g blocks
+    ooff: np.ndarray
+    label: Optional[np.ndarray]  # concatenated per-graph labels
+    stats: np.ndarray  # (count, 2): num_aut, nodes
+    status: np.ndarray
+    arena: Arena
+
+    def matrix(self, g: int) -> np.ndarray:
+        n = int(self.arena.voff[g + 1] - self.arena.voff[g])
+        return self.dense[self.ooff[g]: self.ooff[g + 1]].reshape(n, n)
+
+    def labeling(self, g: int) -> np.ndarray:
+        return self.label[self.arena.voff[g]: self.arena.voff[g + 1]]
+
+
+def canon_batch(graphs: Union[Arena, Sequence[Graph]], max_aut: int = 10000,
+                ctx: Optional[Context] = None, dense: bool = True,
+                label: bool = True) -> BatchResult:
+    """Canonize every graph of a ragged arena in one batched call."""
+    ctx = ctx or default_context()
+    arena = graphs if isinstance(graphs, Arena) else pack(graphs)
+    ooff = arena.out_offsets()
+    out = np.zeros(max(int(ooff[-1]), 1), dtype=np.uint8) if dense else None
+    lab = np.zeros(max(int(arena.voff[-1]), 1), dtype=np.int32) if label else None
+    stats = np.zeros((max(arena.count, 1), 2), dtype=np.int64)
+    status = np.zeros(max(arena.count, 1), dtype=np.int32)
+    col = arena.col if arena.col.size else np.zeros(1, np.int32)
+    color = arena.color if arena.color.any() else None
+    rc = ctx.lib.gcl_canon_batch(ctx.handle, arena.count, _ptr(arena.voff), _ptr(arena.eoff),
+                                 _ptr(arena.rowptr), _ptr(col), _ptr(color), max_aut, _ptr(out),
+                                 _ptr(ooff), _ptr(lab), _ptr(stats), _ptr(status))
+    _check(rc, "gcl_canon_batch")
+    return BatchResult(out, ooff, lab, stats[:arena.count], status[:arena.count], arena)
+
+
+def is_isomorphic(g1: Graph, g2: Graph, max_aut: int = 10000,
+                  ctx: Optional[Context] = None) -> bool:
+    """main.cpp:172-197: canonize both, compare the upper triangles."""
+    ctx = ctx or default_context()
+    a, b = _csr(g1), _csr(g2)
+    v = ctypes.c_int()
+    rc = ctx.lib.gcl_iso(ctx.handle, _ptr(a[0]), _ptr(a[1]), _ptr(a[2]), g1.n, _ptr(b[0]),
+                         _ptr(b[1]), _ptr(b[2]), g2.n, max_aut, ctypes.byref(v))
+    _check(rc, "gcl_iso")
+    return bool(v.value)

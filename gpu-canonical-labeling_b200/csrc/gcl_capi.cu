@@ -1,0 +1,432 @@
+// gcl_capi.cu -- the C ABI (include/gcl.h) and its host-side context.
+//
+// Dispatch: every batch first runs the warp-per-graph kernel for n <= 64
+// (canon_warp64.cuh).  Graphs it cannot finish are appended to device-side
+// lists and picked up by later launches on the same stream, so the batched
+// device path never synchronizes with the host:
+//   * an automorphism ring that outgrew its per-slot capacity -> rerun with a
+//     workspace holding the full max_aut ring;
+//   * n > 64 -> the block-per-graph kernel (canon_block.cuh).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "../../include/gcl.h"
+#include "canon_block.cuh"
+#include "canon_warp64.cuh"
+
+namespace gcl {
+
+constexpr int kW64Threads = 128;  // 4 warps, one graph per warp
+constexpr int kW64Warps = kW64Threads / 32;
+constexpr uint32_t kW64AutCap = 256;  // ring slots per warp in the fast pass
+
+// Device-side lists of deferred graphs.
+struct Deferred {
+  int overflow_count;
+  int large_count;
+  int next_overflow;
+  int next_large;
+  int next;  // work counter of the first pass
+};
+
+__global__ void __launch_bounds__(kW64Threads)
+    w64_batch_kernel(BatchArgs A, Deferred* D, int* overflow_list, int* large_list, int pass) {
+  __shared__ W64Smem smem[kW64Warps];
+  const int warp = (int)(threadIdx.x >> 5);
+  const uint32_t lane = lane_id();
+  W64Smem& S = smem[warp];
+  uint8_t* slot = A.work + ((uint64_t)blockIdx.x * kW64Warps + (uint64_t)warp) * A.slot_bytes;
+  int* ctr = pass == 0 ? &D->next : &D->next_overflow;
+  const int total = pass == 0 ? A.count : *(volatile int*)&D->overflow_count;
+  while (true) {
+    int i = 0;
+    if (lane == 0) i = atomicAdd(ctr, 1);
+    i = __shfl_sync(GCL_FULL, i, 0);
+    if (i >= total) break;
+    const int g = pass == 0 ? (A.order ? A.order[i] : i) : overflow_list[i];
+    const int n = (int)(A.voff[g + 1] - A.voff[g]);
+    if (n > kW64MaxN) {
+      if (lane == 0) {
+        A.status[g] = kTooLarge;
+        large_list[atomicAdd(&D->large_count, 1)] = g;
+      }
+      continue;
+    }
+    if (n <= 32)
+      w64_canon_one<1>(S, A, g, slot);
+    else
+      w64_canon_one<2>(S, A, g, slot);
+    if (pass == 0 && lane == 0 && *(volatile int32_t*)&A.status[g] == kAutOverflow)
+      overflow_list[atomicAdd(&D->overflow_count, 1)] = g;
+    __syncwarp();
+  }
+}
+
+}  // namespace gcl
+
+using namespace gcl;
+
+namespace {
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+  cudaError_t ensure(size_t bytes) {
+    if (bytes <= cap && p) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    size_t want = std::max<size_t>(bytes, 256);
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e == cudaSuccess) cap = want;
+    return e;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+};
+
+}  // namespace
+
+struct gcl_context {
+  int device = 0;
+  int sms = 0;
+  cudaStream_t stream = nullptr;
+  int w64_grid = 0;
+  int blk_grid = 0;
+  // fast-pass workspace
+  DevBuf work;
+  // rerun workspace (full max_aut ring), sized on demand
+  DevBuf work_big;
+  uint32_t work_big_aut = 0;
+  int big_slots = 0;
+  DevBuf block_work;
+  uint64_t block_work_n = 0, block_work_aut = 0;
+  int block_slots = 0;
+  DevBuf deferred, overflow_list, large_list;
+  // staging for host-pointer calls
+  DevBuf voff, eoff, rowptr, col, color, ooff, dense, label, stats, status;
+};
+
+// Per-graph time budget of the search loop (GCL_GRAPH_BUDGET_S, default
+// 600 s); a graph that exceeds it reports GCL_ERR_TIMEOUT instead of holding
+// its warp forever.
+static uint64_t graph_budget_ns() {
+  const char* e = std::getenv("GCL_GRAPH_BUDGET_S");
+  double s = e ? std::atof(e) : 600.0;
+  if (!(s > 0)) return 0;
+  return (uint64_t)(s * 1e9);
+}
+
+static int cuda_status(cudaError_t e) {
+  if (e == cudaSuccess) return GCL_OK;
+  if (e == cudaErrorMemoryAllocation) return GCL_ERR_NOMEM;
+  return GCL_ERR_CUDA;
+}
+#define GCL_TRY(x)                          \
+  do {                                      \
+    cudaError_t e_ = (x);                   \
+    if (e_ != cudaSuccess) return cuda_status(e_); \
+  } while (0)
+
+extern "C" {
+
+const char* gcl_status_string(int s) {
+  switch (s) {
+    case GCL_OK: return "ok";
+    case GCL_ERR_ARG: return "invalid argument";
+    case GCL_ERR_CUDA: return "CUDA error";
+    case GCL_ERR_NOMEM: return "out of memory";
+    case GCL_ERR_BAD_INPUT: return "bad input graph (loop, duplicate or one-directional edge)";
+    case GCL_ERR_TOO_LARGE: return "graph too large";
+    case GCL_ERR_TIMEOUT: return "bounded device wait timed out";
+    default: return "internal error";
+  }
+}
+
+int gcl_version(void) { return 100; }
+
+int gcl_create(int device, gcl_context** out) {
+  if (!out) return GCL_ERR_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  GCL_TRY(cudaGetDeviceCount(&ndev));
+  if (device < 0 || device >= ndev) return GCL_ERR_ARG;
+  GCL_TRY(cudaSetDevice(device));
+  gcl_context* c = new (std::nothrow) gcl_context();
+  if (!c) return GCL_ERR_NOMEM;
+  c->device = device;
+  cudaError_t e = cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  int per_sm = 0;
+  if (e == cudaSuccess)
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, w64_batch_kernel, kW64Threads, 0);
+  if (e == cudaSuccess) {
+    c->w64_grid = c->sms * std::max(per_sm, 1);
+    e = c->deferred.ensure(sizeof(Deferred));
+  }
+  if (e == cudaSuccess) e = block_occupancy(&c->blk_grid, c->sms);
+  if (e != cudaSuccess) {
+    if (c->stream) cudaStreamDestroy(c->stream);
+    c->deferred.release();
+    delete c;
+    return cuda_status(e);
+  }
+  *out = c;
+  return GCL_OK;
+}
+
+int gcl_destroy(gcl_context* c) {
+  if (!c) return GCL_ERR_ARG;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  DevBuf* bufs[] = {&c->work, &c->work_big, &c->block_work, &c->deferred, &c->overflow_list,
+                    &c->large_list, &c->voff, &c->eoff, &c->rowptr, &c->col, &c->color,
+                    &c->ooff, &c->dense, &c->label, &c->stats, &c->status};
+  for (DevBuf* b : bufs) b->release();
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return GCL_OK;
+}
+
+void* gcl_stream(gcl_context* c) { return c ? (void*)c->stream : nullptr; }
+
+int gcl_sync(gcl_context* c) {
+  if (!c) return GCL_ERR_ARG;
+  GCL_TRY(cudaStreamSynchronize(c->stream));
+  return GCL_OK;
+}
+
+int gcl_canon_batch_device_async(gcl_context* c, int count, const int64_t* d_voff,
+                                 const int64_t* d_eoff, const int32_t* d_rowptr,
+                                 const int32_t* d_col, const int32_t* d_color, int max_aut,
+                                 int max_n, uint8_t* d_out_dense, const int64_t* d_ooff,
+                                 int32_t* d_out_label, int64_t* d_out_stats,
+                                 int32_t* d_out_status) {
+  if (!c || count < 0 || max_aut <= 0 || !d_voff || !d_eoff || !d_rowptr || !d_out_status ||
+      (d_out_dense && !d_ooff) || max_n < 0 || max_n > GCL_MAX_N)
+    return GCL_ERR_ARG;
+  if (count == 0) return GCL_OK;
+  GCL_TRY(cudaSetDevice(c->device));
+  const uint32_t maut = (uint32_t)max_aut;
+  const uint32_t cap = std::min<uint32_t>(maut, kW64AutCap);
+  const uint64_t slot_bytes = w64_slot_bytes(cap);
+  const uint64_t slots = (uint64_t)c->w64_grid * kW64Warps;
+  GCL_TRY(c->work.ensure(slots * slot_bytes));
+  GCL_TRY(c->overflow_list.ensure((size_t)count * sizeof(int)));
+  GCL_TRY(c->large_list.ensure((size_t)count * sizeof(int)));
+  GCL_TRY(cudaMemsetAsync(c->deferred.p, 0, sizeof(Deferred), c->stream));
+
+  BatchArgs A;
+  std::memset(&A, 0, sizeof A);
+  A.count = count;
+  A.voff = d_voff;
+  A.eoff = d_eoff;
+  A.rowptr = d_rowptr;
+  A.col = d_col;
+  A.color = d_color;
+  A.order = nullptr;
+  A.max_aut = maut;
+  A.aut_cap = cap;
+  A.out_dense = d_out_dense;
+  A.ooff = d_ooff;
+  A.out_cert = nullptr;
+  A.out_label = d_out_label;
+  A.out_stats = d_out_stats;
+  A.status = d_out_status;
+  A.work = (uint8_t*)c->work.p;
+  A.slot_bytes = slot_bytes;
+  A.budget_ns = graph_budget_ns();
+  Deferred* D = (Deferred*)c->deferred.p;
+  const int grid1 = (int)std::min<int64_t>(c->w64_grid, ((int64_t)count + kW64Warps - 1) / kW64Warps);
+  w64_batch_kernel<<<grid1, kW64Threads, 0, c->stream>>>(A, D, (int*)c->overflow_list.p,
+                                                         (int*)c->large_list.p, 0);
+  GCL_TRY(cudaGetLastError());
+
+  if (cap < maut) {
+    // graphs whose ring outgrew `cap`: rerun with the full ring
+    if (c->work_big_aut < maut || !c->work_big.p) {
+      c->big_slots = std::max(c->sms, 1);
+      GCL_TRY(c->work_big.ensure((uint64_t)c->big_slots * kW64Warps * w64_slot_bytes(maut)));
+      c->work_big_aut = maut;
+    }
+    BatchArgs B = A;
+    B.aut_cap = maut;
+    B.work = (uint8_t*)c->work_big.p;
+    B.slot_bytes = w64_slot_bytes(maut);
+    w64_batch_kernel<<<c->big_slots, kW64Threads, 0, c->stream>>>(
+        B, D, (int*)c->overflow_list.p, (int*)c->large_list.p, 1);
+    GCL_TRY(cudaGetLastError());
+  }
+
+  if (max_n > kW64MaxN) {
+    int rc = block_pass_async(c, A, D, (int*)c->large_list.p, max_n, maut);
+    if (rc != GCL_OK) return rc;
+  }
+  return GCL_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Host-pointer entry points.
+// ---------------------------------------------------------------------------
+namespace {
+
+std::once_flag g_default_once;
+gcl_context* g_default = nullptr;
+int g_default_rc = GCL_OK;
+
+int default_context(gcl_context** out) {
+  std::call_once(g_default_once, [] { g_default_rc = gcl_create(0, &g_default); });
+  *out = g_default;
+  return g_default_rc;
+}
+
+int graph_status_to_rc(int32_t s) {
+  switch (s) {
+    case kOk: return GCL_OK;
+    case kBadInput: return GCL_ERR_BAD_INPUT;
+    case kTooLarge: return GCL_ERR_TOO_LARGE;
+    case kTimeout: return GCL_ERR_TIMEOUT;
+    default: return GCL_ERR_INTERNAL;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int gcl_canon_batch(gcl_context* c, int count, const int64_t* voff, const int64_t* eoff,
+                    const int32_t* rowptr, const int32_t* col, const int32_t* color, int max_aut,
+                    uint8_t* out_dense, const int64_t* ooff, int32_t* out_label,
+                    int64_t* out_stats, int32_t* out_status) {
+  if (!c || count < 0 || max_aut <= 0 || !voff || !eoff || !rowptr || !out_status ||
+      (out_dense && !ooff))
+    return GCL_ERR_ARG;
+  if (count == 0) return GCL_OK;
+  if (voff[0] != 0 || eoff[0] != 0) return GCL_ERR_ARG;
+  int max_n = 0;
+  for (int g = 0; g < count; ++g) {
+    const int64_t n = voff[g + 1] - voff[g], m = eoff[g + 1] - eoff[g];
+    if (n < 0 || m < 0 || n > GCL_MAX_N) return n > GCL_MAX_N ? GCL_ERR_TOO_LARGE : GCL_ERR_ARG;
+    if (rowptr[voff[g] + g] != 0 || rowptr[voff[g + 1] + g] != m) return GCL_ERR_BAD_INPUT;
+    if (out_dense && ooff[g + 1] - ooff[g] != n * n) return GCL_ERR_ARG;
+    max_n = std::max<int>(max_n, (int)n);
+  }
+  if (eoff[count] > 0 && !col) return GCL_ERR_ARG;
+  GCL_TRY(cudaSetDevice(c->device));
+  const size_t nv = (size_t)voff[count], ne = (size_t)eoff[count];
+  const size_t nrp = nv + (size_t)count;
+  GCL_TRY(c->voff.ensure((count + 1) * sizeof(int64_t)));
+  GCL_TRY(c->eoff.ensure((count + 1) * sizeof(int64_t)));
+  GCL_TRY(c->rowptr.ensure(nrp * sizeof(int32_t)));
+  GCL_TRY(c->col.ensure(std::max<size_t>(ne, 1) * sizeof(int32_t)));
+  GCL_TRY(c->status.ensure(count * sizeof(int32_t)));
+  cudaStream_t s = c->stream;
+  GCL_TRY(cudaMemcpyAsync(c->voff.p, voff, (count + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+  GCL_TRY(cudaMemcpyAsync(c->eoff.p, eoff, (count + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+  GCL_TRY(cudaMemcpyAsync(c->rowptr.p, rowptr, nrp * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+  if (ne) GCL_TRY(cudaMemcpyAsync(c->col.p, col, ne * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+  int32_t* d_color = nullptr;
+  if (color && nv) {
+    GCL_TRY(c->color.ensure(nv * sizeof(int32_t)));
+    GCL_TRY(cudaMemcpyAsync(c->color.p, color, nv * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    d_color = (int32_t*)c->color.p;
+  }
+  uint8_t* d_dense = nullptr;
+  int64_t* d_ooff = nullptr;
+  size_t dense_bytes = 0;
+  if (out_dense) {
+    dense_bytes = (size_t)ooff[count];
+    GCL_TRY(c->ooff.ensure((count + 1) * sizeof(int64_t)));
+    GCL_TRY(c->dense.ensure(std::max<size_t>(dense_bytes, 1)));
+    GCL_TRY(cudaMemcpyAsync(c->ooff.p, ooff, (count + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+    d_dense = (uint8_t*)c->dense.p;
+    d_ooff = (int64_t*)c->ooff.p;
+  }
+  int32_t* d_label = nullptr;
+  if (out_label && nv) {
+    GCL_TRY(c->label.ensure(nv * sizeof(int32_t)));
+    d_label = (int32_t*)c->label.p;
+  }
+  int64_t* d_stats = nullptr;
+  if (out_stats) {
+    GCL_TRY(c->stats.ensure(2 * count * sizeof(int64_t)));
+    d_stats = (int64_t*)c->stats.p;
+  }
+  int rc = gcl_canon_batch_device_async(c, count, (int64_t*)c->voff.p, (int64_t*)c->eoff.p,
+                                        (int32_t*)c->rowptr.p, (int32_t*)c->col.p, d_color,
+                                        max_aut, max_n, d_dense, d_ooff, d_label, d_stats,
+                                        (int32_t*)c->status.p);
+  if (rc != GCL_OK) return rc;
+  if (out_dense && dense_bytes)
+    GCL_TRY(cudaMemcpyAsync(out_dense, d_dense, dense_bytes, cudaMemcpyDeviceToHost, s));
+  if (d_label) GCL_TRY(cudaMemcpyAsync(out_label, d_label, nv * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  if (d_stats)
+    GCL_TRY(cudaMemcpyAsync(out_stats, d_stats, 2 * count * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+  GCL_TRY(cudaMemcpyAsync(out_status, c->status.p, count * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  GCL_TRY(cudaStreamSynchronize(s));
+  for (int g = 0; g < count; ++g)
+    if (out_status[g] != kOk) return graph_status_to_rc(out_status[g]);
+  return GCL_OK;
+}
+
+int gcl_canon_one(gcl_context* c, const int32_t* rowptr, const int32_t* col, const int32_t* color,
+                  int n, int max_aut, uint8_t* out_nxn, int64_t* node_count, int64_t* num_aut) {
+  if (n < 0 || !rowptr || max_aut <= 0 || (n > 0 && !out_nxn)) return GCL_ERR_ARG;
+  if (!c) {
+    int rc = default_context(&c);
+    if (rc != GCL_OK) return rc;
+  }
+  if (n == 0) {  // the reference's search visits the (discrete) root only
+    if (node_count) *node_count = 1;
+    if (num_aut) *num_aut = 0;
+    return GCL_OK;
+  }
+  const int64_t voff[2] = {0, n};
+  const int64_t eoff[2] = {0, rowptr[n]};
+  const int64_t ooff[2] = {0, (int64_t)n * n};
+  int64_t st[2] = {0, 0};
+  int32_t status = 0;
+  int rc = gcl_canon_batch(c, 1, voff, eoff, rowptr, col, color, max_aut, out_nxn, ooff, nullptr,
+                           st, &status);
+  if (rc != GCL_OK) return rc;
+  if (num_aut) *num_aut = st[0];
+  if (node_count) *node_count = st[1];
+  return GCL_OK;
+}
+
+int gcl_iso(gcl_context* c, const int32_t* rp1, const int32_t* col1, const int32_t* color1, int n1,
+            const int32_t* rp2, const int32_t* col2, const int32_t* color2, int n2, int max_aut,
+            int* verdict) {
+  if (!verdict || n1 < 0 || n2 < 0 || !rp1 || !rp2 || max_aut <= 0) return GCL_ERR_ARG;
+  if (!c) {
+    int rc = default_context(&c);
+    if (rc != GCL_OK) return rc;
+  }
+  std::vector<uint8_t> a((size_t)n1 * n1 + 1), b((size_t)n2 * n2 + 1);
+  int rc = gcl_canon_one(c, rp1, col1, color1, n1, max_aut, a.data(), nullptr, nullptr);
+  if (rc == GCL_OK) rc = gcl_canon_one(c, rp2, col2, color2, n2, max_aut, b.data(), nullptr, nullptr);
+  if (rc != GCL_OK) return rc;
+  int same = n1 == n2;
+  for (int i = 0; same && i < n1; ++i)
+    for (int j = i + 1; j < n1; ++j)
+      if ((a[(size_t)i * n1 + j] != 0) != (b[(size_t)i * n1 + j] != 0)) {
+        same = 0;
+        break;
+      }
+  *verdict = same;
+  return GCL_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,117 @@
+/* gcl.h -- C ABI of the B200 canonical-labeling library (libgcl_b200.so).
+ *
+ * The reference (rana-dbouk/gpu-canonical-labeling) has no FFI layer; its
+ * boundary is the C++ entry points main.cpp calls:
+ *
+ *   std::vector<unsigned char> Nauty_Parallel(CSRGraph& graph, int max_aut,
+ *       unsigned* node_count = nullptr, const std::string& prefix = "")
+ *                                          -- src/nauty_parallel.h:9-13
+ *   Nauty_Sequential(CSRGraph&, unsigned max_aut), result in
+ *       best_leaf.hash_of_perm_graph       -- src/sequential.h:12-30
+ *   canonical-form compare for the isomorphism verdict
+ *                                          -- main.cpp:73-90, 172-197
+ *
+ * Every entry point here takes plain pointers and sizes.  Graphs are CSR with
+ * both directions of every undirected edge stored (the shape
+ * CSRGraph::fromDIMACS builds, src/CSRGraph.cpp:40-119): rowptr[n+1],
+ * col[rowptr[n]], optional color[n] (NULL = uncoloured).  Rows need not be
+ * sorted; self loops, duplicate entries and one-directional edges are
+ * rejected with GCL_ERR_BAD_INPUT (the reference's refinement is undefined on
+ * parallel edges).  Results are bit-identical to the reference's sequential
+ * path: the canonical matrix, its best-leaf labeling, the number of stored
+ * automorphisms and the number of search-tree nodes.
+ *
+ * Errors are returned as negative status codes; nothing calls exit().  All
+ * calls are synchronous unless named *_async.
+ */
+#ifndef GCL_H
+#define GCL_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define GCL_OK 0
+#define GCL_ERR_ARG (-1)        /* bad argument (null pointer, n < 0, ...)  */
+#define GCL_ERR_CUDA (-2)       /* CUDA runtime error                        */
+#define GCL_ERR_NOMEM (-3)      /* device or host allocation failed          */
+#define GCL_ERR_BAD_INPUT (-4)  /* loop / duplicate / asymmetric edge, index */
+#define GCL_ERR_TOO_LARGE (-5)  /* graph above the supported vertex count    */
+#define GCL_ERR_TIMEOUT (-6)    /* a bounded device wait ran out             */
+#define GCL_ERR_INTERNAL (-7)
+
+/* Per-graph status as written by the batched calls (out_status[g]). */
+#define GCL_GRAPH_OK 0
+#define GCL_GRAPH_BAD_INPUT 3
+#define GCL_GRAPH_TOO_LARGE 2
+
+/* Largest vertex count the library canonizes. */
+#define GCL_MAX_N 65536
+
+const char* gcl_status_string(int status);
+int gcl_version(void);
+
+/* ---- context ------------------------------------------------------------ */
+/* A context owns device workspace, a stream and staging buffers on one GPU.
+ * It is not thread-safe; use one context per host thread. */
+typedef struct gcl_context gcl_context;
+
+int gcl_create(int device, gcl_context** out);
+int gcl_destroy(gcl_context* ctx);
+/* The CUDA stream (cudaStream_t) the context launches on. */
+void* gcl_stream(gcl_context* ctx);
+
+/* ---- one graph (drop-in for Nauty_Parallel, src/nauty_parallel.h:9-13) ---
+ * out_nxn receives the n*n canonical adjacency matrix (row-major, 0/1 bytes,
+ * canonical vertex i = row i), the value Nauty_Parallel returns.  node_count
+ * and num_aut (either may be NULL) receive the search statistics.  ctx may be
+ * NULL: a process-wide context on device 0 is created on first use (the
+ * reference hard-codes device 0, src/nauty_parallel.cu:642-643). */
+int gcl_canon_one(gcl_context* ctx, const int32_t* rowptr, const int32_t* col,
+                  const int32_t* color, int n, int max_aut, uint8_t* out_nxn,
+                  int64_t* node_count, int64_t* num_aut);
+
+/* ---- batched: many graphs in one ragged CSR arena ----------------------
+ * Graph g has n_g = voff[g+1]-voff[g] vertices; its local rowptr (n_g + 1
+ * entries starting at 0) is at rowptr + voff[g] + g, its col entries at
+ * col + eoff[g], its colours at color + voff[g] (color may be NULL).
+ * Outputs (each may be NULL):
+ *   out_dense + ooff[g]     n_g*n_g canonical matrix bytes
+ *   out_label + voff[g]     best-leaf labeling, position -> vertex
+ *   out_stats + 2*g         {num_aut, nodes}
+ *   out_status[g]           GCL_GRAPH_* (required)
+ * gcl_canon_batch takes HOST pointers and performs the copies; the _device
+ * form takes DEVICE pointers and only enqueues work on the context stream
+ * (call gcl_sync before reading results).  Both return GCL_OK when every
+ * graph was processed, else the first failing graph's error. */
+int gcl_canon_batch(gcl_context* ctx, int count, const int64_t* voff,
+                    const int64_t* eoff, const int32_t* rowptr,
+                    const int32_t* col, const int32_t* color, int max_aut,
+                    uint8_t* out_dense, const int64_t* ooff, int32_t* out_label,
+                    int64_t* out_stats, int32_t* out_status);
+
+int gcl_canon_batch_device_async(gcl_context* ctx, int count,
+                                 const int64_t* d_voff, const int64_t* d_eoff,
+                                 const int32_t* d_rowptr, const int32_t* d_col,
+                                 const int32_t* d_color, int max_aut, int max_n,
+                                 uint8_t* d_out_dense, const int64_t* d_ooff,
+                                 int32_t* d_out_label, int64_t* d_out_stats,
+                                 int32_t* d_out_status);
+int gcl_sync(gcl_context* ctx);
+
+/* ---- isomorphism (main.cpp:172-197) --------------------------------------
+ * *verdict = 1 when the canonical upper triangles are equal (ISOMORPHIC),
+ * 0 otherwise.  Graphs with different vertex counts are NOT ISOMORPHIC (the
+ * reference compares n1 x n1 entries and reads out of bounds when n2 < n1). */
+int gcl_iso(gcl_context* ctx, const int32_t* rowptr1, const int32_t* col1,
+            const int32_t* color1, int n1, const int32_t* rowptr2,
+            const int32_t* col2, const int32_t* color2, int n2, int max_aut,
+            int* verdict);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GCL_H */

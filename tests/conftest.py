@@ -1,0 +1,48 @@
+import importlib
+import json
+import os
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+for p in (ROOT, os.path.join(ROOT, "oracle")):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+PKG_NAME = "gpu-canonical-labeling_b200"
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200)")
+
+
+@pytest.fixture(scope="session")
+def pkg():
+    return importlib.import_module(PKG_NAME)
+
+
+@pytest.fixture(scope="session")
+def G():
+    return importlib.import_module(PKG_NAME + ".graphs")
+
+
+@pytest.fixture(scope="session")
+def golden():
+    with open(os.path.join(ROOT, "tests", "golden", "golden.json")) as f:
+        return json.load(f)["records"]
+
+
+@pytest.fixture(scope="session")
+def oracle_mod():
+    import oracle  # noqa: F401  (oracle/oracle.py, test infrastructure)
+    if not oracle.available("port"):
+        import subprocess
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
+    return oracle
+
+
+def golden_graph(G, rec):
+    import numpy as np
+    e = np.asarray(rec["edges"], dtype=np.int64).reshape(-1, 2)
+    return G.from_edges(rec["n"], e, rec["color"])

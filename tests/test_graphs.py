@@ -1,0 +1,44 @@
+"""Graph model, DIMACS parsing (CSRGraph::fromDIMACS semantics) and arenas."""
+import numpy as np
+import pytest
+
+
+def test_dimacs_semantics(G):
+    txt = "c comment\n\np edge 5 99\nn 2 7\nn 0 3\nn 9 1\ne 1 2\ne 3 3\ne 5 1\ne 2 4\n"
+    g = G.parse_dimacs(txt)
+    assert g.n == 5
+    assert g.rowptr.tolist() == [0, 2, 4, 4, 5, 6]
+    assert g.col.tolist() == [1, 4, 0, 3, 1, 0]
+    assert g.color.tolist() == [0, 7, 0, 0, 0]
+    h = G.parse_dimacs(G.to_dimacs(g))
+    assert np.array_equal(h.rowptr, g.rowptr) and np.array_equal(h.col, g.col)
+    assert np.array_equal(h.color, g.color)
+
+
+def test_duplicate_edges_rejected(G):
+    with pytest.raises(ValueError):
+        G.parse_dimacs("p edge 3 2\ne 1 2\ne 2 1\n")
+
+
+def test_arena_roundtrip(G):
+    gs = G.small_batch(30, seed=2)
+    a = G.pack(gs)
+    assert a.count == 30
+    for i, g in enumerate(gs):
+        h = a.graph(i)
+        assert h.n == g.n and np.array_equal(h.rowptr, g.rowptr) and np.array_equal(h.col, g.col)
+    assert a.out_offsets()[-1] == sum(g.n * g.n for g in gs)
+
+
+def test_generators(G):
+    rng = np.random.default_rng(0)
+    r = G.random_regular(64, 3, rng)
+    assert (np.diff(r.rowptr) == 3).all()
+    t = G.torus(5)
+    assert t.n == 25 and (np.diff(t.rowptr) == 4).all()
+    u = G.disjoint_union(r, 3)
+    assert u.n == 192 and u.m == 3 * r.m
+    for g in G.small_batch(100, seed=1):
+        assert 10 <= g.n <= 64
+        assert np.diff(g.rowptr).max() <= 4
+        assert g.m >= g.n - 1
