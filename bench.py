@@ -59,6 +59,7 @@ def parse():
                    help="wall-clock budget of the CPU-baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-plain", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
     return p.parse_args()
 
 
@@ -174,51 +175,62 @@ def reference_arm(args):
 # GPU side
 # --------------------------------------------------------------------------
 class Clocks:
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    """SM clock and throttle reasons sampled through NVML every ~2 ms on a
+    background thread (read-only queries; no setting is changed)."""
+
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+               "sw_power_cap": 0x4}
 
     def __init__(self, device):
+        import threading
         self.device = device
-        self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{device}.csv")
+        self.samples = []
+        self.stop_ev = threading.Event()
+        self.thread = None
+        self.window = None
+
+    def _loop(self):
+        import pynvml as N
+        h = N.nvmlDeviceGetHandleByIndex(self.device)
+        while not self.stop_ev.is_set():
+            try:
+                sm = N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM)
+                rs = N.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.samples.append((time.perf_counter(), sm, rs))
+            except Exception:
+                pass
+            time.sleep(0.002)
 
     def start(self):
-        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        import threading
         try:
-            self.f = open(self.path, "w")
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
-                stderr=subprocess.DEVNULL)
+            import pynvml as N
+            N.nvmlInit()
+            h = N.nvmlDeviceGetHandleByIndex(self.device)
+            self.max_mhz = N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM)
         except Exception:
-            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._loop, daemon=True)
+        self.thread.start()
+
+    def mark(self, t0, t1):
+        self.window = (t0, t1)
 
     def stop(self):
-        if not self.proc:
+        if not self.thread:
             return None
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except Exception:
-            self.proc.kill()
-        self.f.close()
-        rows = []
-        for ln in open(self.path):
-            parts = [x.strip() for x in ln.split(",")]
-            if len(parts) >= 9:
-                rows.append(parts)
+        self.stop_ev.set()
+        self.thread.join()
+        rows = self.samples
+        if self.window:
+            t0, t1 = self.window
+            inside = [r for r in rows if t0 <= r[0] <= t1]
+            rows = inside or [min(rows, key=lambda r: abs(r[0] - t1))] if rows else []
         if not rows:
             return None
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if "Active" in r[5 + i]
-                          and "Not" not in r[5 + i]})
-        load = [s for s in sm if s > 0.5 * (max(mx) if mx else 1)]
-        return {"sm_mhz": float(np.median(load or sm or [0])),
-                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
-                "samples": len(rows)}
+        reasons = sorted({k for _, _, rs in rows for k, bit in self.REASONS.items() if rs & bit})
+        return {"sm_mhz": float(np.median([r[1] for r in rows])), "sm_max_mhz": self.max_mhz,
+                "reasons": reasons, "samples": len(rows), "source": "nvml, 2 ms period"}
 
 
 def read_traffic():
@@ -302,6 +314,7 @@ def gpu_arm(args):
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
            for _ in range(args.steps)]
     barrier()
+    tw0 = time.perf_counter()
     for i in range(args.steps):
         flush.zero_()  # L2 flush outside the timed events
         stream.wait_stream(torch.cuda.current_stream())
@@ -310,6 +323,7 @@ def gpu_arm(args):
         evs[i][1].record(stream)
         torch.cuda.current_stream().wait_stream(stream)
     barrier()
+    clocks.mark(tw0, time.perf_counter())
     clk = clocks.stop()
     per = np.array([a.elapsed_time(b) for a, b in evs])  # ms
     dev_ms = float(per.sum())
@@ -335,16 +349,16 @@ def gpu_arm(args):
         if rc != 0:
             raise RuntimeError(f"gcl_canon_batch failed: {rc}")
 
-    for _ in range(max(2, args.warmup // 2)):
+    for _ in range(max(2, args.warmup // 2) if not args.no_e2e else 0):
         e2e_call()
     barrier()
     e2e_t = []
-    for _ in range(args.steps):
+    for _ in range(args.steps if not args.no_e2e else 0):
         t0 = time.perf_counter()
         e2e_call()
         e2e_t.append(time.perf_counter() - t0)
     barrier()
-    e2e_s = float(np.sum(e2e_t))
+    e2e_s = float(np.sum(e2e_t)) if e2e_t else float("nan")
     if world > 1:
         t = torch.tensor([e2e_s], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)

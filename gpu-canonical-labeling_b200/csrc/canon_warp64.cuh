@@ -5,23 +5,29 @@
 // number of stored automorphisms and the number of search-tree nodes equal
 // the reference's on every input.  What changes is the representation:
 //
-//   * a vertex set is one 64-bit mask; lane L owns vertices L and L+32;
+//   * a vertex set is one 64-bit mask; lane L owns vertices L and L+32 and
+//     positions L and L+32;
 //   * the ordered partition is vertex-indexed: each vertex knows the start
-//     position `cs` of its cell and the member mask `cm` of that cell, and the
-//     warp holds `starts`, the mask of cell start positions.  The order of
-//     vertices inside a cell is never stored: the reference's refinement and
-//     search depend only on the cells as sets (fragments are ordered by count,
-//     targets and branch vertices are chosen by position and by vertex id),
-//     so leaves, codes and pruning decisions are unchanged;
+//     position `cs` of its cell, each cell start knows the member mask of its
+//     cell, and the warp holds `starts`, the mask of cell start positions.  The
+//     order of vertices inside a cell is never stored: the reference's
+//     refinement and search depend only on the cells as sets (fragments are
+//     ordered by count, targets and branch vertices are chosen by position and
+//     by vertex id), so leaves, codes and pruning decisions are unchanged;
 //   * counting neighbours in a splitter is popc(adj[v] & splitter); splitting
 //     every cell at once is a radix pass over the count bits with warp
-//     ballots; only the invariant hash (a serial chain, order-dependent) is
-//     folded by lane 0 over the split cells in position order;
+//     ballots; only the invariant hash (a serial, order-dependent chain) is
+//     folded over a mask of hash items in position order;
 //   * a leaf certificate is one 64-bit row per canonical vertex; the
 //     reference's n^2 upper-triangle compare (sequential.cpp:114-124) becomes
 //     a masked row compare plus a warp min, and the isAutomorphism test
 //     against the first leaf (sequential.cpp:127-167) becomes certificate
 //     equality, which is the same predicate for a bijection.
+//
+// Code layout: the warp's state lives in shared memory between phases and
+// each phase (refine, individualize, backtrack, orbits, leaf work) is one
+// non-inlined function, so the hot instruction footprint stays small enough
+// for the instruction caches when many warps per SM sit in different phases.
 #pragma once
 #include <cstdint>
 
@@ -31,6 +37,8 @@ namespace gcl {
 
 constexpr int kW64MaxN = 64;
 constexpr int kW64Levels = kW64MaxN + 2;
+constexpr int kW64Threads = 128;  // 4 warps per block, one graph per warp
+constexpr int kW64Warps = kW64Threads / 32;
 
 enum GraphStatus : int32_t {
   kOk = 0,
@@ -61,20 +69,30 @@ struct TcHdr {
 };
 
 struct __align__(16) W64Smem {
-  uint64_t adj[kW64MaxN];
-  uint64_t first_cert[kW64MaxN];  // first leaf, row per canonical vertex
+  uint64_t adj[kW64MaxN];         // vertex -> neighbour mask
+  uint64_t cmask[kW64MaxN];       // cell start position -> member mask
+  uint64_t first_cert[kW64MaxN];  // first leaf, one row per canonical vertex
   uint64_t best_cert[kW64MaxN];   // best leaf
   TcHdr tc[kW64Levels];
   uint32_t dsu[kW64MaxN];
   uint16_t firstcode[kW64Levels];
   uint16_t canoncode[kW64Levels];
-  uint8_t inlev[kW64MaxN];  // in_level of the cell starting at a position
-  uint8_t fk[kW64MaxN];     // count value of the fragment starting at a position
+  uint8_t cs[kW64MaxN];     // vertex -> start position of its cell
+  uint8_t inlev[kW64MaxN];  // cell start position -> in_level
+  uint8_t fk[kW64MaxN];     // fragment start position -> its neighbour count
   uint8_t seq[kW64MaxN];
   uint8_t first_seq[kW64MaxN];
   uint8_t best_seq[kW64MaxN];
+  uint8_t fpos[kW64MaxN];  // vertex -> position in the first leaf
+  uint8_t bpos[kW64MaxN];  // vertex -> position in the best leaf
   uint8_t map[kW64MaxN];
 };
+
+// One W64Smem per warp of the block, at namespace scope so every phase
+// function addresses it directly in the shared window.
+__shared__ W64Smem g_w64[kW64Warps];
+
+__device__ __forceinline__ W64Smem& w64_smem() { return g_w64[threadIdx.x >> 5]; }
 
 struct BatchArgs {
   int count;
@@ -102,891 +120,906 @@ __host__ __device__ constexpr uint64_t w64_slot_bytes(uint32_t aut_cap) {
   return ((uint64_t)kW64Levels * 64u + (uint64_t)aut_cap * 64u + 255u) & ~255ull;
 }
 
-template <int VPL>
-struct W64Lane {
-  uint64_t adj[VPL];
-  uint64_t cm[VPL];
-  uint32_t cs[VPL];
-  uint32_t fpos[VPL];
-  uint32_t bpos[VPL];
+__device__ __forceinline__ uint64_t ballot2(bool a, bool b) {
+  return (uint64_t)__ballot_sync(GCL_FULL, a) | ((uint64_t)__ballot_sync(GCL_FULL, b) << 32);
+}
+__device__ __forceinline__ uint64_t bit64(uint32_t p) { return 1ull << p; }
+
+// ---------------------------------------------------------------------------
+// Partition_s_refinement (partition_refinement.cpp:150-485).
+// `active` holds the start positions of the initially active cells.  Returns
+// the new starts mask and the refinement code (the caller increments level).
+// ---------------------------------------------------------------------------
+struct W64Refined {
+  uint64_t starts;
+  int code;
+  int ok;
 };
 
-template <int VPL>
-__device__ __forceinline__ uint64_t ballot64(const bool (&b)[VPL]) {
-  uint64_t m = __ballot_sync(GCL_FULL, b[0]);
-  if (VPL > 1) m |= (uint64_t)__ballot_sync(GCL_FULL, b[VPL > 1 ? 1 : 0]) << 32;
-  return m;
+__device__ __noinline__ W64Refined w64_refine(int n, uint64_t starts, uint32_t level,
+                                              uint64_t active) {
+  W64Smem& S = w64_smem();
+  const uint32_t lane = lane_id();
+  const uint64_t full = low_mask((uint32_t)n);
+  const uint32_t v0 = lane, v1 = lane + 32;
+  const bool ok0 = v0 < (uint32_t)n, ok1 = v1 < (uint32_t)n;
+  const uint64_t adj0 = ok0 ? S.adj[v0] : 0ull, adj1 = ok1 ? S.adj[v1] : 0ull;
+  uint32_t cs0 = ok0 ? S.cs[v0] : 0u, cs1 = ok1 ? S.cs[v1] : 0u;
+  uint64_t cm0 = ok0 ? S.cmask[cs0] : 0ull, cm1 = ok1 ? S.cmask[cs1] : 0ull;
+  const uint32_t lvl1 = level + 1;
+  const uint64_t lastbit = bit64((uint32_t)n - 1);
+  uint32_t lc = popc64(starts), hint = 0, iters = 0;
+  int ok = 1;
+  while (starts != full && active) {
+    if (++iters > 64u * 64u + 64u) {  // every step removes an active cell or splits one
+      ok = 0;
+      break;
+    }
+    // splitter: hint if active, else the next active after it, else wrap
+    uint32_t s;
+    if ((active >> hint) & 1ull) {
+      s = hint;
+    } else {
+      const uint64_t a = active & ge_mask(hint + 1);
+      s = ctz64(a ? a : active);
+    }
+    active &= ~bit64(s);
+    const uint64_t nx = starts & ge_mask(s + 1);
+    const uint32_t e = nx ? ctz64(nx) : (uint32_t)n;
+    lc = mash(lc, s + e - 1);  // split1 + split2
+    const uint64_t spl = ballot2(ok0 && cs0 == s, ok1 && cs1 == s);
+    if (e - s == 1) {
+      // Singleton splitter {w}: every cell meeting N(w) partially splits into
+      // [neighbours, non-neighbours].
+      if (popc64(spl) != 1) {
+        ok = 0;
+        break;
+      }
+      const uint64_t N = S.adj[ctz64(spl)];
+      uint64_t ns = 0;
+      {
+        const uint64_t CN = cm0 & N;
+        if (ok0 && CN != 0 && CN != cm0) {
+          if ((N >> v0) & 1ull) {
+            cm0 = CN;
+          } else {
+            cm0 &= ~N;
+            cs0 += popc64(CN);
+            ns |= bit64(cs0);
+          }
+        }
+      }
+      {
+        const uint64_t CN = cm1 & N;
+        if (ok1 && CN != 0 && CN != cm1) {
+          if ((N >> v1) & 1ull) {
+            cm1 = CN;
+          } else {
+            cm1 &= ~N;
+            cs1 += popc64(CN);
+            ns |= bit64(cs1);
+          }
+        }
+      }
+      const uint64_t NS = warp_or64(ns);
+      if (NS) {
+        // in_level: the neighbour fragment is new (level+1), the
+        // non-neighbour fragment keeps the cell's old in_level (:463-465)
+        uint32_t w0 = 0xffu, w1 = 0xffu;
+        if ((NS >> v0) & 1ull) w0 = S.inlev[msb64(starts & low_mask(v0))];
+        if ((NS >> v1) & 1ull) w1 = S.inlev[msb64(starts & low_mask(v1))];
+        const uint64_t all = starts | NS;
+        uint64_t t = NS, splitc = 0;
+        while (t) {
+          const uint32_t p = ctz64(t);
+          t &= t - 1;
+          const uint32_t c = msb64(starts & low_mask(p));
+          splitc |= bit64(c);
+          const uint64_t q = all & ge_mask(p + 1);
+          const uint32_t nb = p - c, nn = (q ? ctz64(q) : (uint32_t)n) - p;
+          lc = mash(lc, p - 1);  // cell.first + neighbors_size - 1 (:399-409)
+          // active set (:414-435)
+          if (((active >> c) & 1ull) || nb >= nn) {
+            active |= bit64(p);
+            if (nn == 1) hint = p;
+          } else {
+            active |= bit64(c);
+            if (nb == 1) hint = c;
+          }
+        }
+        __syncwarp();
+        if (w0 != 0xffu) S.inlev[v0] = (uint8_t)w0;
+        else if ((splitc >> v0) & 1ull) S.inlev[v0] = (uint8_t)lvl1;
+        if (w1 != 0xffu) S.inlev[v1] = (uint8_t)w1;
+        else if ((splitc >> v1) & 1ull) S.inlev[v1] = (uint8_t)lvl1;
+        starts = all;
+      }
+    } else {
+      // Non-singleton splitter: fragments in ascending neighbour count.
+      lc = mash(lc, e - s);
+      const uint32_t k0 = ok0 ? popc64(adj0 & spl) : 0u, k1 = ok1 ? popc64(adj1 & spl) : 0u;
+      const uint32_t mx = __reduce_max_sync(GCL_FULL, max(k0, k1));
+      uint64_t eq0 = cm0, eq1 = cm1;
+      uint32_t lt0 = 0, lt1 = 0;
+      for (int b = mx ? 31 - __clz((int)mx) : -1; b >= 0; --b) {
+        const bool b0 = (k0 >> b) & 1u, b1 = (k1 >> b) & 1u;
+        const uint64_t M = ballot2(b0, b1);
+        if (b0) {
+          lt0 += popc64(eq0 & ~M);
+          eq0 &= M;
+        } else {
+          eq0 &= ~M;
+        }
+        if (b1) {
+          lt1 += popc64(eq1 & ~M);
+          eq1 &= M;
+        } else {
+          eq1 &= ~M;
+        }
+      }
+      uint64_t ns = 0;
+      if (ok0) {
+        cs0 += lt0;
+        cm0 = eq0;
+        ns |= bit64(cs0);
+        S.fk[cs0] = (uint8_t)k0;
+      }
+      if (ok1) {
+        cs1 += lt1;
+        cm1 = eq1;
+        ns |= bit64(cs1);
+        S.fk[cs1] = (uint8_t)k1;
+      }
+      const uint64_t NS = warp_or64(ns) & ~starts;
+      __syncwarp();
+      // hash items in position order: every start of a non-singleton old
+      // cell (common count) and every new fragment start (:253-373)
+      const uint64_t singles = starts & ((starts >> 1) | lastbit);
+      uint64_t t = (starts & ~singles) | NS;
+      while (t) {
+        const uint32_t p = ctz64(t);
+        t &= t - 1;
+        lc = mash(lc, (uint32_t)S.fk[p] + p);
+      }
+      if (NS) {
+        const uint64_t all = starts | NS;
+        // in_level of the fragments of split cells: level+1, the last one
+        // keeps the cell's old in_level (:342, 463-465)
+        uint32_t w0 = 0xffu, w1 = 0xffu;
+        if ((all >> v0) & 1ull) {
+          const uint32_t c = msb64(starts & low_mask(v0 + 1));
+          const uint64_t nc = starts & ge_mask(c + 1);
+          const uint32_t end = nc ? ctz64(nc) : (uint32_t)n;
+          if (NS & low_mask(end) & ge_mask(c + 1))
+            w0 = (v0 == msb64(all & low_mask(end))) ? S.inlev[c] : lvl1;
+        }
+        if ((all >> v1) & 1ull) {
+          const uint32_t c = msb64(starts & low_mask(v1 + 1));
+          const uint64_t nc = starts & ge_mask(c + 1);
+          const uint32_t end = nc ? ctz64(nc) : (uint32_t)n;
+          if (NS & low_mask(end) & ge_mask(c + 1))
+            w1 = (v1 == msb64(all & low_mask(end))) ? S.inlev[c] : lvl1;
+        }
+        // active set (:436-460): every new fragment; for a cell that was not
+        // active, its first fragment in and its first largest fragment out.
+        // hint: the last new singleton fragment in position order.
+        const uint64_t single_all = all & ((all >> 1) | lastbit);
+        const uint64_t hs = NS & single_all;
+        if (hs) hint = msb64(hs);
+        const uint64_t was = active;
+        active |= NS;
+        t = NS;
+        while (t) {
+          const uint32_t c = msb64(starts & low_mask(ctz64(t)));
+          const uint64_t nc = starts & ge_mask(c + 1);
+          const uint32_t end = nc ? ctz64(nc) : (uint32_t)n;
+          t &= ~low_mask(end);
+          if ((was >> c) & 1ull) continue;
+          uint64_t fr = all & ge_mask(c) & low_mask(end);
+          uint32_t maxsz = 0, maxp = c;
+          while (fr) {
+            const uint32_t f = ctz64(fr);
+            fr &= fr - 1;
+            const uint32_t sz = (fr ? ctz64(fr) : end) - f;
+            if (sz > maxsz) {
+              maxsz = sz;
+              maxp = f;
+            }
+          }
+          active |= bit64(c);
+          active &= ~bit64(maxp);
+        }
+        __syncwarp();
+        if (w0 != 0xffu) S.inlev[v0] = (uint8_t)w0;
+        if (w1 != 0xffu) S.inlev[v1] = (uint8_t)w1;
+        starts = all;
+      }
+    }
+  }
+  __syncwarp();
+  if (ok0) {
+    S.cs[v0] = (uint8_t)cs0;
+    S.cmask[cs0] = cm0;
+  }
+  if (ok1) {
+    S.cs[v1] = (uint8_t)cs1;
+    S.cmask[cs1] = cm1;
+  }
+  __syncwarp();
+  return {starts, cleanup(mash(lc, popc64(starts))), ok};
 }
 
-template <int VPL>
-class W64Search {
- public:
-  __device__ W64Search(W64Smem& s, const BatchArgs& a, int n, uint8_t* slot)
-      : S(s), A(a), n(n), reps(slot), auts(slot + (uint64_t)kW64Levels * 64u) {
-    lane = lane_id();
-    full = low_mask((uint32_t)n);
+// split_by_and_refine's split (partition_refinement.cpp:486-528): vertex v
+// moves to a singleton cell at t, the rest of the cell starts at t+1.
+// Returns false when the cell is already a singleton (nothing to refine).
+__device__ __noinline__ bool w64_individualize(int n, uint32_t level, uint32_t v, uint32_t t) {
+  W64Smem& S = w64_smem();
+  const uint32_t lane = lane_id();
+  const uint64_t mem = S.cmask[t];
+  if (popc64(mem) <= 1) return false;
+  const uint32_t v0 = lane, v1 = lane + 32;
+  __syncwarp();
+  if (v0 < (uint32_t)n && ((mem >> v0) & 1ull) && v0 != v) S.cs[v0] = (uint8_t)(t + 1);
+  if (v1 < (uint32_t)n && ((mem >> v1) & 1ull) && v1 != v) S.cs[v1] = (uint8_t)(t + 1);
+  if (lane == 0) {
+    S.cmask[t] = bit64(v);
+    S.cmask[t + 1] = mem & ~bit64(v);
+    S.inlev[t + 1] = S.inlev[t];
+    S.inlev[t] = (uint8_t)(level + 1);
   }
+  __syncwarp();
+  return true;
+}
 
-  W64Smem& S;
-  const BatchArgs& A;
-  const int n;
-  uint8_t* reps;
-  uint8_t* auts;
-  uint32_t lane;
-  uint64_t full;
-  W64Lane<VPL> L;
+// reconstruct_at_level (partition_refinement.cpp:541-604): every maximal run
+// of cells created after level Lv merges with the cell that follows it, and
+// the merged cell takes that cell's in_level.  Returns the new starts mask
+// (0 if the partition is inconsistent).
+__device__ __noinline__ uint64_t w64_backtrack(int n, uint64_t starts, uint32_t Lv) {
+  W64Smem& S = w64_smem();
+  const uint32_t lane = lane_id();
+  const uint32_t q0 = lane, q1 = lane + 32;
+  const bool st0 = q0 < (uint32_t)n && ((starts >> q0) & 1ull);
+  const bool st1 = q1 < (uint32_t)n && ((starts >> q1) & 1ull);
+  const bool big0 = st0 && S.inlev[q0] > Lv, big1 = st1 && S.inlev[q1] > Lv;
+  const uint64_t BIG = ballot2(big0, big1);
+  if (!BIG) return starts;
+  bool sv0 = st0, sv1 = st1;
+  if (st0 && q0 > 0 && ((BIG >> msb64(starts & low_mask(q0))) & 1ull)) sv0 = false;
+  if (st1 && ((BIG >> msb64(starts & low_mask(q1))) & 1ull)) sv1 = false;
+  const uint64_t NST = ballot2(sv0, sv1);
+  uint32_t nl0 = 0, nl1 = 0;
+  uint64_t m0 = 0, m1 = 0;
+  bool bad = false, w0 = false, w1 = false;
+  if (sv0 && big0) {
+    const uint64_t j = starts & ~BIG & ge_mask(q0 + 1);
+    if (!j) bad = true;
+    else nl0 = S.inlev[ctz64(j)];
+    const uint64_t nn = NST & ge_mask(q0 + 1);
+    uint64_t r = starts & ge_mask(q0) & low_mask(nn ? ctz64(nn) : (uint32_t)n);
+    while (r) {
+      m0 |= S.cmask[ctz64(r)];
+      r &= r - 1;
+    }
+    w0 = true;
+  }
+  if (sv1 && big1) {
+    const uint64_t j = starts & ~BIG & ge_mask(q1 + 1);
+    if (!j) bad = true;
+    else nl1 = S.inlev[ctz64(j)];
+    const uint64_t nn = NST & ge_mask(q1 + 1);
+    uint64_t r = starts & ge_mask(q1) & low_mask(nn ? ctz64(nn) : (uint32_t)n);
+    while (r) {
+      m1 |= S.cmask[ctz64(r)];
+      r &= r - 1;
+    }
+    w1 = true;
+  }
+  if (__any_sync(GCL_FULL, bad)) return 0;
+  __syncwarp();
+  if (w0) {
+    S.inlev[q0] = (uint8_t)nl0;
+    S.cmask[q0] = m0;
+  }
+  if (w1) {
+    S.inlev[q1] = (uint8_t)nl1;
+    S.cmask[q1] = m1;
+  }
+  if (q0 < (uint32_t)n) S.cs[q0] = (uint8_t)msb64(NST & low_mask((uint32_t)S.cs[q0] + 1));
+  if (q1 < (uint32_t)n) S.cs[q1] = (uint8_t)msb64(NST & low_mask((uint32_t)S.cs[q1] + 1));
+  __syncwarp();
+  return NST;
+}
 
-  // search state (warp-uniform), Nauty_Sequential members (sequential.h:24-45)
-  uint64_t starts = 0;
-  uint32_t level = 0, seqlen = 0;
-  int code = 0;
-  int canon_level = 0, eqlevcanon = 0, comp_canon = 0;
-  uint32_t eqlevfirst = 0;
-  int tcl = 0;
-  bool first_found = false;
-  uint32_t first_seqlen = 0, best_seqlen = 0;
-  int num_aut = 0;
-  int64_t nodes = 0;
-  int32_t status = kOk;
+// Certificate rows of the lane's two vertices in a discrete partition: the
+// neighbours renamed to positions (buildPermutedFlatAdjacencyMatrixArray,
+// CSRGraph.cpp:332-351).  Row of vertex v belongs to canonical vertex cs[v].
+struct Rows2 {
+  uint64_t r0, r1;
+};
+
+__device__ __noinline__ Rows2 w64_leaf_rows(int n) {
+  W64Smem& S = w64_smem();
+  const uint32_t lane = lane_id();
+  Rows2 R{0ull, 0ull};
+  if (lane < (uint32_t)n) {
+    uint64_t a = S.adj[lane];
+    while (a) {
+      R.r0 |= bit64(S.cs[ctz64(a)]);
+      a &= a - 1;
+    }
+  }
+  if (lane + 32 < (uint32_t)n) {
+    uint64_t a = S.adj[lane + 32];
+    while (a) {
+      R.r1 |= bit64(S.cs[ctz64(a)]);
+      a &= a - 1;
+    }
+  }
+  return R;
+}
+
+// compare_adj_upper(current, stored) (sequential.cpp:114-124)
+__device__ __noinline__ int w64_cmp_upper(int n, Rows2 R, const uint64_t* B) {
+  W64Smem& S = w64_smem();
+  const uint32_t lane = lane_id();
+  uint32_t row = 64u;
+  bool s0 = false, s1 = false;
+  uint32_t p0 = 64u, p1 = 64u;
+  if (lane < (uint32_t)n) {
+    p0 = S.cs[lane];
+    const uint64_t d = (R.r0 ^ B[p0]) & ge_mask(p0 + 1);
+    if (d) {
+      row = p0;
+      s0 = (R.r0 >> ctz64(d)) & 1ull;
+    }
+  }
+  if (lane + 32 < (uint32_t)n) {
+    p1 = S.cs[lane + 32];
+    const uint64_t d = (R.r1 ^ B[p1]) & ge_mask(p1 + 1);
+    if (d) {
+      row = min(row, p1);
+      s1 = (R.r1 >> ctz64(d)) & 1ull;
+    }
+  }
+  const uint32_t mrow = __reduce_min_sync(GCL_FULL, row);
+  if (mrow == 64u) return 0;
+  return ballot2(p0 == mrow && s0, p1 == mrow && s1) ? 1 : -1;
+}
+
+__device__ __forceinline__ bool w64_rows_equal(int n, Rows2 R, const uint64_t* B) {
+  W64Smem& S = w64_smem();
+  const uint32_t lane = lane_id();
+  const bool d0 = lane < (uint32_t)n && R.r0 != B[S.cs[lane]];
+  const bool d1 = lane + 32 < (uint32_t)n && R.r1 != B[S.cs[lane + 32]];
+  return ballot2(d0, d1) == 0;
+}
+
+// Rows into a stored certificate and the vertex positions into `pos`.
+__device__ __noinline__ void w64_store_leaf(int n, Rows2 R, uint64_t* B, uint8_t* pos) {
+  W64Smem& S = w64_smem();
+  const uint32_t lane = lane_id();
+  __syncwarp();
+  if (lane < (uint32_t)n) {
+    B[S.cs[lane]] = R.r0;
+    pos[lane] = S.cs[lane];
+  }
+  if (lane + 32 < (uint32_t)n) {
+    B[S.cs[lane + 32]] = R.r1;
+    pos[lane + 32] = S.cs[lane + 32];
+  }
+  __syncwarp();
+}
+
+// aut[label[j]] = elem[j] with the stored leaf given by its vertex positions
+// (sequential.cpp:505-520, 544-555), written to one ring slot.
+__device__ __noinline__ void w64_store_aut(int n, const uint8_t* pos, uint8_t* dst) {
+  W64Smem& S = w64_smem();
+  const uint32_t lane = lane_id();
+  __syncwarp();
+  if (lane < (uint32_t)n) S.map[S.cs[lane]] = (uint8_t)lane;  // position -> vertex
+  if (lane + 32 < (uint32_t)n) S.map[S.cs[lane + 32]] = (uint8_t)(lane + 32);
+  __syncwarp();
+  if (lane < (uint32_t)n) dst[lane] = S.map[pos[lane]];
+  if (lane + 32 < (uint32_t)n) dst[lane + 32] = S.map[pos[lane + 32]];
+  __syncwarp();
+}
+
+// get_gca_level (sequential.cpp:183-213)
+__device__ __forceinline__ int w64_gca(const uint8_t* a, uint32_t na, uint32_t seqlen) {
+  W64Smem& S = w64_smem();
+  const uint32_t lane = lane_id();
+  const uint32_t m = min(na, seqlen);
+  const bool d0 = lane < m && a[lane] != S.seq[lane];
+  const bool d1 = lane + 32 < m && a[lane + 32] != S.seq[lane + 32];
+  const uint64_t b = ballot2(d0, d1);
+  return b ? (int)ctz64(b) + 1 : -1;
+}
+
+// target_cell_selector (partition_refinement.cpp:607-655) with hint -1: the
+// first non-singleton cell.
+__device__ __forceinline__ void w64_select_tc(int n, uint64_t starts, int tcl) {
+  W64Smem& S = w64_smem();
+  const uint64_t singles = starts & ((starts >> 1) | bit64((uint32_t)n - 1));
+  const uint32_t t = ctz64(starts & ~singles);
+  const uint64_t mem = S.cmask[t];
+  __syncwarp();
+  if (lane_id() == 0) {
+    TcHdr& h = S.tc[tcl];
+    h.members = mem;
+    h.repmask = mem;
+    h.last = 0;
+    h.counter = 0;
+    h.first = (uint8_t)t;
+    h.reps_valid = 0;
+  }
+  __syncwarp();
+}
+
+// Root of x in the shared union-find; parents only point to smaller
+// vertices, so a path has at most n steps.
+__device__ __forceinline__ uint32_t w64_find(volatile uint32_t* d, uint32_t x) {
+  uint32_t p = d[x];
+  for (int step = 0; p < x && step < kW64MaxN; ++step) {
+    x = p;
+    p = d[x];
+  }
+  return x;
+}
+
+// subgroup_fixing_sequence + compute_orbits_fast (perm_group.cpp:5-116):
+// orbits of the stored automorphisms that fix the current vertex sequence,
+// merged into the target cell's representatives.  Returns false when a
+// consistency bound was hit.
+__device__ __noinline__ bool w64_orbits(int n, int idx, int num_aut, uint32_t max_aut,
+                                        uint32_t seqlen, uint8_t* reps, const uint8_t* auts) {
+  W64Smem& S = w64_smem();
+  const uint32_t lane = lane_id();
+  const int limit = num_aut < (int)max_aut ? num_aut : (int)max_aut;
+  int from = S.tc[idx].last;
+  if (from == -1) from = 0;
+  const uint64_t mem = S.tc[idx].members;
+  const bool rv = S.tc[idx].reps_valid;
+  uint8_t* rp = reps + (uint64_t)idx * 64u;
+  const uint32_t v0 = lane, v1 = lane + 32;
+  const bool ok0 = v0 < (uint32_t)n, ok1 = v1 < (uint32_t)n;
+  volatile uint32_t* dsu = S.dsu;
+  __syncwarp();
+  if (ok0) dsu[v0] = ((mem >> v0) & 1ull) && rv ? (uint32_t)rp[v0] : v0;
+  if (ok1) dsu[v1] = ((mem >> v1) & 1ull) && rv ? (uint32_t)rp[v1] : v1;
+  __syncwarp();
+  bool any = false;
+  for (int i = from; i < limit; ++i) {
+    const uint8_t* pm = auts + (uint64_t)i * 64u;
+    const bool bad0 = lane < seqlen && pm[S.seq[lane]] != S.seq[lane];
+    const bool bad1 = lane + 32 < seqlen && pm[S.seq[lane + 32]] != S.seq[lane + 32];
+    if (__any_sync(GCL_FULL, bad0 || bad1)) continue;
+    any = true;
+    const uint32_t i0 = ok0 ? pm[v0] : v0, i1 = ok1 ? pm[v1] : v1;
+    // hook roots (larger under smaller) until every (v, pm[v]) joins two
+    // vertices of one tree; each round merges at least two trees
+    for (int round = 0;; ++round) {
+      if (round > kW64MaxN + 1) return false;
+      bool changed = false;
+      if (i0 != v0) {
+        const uint32_t a = w64_find(dsu, v0), b = w64_find(dsu, i0);
+        if (a != b) {
+          atomicMin((uint32_t*)&dsu[max(a, b)], min(a, b));
+          changed = true;
+        }
+      }
+      if (i1 != v1) {
+        const uint32_t a = w64_find(dsu, v1), b = w64_find(dsu, i1);
+        if (a != b) {
+          atomicMin((uint32_t*)&dsu[max(a, b)], min(a, b));
+          changed = true;
+        }
+      }
+      __syncwarp();
+      if (ok0) atomicMin((uint32_t*)&dsu[v0], w64_find(dsu, v0));
+      if (ok1) atomicMin((uint32_t*)&dsu[v1], w64_find(dsu, v1));
+      __syncwarp();
+      if (!__any_sync(GCL_FULL, changed)) break;
+    }
+  }
+  if (!any) return true;
+  bool r0 = false, r1 = false;
+  if (ok0 && ((mem >> v0) & 1ull)) {
+    const uint32_t r = w64_find(dsu, v0);
+    rp[v0] = (uint8_t)r;
+    r0 = r == v0;
+  }
+  if (ok1 && ((mem >> v1) & 1ull)) {
+    const uint32_t r = w64_find(dsu, v1);
+    rp[v1] = (uint8_t)r;
+    r1 = r == v1;
+  }
+  const uint64_t rm = ballot2(r0, r1);
+  __syncwarp();
+  if (lane == 0) {
+    S.tc[idx].repmask = rm;
+    S.tc[idx].reps_valid = 1;
+  }
+  __syncwarp();
+  return true;
+}
+
+// Adjacency masks and the colour partition (initializePartition_s,
+// partition_refinement.cpp:28-68: cells are the colour classes in ascending
+// colour order).  Returns the starts mask, or 0 for invalid input.
+__device__ __noinline__ uint64_t w64_load(int n, const int32_t* rp, const int32_t* cl,
+                                          const int32_t* color, int64_t m) {
+  W64Smem& S = w64_smem();
+  const uint32_t lane = lane_id();
+  bool bad = false;
+  uint64_t a0 = 0, a1 = 0;
+  for (int k = 0; k < 2; ++k) {
+    const uint32_t v = lane + 32u * k;
+    if (v >= (uint32_t)n) continue;
+    uint64_t a = 0;
+    const int32_t b = rp[v], e = rp[v + 1];
+    if (b < 0 || e < b || (int64_t)e > m) bad = true;
+    for (int32_t i = b; i < e && !bad; ++i) {
+      const int32_t u = cl[i];
+      if (u < 0 || u >= n || (uint32_t)u == v || ((a >> u) & 1ull)) {
+        bad = true;
+        break;
+      }
+      a |= bit64((uint32_t)u);
+    }
+    S.adj[v] = a;
+    if (k)
+      a1 = a;
+    else
+      a0 = a;
+  }
+  __syncwarp();
+  // both directions stored (CSRGraph::fromDIMACS inserts both)
+  for (int k = 0; k < 2; ++k) {
+    uint64_t a = k ? a1 : a0;
+    const uint32_t v = lane + 32u * k;
+    while (a && !bad) {
+      if (!((S.adj[ctz64(a)] >> v) & 1ull)) bad = true;
+      a &= a - 1;
+    }
+  }
+  if (__any_sync(GCL_FULL, bad)) return 0;
+  const int32_t c0 = (color && lane < (uint32_t)n) ? color[lane] : 0;
+  const int32_t c1 = (color && lane + 32 < (uint32_t)n) ? color[lane + 32] : 0;
+  uint64_t starts;
+  if (!__any_sync(GCL_FULL, c0 != 0 || c1 != 0)) {
+    if (lane < (uint32_t)n) S.cs[lane] = 0;
+    if (lane + 32 < (uint32_t)n) S.cs[lane + 32] = 0;
+    if (lane == 0) S.cmask[0] = low_mask((uint32_t)n);
+    starts = 1ull;
+  } else {
+    int32_t* ct = reinterpret_cast<int32_t*>(S.dsu);
+    if (lane < (uint32_t)n) ct[lane] = c0;
+    if (lane + 32 < (uint32_t)n) ct[lane + 32] = c1;
+    __syncwarp();
+    uint32_t b0 = 0, b1 = 0;
+    uint64_t same0 = 0, same1 = 0;
+    for (int u = 0; u < n; ++u) {
+      const int32_t cu = ct[u];
+      b0 += cu < c0;
+      b1 += cu < c1;
+      same0 |= (uint64_t)(cu == c0) << u;
+      same1 |= (uint64_t)(cu == c1) << u;
+    }
+    uint64_t st = 0;
+    __syncwarp();
+    if (lane < (uint32_t)n) {
+      S.cs[lane] = (uint8_t)b0;
+      S.cmask[b0] = same0;
+      st |= bit64(b0);
+    }
+    if (lane + 32 < (uint32_t)n) {
+      S.cs[lane + 32] = (uint8_t)b1;
+      S.cmask[b1] = same1;
+      st |= bit64(b1);
+    }
+    starts = warp_or64(st);
+  }
+  if (lane < (uint32_t)n) S.inlev[lane] = 0;
+  if (lane + 32 < (uint32_t)n) S.inlev[lane + 32] = 0;
+  __syncwarp();
+  return starts;
+}
+
+// The search (sequential.cpp:216-670) for one graph.
+struct W64Result {
+  int32_t status;
+  int num_aut;
+  int64_t nodes;
+};
+
+__device__ __noinline__ W64Result w64_search(const BatchArgs& A, int n, int64_t vo, int64_t eo,
+                                             int64_t m, const int32_t* rp, uint8_t* slot) {
+  W64Smem& S = w64_smem();
+  const uint32_t lane = lane_id();
+  uint8_t* reps = slot;
+  uint8_t* auts = slot + (uint64_t)kW64Levels * 64u;
+  W64Result res{kOk, 0, 1};
+  if (n == 0) return res;  // the reference visits the (discrete) root only
   uint64_t deadline = 0;
+  if (A.budget_ns)
+    deadline = __shfl_sync(GCL_FULL, lane == 0 ? global_ns() : 0ull, 0) + A.budget_ns;
 
-  // Records a failure (warp-uniform); every caller that indexes by level
-  // checks `status` afterwards and the search loop stops.
-  __device__ __forceinline__ void fail(int32_t st) {
-    if (status == kOk) status = st;
+  uint64_t starts = w64_load(n, rp, A.col + eo, A.color ? A.color + vo : nullptr, m);
+  if (!starts) {
+    res.status = kBadInput;
+    return res;
   }
-  __device__ __forceinline__ bool out_of_time() {
-    if (!deadline) return false;
-    const uint64_t t = __shfl_sync(GCL_FULL, lane == 0 ? global_ns() : 0ull, 0);
-    return t > deadline;
-  }
+  const uint64_t full = low_mask((uint32_t)n);
+  // Nauty_Sequential state (sequential.h:24-45)
+  uint32_t level = 0, seqlen = 0, eqlevfirst = 0, first_seqlen = 0, best_seqlen = 0;
+  int code = 0, canon_level = 0, eqlevcanon = 0, comp_canon = 0, tcl = 0, num_aut = 0;
+  bool first_found = false;
+  int64_t nodes = 1;
+  int32_t status = kOk;
 
-  __device__ __forceinline__ uint32_t vid(int k) const { return lane + 32u * (uint32_t)k; }
-  __device__ __forceinline__ bool valid(int k) const { return vid(k) < (uint32_t)n; }
-
-  // ---- set-up: adjacency masks and the colour partition -------------------
-  __device__ bool load(int64_t vo, const int32_t* rp, const int32_t* cl, const int32_t* color,
-                       int64_t m) {
-    bool bad = false;
-#pragma unroll
-    for (int k = 0; k < VPL; ++k) {
-      uint64_t a = 0;
-      if (valid(k)) {
-        const uint32_t v = vid(k);
-        const int32_t b = rp[v], e = rp[v + 1];
-        if (b < 0 || e < b || (int64_t)e > m) bad = true;
-        for (int32_t i = b; i < e && !bad; ++i) {
-          const int32_t u = cl[i];
-          if (u < 0 || u >= n || (uint32_t)u == v || ((a >> u) & 1ull)) { bad = true; break; }
-          a |= 1ull << u;
-        }
-        S.adj[v] = a;
+  // the next refinement to run, given by its initially active cells; the
+  // root refinement starts with every cell active (sequential.cpp:628)
+  uint64_t pending = starts;
+  while (true) {
+    if (pending) {
+      const W64Refined r = w64_refine(n, starts, level, pending);
+      pending = 0;
+      if (!r.ok) {
+        status = kInternal;
+        break;
       }
-      L.adj[k] = a;
-    }
-    __syncwarp();
-    // symmetric adjacency (CSRGraph::fromDIMACS inserts both directions)
-#pragma unroll
-    for (int k = 0; k < VPL; ++k) {
-      uint64_t a = L.adj[k];
-      while (a && !bad) {
-        const uint32_t u = ctz64(a);
-        a &= a - 1;
-        if (!((S.adj[u] >> vid(k)) & 1ull)) bad = true;
-      }
-    }
-    if (__any_sync(GCL_FULL, bad)) return false;
-
-    // initializePartition_s (partition_refinement.cpp:28-68): cells are the
-    // colour classes in ascending colour order.
-    int32_t c[VPL];
-    bool colored = false;
-#pragma unroll
-    for (int k = 0; k < VPL; ++k) {
-      c[k] = (color && valid(k)) ? color[vo + vid(k)] : 0;
-      colored |= c[k] != 0;
-    }
-    if (!__any_sync(GCL_FULL, colored)) {
-#pragma unroll
-      for (int k = 0; k < VPL; ++k) {
-        L.cs[k] = 0;
-        L.cm[k] = full;
-      }
-      starts = n > 0 ? 1ull : 0ull;
-    } else {
-      int32_t* ctmp = reinterpret_cast<int32_t*>(S.dsu);
-#pragma unroll
-      for (int k = 0; k < VPL; ++k)
-        if (valid(k)) ctmp[vid(k)] = c[k];
+      starts = r.starts;
+      code = r.code;
+      ++level;
+      // the first path records its codes (sequential.cpp:254, 630)
       __syncwarp();
-      uint64_t st = 0;
-#pragma unroll
-      for (int k = 0; k < VPL; ++k) {
-        uint32_t below = 0;
-        uint64_t same = 0;
-        if (valid(k))
-          for (int u = 0; u < n; ++u) {
-            const int32_t cu = ctmp[u];
-            below += cu < c[k];
-            same |= (uint64_t)(cu == c[k]) << u;
-          }
-        L.cs[k] = below;
-        L.cm[k] = same;
-        if (valid(k)) st |= 1ull << below;
-      }
-      starts = warp_or64(st);
+      if (lane == 0) S.firstcode[level - 1] = (uint16_t)code;
       __syncwarp();
+      continue;
     }
-#pragma unroll
-    for (int k = 0; k < VPL; ++k)
-      if (valid(k)) S.inlev[vid(k)] = 0;
-    __syncwarp();
-    return true;
-  }
-
-  // ---- Partition_s_refinement (partition_refinement.cpp:150-485) -----------
-  __device__ int refine(uint64_t active) {
-    uint32_t lc = popc64(starts);
-    uint32_t hint = 0;
-    uint32_t iters = 0;
-    while (starts != full && active) {
-      if (++iters > 64u * 64u + 64u) {  // each step removes an active cell or splits one
-        fail(kInternal);
-        return 0;
-      }
-      uint32_t s;
-      if ((active >> hint) & 1ull) {
-        s = hint;
-      } else {
-        const uint64_t a = active & ge_mask(hint + 1);
-        s = ctz64(a ? a : active);
-      }
-      active &= ~(1ull << s);
-      const uint64_t nx = starts & ge_mask(s + 1);
-      const uint32_t e = nx ? ctz64(nx) : (uint32_t)n;
-      const uint32_t len = e - s;
-      lc = mash(lc, s + e - 1);  // split1 + split2
-      if (len > 1) lc = mash(lc, len);
-
-      bool insp[VPL];
-#pragma unroll
-      for (int k = 0; k < VPL; ++k) insp[k] = valid(k) && L.cs[k] == s;
-      const uint64_t spl = ballot64<VPL>(insp);  // splitter members
-
-      if (len == 1) {
-        // singleton splitter: every cell meeting N(w) partially splits into
-        // [neighbours, non-neighbours]
-        if (popc64(spl) != 1) {
-          fail(kInternal);
-          return 0;
-        }
-        const uint64_t N = S.adj[ctz64(spl)];
-        uint64_t ns = 0;
-#pragma unroll
-        for (int k = 0; k < VPL; ++k) {
-          if (!valid(k)) continue;
-          const uint64_t C = L.cm[k], CN = C & N;
-          if (CN != 0 && CN != C) {
-            if ((N >> vid(k)) & 1ull) {
-              L.cm[k] = CN;
-            } else {
-              L.cm[k] = C & ~N;
-              L.cs[k] += popc64(CN);
-              ns |= 1ull << L.cs[k];
-            }
-          }
-        }
-        const uint64_t NS = warp_or64(ns);
-        if (NS) {
-          uint32_t o_lc = lc, o_hint = hint;
-          uint64_t o_act = active;
-          if (lane == 0) {
-            const uint64_t all = starts | NS;
-            uint64_t t = NS;
-            while (t) {
-              const uint32_t p = ctz64(t);
-              t &= t - 1;
-              const uint32_t c = msb64(starts & low_mask(p));
-              const uint64_t q = all & ge_mask(p + 1);
-              const uint32_t qe = q ? ctz64(q) : (uint32_t)n;
-              const uint32_t nb = p - c, nn = qe - p;
-              o_lc = mash(o_lc, p - 1);  // cell.first + neighbors_size - 1
-              const uint8_t old = S.inlev[c];
-              S.inlev[c] = (uint8_t)(level + 1);
-              S.inlev[p] = old;
-              if (((o_act >> c) & 1ull) || nb >= nn) {
-                o_act |= 1ull << p;
-                if (nn == 1) o_hint = p;
-              } else {
-                o_act |= 1ull << c;
-                if (nb == 1) o_hint = c;
-              }
-            }
-          }
-          __syncwarp();
-          lc = __shfl_sync(GCL_FULL, o_lc, 0);
-          hint = __shfl_sync(GCL_FULL, o_hint, 0);
-          active = bcast64(o_act, 0);
-          starts |= NS;
-        }
-      } else {
-        // non-singleton splitter: split by neighbour count, fragments in
-        // ascending count order
-        uint32_t cnt[VPL];
-        uint32_t mx = 0;
-#pragma unroll
-        for (int k = 0; k < VPL; ++k) {
-          cnt[k] = valid(k) ? popc64(L.adj[k] & spl) : 0u;
-          mx = max(mx, cnt[k]);
-        }
-        mx = __reduce_max_sync(GCL_FULL, mx);
-        uint64_t eq[VPL];
-        uint32_t lt[VPL];
-#pragma unroll
-        for (int k = 0; k < VPL; ++k) {
-          eq[k] = L.cm[k];
-          lt[k] = 0;
-        }
-        for (int b = mx ? 31 - __clz(mx) : -1; b >= 0; --b) {
-          bool bit[VPL];
-#pragma unroll
-          for (int k = 0; k < VPL; ++k) bit[k] = (cnt[k] >> b) & 1u;
-          const uint64_t M = ballot64<VPL>(bit);
-#pragma unroll
-          for (int k = 0; k < VPL; ++k) {
-            if (bit[k]) {
-              lt[k] += popc64(eq[k] & ~M);
-              eq[k] &= M;
-            } else {
-              eq[k] &= ~M;
-            }
-          }
-        }
-        uint64_t ns = 0;
-#pragma unroll
-        for (int k = 0; k < VPL; ++k) {
-          if (!valid(k)) continue;
-          L.cs[k] += lt[k];
-          L.cm[k] = eq[k];
-          ns |= 1ull << L.cs[k];
-          S.fk[L.cs[k]] = (uint8_t)cnt[k];
-        }
-        const uint64_t NS = warp_or64(ns) & ~starts;
+    if (level == 0) break;
+    if ((nodes & 63) == 0 && deadline &&
+        __shfl_sync(GCL_FULL, lane == 0 ? global_ns() : 0ull, 0) > deadline) {
+      status = kTimeout;
+      break;
+    }
+    int bt = -1;       // backtrack target level
+    int descend = -1;  // index of the target cell to branch from
+    bool classify = false;
+    const bool disc = starts == full;
+    if (!first_found) {
+      // first_path_node (sequential.cpp:216-257)
+      if (disc) {
+        // first_terminal (sequential.cpp:259-303)
+        const Rows2 R = w64_leaf_rows(n);
+        w64_store_leaf(n, R, S.first_cert, S.fpos);
+        w64_store_leaf(n, R, S.best_cert, S.bpos);
+        if (lane < seqlen) S.first_seq[lane] = S.best_seq[lane] = S.seq[lane];
+        if (lane + 32 < seqlen) S.first_seq[lane + 32] = S.best_seq[lane + 32] = S.seq[lane + 32];
+        if (lane < level) S.canoncode[lane] = S.firstcode[lane];
+        if (lane + 32 < level) S.canoncode[lane + 32] = S.firstcode[lane + 32];
         __syncwarp();
-        uint32_t o_lc = lc, o_hint = hint;
-        uint64_t o_act = active;
         if (lane == 0) {
-          const uint64_t singles = starts & ((starts >> 1) | (1ull << (n - 1)));
-          uint64_t t = starts & ~singles;
-          const uint64_t all = starts | NS;
-          const uint32_t lvl1 = level + 1;
-          while (t) {
-            const uint32_t c = ctz64(t);
-            t &= t - 1;
-            const uint64_t nx2 = starts & ge_mask(c + 1);
-            const uint32_t end = nx2 ? ctz64(nx2) : (uint32_t)n;
-            uint64_t fr = all & ge_mask(c) & low_mask(end);
-            if (fr == (1ull << c)) {
-              o_lc = mash(o_lc, (uint32_t)S.fk[c] + c);  // common count
-              continue;
-            }
-            const bool was = (o_act >> c) & 1ull;
-            const uint8_t old = S.inlev[c];
-            uint32_t maxsz = 0, maxp = c, lastp = c;
-            while (fr) {
-              const uint32_t p = ctz64(fr);
-              fr &= fr - 1;
-              const uint32_t pe = fr ? ctz64(fr) : end;
-              const uint32_t sz = pe - p;
-              o_lc = mash(o_lc, (uint32_t)S.fk[p] + p);
-              S.inlev[p] = (uint8_t)lvl1;
-              if (sz > maxsz) {
-                maxsz = sz;
-                maxp = p;
-              }
-              if (p != c) {
-                o_act |= 1ull << p;
-                if (sz == 1) o_hint = p;
-              }
-              lastp = p;
-            }
-            if (!was) {
-              o_act |= 1ull << c;
-              o_act &= ~(1ull << maxp);
-            }
-            S.inlev[lastp] = old;
-          }
+          S.firstcode[level] = (uint16_t)kSentinel;
+          S.canoncode[level] = (uint16_t)kSentinel;
         }
         __syncwarp();
-        lc = __shfl_sync(GCL_FULL, o_lc, 0);
-        hint = __shfl_sync(GCL_FULL, o_hint, 0);
-        active = bcast64(o_act, 0);
-        starts |= NS;
-      }
-    }
-    lc = mash(lc, popc64(starts));
-    ++level;
-    return cleanup(lc);
-  }
-
-  // ---- split_by_and_refine (partition_refinement.cpp:486-539) -------------
-  __device__ void individualize(uint32_t v, uint32_t t) {
-    bool in[VPL];
-#pragma unroll
-    for (int k = 0; k < VPL; ++k) in[k] = valid(k) && L.cs[k] == t;
-    const uint64_t mem = ballot64<VPL>(in);
-    if (popc64(mem) == 1) return;  // singleton: nothing to split, code kept
-#pragma unroll
-    for (int k = 0; k < VPL; ++k) {
-      if (!in[k]) continue;
-      if (vid(k) == v) {
-        L.cm[k] = 1ull << v;
-      } else {
-        L.cm[k] = mem & ~(1ull << v);
-        L.cs[k] = t + 1;
-      }
-    }
-    starts |= 1ull << (t + 1);
-    if (lane == 0) {
-      S.inlev[t + 1] = S.inlev[t];
-      S.inlev[t] = (uint8_t)(level + 1);
-    }
-    __syncwarp();
-    code = refine(1ull << t);
-  }
-
-  // ---- reconstruct_at_level + backtrack_to (partition_refinement.cpp:541-604,
-  //      sequential.cpp:650-670) -----------------------------------------
-  __device__ void backtrack(uint32_t Lv) {
-    if (Lv == 0) {
-      level = 0;
-      return;
-    }
-    bool big[VPL];
-    uint32_t lv[VPL];
-#pragma unroll
-    for (int k = 0; k < VPL; ++k) {
-      const uint32_t p = vid(k);
-      const bool st = valid(k) && ((starts >> p) & 1ull);
-      lv[k] = st ? S.inlev[p] : 0u;
-      big[k] = st && lv[k] > Lv;
-    }
-    const uint64_t BIG = ballot64<VPL>(big);
-    if (BIG) {
-      bool surv[VPL];
-      uint32_t nlv[VPL];
-#pragma unroll
-      for (int k = 0; k < VPL; ++k) {
-        const uint32_t p = vid(k);
-        const bool st = valid(k) && ((starts >> p) & 1ull);
-        bool sv = st;
-        if (st && p > 0) {
-          const uint64_t prev = starts & low_mask(p);
-          if (prev && ((BIG >> msb64(prev)) & 1ull)) sv = false;
-        }
-        surv[k] = sv;
-        nlv[k] = lv[k];
-        if (sv && big[k]) {
-          // the run is closed by the first following cell created at or
-          // before level Lv; the merged cell takes that cell's in_level
-          const uint64_t j = starts & ~BIG & ge_mask(p + 1);
-          nlv[k] = j ? S.inlev[ctz64(j)] : 0xffu;
-        }
-      }
-      const uint64_t NST = ballot64<VPL>(surv);
-      bool broken[VPL];
-#pragma unroll
-      for (int k = 0; k < VPL; ++k) broken[k] = nlv[k] == 0xffu;
-      if (ballot64<VPL>(broken)) {  // a run of new cells reached the last cell
-        fail(kInternal);
-        return;
-      }
-      __syncwarp();
-#pragma unroll
-      for (int k = 0; k < VPL; ++k)
-        if (surv[k] && big[k]) S.inlev[vid(k)] = (uint8_t)nlv[k];
-      starts = NST;
-#pragma unroll
-      for (int k = 0; k < VPL; ++k)
-        if (valid(k)) L.cs[k] = msb64(NST & low_mask(L.cs[k] + 1));
-      rebuild_cell_masks();
-      __syncwarp();
-    }
-    if (Lv < eqlevfirst) eqlevfirst = Lv;
-    if ((int)Lv <= eqlevcanon) {
-      eqlevcanon = (int)Lv;
-      comp_canon = 0;
-    }
-    seqlen = Lv - 1;
-    tcl = (int)Lv;
-    level = Lv;
-  }
-
-  __device__ void rebuild_cell_masks() {
-    uint64_t eq[VPL];
-    bool vb[VPL];
-#pragma unroll
-    for (int k = 0; k < VPL; ++k) vb[k] = valid(k);
-    const uint64_t vm = ballot64<VPL>(vb);
-#pragma unroll
-    for (int k = 0; k < VPL; ++k) eq[k] = vm;
-    const int nb = 32 - __clz(max(n - 1, 1));
-    for (int b = nb - 1; b >= 0; --b) {
-      bool bit[VPL];
-#pragma unroll
-      for (int k = 0; k < VPL; ++k) bit[k] = (L.cs[k] >> b) & 1u;
-      const uint64_t M = ballot64<VPL>(bit);
-#pragma unroll
-      for (int k = 0; k < VPL; ++k) eq[k] &= bit[k] ? M : ~M;
-    }
-#pragma unroll
-    for (int k = 0; k < VPL; ++k) L.cm[k] = valid(k) ? eq[k] : 0ull;
-  }
-
-  __device__ __forceinline__ bool discrete() const { return starts == full; }
-
-  // target_cell_selector (partition_refinement.cpp:607-655), hint -1
-  __device__ void select_tc() {
-    const uint64_t singles = starts & ((starts >> 1) | (1ull << (n - 1)));
-    const uint64_t ns = starts & ~singles;
-    if (!ns) return;
-    const uint32_t t = ctz64(ns);
-    bool in[VPL];
-#pragma unroll
-    for (int k = 0; k < VPL; ++k) in[k] = valid(k) && L.cs[k] == t;
-    const uint64_t mem = ballot64<VPL>(in);
-    if (tcl >= kW64Levels) {
-      fail(kInternal);
-      return;
-    }
-    if (lane == 0) {
-      TcHdr& h = S.tc[tcl];
-      h.members = mem;
-      h.repmask = mem;
-      h.last = 0;
-      h.counter = 0;
-      h.first = (uint8_t)t;
-      h.reps_valid = 0;
-    }
-    __syncwarp();
-    ++tcl;
-  }
-
-  // next branch vertex: smallest v >= counter with elems[v] == v
-  __device__ __forceinline__ bool next_rep(int idx) {
-    const TcHdr& h = S.tc[idx];
-    const uint64_t r = h.repmask & ge_mask(h.counter);
-    const uint32_t c = r ? ctz64(r) : (uint32_t)n;
-    __syncwarp();
-    if (lane == 0) S.tc[idx].counter = (uint16_t)c;
-    __syncwarp();
-    return c < (uint32_t)n;
-  }
-
-  __device__ void push_and_split(int idx) {
-    const uint32_t v = S.tc[idx].counter;
-    const uint32_t t = S.tc[idx].first;
-    __syncwarp();
-    if (lane == 0) {
-      S.tc[idx].counter = (uint16_t)(v + 1);
-      S.seq[seqlen] = (uint8_t)v;
-    }
-    __syncwarp();
-    ++seqlen;
-    ++nodes;
-    individualize(v, t);
-  }
-
-  // ---- leaves --------------------------------------------------------------
-  // Certificate row of each own vertex: its neighbours renamed to positions
-  // (buildPermutedFlatAdjacencyMatrixArray, CSRGraph.cpp:332-351).
-  __device__ void leaf_rows(uint64_t (&R)[VPL]) {
-#pragma unroll
-    for (int k = 0; k < VPL; ++k)
-      if (valid(k)) S.map[vid(k)] = (uint8_t)L.cs[k];
-    __syncwarp();
-#pragma unroll
-    for (int k = 0; k < VPL; ++k) {
-      uint64_t a = L.adj[k], r = 0;
-      while (a) {
-        const uint32_t u = ctz64(a);
-        a &= a - 1;
-        r |= 1ull << S.map[u];
-      }
-      R[k] = r;
-    }
-    __syncwarp();
-  }
-
-  // compare_adj_upper(current, stored) (sequential.cpp:114-124)
-  __device__ int cmp_upper(const uint64_t (&R)[VPL], const uint64_t* B) {
-    uint32_t row = 64u;
-    bool sgn[VPL];
-#pragma unroll
-    for (int k = 0; k < VPL; ++k) {
-      sgn[k] = false;
-      if (!valid(k)) continue;
-      const uint32_t p = L.cs[k];
-      const uint64_t d = (R[k] ^ B[p]) & ge_mask(p + 1);
-      if (d) {
-        row = min(row, p);
-        sgn[k] = (R[k] >> ctz64(d)) & 1ull;
-      }
-    }
-    const uint32_t mrow = __reduce_min_sync(GCL_FULL, row);
-    if (mrow == 64u) return 0;
-    bool win[VPL];
-#pragma unroll
-    for (int k = 0; k < VPL; ++k) win[k] = valid(k) && L.cs[k] == mrow && sgn[k];
-    return ballot64<VPL>(win) ? 1 : -1;
-  }
-
-  __device__ bool rows_equal(const uint64_t (&R)[VPL], const uint64_t* B) {
-    bool ne[VPL];
-#pragma unroll
-    for (int k = 0; k < VPL; ++k) ne[k] = valid(k) && R[k] != B[L.cs[k]];
-    return ballot64<VPL>(ne) == 0;
-  }
-
-  __device__ void store_rows(const uint64_t (&R)[VPL], uint64_t* B) {
-#pragma unroll
-    for (int k = 0; k < VPL; ++k)
-      if (valid(k)) B[L.cs[k]] = R[k];
-    __syncwarp();
-  }
-
-  __device__ void copy_seq(uint8_t* dst) {
-    for (uint32_t j = lane; j < seqlen; j += 32) dst[j] = S.seq[j];
-    __syncwarp();
-  }
-
-  // get_gca_level (sequential.cpp:183-213)
-  __device__ int gca(const uint8_t* a, uint32_t na) {
-    const uint32_t m = min(na, seqlen);
-    uint32_t first = 0xffffffffu;
-    for (uint32_t j0 = 0; j0 < m; j0 += 32) {
-      const uint32_t j = j0 + lane;
-      const bool d = j < m && a[j] != S.seq[j];
-      const uint32_t b = __ballot_sync(GCL_FULL, d);
-      if (b) {
-        first = j0 + (uint32_t)(__ffs(b) - 1);
-        break;
-      }
-    }
-    return first == 0xffffffffu ? -1 : (int)first + 1;
-  }
-
-  // aut[label[j]] = elem[j] with the stored leaf given by its positions
-  // (sequential.cpp:505-520, 544-555), written to ring slot num_aut % max_aut
-  __device__ bool store_aut(const uint32_t (&pos)[VPL]) {
-    const uint32_t idx = (uint32_t)num_aut % A.max_aut;
-    if (idx >= A.aut_cap) {
-      status = kAutOverflow;
-      return false;
-    }
-#pragma unroll
-    for (int k = 0; k < VPL; ++k)
-      if (valid(k)) S.map[L.cs[k]] = (uint8_t)vid(k);  // position -> vertex
-    __syncwarp();
-    uint8_t* dst = auts + (uint64_t)idx * 64u;
-#pragma unroll
-    for (int k = 0; k < VPL; ++k)
-      if (valid(k)) dst[vid(k)] = S.map[pos[k]];
-    __syncwarp();
-    ++num_aut;
-    return true;
-  }
-
-  // ---- orbits of the stored automorphisms fixing the current sequence
-  //      (perm_group.cpp:5-116) ------------------------------------------
-  // Root of x: parents only point to smaller vertices, so at most n steps.
-  __device__ uint32_t find(uint32_t x) {
-    volatile uint32_t* d = S.dsu;
-    uint32_t p = d[x];
-    for (int step = 0; p != x && p < x && step < kW64MaxN; ++step) {
-      x = p;
-      p = d[x];
-    }
-    return x;
-  }
-
-  __device__ void orbits(int idx) {
-    const int limit = num_aut < (int)A.max_aut ? num_aut : (int)A.max_aut;
-    int from = S.tc[idx].last;
-    if (from == -1) from = 0;
-    const uint64_t mem = S.tc[idx].members;
-    const bool rv = S.tc[idx].reps_valid;
-    uint8_t* rp = reps + (uint64_t)idx * 64u;
-#pragma unroll
-    for (int k = 0; k < VPL; ++k) {
-      if (!valid(k)) continue;
-      const uint32_t v = vid(k);
-      S.dsu[v] = ((mem >> v) & 1ull) ? (rv ? (uint32_t)rp[v] : v) : v;
-    }
-    __syncwarp();
-    bool any = false;
-    for (int i = from; i < limit; ++i) {
-      const uint8_t* pm = auts + (uint64_t)i * 64u;
-      bool bad = false;
-      for (uint32_t j = lane; j < seqlen; j += 32) {
-        const uint32_t sv = S.seq[j];
-        if (pm[sv] != sv) bad = true;
-      }
-      if (__any_sync(GCL_FULL, bad)) continue;
-      any = true;
-      uint32_t img[VPL];
-#pragma unroll
-      for (int k = 0; k < VPL; ++k) img[k] = valid(k) ? pm[vid(k)] : vid(k);
-      // union every (v, pm[v]) with min-root hooking until no edge is left
-      // between two roots; a root is always the minimum of its tree.  Each
-      // round merges at least two trees, so n rounds always suffice.
-      for (int round = 0;; ++round) {
-        if (round > kW64MaxN + 1) {
-          fail(kInternal);
-          return;
-        }
-        bool changed = false;
-#pragma unroll
-        for (int k = 0; k < VPL; ++k) {
-          if (!valid(k) || img[k] == vid(k)) continue;
-          const uint32_t a = find(vid(k)), b = find(img[k]);
-          if (a != b) {
-            atomicMin(&S.dsu[max(a, b)], min(a, b));
-            changed = true;
-          }
-        }
-        __syncwarp();
-#pragma unroll
-        for (int k = 0; k < VPL; ++k)
-          if (valid(k)) {
-            const uint32_t r = find(vid(k));
-            atomicMin(&S.dsu[vid(k)], r);
-          }
-        __syncwarp();
-        if (!__any_sync(GCL_FULL, changed)) break;
-      }
-    }
-    if (!any) return;
-    bool isrep[VPL];
-#pragma unroll
-    for (int k = 0; k < VPL; ++k) {
-      isrep[k] = false;
-      if (!valid(k)) continue;
-      const uint32_t v = vid(k);
-      if ((mem >> v) & 1ull) {
-        const uint32_t r = find(v);
-        rp[v] = (uint8_t)r;
-        isrep[k] = r == v;
-      }
-    }
-    const uint64_t rm = ballot64<VPL>(isrep);
-    __syncwarp();
-    if (lane == 0) {
-      S.tc[idx].repmask = rm;
-      S.tc[idx].reps_valid = 1;
-    }
-    __syncwarp();
-  }
-
-  // ---- first_terminal (sequential.cpp:259-303) ---------------------------
-  __device__ void first_terminal() {
-    uint64_t R[VPL];
-    leaf_rows(R);
-    eqlevfirst = level;
-#pragma unroll
-    for (int k = 0; k < VPL; ++k) {
-      if (!valid(k)) continue;
-      S.first_cert[L.cs[k]] = R[k];
-      S.best_cert[L.cs[k]] = R[k];
-      L.fpos[k] = L.bpos[k] = L.cs[k];
-    }
-    for (uint32_t j = lane; j < seqlen; j += 32) S.first_seq[j] = S.best_seq[j] = S.seq[j];
-    for (uint32_t j = lane; j < level; j += 32) S.canoncode[j] = S.firstcode[j];
-    __syncwarp();
-    if (lane == 0) {
-      S.firstcode[level] = (uint16_t)kSentinel;
-      S.canoncode[level] = (uint16_t)kSentinel;
-    }
-    __syncwarp();
-    first_seqlen = best_seqlen = seqlen;
-    first_found = true;
-    canon_level = eqlevcanon = (int)level;
-    comp_canon = 0;
-  }
-
-  __device__ void first_path_node() {
-    if (discrete()) {
-      first_terminal();
-      backtrack(level - 1);
-      return;
-    }
-    select_tc();
-    if (status != kOk) return;
-    const int idx = tcl - 1;
-    next_rep(idx);
-    push_and_split(idx);
-    if (status != kOk) return;
-    if (lane == 0) S.firstcode[level - 1] = (uint16_t)code;
-    __syncwarp();
-  }
-
-  // ---- classify_node (sequential.cpp:396-624) ----------------------------
-  __device__ bool classify() {
-    const uint32_t Lv = level;
-    if (eqlevfirst == Lv - 1 && code == (int)S.firstcode[Lv - 1]) eqlevfirst = Lv;
-    if (eqlevcanon == (int)Lv - 1) {
-      const int cc = S.canoncode[Lv - 1];
-      if (code < cc) {
-        comp_canon = -1;
-      } else if (code > cc) {
-        comp_canon = 1;
-      } else {
+        eqlevfirst = level;
+        first_seqlen = best_seqlen = seqlen;
+        first_found = true;
+        canon_level = eqlevcanon = (int)level;
         comp_canon = 0;
-        eqlevcanon = (int)Lv;
-      }
-    }
-    if (comp_canon > 0) {
-      __syncwarp();
-      if (lane == 0) S.canoncode[Lv - 1] = (uint16_t)code;
-      __syncwarp();
-    }
-    int dec = 0;
-    uint64_t R[VPL];
-    if (eqlevfirst != Lv && comp_canon < 0) {
-      dec = 4;
-    } else if (discrete()) {
-      leaf_rows(R);
-      if (eqlevfirst == Lv && rows_equal(R, S.first_cert)) dec = 1;
-      if (dec == 0) {
-        if (comp_canon == 0) {
-          if ((int)Lv < canon_level)
-            comp_canon = 1;
-          else
-            comp_canon = cmp_upper(R, S.best_cert);
+        bt = (int)level - 1;
+      } else {
+        if (tcl >= kW64Levels) {
+          status = kInternal;
+          break;
         }
-        dec = comp_canon == 0 ? 2 : (comp_canon > 0 ? 3 : 4);
+        w64_select_tc(n, starts, tcl);
+        ++tcl;
+        descend = tcl - 1;
+      }
+    } else {
+      // other_path_node (sequential.cpp:304-392)
+      classify = true;
+      if (!disc && (eqlevfirst == level || comp_canon >= 0)) {
+        if (tcl < (int)level) {
+          if (tcl >= kW64Levels) {
+            status = kInternal;
+            break;
+          }
+          w64_select_tc(n, starts, tcl);
+          ++tcl;
+        }
+        const int idx = (int)level - 1;
+        if (S.tc[idx].counter >= (uint32_t)n) {
+          bt = (int)level - 1;
+          classify = false;
+        } else {
+          if (num_aut > 0 && num_aut > S.tc[idx].last) {
+            if (!w64_orbits(n, idx, num_aut, A.max_aut, seqlen, reps, auts)) {
+              status = kInternal;
+              break;
+            }
+            __syncwarp();
+            if (lane == 0) S.tc[idx].last = num_aut;
+            __syncwarp();
+          }
+          descend = idx;
+        }
       }
     }
-    switch (dec) {
-      case 1: {
-        if (!store_aut(L.fpos)) return false;
-        const int g = gca(S.first_seq, first_seqlen);
-        backtrack(g >= 0 ? (uint32_t)g : Lv - 1);
-        break;
+    if (descend >= 0) {
+      // next representative: smallest v >= counter with elems[v] == v
+      const uint64_t r = S.tc[descend].repmask & ge_mask(S.tc[descend].counter);
+      if (!r) {
+        // the counter runs past the last vertex (sequential.cpp:359-365)
+        __syncwarp();
+        if (lane == 0) S.tc[descend].counter = (uint16_t)n;
+        __syncwarp();
+        bt = (int)level - 1;
+        classify = false;
+      } else {
+        const uint32_t v = ctz64(r), t = S.tc[descend].first;
+        __syncwarp();
+        if (lane == 0) {
+          S.tc[descend].counter = (uint16_t)(v + 1);
+          S.seq[seqlen] = (uint8_t)v;
+        }
+        __syncwarp();
+        ++seqlen;
+        ++nodes;
+        if (w64_individualize(n, level, v, t)) {
+          starts |= bit64(t + 1);
+          if (!first_found) {
+            pending = bit64(t);  // refine and record firstcode
+            continue;
+          }
+          const W64Refined rr = w64_refine(n, starts, level, bit64(t));
+          if (!rr.ok) {
+            status = kInternal;
+            break;
+          }
+          starts = rr.starts;
+          code = rr.code;
+          ++level;
+        } else if (!first_found) {
+          __syncwarp();
+          if (lane == 0) S.firstcode[level - 1] = (uint16_t)code;
+          __syncwarp();
+          continue;
+        }
       }
-      case 2: {
-        if (!store_aut(L.bpos)) return false;
-        const int g = gca(S.best_seq, best_seqlen);
-        backtrack(g >= 0 ? (uint32_t)g : Lv - 1);
-        break;
+    }
+    if (classify) {
+      // classify_node (sequential.cpp:396-624)
+      const uint32_t Lv = level;
+      if (eqlevfirst == Lv - 1 && code == (int)S.firstcode[Lv - 1]) eqlevfirst = Lv;
+      if (eqlevcanon == (int)Lv - 1) {
+        const int cc = S.canoncode[Lv - 1];
+        if (code < cc) {
+          comp_canon = -1;
+        } else if (code > cc) {
+          comp_canon = 1;
+        } else {
+          comp_canon = 0;
+          eqlevcanon = (int)Lv;
+        }
       }
-      case 3: {
+      if (comp_canon > 0) {
+        __syncwarp();
+        if (lane == 0) S.canoncode[Lv - 1] = (uint16_t)code;
+        __syncwarp();
+      }
+      int dec = 0;
+      Rows2 R{0ull, 0ull};
+      if (eqlevfirst != Lv && comp_canon < 0) {
+        dec = 4;
+      } else if (starts == full) {
+        R = w64_leaf_rows(n);
+        if (eqlevfirst == Lv && w64_rows_equal(n, R, S.first_cert)) dec = 1;
+        if (dec == 0) {
+          if (comp_canon == 0) {
+            if ((int)Lv < canon_level)
+              comp_canon = 1;
+            else
+              comp_canon = w64_cmp_upper(n, R, S.best_cert);
+          }
+          dec = comp_canon == 0 ? 2 : (comp_canon > 0 ? 3 : 4);
+        }
+      }
+      if (dec == 1 || dec == 2) {
+        const uint32_t slot_i = (uint32_t)num_aut % A.max_aut;
+        if (slot_i >= A.aut_cap) {
+          status = kAutOverflow;
+          break;
+        }
+        w64_store_aut(n, dec == 1 ? S.fpos : S.bpos, auts + (uint64_t)slot_i * 64u);
+        ++num_aut;
+        const int g = dec == 1 ? w64_gca(S.first_seq, first_seqlen, seqlen)
+                               : w64_gca(S.best_seq, best_seqlen, seqlen);
+        bt = g >= 0 ? g : (int)Lv - 1;
+      } else if (dec == 3) {
         canon_level = eqlevcanon = (int)Lv;
         comp_canon = 0;
-        store_rows(R, S.best_cert);
-#pragma unroll
-        for (int k = 0; k < VPL; ++k) L.bpos[k] = L.cs[k];
-        copy_seq(S.best_seq);
+        w64_store_leaf(n, R, S.best_cert, S.bpos);
+        if (lane < seqlen) S.best_seq[lane] = S.seq[lane];
+        if (lane + 32 < seqlen) S.best_seq[lane + 32] = S.seq[lane + 32];
+        __syncwarp();
         if (lane == 0) S.canoncode[Lv] = (uint16_t)kSentinel;
         __syncwarp();
         best_seqlen = seqlen;
-        backtrack(Lv - 1);
+        bt = (int)Lv - 1;
+      } else if (dec == 4) {
+        bt = (int)Lv - 1;
+      }
+    }
+    if (bt >= 0) {
+      // backtrack_to (sequential.cpp:650-670)
+      const uint32_t Lv = (uint32_t)bt;
+      if (Lv == 0) {
+        level = 0;
+        continue;
+      }
+      starts = w64_backtrack(n, starts, Lv);
+      if (!starts) {
+        status = kInternal;
         break;
       }
-      case 4:
-        backtrack(Lv - 1);
-        break;
-      default:
-        break;
+      if (Lv < eqlevfirst) eqlevfirst = Lv;
+      if ((int)Lv <= eqlevcanon) {
+        eqlevcanon = (int)Lv;
+        comp_canon = 0;
+      }
+      seqlen = Lv - 1;
+      tcl = (int)Lv;
+      level = Lv;
     }
-    return true;
   }
+  res.status = status;
+  res.num_aut = num_aut;
+  res.nodes = nodes;
+  return res;
+}
 
-  // ---- other_path_node (sequential.cpp:304-392) ---------------------------
-  __device__ bool other_path_node() {
-    if (!discrete() && (eqlevfirst == level || comp_canon >= 0)) {
-      if (tcl < (int)level) select_tc();
-      if (status != kOk) return false;
-      const int idx = (int)level - 1;
-      if (S.tc[idx].counter >= (uint32_t)n) {
-        backtrack(level - 1);
-        return true;
-      }
-      if (num_aut > 0 && num_aut > S.tc[idx].last) {
-        orbits(idx);
-        if (status != kOk) return false;
-        __syncwarp();
-        if (lane == 0) S.tc[idx].last = num_aut;
-        __syncwarp();
-      }
-      if (!next_rep(idx)) {
-        backtrack(level - 1);
-        return true;
-      }
-      push_and_split(idx);
-      if (status != kOk) return false;
-    }
-    return classify();
-  }
-
-  // ---- search_tree_traversal (sequential.cpp:626-648) ---------------------
-  __device__ void run() {
-    code = refine(starts);
-    if (status != kOk) return;
-    if (lane == 0) S.firstcode[level - 1] = (uint16_t)code;
-    __syncwarp();
-    nodes = 1;
-    while (level >= 1 && status == kOk) {
-      if ((nodes & 63) == 0 && out_of_time()) {
-        fail(kTimeout);
-        break;
-      }
-      if (!first_found) {
-        first_path_node();
-      } else if (!other_path_node()) {
-        return;  // overflow of the automorphism ring or a failed check
-      }
-    }
-  }
-};
-
-template <int VPL>
-__device__ void w64_canon_one(W64Smem& S, const BatchArgs& A, int g, uint8_t* slot) {
-  const int64_t vo = A.voff[g];
-  const int n = (int)(A.voff[g + 1] - vo);
-  W64Search<VPL> W(S, A, n, slot);
-  const uint32_t lane = W.lane;
-  if (A.budget_ns) W.deadline = __shfl_sync(GCL_FULL, lane == 0 ? global_ns() : 0ull, 0) + A.budget_ns;
-  if (!W.load(vo, A.rowptr + vo + g, A.col + A.eoff[g], A.color, A.eoff[g + 1] - A.eoff[g])) {
-    if (lane == 0) A.status[g] = kBadInput;
-    return;
-  }
-  W.run();
-  if (lane == 0) {
-    A.status[g] = W.status;
-    if (A.out_stats) {
-      A.out_stats[2 * (int64_t)g] = W.num_aut;
-      A.out_stats[2 * (int64_t)g + 1] = W.nodes;
-    }
-  }
-  if (W.status != kOk) return;
-  // canonical labeling: position -> vertex of the best leaf
+__device__ __noinline__ void w64_write_outputs(const BatchArgs& A, int g, int n, int64_t vo) {
+  W64Smem& S = w64_smem();
+  const uint32_t lane = lane_id();
   if (A.out_label) {
-#pragma unroll
-    for (int k = 0; k < VPL; ++k)
-      if (W.valid(k)) A.out_label[vo + W.L.bpos[k]] = (int32_t)W.vid(k);
+    if (lane < (uint32_t)n) A.out_label[vo + S.bpos[lane]] = (int32_t)lane;
+    if (lane + 32 < (uint32_t)n) A.out_label[vo + S.bpos[lane + 32]] = (int32_t)(lane + 32);
   }
   if (A.out_cert) {
-    for (int p = lane; p < n; p += 32) A.out_cert[vo + p] = S.best_cert[p];
+    if (lane < (uint32_t)n) A.out_cert[vo + lane] = S.best_cert[lane];
+    if (lane + 32 < (uint32_t)n) A.out_cert[vo + lane + 32] = S.best_cert[lane + 32];
   }
   if (A.out_dense) {
     uint8_t* o = A.out_dense + A.ooff[g];
-    const int nn = n * n;
-    for (int i = lane; i < nn; i += 32) {
-      const int r = i / n, c = i - r * n;
-      o[i] = (uint8_t)((S.best_cert[r] >> c) & 1ull);
+    for (int r = 0; r < n; ++r) {
+      const uint64_t row = S.best_cert[r];
+      uint8_t* orow = o + (int64_t)r * n;
+      if (lane < (uint32_t)n) orow[lane] = (uint8_t)((row >> lane) & 1ull);
+      if (lane + 32 < (uint32_t)n) orow[lane + 32] = (uint8_t)((row >> (lane + 32)) & 1ull);
     }
   }
+}
+
+__device__ __forceinline__ void w64_canon_one(const BatchArgs& A, int g, uint8_t* slot) {
+  const int64_t vo = A.voff[g];
+  const int n = (int)(A.voff[g + 1] - vo);
+  const int64_t eo = A.eoff[g];
+  const W64Result r = w64_search(A, n, vo, eo, A.eoff[g + 1] - eo, A.rowptr + vo + g, slot);
+  const uint32_t lane = lane_id();
+  if (lane == 0) {
+    A.status[g] = r.status;
+    if (A.out_stats) {
+      A.out_stats[2 * (int64_t)g] = r.num_aut;
+      A.out_stats[2 * (int64_t)g + 1] = r.nodes;
+    }
+  }
+  if (r.status == kOk) w64_write_outputs(A, g, n, vo);
+  __syncwarp();
 }
 
 }  // namespace gcl

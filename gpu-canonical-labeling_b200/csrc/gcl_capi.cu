@@ -23,8 +23,6 @@
 
 namespace gcl {
 
-constexpr int kW64Threads = 128;  // 4 warps, one graph per warp
-constexpr int kW64Warps = kW64Threads / 32;
 constexpr uint32_t kW64AutCap = 256;  // ring slots per warp in the fast pass
 
 // Device-side lists of deferred graphs.
@@ -36,12 +34,10 @@ struct Deferred {
   int next;  // work counter of the first pass
 };
 
-__global__ void __launch_bounds__(kW64Threads)
+__global__ void __launch_bounds__(kW64Threads, 8)
     w64_batch_kernel(BatchArgs A, Deferred* D, int* overflow_list, int* large_list, int pass) {
-  __shared__ W64Smem smem[kW64Warps];
   const int warp = (int)(threadIdx.x >> 5);
   const uint32_t lane = lane_id();
-  W64Smem& S = smem[warp];
   uint8_t* slot = A.work + ((uint64_t)blockIdx.x * kW64Warps + (uint64_t)warp) * A.slot_bytes;
   int* ctr = pass == 0 ? &D->next : &D->next_overflow;
   const int total = pass == 0 ? A.count : *(volatile int*)&D->overflow_count;
@@ -59,10 +55,7 @@ __global__ void __launch_bounds__(kW64Threads)
       }
       continue;
     }
-    if (n <= 32)
-      w64_canon_one<1>(S, A, g, slot);
-    else
-      w64_canon_one<2>(S, A, g, slot);
+    w64_canon_one(A, g, slot);
     if (pass == 0 && lane == 0 && *(volatile int32_t*)&A.status[g] == kAutOverflow)
       overflow_list[atomicAdd(&D->overflow_count, 1)] = g;
     __syncwarp();
