@@ -272,6 +272,7 @@ def gpu_arm(args):
     stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
     ooff = arena.out_offsets()
     max_n = int(arena.sizes().max())
+    max_m2 = int(np.diff(arena.eoff).max())
 
     # device-resident inputs and outputs
     def d(a, dtype):
@@ -290,7 +291,7 @@ def gpu_arm(args):
     def launch():
         rc = lib.gcl_canon_batch_device_async(
             ctx.handle, count, P(t_voff.data_ptr()), P(t_eoff.data_ptr()), P(t_rp.data_ptr()),
-            P(t_col.data_ptr()), None, args.max_aut, max_n, P(t_dense.data_ptr()),
+            P(t_col.data_ptr()), None, args.max_aut, max_n, max_m2, P(t_dense.data_ptr()),
             P(t_ooff.data_ptr()), None, P(t_stats.data_ptr()), P(t_status.data_ptr()))
         if rc != 0:
             raise RuntimeError(f"gcl_canon_batch_device_async failed: {rc}")
@@ -413,7 +414,7 @@ def gpu_arm(args):
             rc = lib.gcl_canon_batch_device_async(
                 ctx.handle, 1, P(vo_all[i].data_ptr()), P(eo_all[i].data_ptr()),
                 P(t_rp.data_ptr() + 4 * int(hv[g] + g)), P(t_col.data_ptr() + 4 * int(hee[g])),
-                None, args.max_aut, n, P(t_dense.data_ptr() + int(ooff[g])),
+                None, args.max_aut, n, m, P(t_dense.data_ptr() + int(ooff[g])),
                 P(oo_all[i].data_ptr()), None, P(t_stats.data_ptr() + 16 * g),
                 P(t_status.data_ptr() + 4 * g))
             if rc != 0:

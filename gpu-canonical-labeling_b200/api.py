@@ -71,7 +71,8 @@ def load_library(path: str = LIB_PATH):
     lib.gcl_canon_batch.argtypes = [_P, ctypes.c_int, _P, _P, _P, _P, _P, ctypes.c_int, _P, _P,
                                     _P, _P, _P]
     lib.gcl_canon_batch_device_async.argtypes = [_P, ctypes.c_int, _P, _P, _P, _P, _P,
-                                                 ctypes.c_int, ctypes.c_int, _P, _P, _P, _P, _P]
+                                                 ctypes.c_int, ctypes.c_int, ctypes.c_int64, _P,
+                                                 _P, _P, _P, _P]
     lib.gcl_iso.argtypes = [_P, _P, _P, _P, ctypes.c_int, _P, _P, _P, ctypes.c_int,
                             ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     for name in ("gcl_create", "gcl_destroy", "gcl_sync", "gcl_canon_one", "gcl_canon_batch",

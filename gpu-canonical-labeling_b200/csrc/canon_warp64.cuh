@@ -761,6 +761,7 @@ __device__ __noinline__ W64Result w64_search(const BatchArgs& A, int n, int64_t 
   // the next refinement to run, given by its initially active cells; the
   // root refinement starts with every cell active (sequential.cpp:628)
   uint64_t pending = starts;
+  uint64_t iter = 0;
   while (true) {
     if (pending) {
       const W64Refined r = w64_refine(n, starts, level, pending);
@@ -779,7 +780,7 @@ __device__ __noinline__ W64Result w64_search(const BatchArgs& A, int n, int64_t 
       continue;
     }
     if (level == 0) break;
-    if ((nodes & 63) == 0 && deadline &&
+    if ((++iter & 63) == 0 && deadline &&
         __shfl_sync(GCL_FULL, lane == 0 ? global_ns() : 0ull, 0) > deadline) {
       status = kTimeout;
       break;

@@ -6,7 +6,9 @@
 // device path never synchronizes with the host:
 //   * an automorphism ring that outgrew its per-slot capacity -> rerun with a
 //     workspace holding the full max_aut ring;
-//   * n > 64 -> the block-per-graph kernel (canon_block.cuh).
+//   * n > 64 -> the sparse warp-per-graph kernel (canon_sparse.cuh), first
+//     with a small pool of per-level orbit arrays and a short ring, then a
+//     rerun of the graphs that outgrew them with both at full size.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -18,7 +20,7 @@
 #include <vector>
 
 #include "../../include/gcl.h"
-#include "canon_block.cuh"
+#include "canon_sparse.cuh"
 #include "canon_warp64.cuh"
 
 namespace gcl {
@@ -27,12 +29,52 @@ constexpr uint32_t kW64AutCap = 256;  // ring slots per warp in the fast pass
 
 // Device-side lists of deferred graphs.
 struct Deferred {
-  int overflow_count;
-  int large_count;
+  int overflow_count;  // n <= 64 graphs that outgrew the ring
+  int large_count;     // n > 64 graphs
   int next_overflow;
   int next_large;
-  int next;  // work counter of the first pass
+  int next;            // work counter of the first pass
+  int sp_fail_count;   // n > 64 graphs that outgrew pool or ring
+  int next_sp_fail;
 };
+
+constexpr uint32_t kSpPool = 8;     // per-level orbit arrays in the first sparse pass
+constexpr uint32_t kSpAutCap = 64;  // ring entries in the first sparse pass
+
+__global__ void __launch_bounds__(kSpThreads)
+    sp_batch_kernel(BatchArgs A, const int* list, const int* count, int* next, int* fail_list,
+                    int* fail_count, uint32_t n_max, uint64_t m2_max, uint32_t pool, uint32_t cap,
+                    uint64_t slot_bytes) {
+  const int warp = (int)(threadIdx.x >> 5);
+  const uint32_t lane = lane_id();
+  uint8_t* slot = A.work + ((uint64_t)blockIdx.x * kSpWarps + (uint64_t)warp) * slot_bytes;
+  const SpLayout Lo = sp_layout(n_max, m2_max, pool, cap);
+  const int total = *(volatile const int*)count;
+  while (true) {
+    int i = 0;
+    if (lane == 0) i = atomicAdd(next, 1);
+    i = __shfl_sync(GCL_FULL, i, 0);
+    if (i >= total) break;
+    const int g = list[i];
+    const int64_t n = A.voff[g + 1] - A.voff[g];
+    const int64_t m2 = A.eoff[g + 1] - A.eoff[g];
+    if (n > (int64_t)n_max || m2 > (int64_t)m2_max) {
+      if (lane == 0) A.status[g] = kTooLarge;
+      continue;
+    }
+    const SpResult r = sp_search(A, g, slot, Lo, pool, cap);
+    if (lane == 0) {
+      A.status[g] = r.status;
+      if (A.out_stats) {
+        A.out_stats[2 * (int64_t)g] = r.num_aut;
+        A.out_stats[2 * (int64_t)g + 1] = r.nodes;
+      }
+      if (r.status == kAutOverflow && fail_list) fail_list[atomicAdd(fail_count, 1)] = g;
+    }
+    if (r.status == kOk) sp_write_outputs(A, g);
+    __syncwarp();
+  }
+}
 
 __global__ void __launch_bounds__(kW64Threads, 8)
     w64_batch_kernel(BatchArgs A, Deferred* D, int* overflow_list, int* large_list, int pass) {
@@ -95,17 +137,15 @@ struct gcl_context {
   int sms = 0;
   cudaStream_t stream = nullptr;
   int w64_grid = 0;
-  int blk_grid = 0;
   // fast-pass workspace
   DevBuf work;
   // rerun workspace (full max_aut ring), sized on demand
   DevBuf work_big;
   uint32_t work_big_aut = 0;
   int big_slots = 0;
-  DevBuf block_work;
-  uint64_t block_work_n = 0, block_work_aut = 0;
-  int block_slots = 0;
-  DevBuf deferred, overflow_list, large_list;
+  DevBuf sp_work, sp_work_big;
+  int sp_grid = 0;
+  DevBuf deferred, overflow_list, large_list, sp_fail_list;
   // staging for host-pointer calls
   DevBuf voff, eoff, rowptr, col, color, ooff, dense, label, stats, status;
 };
@@ -118,6 +158,15 @@ static uint64_t graph_budget_ns() {
   double s = e ? std::atof(e) : 600.0;
   if (!(s > 0)) return 0;
   return (uint64_t)(s * 1e9);
+}
+
+// Device memory the per-warp workspaces of one pass may take
+// (GCL_WORKSPACE_GB, default 4 GiB).
+static uint64_t workspace_budget() {
+  const char* e = std::getenv("GCL_WORKSPACE_GB");
+  double g = e ? std::atof(e) : 4.0;
+  if (!(g > 0)) g = 4.0;
+  return (uint64_t)(g * (1ull << 30));
 }
 
 static int cuda_status(cudaError_t e) {
@@ -167,7 +216,10 @@ int gcl_create(int device, gcl_context** out) {
     c->w64_grid = c->sms * std::max(per_sm, 1);
     e = c->deferred.ensure(sizeof(Deferred));
   }
-  if (e == cudaSuccess) e = block_occupancy(&c->blk_grid, c->sms);
+  int sp_per_sm = 0;
+  if (e == cudaSuccess)
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sp_per_sm, sp_batch_kernel, kSpThreads, 0);
+  if (e == cudaSuccess) c->sp_grid = c->sms * std::max(sp_per_sm, 1);
   if (e != cudaSuccess) {
     if (c->stream) cudaStreamDestroy(c->stream);
     c->deferred.release();
@@ -182,8 +234,8 @@ int gcl_destroy(gcl_context* c) {
   if (!c) return GCL_ERR_ARG;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
-  DevBuf* bufs[] = {&c->work, &c->work_big, &c->block_work, &c->deferred, &c->overflow_list,
-                    &c->large_list, &c->voff, &c->eoff, &c->rowptr, &c->col, &c->color,
+  DevBuf* bufs[] = {&c->work, &c->work_big, &c->sp_work, &c->sp_work_big, &c->deferred,
+                    &c->overflow_list, &c->large_list, &c->sp_fail_list, &c->voff, &c->eoff, &c->rowptr, &c->col, &c->color,
                     &c->ooff, &c->dense, &c->label, &c->stats, &c->status};
   for (DevBuf* b : bufs) b->release();
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -202,7 +254,8 @@ int gcl_sync(gcl_context* c) {
 int gcl_canon_batch_device_async(gcl_context* c, int count, const int64_t* d_voff,
                                  const int64_t* d_eoff, const int32_t* d_rowptr,
                                  const int32_t* d_col, const int32_t* d_color, int max_aut,
-                                 int max_n, uint8_t* d_out_dense, const int64_t* d_ooff,
+                                 int max_n, int64_t max_m2, uint8_t* d_out_dense,
+                                 const int64_t* d_ooff,
                                  int32_t* d_out_label, int64_t* d_out_stats,
                                  int32_t* d_out_status) {
   if (!c || count < 0 || max_aut <= 0 || !d_voff || !d_eoff || !d_rowptr || !d_out_status ||
@@ -262,8 +315,35 @@ int gcl_canon_batch_device_async(gcl_context* c, int count, const int64_t* d_vof
   }
 
   if (max_n > kW64MaxN) {
-    int rc = block_pass_async(c, A, D, (int*)c->large_list.p, max_n, maut);
-    if (rc != GCL_OK) return rc;
+    // graphs with n > 64: the sparse kernel over the deferred list
+    const uint32_t nmax = (uint32_t)max_n;
+    const uint64_t m2max = (uint64_t)std::max<int64_t>(max_m2, 1);
+    const uint32_t cap1 = std::min<uint32_t>(maut, kSpAutCap);
+    const uint64_t sb1 = sp_layout(nmax, m2max, kSpPool, cap1).bytes;
+    const uint64_t budget = workspace_budget();
+    int64_t slots = std::min<int64_t>((int64_t)c->sp_grid * kSpWarps,
+                                      std::max<int64_t>(kSpWarps, (int64_t)(budget / sb1)));
+    slots = std::min<int64_t>(slots, ((int64_t)count + kSpWarps - 1) / kSpWarps * kSpWarps);
+    slots = std::max<int64_t>(kSpWarps, slots / kSpWarps * kSpWarps);
+    GCL_TRY(c->sp_work.ensure((size_t)(slots * sb1)));
+    GCL_TRY(c->sp_fail_list.ensure((size_t)count * sizeof(int)));
+    BatchArgs Sa = A;
+    Sa.work = (uint8_t*)c->sp_work.p;
+    sp_batch_kernel<<<(int)(slots / kSpWarps), kSpThreads, 0, c->stream>>>(
+        Sa, (const int*)c->large_list.p, &D->large_count, &D->next_large,
+        (int*)c->sp_fail_list.p, &D->sp_fail_count, nmax, m2max, kSpPool, cap1, sb1);
+    GCL_TRY(cudaGetLastError());
+    // rerun with a representative array per level and the full ring
+    const uint32_t pool2 = nmax + 2;
+    const uint64_t sb2 = sp_layout(nmax, m2max, pool2, maut).bytes;
+    int64_t slots2 = std::max<int64_t>(1, std::min<int64_t>((int64_t)c->sms,
+                                                          (int64_t)(budget / (sb2 * kSpWarps))));
+    GCL_TRY(c->sp_work_big.ensure((size_t)(slots2 * kSpWarps * sb2)));
+    Sa.work = (uint8_t*)c->sp_work_big.p;
+    sp_batch_kernel<<<(int)slots2, kSpThreads, 0, c->stream>>>(
+        Sa, (const int*)c->sp_fail_list.p, &D->sp_fail_count, &D->next_sp_fail, nullptr, nullptr,
+        nmax, m2max, pool2, maut, sb2);
+    GCL_TRY(cudaGetLastError());
   }
   return GCL_OK;
 }
@@ -309,8 +389,10 @@ int gcl_canon_batch(gcl_context* c, int count, const int64_t* voff, const int64_
   if (count == 0) return GCL_OK;
   if (voff[0] != 0 || eoff[0] != 0) return GCL_ERR_ARG;
   int max_n = 0;
+  int64_t max_m2 = 0;
   for (int g = 0; g < count; ++g) {
     const int64_t n = voff[g + 1] - voff[g], m = eoff[g + 1] - eoff[g];
+    if (n > kW64MaxN) max_m2 = std::max(max_m2, m);
     if (n < 0 || m < 0 || n > GCL_MAX_N) return n > GCL_MAX_N ? GCL_ERR_TOO_LARGE : GCL_ERR_ARG;
     if (rowptr[voff[g] + g] != 0 || rowptr[voff[g + 1] + g] != m) return GCL_ERR_BAD_INPUT;
     if (out_dense && ooff[g + 1] - ooff[g] != n * n) return GCL_ERR_ARG;
@@ -359,7 +441,7 @@ int gcl_canon_batch(gcl_context* c, int count, const int64_t* voff, const int64_
   }
   int rc = gcl_canon_batch_device_async(c, count, (int64_t*)c->voff.p, (int64_t*)c->eoff.p,
                                         (int32_t*)c->rowptr.p, (int32_t*)c->col.p, d_color,
-                                        max_aut, max_n, d_dense, d_ooff, d_label, d_stats,
+                                        max_aut, max_n, max_m2, d_dense, d_ooff, d_label, d_stats,
                                         (int32_t*)c->status.p);
   if (rc != GCL_OK) return rc;
   if (out_dense && dense_bytes)

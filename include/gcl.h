@@ -12,12 +12,12 @@
  *                                          -- main.cpp:73-90, 172-197
  *
  * Every entry point here takes plain pointers and sizes.  Graphs are CSR with
- * both directions of every undirected edge stored (the shape
- * CSRGraph::fromDIMACS builds, src/CSRGraph.cpp:40-119): rowptr[n+1],
- * col[rowptr[n]], optional color[n] (NULL = uncoloured).  Rows need not be
- * sorted; self loops, duplicate entries and one-directional edges are
- * rejected with GCL_ERR_BAD_INPUT (the reference's refinement is undefined on
- * parallel edges).  Results are bit-identical to the reference's sequential
+ * both directions of every undirected edge stored and every row strictly
+ * ascending (the shape CSRGraph::fromDIMACS builds, src/CSRGraph.cpp:40-119):
+ * rowptr[n+1], col[rowptr[n]], optional color[n] (NULL = uncoloured).
+ * Self loops, duplicate entries, unsorted rows (n > 64) and one-directional
+ * edges are rejected with GCL_ERR_BAD_INPUT (the reference's refinement is
+ * undefined on parallel edges).  Results are bit-identical to the reference's sequential
  * path: the canonical matrix, its best-leaf labeling, the number of stored
  * automorphisms and the number of search-tree nodes.
  *
@@ -85,7 +85,9 @@ int gcl_canon_one(gcl_context* ctx, const int32_t* rowptr, const int32_t* col,
  *   out_status[g]           GCL_GRAPH_* (required)
  * gcl_canon_batch takes HOST pointers and performs the copies; the _device
  * form takes DEVICE pointers and only enqueues work on the context stream
- * (call gcl_sync before reading results).  Both return GCL_OK when every
+ * (call gcl_sync before reading results); it needs two host-side bounds:
+ * max_n >= every n_g, and max_m2 >= every CSR entry count of a graph with
+ * n_g > 64 (graphs up to 64 vertices never need it).  Both return GCL_OK when every
  * graph was processed, else the first failing graph's error. */
 int gcl_canon_batch(gcl_context* ctx, int count, const int64_t* voff,
                     const int64_t* eoff, const int32_t* rowptr,
@@ -97,7 +99,8 @@ int gcl_canon_batch_device_async(gcl_context* ctx, int count,
                                  const int64_t* d_voff, const int64_t* d_eoff,
                                  const int32_t* d_rowptr, const int32_t* d_col,
                                  const int32_t* d_color, int max_aut, int max_n,
-                                 uint8_t* d_out_dense, const int64_t* d_ooff,
+                                 int64_t max_m2, uint8_t* d_out_dense,
+                                 const int64_t* d_ooff,
                                  int32_t* d_out_label, int64_t* d_out_stats,
                                  int32_t* d_out_status);
 int gcl_sync(gcl_context* ctx);

@@ -12,6 +12,10 @@ for p in (ROOT, os.path.join(ROOT, "oracle")):
 
 PKG_NAME = "gpu-canonical-labeling_b200"
 
+# Bound every graph's device search in tests: a regression that loops stops
+# with GCL_ERR_TIMEOUT instead of holding the GPU.
+os.environ.setdefault("GCL_GRAPH_BUDGET_S", "30")
+
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200)")

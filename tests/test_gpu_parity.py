@@ -104,3 +104,69 @@ def test_bad_input_rejected(pkg, G, ctx):
         pkg.canon(asym, ctx=ctx)
     # the context is still usable afterwards
     assert pkg.canon(g, ctx=ctx).matrix.shape == (4, 4)
+
+
+# ---- graphs above 64 vertices (the sparse warp kernel) --------------------
+
+def test_large_random_vs_oracle(pkg, G, oracle_mod, ctx):
+    rng = np.random.default_rng(77)
+    graphs = []
+    for i in range(60):
+        n = int(rng.integers(65, 260))
+        fam = i % 5
+        if fam == 0:
+            g = G.erdos_renyi(n, float(rng.uniform(0.01, 0.08)), rng)
+        elif fam == 1:
+            g = G.random_regular(n + (n % 2), 3, rng)
+        elif fam == 2:
+            g = G.from_edges(n, G.erdos_renyi(n, 0.05, rng).edges(), rng.integers(0, 3, n))
+        elif fam == 3:
+            g = G.tree_plus_edges(n, rng)
+        else:
+            g = G.erdos_renyi(n, float(rng.uniform(0.2, 0.5)), rng)
+        graphs.append(g)
+    _check_batch(pkg, G, oracle_mod, graphs, ctx)
+
+
+def test_large_symmetric_vs_oracle(pkg, G, oracle_mod, ctx):
+    rng = np.random.default_rng(5)
+    graphs = [G.torus(k) for k in (9, 10, 12, 16)] + [G.torus(7, 11)]
+    graphs += [G.disjoint_union(G.random_regular(16, 3, rng), k) for k in (5, 8)]
+    graphs += [G.disjoint_union(G.random_regular(64, 4, rng), 2)]
+    graphs += [G.from_edges(n, []) for n in (65, 100)]
+    graphs += [G.from_edges(70, [(i, j) for i in range(70) for j in range(i + 1, 70)])]
+    graphs += [G.from_edges(200, [(0, i) for i in range(1, 200)])]
+    graphs += [G.from_edges(128, [(i, (i + 1) % 128) for i in range(128)])]
+    for max_aut in (10000, 3, 1):
+        _check_batch(pkg, G, oracle_mod, graphs, ctx, max_aut=max_aut)
+
+
+def test_mixed_small_and_large(pkg, G, oracle_mod, ctx):
+    rng = np.random.default_rng(12)
+    graphs = G.small_batch(300, seed=4) + [G.erdos_renyi(int(rng.integers(65, 200)), 0.04, rng)
+                                          for _ in range(30)]
+    order = rng.permutation(len(graphs))
+    _check_batch(pkg, G, oracle_mod, [graphs[i] for i in order], ctx)
+
+
+def test_er256_triple_iso(pkg, G, oracle_mod, ctx):
+    # plain single-graph workload: G(256, 0.05), a relabeling, one edge moved
+    rng = np.random.default_rng(1000)
+    er = G.erdos_renyi(256, 0.05, rng)
+    rel = G.random_relabel(er, rng)
+    moved = G.move_one_edge(er, rng)
+    for g in (er, rel, moved):
+        r = pkg.canon(g, ctx=ctx)
+        mat, _, na, nd = oracle_mod.canon(g)
+        assert np.array_equal(r.matrix, mat) and (r.num_aut, r.nodes) == (na, nd)
+    assert pkg.is_isomorphic(er, rel, ctx=ctx)
+    assert not pkg.is_isomorphic(er, moved, ctx=ctx)
+
+
+def test_uncoloured_single_large(pkg, G, oracle_mod, ctx):
+    # one graph per call with no colour array at all (color == NULL)
+    rng = np.random.default_rng(21)
+    for g in (G.torus(9), G.random_regular(100, 3, rng), G.erdos_renyi(120, 0.05, rng)):
+        r = pkg.canon(g, ctx=ctx)
+        mat, _, na, nd = oracle_mod.canon(g)
+        assert np.array_equal(r.matrix, mat) and (r.num_aut, r.nodes) == (na, nd)
