@@ -58,7 +58,7 @@ def build_cli(force: bool = False) -> str:
         os.makedirs(os.path.dirname(CLI_BIN), exist_ok=True)
         cmd = [HOST_CXX, "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"), CLI_SRC,
                "-o", CLI_BIN, "-L", PKG, "-lgcl_b200", "-Wl,-rpath,$ORIGIN/..",
-               "-L/usr/local/cuda/lib64", "-lcudart"]
+               ]
         subprocess.run(cmd, check=True)
     return CLI_BIN
 
