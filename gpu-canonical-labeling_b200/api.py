@@ -37,6 +37,7 @@ ERRORS = {
 EXPORTS = [
     "gcl_status_string", "gcl_version", "gcl_create", "gcl_destroy", "gcl_stream",
     "gcl_canon_one", "gcl_canon_batch", "gcl_canon_batch_device_async", "gcl_sync", "gcl_iso",
+    "gcl_canon_batch_noalloc",
 ]
 
 
@@ -75,8 +76,10 @@ def load_library(path: str = LIB_PATH):
                                                  _P, _P, _P, _P]
     lib.gcl_iso.argtypes = [_P, _P, _P, _P, ctypes.c_int, _P, _P, _P, ctypes.c_int,
                             ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+    lib.gcl_canon_batch_noalloc.argtypes = [_P, ctypes.c_int, _P, _P, _P, _P, _P, ctypes.c_int,
+                                            ctypes.c_int, _P, _P, _P, _P, _P]
     for name in ("gcl_create", "gcl_destroy", "gcl_sync", "gcl_canon_one", "gcl_canon_batch",
-                 "gcl_canon_batch_device_async", "gcl_iso"):
+                 "gcl_canon_batch_device_async", "gcl_iso", "gcl_canon_batch_noalloc"):
         getattr(lib, name).restype = ctypes.c_int
     _lib = lib
     return lib

@@ -42,8 +42,8 @@ def _stale(target, deps):
 def build_lib(force: bool = False, verbose: bool = False) -> str:
     deps = _sources() + [os.path.join(ROOT, "include", "gcl.h")]
     if force or _stale(LIB, deps):
-        cmd = [NVCC, *ARCH, *NVCC_FLAGS, "-ccbin", HOST_CXX, "-shared", "-o", LIB,
-               os.path.join(CSRC, "gcl_capi.cu")]
+        units = sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cu"))
+        cmd = [NVCC, *ARCH, *NVCC_FLAGS, "-ccbin", HOST_CXX, "-shared", "-o", LIB, *units]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
         subprocess.run(cmd, check=True)

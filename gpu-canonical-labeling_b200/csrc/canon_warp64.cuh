@@ -136,7 +136,7 @@ struct W64Refined {
   int ok;
 };
 
-__device__ __noinline__ W64Refined w64_refine(int n, uint64_t starts, uint32_t level,
+static __device__ __noinline__ W64Refined w64_refine(int n, uint64_t starts, uint32_t level,
                                               uint64_t active) {
   W64Smem& S = w64_smem();
   const uint32_t lane = lane_id();
@@ -352,7 +352,7 @@ __device__ __noinline__ W64Refined w64_refine(int n, uint64_t starts, uint32_t l
 // split_by_and_refine's split (partition_refinement.cpp:486-528): vertex v
 // moves to a singleton cell at t, the rest of the cell starts at t+1.
 // Returns false when the cell is already a singleton (nothing to refine).
-__device__ __noinline__ bool w64_individualize(int n, uint32_t level, uint32_t v, uint32_t t) {
+static __device__ __noinline__ bool w64_individualize(int n, uint32_t level, uint32_t v, uint32_t t) {
   W64Smem& S = w64_smem();
   const uint32_t lane = lane_id();
   const uint64_t mem = S.cmask[t];
@@ -375,7 +375,7 @@ __device__ __noinline__ bool w64_individualize(int n, uint32_t level, uint32_t v
 // of cells created after level Lv merges with the cell that follows it, and
 // the merged cell takes that cell's in_level.  Returns the new starts mask
 // (0 if the partition is inconsistent).
-__device__ __noinline__ uint64_t w64_backtrack(int n, uint64_t starts, uint32_t Lv) {
+static __device__ __noinline__ uint64_t w64_backtrack(int n, uint64_t starts, uint32_t Lv) {
   W64Smem& S = w64_smem();
   const uint32_t lane = lane_id();
   const uint32_t q0 = lane, q1 = lane + 32;
@@ -438,7 +438,7 @@ struct Rows2 {
   uint64_t r0, r1;
 };
 
-__device__ __noinline__ Rows2 w64_leaf_rows(int n) {
+static __device__ __noinline__ Rows2 w64_leaf_rows(int n) {
   W64Smem& S = w64_smem();
   const uint32_t lane = lane_id();
   Rows2 R{0ull, 0ull};
@@ -460,7 +460,7 @@ __device__ __noinline__ Rows2 w64_leaf_rows(int n) {
 }
 
 // compare_adj_upper(current, stored) (sequential.cpp:114-124)
-__device__ __noinline__ int w64_cmp_upper(int n, Rows2 R, const uint64_t* B) {
+static __device__ __noinline__ int w64_cmp_upper(int n, Rows2 R, const uint64_t* B) {
   W64Smem& S = w64_smem();
   const uint32_t lane = lane_id();
   uint32_t row = 64u;
@@ -496,7 +496,7 @@ __device__ __forceinline__ bool w64_rows_equal(int n, Rows2 R, const uint64_t* B
 }
 
 // Rows into a stored certificate and the vertex positions into `pos`.
-__device__ __noinline__ void w64_store_leaf(int n, Rows2 R, uint64_t* B, uint8_t* pos) {
+static __device__ __noinline__ void w64_store_leaf(int n, Rows2 R, uint64_t* B, uint8_t* pos) {
   W64Smem& S = w64_smem();
   const uint32_t lane = lane_id();
   __syncwarp();
@@ -513,7 +513,7 @@ __device__ __noinline__ void w64_store_leaf(int n, Rows2 R, uint64_t* B, uint8_t
 
 // aut[label[j]] = elem[j] with the stored leaf given by its vertex positions
 // (sequential.cpp:505-520, 544-555), written to one ring slot.
-__device__ __noinline__ void w64_store_aut(int n, const uint8_t* pos, uint8_t* dst) {
+static __device__ __noinline__ void w64_store_aut(int n, const uint8_t* pos, uint8_t* dst) {
   W64Smem& S = w64_smem();
   const uint32_t lane = lane_id();
   __syncwarp();
@@ -571,7 +571,7 @@ __device__ __forceinline__ uint32_t w64_find(volatile uint32_t* d, uint32_t x) {
 // orbits of the stored automorphisms that fix the current vertex sequence,
 // merged into the target cell's representatives.  Returns false when a
 // consistency bound was hit.
-__device__ __noinline__ bool w64_orbits(int n, int idx, int num_aut, uint32_t max_aut,
+static __device__ __noinline__ bool w64_orbits(int n, int idx, int num_aut, uint32_t max_aut,
                                         uint32_t seqlen, uint8_t* reps, const uint8_t* auts) {
   W64Smem& S = w64_smem();
   const uint32_t lane = lane_id();
@@ -647,7 +647,7 @@ __device__ __noinline__ bool w64_orbits(int n, int idx, int num_aut, uint32_t ma
 // Adjacency masks and the colour partition (initializePartition_s,
 // partition_refinement.cpp:28-68: cells are the colour classes in ascending
 // colour order).  Returns the starts mask, or 0 for invalid input.
-__device__ __noinline__ uint64_t w64_load(int n, const int32_t* rp, const int32_t* cl,
+static __device__ __noinline__ uint64_t w64_load(int n, const int32_t* rp, const int32_t* cl,
                                           const int32_t* color, int64_t m) {
   W64Smem& S = w64_smem();
   const uint32_t lane = lane_id();
@@ -733,7 +733,7 @@ struct W64Result {
   int64_t nodes;
 };
 
-__device__ __noinline__ W64Result w64_search(const BatchArgs& A, int n, int64_t vo, int64_t eo,
+static __device__ __noinline__ W64Result w64_search(const BatchArgs& A, int n, int64_t vo, int64_t eo,
                                              int64_t m, const int32_t* rp, uint8_t* slot) {
   W64Smem& S = w64_smem();
   const uint32_t lane = lane_id();
@@ -984,7 +984,7 @@ __device__ __noinline__ W64Result w64_search(const BatchArgs& A, int n, int64_t 
   return res;
 }
 
-__device__ __noinline__ void w64_write_outputs(const BatchArgs& A, int g, int n, int64_t vo) {
+static __device__ __noinline__ void w64_write_outputs(const BatchArgs& A, int g, int n, int64_t vo) {
   W64Smem& S = w64_smem();
   const uint32_t lane = lane_id();
   if (A.out_label) {

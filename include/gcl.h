@@ -105,6 +105,35 @@ int gcl_canon_batch_device_async(gcl_context* ctx, int count,
                                  int32_t* d_out_status);
 int gcl_sync(gcl_context* ctx);
 
+/* ---- batched, allocation-free (n <= 64) ---------------------------------
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc
+ * where they canonize: a framework that owns all device memory through its
+ * own allocator, a plugin in a process that forbids device allocations after
+ * start-up, or a latency-critical path where an allocate/free pair would
+ * synchronize the device.  Every pointer is a caller-owned DEVICE buffer in
+ * the batched layout above; work is enqueued on `stream` (a cudaStream_t,
+ * NULL = legacy default stream) of the current device and the call returns
+ * without waiting.  Nothing is allocated: the per-warp scratch is one device
+ * array of about 6.1 MiB that the library reserves statically on every GPU
+ * it is loaded on, held until the process exits.
+ *   Limits: max_n must be <= 64 (else GCL_ERR_TOO_LARGE, nothing launched);
+ *   up to 128 stored automorphisms per graph when max_aut > 128 -- a graph
+ *   that would store more reports GCL_GRAPH_AUT_OVERFLOW in out_status and
+ *   no result.
+ *   The first call on a device resolves the scratch's device address and the
+ *   launch shape for that device; make that first call before any stream
+ *   capture on the device.
+ *   All calls share the one scratch array, which keeps the last call's
+ *   contents: calls that overlap on the GPU (other streams, other threads)
+ *   race and corrupt each other; serialize them. */
+#define GCL_GRAPH_AUT_OVERFLOW 1
+int gcl_canon_batch_noalloc(void* stream, int count, const int64_t* d_voff,
+                            const int64_t* d_eoff, const int32_t* d_rowptr,
+                            const int32_t* d_col, const int32_t* d_color,
+                            int max_aut, int max_n, uint8_t* d_out_dense,
+                            const int64_t* d_ooff, int32_t* d_out_label,
+                            int64_t* d_out_stats, int32_t* d_out_status);
+
 /* ---- isomorphism (main.cpp:172-197) --------------------------------------
  * *verdict = 1 when the canonical upper triangles are equal (ISOMORPHIC),
  * 0 otherwise.  Graphs with different vertex counts are NOT ISOMORPHIC (the
