@@ -39,6 +39,7 @@ constexpr int kW64MaxN = 64;
 constexpr int kW64Levels = kW64MaxN + 2;
 constexpr int kW64Threads = 128;  // 4 warps per block, one graph per warp
 constexpr int kW64Warps = kW64Threads / 32;
+constexpr int kW64AutHead = 8;  // first ring entries kept in shared memory
 
 enum GraphStatus : int32_t {
   kOk = 0,
@@ -86,6 +87,13 @@ struct __align__(16) W64Smem {
   uint8_t fpos[kW64MaxN];  // vertex -> position in the first leaf
   uint8_t bpos[kW64MaxN];  // vertex -> position in the best leaf
   uint8_t map[kW64MaxN];
+  uint8_t pv[kW64MaxN];  // singleton cell start position -> its vertex
+  uint64_t sing;         // vertices whose cell is a singleton
+  // ring entries 0..kW64AutHead-1 and their fixed-point masks; later entries
+  // live in the slot workspace
+  uint8_t aut_head[kW64AutHead][kW64MaxN];
+  uint64_t fix_head[kW64AutHead];
+  uint64_t cls[kW64MaxN];  // orbit computation: previous orbit -> member mask
 };
 
 // One W64Smem per warp of the block, at namespace scope so every phase
@@ -115,9 +123,12 @@ struct BatchArgs {
   uint64_t budget_ns;    // per-graph time budget (0 = unlimited)
 };
 
-// Per-slot workspace layout: reps[kW64Levels][64] then the automorphism ring.
+// Per-slot workspace layout: reps[kW64Levels][64], the automorphism ring
+// (aut_cap x 64 bytes), then one fixed-point mask per ring entry (aut_cap x
+// 8 bytes).  The first kW64AutHead entries of both are used from shared
+// memory instead.
 __host__ __device__ constexpr uint64_t w64_slot_bytes(uint32_t aut_cap) {
-  return ((uint64_t)kW64Levels * 64u + (uint64_t)aut_cap * 64u + 255u) & ~255ull;
+  return ((uint64_t)kW64Levels * 64u + (uint64_t)aut_cap * 72u + 255u) & ~255ull;
 }
 
 __device__ __forceinline__ uint64_t ballot2(bool a, bool b) {
@@ -137,17 +148,16 @@ struct W64Refined {
 };
 
 static __device__ __noinline__ W64Refined w64_refine(int n, uint64_t starts, uint32_t level,
-                                              uint64_t active) {
+                                                     uint64_t active) {
   W64Smem& S = w64_smem();
   const uint32_t lane = lane_id();
   const uint64_t full = low_mask((uint32_t)n);
   const uint32_t v0 = lane, v1 = lane + 32;
   const bool ok0 = v0 < (uint32_t)n, ok1 = v1 < (uint32_t)n;
   const uint64_t adj0 = ok0 ? S.adj[v0] : 0ull, adj1 = ok1 ? S.adj[v1] : 0ull;
-  uint32_t cs0 = ok0 ? S.cs[v0] : 0u, cs1 = ok1 ? S.cs[v1] : 0u;
-  uint64_t cm0 = ok0 ? S.cmask[cs0] : 0ull, cm1 = ok1 ? S.cmask[cs1] : 0ull;
   const uint32_t lvl1 = level + 1;
   const uint64_t lastbit = bit64((uint32_t)n - 1);
+  uint64_t sing = S.sing;
   uint32_t lc = popc64(starts), hint = 0, iters = 0;
   int ok = 1;
   while (starts != full && active) {
@@ -167,108 +177,93 @@ static __device__ __noinline__ W64Refined w64_refine(int n, uint64_t starts, uin
     const uint64_t nx = starts & ge_mask(s + 1);
     const uint32_t e = nx ? ctz64(nx) : (uint32_t)n;
     lc = mash(lc, s + e - 1);  // split1 + split2
-    const uint64_t spl = ballot2(ok0 && cs0 == s, ok1 && cs1 == s);
     if (e - s == 1) {
-      // Singleton splitter {w}: every cell meeting N(w) partially splits into
-      // [neighbours, non-neighbours].
-      if (popc64(spl) != 1) {
-        ok = 0;
-        break;
+      // Singleton splitter {w}: a cell splits into [neighbours, non-neighbours]
+      // when N(w) meets it partially.  Only neighbours outside singleton
+      // cells can be in such a cell, so most steps end here.
+      const uint64_t N = S.adj[S.pv[s]];
+      uint64_t X = N & ~sing;
+      if (!X) continue;
+      uint64_t splitc = 0;
+      while (X) {
+        const uint32_t c = S.cs[ctz64(X)];
+        const uint64_t C = S.cmask[c];
+        X &= ~C;
+        if (C & ~N) splitc |= bit64(c);
       }
-      const uint64_t N = S.adj[ctz64(spl)];
-      uint64_t ns = 0;
-      {
-        const uint64_t CN = cm0 & N;
-        if (ok0 && CN != 0 && CN != cm0) {
-          if ((N >> v0) & 1ull) {
-            cm0 = CN;
-          } else {
-            cm0 &= ~N;
-            cs0 += popc64(CN);
-            ns |= bit64(cs0);
-          }
+      // split cells in position order: hash, active set, in_level (:296-465)
+      while (splitc) {
+        const uint32_t c = ctz64(splitc);
+        splitc &= splitc - 1;
+        const uint64_t C = S.cmask[c], CN = C & N, CR = C & ~N;
+        const uint32_t nb = popc64(CN), nn = popc64(CR), p = c + nb;
+        const uint32_t old = S.inlev[c];
+        lc = mash(lc, p - 1);  // cell.first + neighbors_size - 1
+        if (((active >> c) & 1ull) || nb >= nn) {
+          active |= bit64(p);
+          if (nn == 1) hint = p;
+        } else {
+          active |= bit64(c);
+          if (nb == 1) hint = c;
         }
-      }
-      {
-        const uint64_t CN = cm1 & N;
-        if (ok1 && CN != 0 && CN != cm1) {
-          if ((N >> v1) & 1ull) {
-            cm1 = CN;
-          } else {
-            cm1 &= ~N;
-            cs1 += popc64(CN);
-            ns |= bit64(cs1);
-          }
-        }
-      }
-      const uint64_t NS = warp_or64(ns);
-      if (NS) {
-        // in_level: the neighbour fragment is new (level+1), the
-        // non-neighbour fragment keeps the cell's old in_level (:463-465)
-        uint32_t w0 = 0xffu, w1 = 0xffu;
-        if ((NS >> v0) & 1ull) w0 = S.inlev[msb64(starts & low_mask(v0))];
-        if ((NS >> v1) & 1ull) w1 = S.inlev[msb64(starts & low_mask(v1))];
-        const uint64_t all = starts | NS;
-        uint64_t t = NS, splitc = 0;
-        while (t) {
-          const uint32_t p = ctz64(t);
-          t &= t - 1;
-          const uint32_t c = msb64(starts & low_mask(p));
-          splitc |= bit64(c);
-          const uint64_t q = all & ge_mask(p + 1);
-          const uint32_t nb = p - c, nn = (q ? ctz64(q) : (uint32_t)n) - p;
-          lc = mash(lc, p - 1);  // cell.first + neighbors_size - 1 (:399-409)
-          // active set (:414-435)
-          if (((active >> c) & 1ull) || nb >= nn) {
-            active |= bit64(p);
-            if (nn == 1) hint = p;
-          } else {
-            active |= bit64(c);
-            if (nb == 1) hint = c;
-          }
-        }
+        starts |= bit64(p);
+        if (nb == 1) sing |= CN;
+        if (nn == 1) sing |= CR;
         __syncwarp();
-        if (w0 != 0xffu) S.inlev[v0] = (uint8_t)w0;
-        else if ((splitc >> v0) & 1ull) S.inlev[v0] = (uint8_t)lvl1;
-        if (w1 != 0xffu) S.inlev[v1] = (uint8_t)w1;
-        else if ((splitc >> v1) & 1ull) S.inlev[v1] = (uint8_t)lvl1;
-        starts = all;
+        if (lane == 0) {
+          S.cmask[c] = CN;
+          S.cmask[p] = CR;
+          S.inlev[c] = (uint8_t)lvl1;
+          S.inlev[p] = (uint8_t)old;
+          if (nb == 1) S.pv[c] = (uint8_t)ctz64(CN);
+          if (nn == 1) S.pv[p] = (uint8_t)ctz64(CR);
+        }
+        if ((CR >> v0) & 1ull) S.cs[v0] = (uint8_t)p;
+        if ((CR >> v1) & 1ull) S.cs[v1] = (uint8_t)p;
+        __syncwarp();
       }
     } else {
       // Non-singleton splitter: fragments in ascending neighbour count.
       lc = mash(lc, e - s);
+      const uint64_t spl = S.cmask[s];
+      uint32_t cs0 = ok0 ? S.cs[v0] : 0u, cs1 = ok1 ? S.cs[v1] : 0u;
+      uint64_t cm0 = ok0 ? S.cmask[cs0] : 0ull, cm1 = ok1 ? S.cmask[cs1] : 0ull;
       const uint32_t k0 = ok0 ? popc64(adj0 & spl) : 0u, k1 = ok1 ? popc64(adj1 & spl) : 0u;
       const uint32_t mx = __reduce_max_sync(GCL_FULL, max(k0, k1));
-      uint64_t eq0 = cm0, eq1 = cm1;
       uint32_t lt0 = 0, lt1 = 0;
       for (int b = mx ? 31 - __clz((int)mx) : -1; b >= 0; --b) {
         const bool b0 = (k0 >> b) & 1u, b1 = (k1 >> b) & 1u;
         const uint64_t M = ballot2(b0, b1);
         if (b0) {
-          lt0 += popc64(eq0 & ~M);
-          eq0 &= M;
+          lt0 += popc64(cm0 & ~M);
+          cm0 &= M;
         } else {
-          eq0 &= ~M;
+          cm0 &= ~M;
         }
         if (b1) {
-          lt1 += popc64(eq1 & ~M);
-          eq1 &= M;
+          lt1 += popc64(cm1 & ~M);
+          cm1 &= M;
         } else {
-          eq1 &= ~M;
+          cm1 &= ~M;
         }
       }
-      uint64_t ns = 0;
+      cs0 += lt0;
+      cs1 += lt1;
+      const uint64_t ns = (ok0 ? bit64(cs0) : 0ull) | (ok1 ? bit64(cs1) : 0ull);
+      const bool s0 = ok0 && popc64(cm0) == 1, s1 = ok1 && popc64(cm1) == 1;
+      sing = ballot2(s0, s1);
+      __syncwarp();  // every lane has read the old cell masks
       if (ok0) {
-        cs0 += lt0;
-        cm0 = eq0;
-        ns |= bit64(cs0);
+        S.cs[v0] = (uint8_t)cs0;
+        S.cmask[cs0] = cm0;
         S.fk[cs0] = (uint8_t)k0;
+        if (s0) S.pv[cs0] = (uint8_t)v0;
       }
       if (ok1) {
-        cs1 += lt1;
-        cm1 = eq1;
-        ns |= bit64(cs1);
+        S.cs[v1] = (uint8_t)cs1;
+        S.cmask[cs1] = cm1;
         S.fk[cs1] = (uint8_t)k1;
+        if (s1) S.pv[cs1] = (uint8_t)v1;
       }
       const uint64_t NS = warp_or64(ns) & ~starts;
       __syncwarp();
@@ -334,17 +329,11 @@ static __device__ __noinline__ W64Refined w64_refine(int n, uint64_t starts, uin
         if (w1 != 0xffu) S.inlev[v1] = (uint8_t)w1;
         starts = all;
       }
+      __syncwarp();
     }
   }
   __syncwarp();
-  if (ok0) {
-    S.cs[v0] = (uint8_t)cs0;
-    S.cmask[cs0] = cm0;
-  }
-  if (ok1) {
-    S.cs[v1] = (uint8_t)cs1;
-    S.cmask[cs1] = cm1;
-  }
+  if (lane == 0) S.sing = sing;
   __syncwarp();
   return {starts, cleanup(mash(lc, popc64(starts))), ok};
 }
@@ -362,10 +351,18 @@ static __device__ __noinline__ bool w64_individualize(int n, uint32_t level, uin
   if (v0 < (uint32_t)n && ((mem >> v0) & 1ull) && v0 != v) S.cs[v0] = (uint8_t)(t + 1);
   if (v1 < (uint32_t)n && ((mem >> v1) & 1ull) && v1 != v) S.cs[v1] = (uint8_t)(t + 1);
   if (lane == 0) {
+    const uint64_t rest = mem & ~bit64(v);
     S.cmask[t] = bit64(v);
-    S.cmask[t + 1] = mem & ~bit64(v);
+    S.cmask[t + 1] = rest;
     S.inlev[t + 1] = S.inlev[t];
     S.inlev[t] = (uint8_t)(level + 1);
+    S.pv[t] = (uint8_t)v;
+    uint64_t sg = S.sing | bit64(v);
+    if (popc64(rest) == 1) {
+      sg |= rest;
+      S.pv[t + 1] = (uint8_t)ctz64(rest);
+    }
+    S.sing = sg;
   }
   __syncwarp();
   return true;
@@ -425,8 +422,22 @@ static __device__ __noinline__ uint64_t w64_backtrack(int n, uint64_t starts, ui
     S.inlev[q1] = (uint8_t)nl1;
     S.cmask[q1] = m1;
   }
-  if (q0 < (uint32_t)n) S.cs[q0] = (uint8_t)msb64(NST & low_mask((uint32_t)S.cs[q0] + 1));
-  if (q1 < (uint32_t)n) S.cs[q1] = (uint8_t)msb64(NST & low_mask((uint32_t)S.cs[q1] + 1));
+  uint32_t c0 = 0, c1 = 0;
+  if (q0 < (uint32_t)n) {
+    c0 = msb64(NST & low_mask((uint32_t)S.cs[q0] + 1));
+    S.cs[q0] = (uint8_t)c0;
+  }
+  if (q1 < (uint32_t)n) {
+    c1 = msb64(NST & low_mask((uint32_t)S.cs[q1] + 1));
+    S.cs[q1] = (uint8_t)c1;
+  }
+  __syncwarp();
+  // vertices in singleton cells after the merge; their pv entries are
+  // unchanged (merging never creates a singleton)
+  const bool g0 = q0 < (uint32_t)n && popc64(S.cmask[c0]) == 1;
+  const bool g1 = q1 < (uint32_t)n && popc64(S.cmask[c1]) == 1;
+  const uint64_t sg = ballot2(g0, g1);
+  if (lane == 0) S.sing = sg;
   __syncwarp();
   return NST;
 }
@@ -512,16 +523,29 @@ static __device__ __noinline__ void w64_store_leaf(int n, Rows2 R, uint64_t* B, 
 }
 
 // aut[label[j]] = elem[j] with the stored leaf given by its vertex positions
-// (sequential.cpp:505-520, 544-555), written to one ring slot.
-static __device__ __noinline__ void w64_store_aut(int n, const uint8_t* pos, uint8_t* dst) {
+// (sequential.cpp:505-520, 544-555), written to one ring slot; its mask of
+// fixed points goes to *fix.
+static __device__ __noinline__ void w64_store_aut(int n, const uint8_t* pos, uint8_t* dst,
+                                                  uint64_t* fix) {
   W64Smem& S = w64_smem();
   const uint32_t lane = lane_id();
   __syncwarp();
   if (lane < (uint32_t)n) S.map[S.cs[lane]] = (uint8_t)lane;  // position -> vertex
   if (lane + 32 < (uint32_t)n) S.map[S.cs[lane + 32]] = (uint8_t)(lane + 32);
   __syncwarp();
-  if (lane < (uint32_t)n) dst[lane] = S.map[pos[lane]];
-  if (lane + 32 < (uint32_t)n) dst[lane + 32] = S.map[pos[lane + 32]];
+  bool f0 = false, f1 = false;
+  if (lane < (uint32_t)n) {
+    const uint8_t im = S.map[pos[lane]];
+    dst[lane] = im;
+    f0 = im == lane;
+  }
+  if (lane + 32 < (uint32_t)n) {
+    const uint8_t im = S.map[pos[lane + 32]];
+    dst[lane + 32] = im;
+    f1 = im == lane + 32;
+  }
+  const uint64_t fm = ballot2(f0, f1);
+  if (lane == 0) *fix = fm;
   __syncwarp();
 }
 
@@ -556,83 +580,124 @@ __device__ __forceinline__ void w64_select_tc(int n, uint64_t starts, int tcl) {
   __syncwarp();
 }
 
-// Root of x in the shared union-find; parents only point to smaller
-// vertices, so a path has at most n steps.
-__device__ __forceinline__ uint32_t w64_find(volatile uint32_t* d, uint32_t x) {
-  uint32_t p = d[x];
-  for (int step = 0; p < x && step < kW64MaxN; ++step) {
-    x = p;
-    p = d[x];
-  }
-  return x;
-}
-
 // subgroup_fixing_sequence + compute_orbits_fast (perm_group.cpp:5-116):
 // orbits of the stored automorphisms that fix the current vertex sequence,
-// merged into the target cell's representatives.  Returns false when a
-// consistency bound was hit.
+// merged into the target cell's previous orbits; each new representative is
+// the least vertex of its merged orbit, as with the reference's min-root
+// union-find.  A permutation fixes the sequence iff the sequence's vertex mask
+// lies inside its fixed-point mask.  Such a permutation maps the target cell
+// onto itself, so one that moves no member of the cell only joins vertices
+// outside it and cannot change a member's orbit: only permutations that fix
+// the sequence and move a member take part.
+//
+// The merge works on labels that are parent pointers to smaller vertices of
+// the same component.  Every previous orbit is turned into one more
+// permutation (a cycle through its members), so every edge of the union lies
+// on a permutation cycle.  A round pulls the least label over all
+// permutation images of a vertex (independent shared-memory loads), hooks the
+// vertex's old parent under it (atomicMin), and shortcuts parents twice; a
+// round that improves no label ends it, and then every vertex points at the
+// least vertex of its component.  Returns false when the round bound was hit.
 static __device__ __noinline__ bool w64_orbits(int n, int idx, int num_aut, uint32_t max_aut,
-                                        uint32_t seqlen, uint8_t* reps, const uint8_t* auts) {
+                                               uint32_t seqlen, uint8_t* reps, const uint8_t* auts,
+                                               const uint64_t* fixes) {
   W64Smem& S = w64_smem();
   const uint32_t lane = lane_id();
   const int limit = num_aut < (int)max_aut ? num_aut : (int)max_aut;
   int from = S.tc[idx].last;
   if (from == -1) from = 0;
   const uint64_t mem = S.tc[idx].members;
+  const uint64_t seqm = warp_or64((lane < seqlen ? bit64(S.seq[lane]) : 0ull) |
+                                  (lane + 32 < seqlen ? bit64(S.seq[lane + 32]) : 0ull));
+  // taking part: a bit per shared-memory head entry, and whether any later
+  // (device-memory) entry does
+  uint32_t selh = 0;
+  bool seltail = false;
+  for (int i = from; i < limit; ++i) {
+    const uint64_t fm = i < kW64AutHead ? S.fix_head[i] : fixes[i];
+    if ((seqm & ~fm) || !(mem & ~fm)) continue;
+    if (i < kW64AutHead)
+      selh |= 1u << i;
+    else
+      seltail = true;
+  }
+  if (!selh && !seltail) return true;  // no member's orbit can change
   const bool rv = S.tc[idx].reps_valid;
   uint8_t* rp = reps + (uint64_t)idx * 64u;
   const uint32_t v0 = lane, v1 = lane + 32;
   const bool ok0 = v0 < (uint32_t)n, ok1 = v1 < (uint32_t)n;
-  volatile uint32_t* dsu = S.dsu;
+  uint32_t L0 = ok0 && ((mem >> v0) & 1ull) && rv ? (uint32_t)rp[v0] : v0;
+  uint32_t L1 = ok1 && ((mem >> v1) & 1ull) && rv ? (uint32_t)rp[v1] : v1;
+  // previous orbits as cycles: next larger member, wrapping to the least
   __syncwarp();
-  if (ok0) dsu[v0] = ((mem >> v0) & 1ull) && rv ? (uint32_t)rp[v0] : v0;
-  if (ok1) dsu[v1] = ((mem >> v1) & 1ull) && rv ? (uint32_t)rp[v1] : v1;
+  S.cls[v0] = 0;
+  S.cls[v1] = 0;
   __syncwarp();
-  bool any = false;
-  for (int i = from; i < limit; ++i) {
-    const uint8_t* pm = auts + (uint64_t)i * 64u;
-    const bool bad0 = lane < seqlen && pm[S.seq[lane]] != S.seq[lane];
-    const bool bad1 = lane + 32 < seqlen && pm[S.seq[lane + 32]] != S.seq[lane + 32];
-    if (__any_sync(GCL_FULL, bad0 || bad1)) continue;
-    any = true;
-    const uint32_t i0 = ok0 ? pm[v0] : v0, i1 = ok1 ? pm[v1] : v1;
-    // hook roots (larger under smaller) until every (v, pm[v]) joins two
-    // vertices of one tree; each round merges at least two trees
-    for (int round = 0;; ++round) {
-      if (round > kW64MaxN + 1) return false;
-      bool changed = false;
-      if (i0 != v0) {
-        const uint32_t a = w64_find(dsu, v0), b = w64_find(dsu, i0);
-        if (a != b) {
-          atomicMin((uint32_t*)&dsu[max(a, b)], min(a, b));
-          changed = true;
-        }
-      }
-      if (i1 != v1) {
-        const uint32_t a = w64_find(dsu, v1), b = w64_find(dsu, i1);
-        if (a != b) {
-          atomicMin((uint32_t*)&dsu[max(a, b)], min(a, b));
-          changed = true;
-        }
-      }
-      __syncwarp();
-      if (ok0) atomicMin((uint32_t*)&dsu[v0], w64_find(dsu, v0));
-      if (ok1) atomicMin((uint32_t*)&dsu[v1], w64_find(dsu, v1));
-      __syncwarp();
-      if (!__any_sync(GCL_FULL, changed)) break;
-    }
+  if (ok0) atomicOr((unsigned long long*)&S.cls[L0], (unsigned long long)bit64(v0));
+  if (ok1) atomicOr((unsigned long long*)&S.cls[L1], (unsigned long long)bit64(v1));
+  __syncwarp();
+  uint32_t sg0 = v0, sg1 = v1;
+  if (ok0) {
+    const uint64_t c = S.cls[L0], up = c & ge_mask(v0 + 1);
+    sg0 = ctz64(up ? up : c);
   }
-  if (!any) return true;
+  if (ok1) {
+    const uint64_t c = S.cls[L1], up = c & ge_mask(v1 + 1);
+    sg1 = ctz64(up ? up : c);
+  }
+  uint32_t* lab = S.dsu;
+  lab[v0] = L0;
+  lab[v1] = L1;
+  for (int round = 0;; ++round) {
+    if (round > 2 * kW64MaxN) return false;
+    __syncwarp();
+    L0 = lab[v0];
+    L1 = lab[v1];
+    uint32_t n0 = min(L0, lab[sg0]), n1 = min(L1, lab[sg1]);
+#pragma unroll
+    for (int k = 0; k < kW64AutHead; ++k) {
+      if (!((selh >> k) & 1u)) continue;
+      if (ok0) n0 = min(n0, lab[S.aut_head[k][v0]]);
+      if (ok1) n1 = min(n1, lab[S.aut_head[k][v1]]);
+    }
+    if (seltail)
+      for (int i = max(from, kW64AutHead); i < limit; ++i) {
+        const uint64_t fm = fixes[i];
+        if ((seqm & ~fm) || !(mem & ~fm)) continue;
+        const uint8_t* pm = auts + (uint64_t)i * 64u;
+        if (ok0) n0 = min(n0, lab[pm[v0]]);
+        if (ok1) n1 = min(n1, lab[pm[v1]]);
+      }
+    const bool changed = n0 < L0 || n1 < L1;
+    __syncwarp();
+    if (n0 < L0) {  // hook the old parent, then the vertex, under the smaller label
+      atomicMin(&lab[L0], n0);
+      atomicMin(&lab[v0], n0);
+    }
+    if (n1 < L1) {
+      atomicMin(&lab[L1], n1);
+      atomicMin(&lab[v1], n1);
+    }
+    for (int j = 0; j < 2; ++j) {  // shortcut: parent := grandparent
+      __syncwarp();
+      const uint32_t g0 = lab[lab[v0]], g1 = lab[lab[v1]];
+      __syncwarp();
+      atomicMin(&lab[v0], g0);
+      atomicMin(&lab[v1], g1);
+    }
+    if (!__any_sync(GCL_FULL, changed)) break;
+  }
+  __syncwarp();
+  L0 = lab[v0];
+  L1 = lab[v1];
   bool r0 = false, r1 = false;
   if (ok0 && ((mem >> v0) & 1ull)) {
-    const uint32_t r = w64_find(dsu, v0);
-    rp[v0] = (uint8_t)r;
-    r0 = r == v0;
+    rp[v0] = (uint8_t)L0;
+    r0 = L0 == v0;
   }
   if (ok1 && ((mem >> v1) & 1ull)) {
-    const uint32_t r = w64_find(dsu, v1);
-    rp[v1] = (uint8_t)r;
-    r1 = r == v1;
+    rp[v1] = (uint8_t)L1;
+    r1 = L1 == v1;
   }
   const uint64_t rm = ballot2(r0, r1);
   __syncwarp();
@@ -690,7 +755,11 @@ static __device__ __noinline__ uint64_t w64_load(int n, const int32_t* rp, const
   if (!__any_sync(GCL_FULL, c0 != 0 || c1 != 0)) {
     if (lane < (uint32_t)n) S.cs[lane] = 0;
     if (lane + 32 < (uint32_t)n) S.cs[lane + 32] = 0;
-    if (lane == 0) S.cmask[0] = low_mask((uint32_t)n);
+    if (lane == 0) {
+      S.cmask[0] = low_mask((uint32_t)n);
+      S.pv[0] = 0;
+      S.sing = n == 1 ? 1ull : 0ull;
+    }
     starts = 1ull;
   } else {
     int32_t* ct = reinterpret_cast<int32_t*>(S.dsu);
@@ -712,13 +781,18 @@ static __device__ __noinline__ uint64_t w64_load(int n, const int32_t* rp, const
       S.cs[lane] = (uint8_t)b0;
       S.cmask[b0] = same0;
       st |= bit64(b0);
+      if (popc64(same0) == 1) S.pv[b0] = (uint8_t)lane;
     }
     if (lane + 32 < (uint32_t)n) {
       S.cs[lane + 32] = (uint8_t)b1;
       S.cmask[b1] = same1;
       st |= bit64(b1);
+      if (popc64(same1) == 1) S.pv[b1] = (uint8_t)(lane + 32);
     }
     starts = warp_or64(st);
+    const uint64_t sg = ballot2(lane < (uint32_t)n && popc64(same0) == 1,
+                                lane + 32 < (uint32_t)n && popc64(same1) == 1);
+    if (lane == 0) S.sing = sg;
   }
   if (lane < (uint32_t)n) S.inlev[lane] = 0;
   if (lane + 32 < (uint32_t)n) S.inlev[lane + 32] = 0;
@@ -839,7 +913,8 @@ static __device__ __noinline__ W64Result w64_search(const BatchArgs& A, int n, i
           classify = false;
         } else {
           if (num_aut > 0 && num_aut > S.tc[idx].last) {
-            if (!w64_orbits(n, idx, num_aut, A.max_aut, seqlen, reps, auts)) {
+            if (!w64_orbits(n, idx, num_aut, A.max_aut, seqlen, reps, auts,
+                            reinterpret_cast<const uint64_t*>(auts + (uint64_t)A.aut_cap * 64u))) {
               status = kInternal;
               break;
             }
@@ -936,7 +1011,12 @@ static __device__ __noinline__ W64Result w64_search(const BatchArgs& A, int n, i
           status = kAutOverflow;
           break;
         }
-        w64_store_aut(n, dec == 1 ? S.fpos : S.bpos, auts + (uint64_t)slot_i * 64u);
+        w64_store_aut(n, dec == 1 ? S.fpos : S.bpos,
+                      slot_i < (uint32_t)kW64AutHead ? S.aut_head[slot_i]
+                                                     : auts + (uint64_t)slot_i * 64u,
+                      slot_i < (uint32_t)kW64AutHead
+                          ? &S.fix_head[slot_i]
+                          : reinterpret_cast<uint64_t*>(auts + (uint64_t)A.aut_cap * 64u) + slot_i);
         ++num_aut;
         const int g = dec == 1 ? w64_gca(S.first_seq, first_seqlen, seqlen)
                                : w64_gca(S.best_seq, best_seqlen, seqlen);

@@ -38,6 +38,35 @@ struct Deferred {
   int next_sp_fail;
 };
 
+// Largest graphs first: a counting sort of the graph ids by descending n
+// (n > 64 first, they only pass through the warp kernel), so the persistent
+// warps do not finish on a few large graphs (longest-processing-time order).
+constexpr int kOrderThreads = 1024;
+__global__ void __launch_bounds__(kOrderThreads)
+    order_by_size_kernel(int count, const int64_t* voff, int* order) {
+  __shared__ int hist[kW64MaxN + 2];
+  __shared__ int start[kW64MaxN + 2];
+  for (int b = threadIdx.x; b < kW64MaxN + 2; b += blockDim.x) hist[b] = 0;
+  __syncthreads();
+  for (int g = threadIdx.x; g < count; g += blockDim.x) {
+    const int64_t n = voff[g + 1] - voff[g];
+    atomicAdd(&hist[n > kW64MaxN ? kW64MaxN + 1 : (int)n], 1);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int run = 0;
+    for (int b = kW64MaxN + 1; b >= 0; --b) {
+      start[b] = run;
+      run += hist[b];
+    }
+  }
+  __syncthreads();
+  for (int g = threadIdx.x; g < count; g += blockDim.x) {
+    const int64_t n = voff[g + 1] - voff[g];
+    order[atomicAdd(&start[n > kW64MaxN ? kW64MaxN + 1 : (int)n], 1)] = g;
+  }
+}
+
 constexpr uint32_t kSpPool = 8;     // per-level orbit arrays in the first sparse pass
 constexpr uint32_t kSpAutCap = 64;  // ring entries in the first sparse pass
 
@@ -145,7 +174,7 @@ struct gcl_context {
   int big_slots = 0;
   DevBuf sp_work, sp_work_big;
   int sp_grid = 0;
-  DevBuf deferred, overflow_list, large_list, sp_fail_list;
+  DevBuf deferred, overflow_list, large_list, sp_fail_list, order;
   // staging for host-pointer calls
   DevBuf voff, eoff, rowptr, col, color, ooff, dense, label, stats, status;
 };
@@ -235,7 +264,7 @@ int gcl_destroy(gcl_context* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   DevBuf* bufs[] = {&c->work, &c->work_big, &c->sp_work, &c->sp_work_big, &c->deferred,
-                    &c->overflow_list, &c->large_list, &c->sp_fail_list, &c->voff, &c->eoff, &c->rowptr, &c->col, &c->color,
+                    &c->overflow_list, &c->large_list, &c->sp_fail_list, &c->order, &c->voff, &c->eoff, &c->rowptr, &c->col, &c->color,
                     &c->ooff, &c->dense, &c->label, &c->stats, &c->status};
   for (DevBuf* b : bufs) b->release();
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -270,7 +299,10 @@ int gcl_canon_batch_device_async(gcl_context* c, int count, const int64_t* d_vof
   GCL_TRY(c->work.ensure(slots * slot_bytes));
   GCL_TRY(c->overflow_list.ensure((size_t)count * sizeof(int)));
   GCL_TRY(c->large_list.ensure((size_t)count * sizeof(int)));
+  GCL_TRY(c->order.ensure((size_t)count * sizeof(int)));
   GCL_TRY(cudaMemsetAsync(c->deferred.p, 0, sizeof(Deferred), c->stream));
+  order_by_size_kernel<<<1, kOrderThreads, 0, c->stream>>>(count, d_voff, (int*)c->order.p);
+  GCL_TRY(cudaGetLastError());
 
   BatchArgs A;
   std::memset(&A, 0, sizeof A);
@@ -280,7 +312,7 @@ int gcl_canon_batch_device_async(gcl_context* c, int count, const int64_t* d_vof
   A.rowptr = d_rowptr;
   A.col = d_col;
   A.color = d_color;
-  A.order = nullptr;
+  A.order = (const int32_t*)c->order.p;
   A.max_aut = maut;
   A.aut_cap = cap;
   A.out_dense = d_out_dense;

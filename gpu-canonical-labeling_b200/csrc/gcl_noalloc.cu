@@ -31,7 +31,7 @@ constexpr uint64_t kNoAllocSlotBytes = w64_slot_bytes(kNoAllocRing);
 constexpr uint64_t kNoAllocHeader = 256;  // the work counter
 constexpr uint64_t kNoAllocBytes = kNoAllocHeader + (uint64_t)kNoAllocSlots * kNoAllocSlotBytes;
 
-// The statically reserved scratch (about 6.1 MiB per GPU).  Host code must
+// The statically reserved scratch (about 6.6 MiB per GPU).  Host code must
 // not pass this name to a kernel: on the host it only stands for the symbol;
 // the device address comes from cudaGetSymbolAddress below.
 static __device__ __align__(256) uint8_t g_noalloc_scratch[kNoAllocBytes];

@@ -114,7 +114,7 @@ int gcl_sync(gcl_context* ctx);
  * the batched layout above; work is enqueued on `stream` (a cudaStream_t,
  * NULL = legacy default stream) of the current device and the call returns
  * without waiting.  Nothing is allocated: the per-warp scratch is one device
- * array of about 6.1 MiB that the library reserves statically on every GPU
+ * array of about 6.6 MiB that the library reserves statically on every GPU
  * it is loaded on, held until the process exits.
  *   Limits: max_n must be <= 64 (else GCL_ERR_TOO_LARGE, nothing launched);
  *   up to 128 stored automorphisms per graph when max_aut > 128 -- a graph
