@@ -239,7 +239,7 @@ def read_traffic():
     if not os.path.exists(p):
         return None
     for ln in open(p):
-        if ln.startswith("dram_bytes_per_launch:"):
+        if ln.strip().startswith("dram_bytes_per_launch:"):
             return float(ln.split(":")[1].split()[0])
     return None
 
@@ -271,6 +271,7 @@ def gpu_arm(args):
     ctx = api.Context(local)
     stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
     ooff = arena.out_offsets()
+    roff = api.rows_offsets(arena)
     max_n = int(arena.sizes().max())
     max_m2 = int(np.diff(arena.eoff).max())
 
@@ -281,7 +282,9 @@ def gpu_arm(args):
     t_voff, t_eoff = d(arena.voff, torch.int64), d(arena.eoff, torch.int64)
     t_rp, t_col = d(arena.rowptr, torch.int32), d(arena.col, torch.int32)
     t_ooff = d(ooff, torch.int64)
+    t_roff = d(roff, torch.int64)
     t_dense = torch.empty(int(ooff[-1]), dtype=torch.uint8, device=dev)
+    t_rows = torch.empty(int(roff[-1]), dtype=torch.int64, device=dev)
     t_stats = torch.empty((count, 2), dtype=torch.int64, device=dev)
     t_status = torch.empty(count, dtype=torch.int32, device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
@@ -291,8 +294,9 @@ def gpu_arm(args):
     def launch():
         rc = lib.gcl_canon_batch_device_async(
             ctx.handle, count, P(t_voff.data_ptr()), P(t_eoff.data_ptr()), P(t_rp.data_ptr()),
-            P(t_col.data_ptr()), None, args.max_aut, max_n, max_m2, P(t_dense.data_ptr()),
-            P(t_ooff.data_ptr()), None, P(t_stats.data_ptr()), P(t_status.data_ptr()))
+            P(t_col.data_ptr()), None, args.max_aut, max_n, max_m2, None, None,
+            P(t_rows.data_ptr()), P(t_roff.data_ptr()), None, P(t_stats.data_ptr()),
+            P(t_status.data_ptr()))
         if rc != 0:
             raise RuntimeError(f"gcl_canon_batch_device_async failed: {rc}")
 
@@ -337,35 +341,46 @@ def gpu_arm(args):
     # end to end through the C ABI: pinned host buffers, copies inside
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
     h_voff, h_eoff, h_rp, h_col = pin(arena.voff), pin(arena.eoff), pin(arena.rowptr), pin(arena.col)
-    h_ooff = pin(ooff)
+    h_ooff, h_roff = pin(ooff), pin(roff)
     h_dense = torch.empty(int(ooff[-1]), dtype=torch.uint8).pin_memory().numpy()
+    h_rows = torch.empty(int(roff[-1]), dtype=torch.int64).pin_memory().numpy()
     h_stats = torch.empty((count, 2), dtype=torch.int64).pin_memory().numpy()
     h_status = torch.empty(count, dtype=torch.int32).pin_memory().numpy()
     pp = lambda a: a.ctypes.data_as(P)  # noqa: E731
 
-    def e2e_call():
+    def e2e_call(dense):
+        if dense:  # the reference's n*n byte matrices
+            outs = (pp(h_dense), pp(h_ooff), None, None)
+        else:  # the same canonical forms bit-packed
+            outs = (None, None, pp(h_rows), pp(h_roff))
         rc = lib.gcl_canon_batch(ctx.handle, count, pp(h_voff), pp(h_eoff), pp(h_rp), pp(h_col),
-                                 None, args.max_aut, pp(h_dense), pp(h_ooff), None, pp(h_stats),
-                                 pp(h_status))
+                                 None, args.max_aut, *outs, None, pp(h_stats), pp(h_status))
         if rc != 0:
             raise RuntimeError(f"gcl_canon_batch failed: {rc}")
 
-    for _ in range(max(2, args.warmup // 2) if not args.no_e2e else 0):
-        e2e_call()
-    barrier()
-    e2e_t = []
-    for _ in range(args.steps if not args.no_e2e else 0):
-        t0 = time.perf_counter()
-        e2e_call()
-        e2e_t.append(time.perf_counter() - t0)
-    barrier()
-    e2e_s = float(np.sum(e2e_t)) if e2e_t else float("nan")
-    if world > 1:
-        t = torch.tensor([e2e_s], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    h2d = sum(a.nbytes for a in (h_voff, h_eoff, h_rp, h_col, h_ooff))
-    d2h = h_dense.nbytes + h_stats.nbytes + h_status.nbytes
+    def e2e_run(dense):
+        for _ in range(max(2, args.warmup // 2) if not args.no_e2e else 0):
+            e2e_call(dense)
+        barrier()
+        ts = []
+        for _ in range(args.steps if not args.no_e2e else 0):
+            t0 = time.perf_counter()
+            e2e_call(dense)
+            ts.append(time.perf_counter() - t0)
+        barrier()
+        s = float(np.sum(ts)) if ts else float("nan")
+        if world > 1:
+            t = torch.tensor([s], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            s = float(t.item())
+        return s
+
+    e2e_s = e2e_run(False)
+    e2e_dense_s = e2e_run(True)
+    h2d = sum(a.nbytes for a in (h_voff, h_eoff, h_rp, h_col, h_roff))
+    d2h = h_rows.nbytes + h_stats.nbytes + h_status.nbytes
+    h2d_dense = sum(a.nbytes for a in (h_voff, h_eoff, h_rp, h_col, h_ooff))
+    d2h_dense = h_dense.nbytes + h_stats.nbytes + h_status.nbytes
 
     line = None
     if rank == 0:
@@ -382,9 +397,15 @@ def gpu_arm(args):
             "config": {"workload": WORKLOAD, "graphs_per_step_per_gpu": count,
                        "max_aut": args.max_aut, "seed": args.seed,
                        "parallelism": f"graph-sharded x{world} (no collective)",
-                       "l2": "flushed between steps (256 MiB write outside the timed events)"},
+                       "l2": "flushed between steps (256 MiB write outside the timed events)",
+                       "output": "bit-packed canonical rows, stats and status per graph"},
             "e2e": {"value": world * count * args.steps / e2e_s, "unit": UNIT,
-                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                    "output": "bit-packed canonical rows (n x ceil(n/64) words per graph)"},
+            "e2e_dense": {"value": world * count * args.steps / e2e_dense_s, "unit": UNIT,
+                          "h2d_bytes_per_step": int(h2d_dense),
+                          "d2h_bytes_per_step": int(d2h_dense),
+                          "output": "n*n byte matrices (the reference's Nauty_Parallel form)"},
             "gpu_launches": 2 * args.steps,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
@@ -415,7 +436,7 @@ def gpu_arm(args):
                 ctx.handle, 1, P(vo_all[i].data_ptr()), P(eo_all[i].data_ptr()),
                 P(t_rp.data_ptr() + 4 * int(hv[g] + g)), P(t_col.data_ptr() + 4 * int(hee[g])),
                 None, args.max_aut, n, m, P(t_dense.data_ptr() + int(ooff[g])),
-                P(oo_all[i].data_ptr()), None, P(t_stats.data_ptr() + 16 * g),
+                P(oo_all[i].data_ptr()), None, None, None, P(t_stats.data_ptr() + 16 * g),
                 P(t_status.data_ptr() + 4 * g))
             if rc != 0:
                 raise RuntimeError("plain launch failed")

@@ -70,10 +70,10 @@ def load_library(path: str = LIB_PATH):
     lib.gcl_sync.argtypes = [_P]
     lib.gcl_canon_one.argtypes = [_P, _P, _P, _P, ctypes.c_int, ctypes.c_int, _P, _P, _P]
     lib.gcl_canon_batch.argtypes = [_P, ctypes.c_int, _P, _P, _P, _P, _P, ctypes.c_int, _P, _P,
-                                    _P, _P, _P]
+                                    _P, _P, _P, _P, _P]
     lib.gcl_canon_batch_device_async.argtypes = [_P, ctypes.c_int, _P, _P, _P, _P, _P,
                                                  ctypes.c_int, ctypes.c_int, ctypes.c_int64, _P,
-                                                 _P, _P, _P, _P]
+                                                 _P, _P, _P, _P, _P, _P]
     lib.gcl_iso.argtypes = [_P, _P, _P, _P, ctypes.c_int, _P, _P, _P, ctypes.c_int,
                             ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     lib.gcl_canon_batch_noalloc.argtypes = [_P, ctypes.c_int, _P, _P, _P, _P, _P, ctypes.c_int,
@@ -168,6 +168,21 @@ def Nauty_Parallel(g: Graph, max_aut: int = 10000) -> bytes:  # noqa: N802 (refe
     return canon(g, max_aut).matrix.tobytes()
 
 
+def rows_offsets(arena: Arena) -> np.ndarray:
+    """Offsets (in 64-bit words) of each graph's packed rows."""
+    n = arena.sizes()
+    o = np.zeros(arena.count + 1, dtype=np.int64)
+    np.cumsum(n * ((n + 63) // 64), out=o[1:])
+    return o
+
+
+def unpack_rows(rows: np.ndarray, n: int) -> np.ndarray:
+    """n x n 0/1 matrix from n packed rows of ceil(n/64) words."""
+    w = (n + 63) // 64
+    bits = np.unpackbits(rows.reshape(n, w).view(np.uint8), axis=1, bitorder="little")
+    return bits[:, :n].astype(np.uint8)
+
+
 @dataclass
 class BatchResult:
     dense: Optional[np.ndarray]  # concatenated n_g*n_g blocks
@@ -176,6 +191,11 @@ class BatchResult:
     stats: np.ndarray  # (count, 2): num_aut, nodes
     status: np.ndarray
     arena: Arena
+    rows: Optional[np.ndarray] = None  # concatenated packed rows
+    roff: Optional[np.ndarray] = None
+
+    def packed(self, g: int) -> np.ndarray:
+        return self.rows[self.roff[g]: self.roff[g + 1]]
 
     def matrix(self, g: int) -> np.ndarray:
         n = int(self.arena.voff[g + 1] - self.arena.voff[g])
@@ -187,12 +207,14 @@ class BatchResult:
 
 def canon_batch(graphs: Union[Arena, Sequence[Graph]], max_aut: int = 10000,
                 ctx: Optional[Context] = None, dense: bool = True,
-                label: bool = True) -> BatchResult:
+                label: bool = True, rows: bool = False) -> BatchResult:
     """Canonize every graph of a ragged arena in one batched call."""
     ctx = ctx or default_context()
     arena = graphs if isinstance(graphs, Arena) else pack(graphs)
     ooff = arena.out_offsets()
+    roff = rows_offsets(arena)
     out = np.zeros(max(int(ooff[-1]), 1), dtype=np.uint8) if dense else None
+    prow = np.zeros(max(int(roff[-1]), 1), dtype=np.uint64) if rows else None
     lab = np.zeros(max(int(arena.voff[-1]), 1), dtype=np.int32) if label else None
     stats = np.zeros((max(arena.count, 1), 2), dtype=np.int64)
     status = np.zeros(max(arena.count, 1), dtype=np.int32)
@@ -200,9 +222,11 @@ def canon_batch(graphs: Union[Arena, Sequence[Graph]], max_aut: int = 10000,
     color = arena.color if arena.color.any() else None
     rc = ctx.lib.gcl_canon_batch(ctx.handle, arena.count, _ptr(arena.voff), _ptr(arena.eoff),
                                  _ptr(arena.rowptr), _ptr(col), _ptr(color), max_aut, _ptr(out),
-                                 _ptr(ooff), _ptr(lab), _ptr(stats), _ptr(status))
+                                 _ptr(ooff), _ptr(prow), _ptr(roff), _ptr(lab), _ptr(stats),
+                                 _ptr(status))
     _check(rc, "gcl_canon_batch")
-    return BatchResult(out, ooff, lab, stats[:arena.count], status[:arena.count], arena)
+    return BatchResult(out, ooff, lab, stats[:arena.count], status[:arena.count], arena,
+                       prow, roff)
 
 
 def is_isomorphic(g1: Graph, g2: Graph, max_aut: int = 10000,

@@ -1341,6 +1341,19 @@ __device__ __noinline__ void sp_write_outputs(const BatchArgs& A, int g) {
   const int64_t vo = A.voff[g];
   if (A.out_label)
     for (uint32_t j = lane; j < n; j += 32) A.out_label[vo + j] = (int32_t)W.blabel[j];
+  if (A.out_rows) {  // row i: bit j set iff canonical i ~ j, ceil(n/64) words
+    const uint32_t words = (n + 63) / 64;
+    uint64_t* o = A.out_rows + A.roff[g];
+    for (uint32_t i = lane; i < n; i += 32) {
+      uint64_t* row = o + (uint64_t)i * words;
+      for (uint32_t w = 0; w < words; ++w) row[w] = 0;
+      const uint32_t v = W.blabel[i];
+      for (int32_t j = W.rp[v]; j < W.rp[v + 1]; ++j) {
+        const uint32_t c = W.bcert[j];
+        row[c >> 6] |= bit64(c & 63);
+      }
+    }
+  }
   if (A.out_dense) {
     uint8_t* o = A.out_dense + A.ooff[g];
     const uint64_t nn = (uint64_t)n * n;

@@ -114,7 +114,8 @@ struct BatchArgs {
   uint32_t aut_cap;      // automorphism slots per workspace slot (<= max_aut)
   uint8_t* out_dense;    // n*n bytes per graph at ooff[g], or null
   const int64_t* ooff;
-  uint64_t* out_cert;    // n rows per graph at voff[g], or null
+  uint64_t* out_rows;    // packed rows per graph at roff[g], or null
+  const int64_t* roff;   // ceil(n/64) words per row, n rows per graph
   int32_t* out_label;    // n per graph at voff[g], or null
   int64_t* out_stats;    // {num_aut, nodes} per graph, or null
   int32_t* status;       // per graph
@@ -1071,9 +1072,10 @@ static __device__ __noinline__ void w64_write_outputs(const BatchArgs& A, int g,
     if (lane < (uint32_t)n) A.out_label[vo + S.bpos[lane]] = (int32_t)lane;
     if (lane + 32 < (uint32_t)n) A.out_label[vo + S.bpos[lane + 32]] = (int32_t)(lane + 32);
   }
-  if (A.out_cert) {
-    if (lane < (uint32_t)n) A.out_cert[vo + lane] = S.best_cert[lane];
-    if (lane + 32 < (uint32_t)n) A.out_cert[vo + lane + 32] = S.best_cert[lane + 32];
+  if (A.out_rows) {  // one word per row for n <= 64
+    uint64_t* o = A.out_rows + A.roff[g];
+    if (lane < (uint32_t)n) o[lane] = S.best_cert[lane];
+    if (lane + 32 < (uint32_t)n) o[lane + 32] = S.best_cert[lane + 32];
   }
   if (A.out_dense) {
     uint8_t* o = A.out_dense + A.ooff[g];

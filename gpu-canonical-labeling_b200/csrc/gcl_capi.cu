@@ -176,7 +176,7 @@ struct gcl_context {
   int sp_grid = 0;
   DevBuf deferred, overflow_list, large_list, sp_fail_list, order;
   // staging for host-pointer calls
-  DevBuf voff, eoff, rowptr, col, color, ooff, dense, label, stats, status;
+  DevBuf voff, eoff, rowptr, col, color, ooff, dense, roff, rows, label, stats, status;
 };
 
 // Per-graph time budget of the search loop (GCL_GRAPH_BUDGET_S, default
@@ -242,6 +242,10 @@ int gcl_create(int device, gcl_context** out) {
   if (e == cudaSuccess)
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, w64_batch_kernel, kW64Threads, 0);
   if (e == cudaSuccess) {
+    // GCL_W64_BLOCKS_PER_SM caps the resident blocks of the warp kernel (fewer
+    // warps per SM run each graph faster; more hide more latency)
+    const char* cap_env = std::getenv("GCL_W64_BLOCKS_PER_SM");
+    if (cap_env && std::atoi(cap_env) > 0) per_sm = std::min(per_sm, std::atoi(cap_env));
     c->w64_grid = c->sms * std::max(per_sm, 1);
     e = c->deferred.ensure(sizeof(Deferred));
   }
@@ -265,7 +269,8 @@ int gcl_destroy(gcl_context* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   DevBuf* bufs[] = {&c->work, &c->work_big, &c->sp_work, &c->sp_work_big, &c->deferred,
                     &c->overflow_list, &c->large_list, &c->sp_fail_list, &c->order, &c->voff, &c->eoff, &c->rowptr, &c->col, &c->color,
-                    &c->ooff, &c->dense, &c->label, &c->stats, &c->status};
+                    &c->ooff, &c->dense, &c->roff, &c->rows, &c->label, &c->stats,
+                    &c->status};
   for (DevBuf* b : bufs) b->release();
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -284,11 +289,12 @@ int gcl_canon_batch_device_async(gcl_context* c, int count, const int64_t* d_vof
                                  const int64_t* d_eoff, const int32_t* d_rowptr,
                                  const int32_t* d_col, const int32_t* d_color, int max_aut,
                                  int max_n, int64_t max_m2, uint8_t* d_out_dense,
-                                 const int64_t* d_ooff,
+                                 const int64_t* d_ooff, uint64_t* d_out_rows,
+                                 const int64_t* d_roff,
                                  int32_t* d_out_label, int64_t* d_out_stats,
                                  int32_t* d_out_status) {
   if (!c || count < 0 || max_aut <= 0 || !d_voff || !d_eoff || !d_rowptr || !d_out_status ||
-      (d_out_dense && !d_ooff) || max_n < 0 || max_n > GCL_MAX_N)
+      (d_out_dense && !d_ooff) || (d_out_rows && !d_roff) || max_n < 0 || max_n > GCL_MAX_N)
     return GCL_ERR_ARG;
   if (count == 0) return GCL_OK;
   GCL_TRY(cudaSetDevice(c->device));
@@ -317,7 +323,8 @@ int gcl_canon_batch_device_async(gcl_context* c, int count, const int64_t* d_vof
   A.aut_cap = cap;
   A.out_dense = d_out_dense;
   A.ooff = d_ooff;
-  A.out_cert = nullptr;
+  A.out_rows = d_out_rows;
+  A.roff = d_roff;
   A.out_label = d_out_label;
   A.out_stats = d_out_stats;
   A.status = d_out_status;
@@ -413,10 +420,11 @@ extern "C" {
 
 int gcl_canon_batch(gcl_context* c, int count, const int64_t* voff, const int64_t* eoff,
                     const int32_t* rowptr, const int32_t* col, const int32_t* color, int max_aut,
-                    uint8_t* out_dense, const int64_t* ooff, int32_t* out_label,
-                    int64_t* out_stats, int32_t* out_status) {
+                    uint8_t* out_dense, const int64_t* ooff, uint64_t* out_rows,
+                    const int64_t* roff, int32_t* out_label, int64_t* out_stats,
+                    int32_t* out_status) {
   if (!c || count < 0 || max_aut <= 0 || !voff || !eoff || !rowptr || !out_status ||
-      (out_dense && !ooff))
+      (out_dense && !ooff) || (out_rows && !roff))
     return GCL_ERR_ARG;
   if (count == 0) return GCL_OK;
   if (voff[0] != 0 || eoff[0] != 0) return GCL_ERR_ARG;
@@ -428,6 +436,7 @@ int gcl_canon_batch(gcl_context* c, int count, const int64_t* voff, const int64_
     if (n < 0 || m < 0 || n > GCL_MAX_N) return n > GCL_MAX_N ? GCL_ERR_TOO_LARGE : GCL_ERR_ARG;
     if (rowptr[voff[g] + g] != 0 || rowptr[voff[g + 1] + g] != m) return GCL_ERR_BAD_INPUT;
     if (out_dense && ooff[g + 1] - ooff[g] != n * n) return GCL_ERR_ARG;
+    if (out_rows && roff[g + 1] - roff[g] != n * ((n + 63) / 64)) return GCL_ERR_ARG;
     max_n = std::max<int>(max_n, (int)n);
   }
   if (eoff[count] > 0 && !col) return GCL_ERR_ARG;
@@ -461,6 +470,17 @@ int gcl_canon_batch(gcl_context* c, int count, const int64_t* voff, const int64_
     d_dense = (uint8_t*)c->dense.p;
     d_ooff = (int64_t*)c->ooff.p;
   }
+  uint64_t* d_rows = nullptr;
+  int64_t* d_roff = nullptr;
+  size_t rows_words = 0;
+  if (out_rows) {
+    rows_words = (size_t)roff[count];
+    GCL_TRY(c->roff.ensure((count + 1) * sizeof(int64_t)));
+    GCL_TRY(c->rows.ensure(std::max<size_t>(rows_words, 1) * sizeof(uint64_t)));
+    GCL_TRY(cudaMemcpyAsync(c->roff.p, roff, (count + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+    d_rows = (uint64_t*)c->rows.p;
+    d_roff = (int64_t*)c->roff.p;
+  }
   int32_t* d_label = nullptr;
   if (out_label && nv) {
     GCL_TRY(c->label.ensure(nv * sizeof(int32_t)));
@@ -473,11 +493,14 @@ int gcl_canon_batch(gcl_context* c, int count, const int64_t* voff, const int64_
   }
   int rc = gcl_canon_batch_device_async(c, count, (int64_t*)c->voff.p, (int64_t*)c->eoff.p,
                                         (int32_t*)c->rowptr.p, (int32_t*)c->col.p, d_color,
-                                        max_aut, max_n, max_m2, d_dense, d_ooff, d_label, d_stats,
+                                        max_aut, max_n, max_m2, d_dense, d_ooff, d_rows, d_roff,
+                                        d_label, d_stats,
                                         (int32_t*)c->status.p);
   if (rc != GCL_OK) return rc;
   if (out_dense && dense_bytes)
     GCL_TRY(cudaMemcpyAsync(out_dense, d_dense, dense_bytes, cudaMemcpyDeviceToHost, s));
+  if (out_rows && rows_words)
+    GCL_TRY(cudaMemcpyAsync(out_rows, d_rows, rows_words * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
   if (d_label) GCL_TRY(cudaMemcpyAsync(out_label, d_label, nv * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
   if (d_stats)
     GCL_TRY(cudaMemcpyAsync(out_stats, d_stats, 2 * count * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
@@ -506,7 +529,7 @@ int gcl_canon_one(gcl_context* c, const int32_t* rowptr, const int32_t* col, con
   int64_t st[2] = {0, 0};
   int32_t status = 0;
   int rc = gcl_canon_batch(c, 1, voff, eoff, rowptr, col, color, max_aut, out_nxn, ooff, nullptr,
-                           st, &status);
+                           nullptr, nullptr, st, &status);
   if (rc != GCL_OK) return rc;
   if (num_aut) *num_aut = st[0];
   if (node_count) *node_count = st[1];

@@ -131,7 +131,8 @@ extern "C" int gcl_canon_batch_noalloc(void* stream, int count, const int64_t* d
   A.aut_cap = std::min<uint32_t>((uint32_t)max_aut, kNoAllocRing);
   A.out_dense = d_out_dense;
   A.ooff = d_ooff;
-  A.out_cert = nullptr;
+  A.out_rows = nullptr;
+  A.roff = nullptr;
   A.out_label = d_out_label;
   A.out_stats = d_out_stats;
   A.status = d_out_status;

@@ -80,6 +80,11 @@ int gcl_canon_one(gcl_context* ctx, const int32_t* rowptr, const int32_t* col,
  * col + eoff[g], its colours at color + voff[g] (color may be NULL).
  * Outputs (each may be NULL):
  *   out_dense + ooff[g]     n_g*n_g canonical matrix bytes
+ *   out_rows + roff[g]      the same matrix bit-packed: n_g rows of
+ *                           ceil(n_g/64) words, bit j of row i (word j/64,
+ *                           bit j%64) set iff canonical vertices i and j are
+ *                           adjacent -- equal exactly when the canonical
+ *                           forms are equal, 8x smaller than out_dense
  *   out_label + voff[g]     best-leaf labeling, position -> vertex
  *   out_stats + 2*g         {num_aut, nodes}
  *   out_status[g]           GCL_GRAPH_* (required)
@@ -92,15 +97,17 @@ int gcl_canon_one(gcl_context* ctx, const int32_t* rowptr, const int32_t* col,
 int gcl_canon_batch(gcl_context* ctx, int count, const int64_t* voff,
                     const int64_t* eoff, const int32_t* rowptr,
                     const int32_t* col, const int32_t* color, int max_aut,
-                    uint8_t* out_dense, const int64_t* ooff, int32_t* out_label,
-                    int64_t* out_stats, int32_t* out_status);
+                    uint8_t* out_dense, const int64_t* ooff, uint64_t* out_rows,
+                    const int64_t* roff, int32_t* out_label, int64_t* out_stats,
+                    int32_t* out_status);
 
 int gcl_canon_batch_device_async(gcl_context* ctx, int count,
                                  const int64_t* d_voff, const int64_t* d_eoff,
                                  const int32_t* d_rowptr, const int32_t* d_col,
                                  const int32_t* d_color, int max_aut, int max_n,
                                  int64_t max_m2, uint8_t* d_out_dense,
-                                 const int64_t* d_ooff,
+                                 const int64_t* d_ooff, uint64_t* d_out_rows,
+                                 const int64_t* d_roff,
                                  int32_t* d_out_label, int64_t* d_out_stats,
                                  int32_t* d_out_status);
 int gcl_sync(gcl_context* ctx);

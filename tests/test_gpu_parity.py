@@ -170,3 +170,13 @@ def test_uncoloured_single_large(pkg, G, oracle_mod, ctx):
         r = pkg.canon(g, ctx=ctx)
         mat, _, na, nd = oracle_mod.canon(g)
         assert np.array_equal(r.matrix, mat) and (r.num_aut, r.nodes) == (na, nd)
+
+
+def test_packed_rows_match_dense(pkg, G, ctx):
+    rng = np.random.default_rng(8)
+    graphs = G.small_batch(200, seed=71) + [G.erdos_renyi(int(rng.integers(65, 300)), 0.03, rng)
+                                           for _ in range(10)] + [G.torus(12), G.from_edges(64, [])]
+    res = pkg.canon_batch(graphs, ctx=ctx, rows=True)
+    for g in range(res.arena.count):
+        n = res.arena.graph(g).n
+        assert np.array_equal(pkg.api.unpack_rows(res.packed(g), n), res.matrix(g))
