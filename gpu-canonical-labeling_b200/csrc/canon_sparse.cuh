@@ -46,7 +46,7 @@ struct SpTc {
 // Byte layout of one slot for graphs with at most n vertices and m2 CSR
 // entries, `pool` per-level representative arrays and `cap` ring slots.
 struct SpLayout {
-  uint64_t u32n[23];  // offsets of the n-sized u32 arrays
+  uint64_t u32n[24];  // offsets of the n-sized u32 arrays
   uint64_t fcode, ccode, pool_owner;
   uint64_t stb, sts, act, acts, tcb, tcbs;
   uint64_t fcert, bcert, ccert;
@@ -67,7 +67,7 @@ __host__ __device__ inline SpLayout sp_layout(uint32_t n, uint64_t m2, uint32_t 
   };
   const uint64_t N1 = (uint64_t)n + 2;
   L.stride = (uint32_t)N1;
-  for (int i = 0; i < 23; ++i) L.u32n[i] = take(4 * N1);
+  for (int i = 0; i < 24; ++i) L.u32n[i] = take(4 * N1);
   L.fcode = take(4 * (N1 + 1));
   L.ccode = take(4 * (N1 + 1));
   L.pool_owner = take(4 * ((uint64_t)pool + 1));
@@ -89,9 +89,19 @@ __host__ __device__ inline SpLayout sp_layout(uint32_t n, uint64_t m2, uint32_t 
   return L;
 }
 
+// Shared-memory staging: the arrays every refinement step touches (elem,
+// pos, in_level, the list of non-singleton cells and the start / active /
+// touched-cell bitmaps with their summaries) live in the warp's
+// shared-memory region when they fit.
+__host__ __device__ inline uint64_t sp_smem_bytes(uint32_t n) {
+  const uint64_t nw = (n + 63) / 64 + 1, nsw = (nw + 63) / 64 + 1;
+  const uint64_t a = ((uint64_t)n + 2) * 4u;
+  return 4 * ((a + 15) & ~15ull) + 3 * 8 * (nw + nsw);
+}
+
 struct SpWarp {
   uint32_t *elem, *pos, *inlev, *cnt, *T, *Tc, *cellcnt, *off, *fill, *G, *tmp, *lst1, *lst2;
-  uint32_t *seq, *fseq, *bseq, *flabel, *blabel, *dsu, *hist, *pre, *fpos, *bpos;
+  uint32_t *seq, *fseq, *bseq, *flabel, *blabel, *dsu, *hist, *pre, *fpos, *bpos, *nsl;
   int32_t *fcode, *ccode, *pool_owner;
   uint64_t *stb, *sts, *act, *acts, *tcb, *tcbs;
   uint32_t *fcert, *bcert, *ccert, *reps;
@@ -181,6 +191,11 @@ __device__ __forceinline__ uint32_t sp_cell_end(const SpWarp& W, uint32_t c) {
 __device__ __forceinline__ uint32_t sp_cell_of(const SpWarp& W, uint32_t p) {
   return bm_prev(W.stb, W.sts, p);
 }
+__device__ __forceinline__ uint32_t lanemask_lt() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
 
 // ---------------------------------------------------------------------------
 // Rearranging a split cell.  `seg` holds the k touched vertices of the cell
@@ -234,6 +249,44 @@ __device__ __noinline__ void sp_regroup(const uint32_t* seg, uint32_t k, uint32_
   __syncwarp();
 }
 
+// Ascending start positions of the non-singleton cells into W.nsl; returns
+// their number.  Each lane scans a contiguous range of start-bitmap words and
+// an exclusive warp scan places its cells.
+__device__ __noinline__ uint32_t sp_list_nonsingleton() {
+  SpWarp& W = sp_w();
+  const uint32_t lane = lane_id();
+  const uint32_t n = W.n, nwr = (n + 63) / 64;
+  const uint32_t per = (nwr + 31) / 32;
+  const uint32_t w0 = min(nwr, lane * per), w1 = min(nwr, w0 + per);
+  const uint64_t lastp = bit64((n - 1) & 63);
+  uint32_t cnt = 0;
+  for (uint32_t w = w0; w < w1; ++w) {
+    const uint64_t b = W.stb[w];
+    uint64_t succ = (b >> 1) | ((w + 1 < nwr ? W.stb[w + 1] : 0ull) << 63);
+    if (w == nwr - 1) succ |= lastp;
+    cnt += popc64(b & ~succ);
+  }
+  uint32_t off = cnt;
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(GCL_FULL, off, o);
+    if (lane >= (uint32_t)o) off += y;
+  }
+  const uint32_t total = __shfl_sync(GCL_FULL, off, 31);
+  off -= cnt;
+  for (uint32_t w = w0; w < w1; ++w) {
+    const uint64_t b = W.stb[w];
+    uint64_t succ = (b >> 1) | ((w + 1 < nwr ? W.stb[w + 1] : 0ull) << 63);
+    if (w == nwr - 1) succ |= lastp;
+    uint64_t ns = b & ~succ;
+    while (ns) {
+      W.nsl[off++] = w * 64 + ctz64(ns);
+      ns &= ns - 1;
+    }
+  }
+  __syncwarp();
+  return total;
+}
+
 // ---------------------------------------------------------------------------
 // Partition_s_refinement (partition_refinement.cpp:150-485).  The active
 // bitmap holds the initially active cells; returns the code (-1 on a failed
@@ -274,6 +327,83 @@ __device__ __noinline__ int sp_refine(uint32_t level) {
     const uint32_t len = e - s;
     lc = mash(lc, s + e - 1);
     if (len > 1) lc = mash(lc, len);
+
+    // Singleton splitter {w} with at most 32 neighbours: lane i holds
+    // neighbour i; lanes whose neighbours share a (non-singleton) cell are
+    // grouped with match_any; a cell that is not all neighbours splits into
+    // [neighbours, non-neighbours]: its misplaced neighbours swap with the
+    // non-neighbours inside its first k positions, then the split cells are
+    // folded in position order (:296-309, 399-435).
+    if (len == 1 && W.rp[W.elem[s] + 1] - W.rp[W.elem[s]] <= 32) {
+      const uint32_t w = W.elem[s];
+      const int32_t b = W.rp[w], d = W.rp[w + 1] - b;
+      const bool have = (int32_t)lane < d;
+      uint32_t u = 0, p = 0, c = kNone, L = 0;
+      if (have) {
+        u = (uint32_t)W.col[b + (int32_t)lane];
+        p = W.pos[u];
+        c = sp_cell_of(W, p);
+        L = sp_cell_end(W, c) - c;
+      }
+      const bool act_l = have && L > 1;
+      const uint32_t grp = __match_any_sync(GCL_FULL, act_l ? c : kNone);
+      const uint32_t k = (uint32_t)__popc(grp);
+      const bool spl_l = act_l && k < L;
+      uint32_t h = 0, x = 0;
+      bool mv = false;
+      if (spl_l) {
+        const bool in = p < c + k;
+        const uint32_t inner = __reduce_or_sync(grp, in ? (1u << (p - c)) : 0u);
+        const uint32_t outs = __ballot_sync(grp, !in);
+        if (!in) {
+          const uint32_t j = (uint32_t)__popc(outs & lanemask_lt());
+          const uint32_t holes = ~inner & (k >= 32 ? 0xffffffffu : ((1u << k) - 1u));
+          h = c + (uint32_t)__fns(holes, 0, (int)j + 1);
+          x = W.elem[h];
+          mv = true;
+        }
+      }
+      __syncwarp();
+      if (mv) {
+        W.elem[h] = u;
+        W.pos[u] = h;
+        W.elem[p] = x;
+        W.pos[x] = p;
+      }
+      __syncwarp();
+      uint32_t leaders = __ballot_sync(GCL_FULL, spl_l && lane == (uint32_t)(__ffs(grp) - 1));
+      while (leaders) {
+        const bool mine = (leaders >> lane) & 1u;
+        const uint32_t cmin = __reduce_min_sync(GCL_FULL, mine ? c : kNone);
+        const uint32_t src = (uint32_t)__ffs(__ballot_sync(GCL_FULL, mine && c == cmin)) - 1;
+        const uint32_t kk = __shfl_sync(GCL_FULL, k, (int)src), LL = __shfl_sync(GCL_FULL, L, (int)src);
+        leaders &= ~(1u << src);
+        const uint32_t pp = cmin + kk;
+        lc = mash(lc, pp - 1);  // cell.first + neighbors_size - 1
+        const bool was = bm_test(W.act, cmin);
+        __syncwarp();
+        if (lane == 0) {
+          W.inlev[pp] = W.inlev[cmin];
+          W.inlev[cmin] = lvl1;
+          bm_set1(W.stb, W.sts, pp);
+          W.ncells += 1;
+          const uint32_t nb = kk, nn = LL - kk;
+          if (was || nb >= nn) {
+            bm_set1(W.act, W.acts, pp);
+            W.nact += 1;
+            if (nn == 1) hint = pp;
+          } else {
+            bm_set1(W.act, W.acts, cmin);
+            W.nact += 1;
+            if (nb == 1) hint = cmin;
+          }
+          W.hint = hint;
+        }
+        __syncwarp();
+        hint = W.hint;
+      }
+      continue;
+    }
 
     // count neighbours in the splitter, record touched vertices and cells
     // (cells that are singletons never split and are skipped, :257-259)
@@ -366,19 +496,21 @@ __device__ __noinline__ int sp_refine(uint32_t level) {
       }
     } else {
       // every non-singleton cell in order: common count, or fragments in
-      // ascending count with the untouched (count 0) fragment first
-      for (uint32_t w = 0; w < nw; ++w) {
-        uint64_t sb = W.stb[w];
-        while (sb) {
-          const uint32_t c = w * 64 + ctz64(sb);
-          sb &= sb - 1;
-          if (c >= n) break;
-          const uint32_t ce = sp_cell_end(W, c), L = ce - c;
-          if (L == 1) continue;
-          if (!bm_test(W.tcb, c)) {
+      // ascending count with the untouched (count 0) fragment first.  Cells
+      // are taken 32 at a time; untouched ones only hash their start.
+      const uint32_t K = sp_list_nonsingleton();
+      for (uint32_t i0 = 0; i0 < K; i0 += 32) {
+        const uint32_t il = i0 + lane;
+        const uint32_t cl = il < K ? W.nsl[il] : 0u;
+        const uint32_t tmask = __ballot_sync(GCL_FULL, il < K && bm_test(W.tcb, cl));
+        const uint32_t cnt32 = min(32u, K - i0);
+        for (uint32_t jj = 0; jj < cnt32; ++jj) {
+          const uint32_t c = __shfl_sync(GCL_FULL, cl, (int)jj);
+          if (!((tmask >> jj) & 1u)) {
             lc = mash(lc, c);  // every member has count 0
             continue;
           }
+          const uint32_t ce = sp_cell_end(W, c), L = ce - c;
           const uint32_t k = W.cellcnt[c];
           const uint32_t* seg = W.G + W.off[c];
           uint32_t mn = 0xffffffffu, mx = 0;
@@ -1018,7 +1150,8 @@ struct SpResult {
 };
 
 __device__ __noinline__ SpResult sp_search(const BatchArgs& A, int g, uint8_t* slot,
-                                           const SpLayout& Lo, uint32_t pool, uint32_t cap) {
+                                           const SpLayout& Lo, uint32_t pool, uint32_t cap,
+                                           uint8_t* smem, uint64_t smem_bytes) {
   SpWarp& W = sp_w();
   const uint32_t lane = lane_id();
   const int64_t vo = A.voff[g];
@@ -1029,8 +1162,8 @@ __device__ __noinline__ SpResult sp_search(const BatchArgs& A, int g, uint8_t* s
   if (n == 0) return res;
   if (lane == 0) {
     // the n-sized u32 arrays
-    uint32_t* base[23];
-    for (int i = 0; i < 23; ++i) base[i] = (uint32_t*)(slot + Lo.u32n[i]);
+    uint32_t* base[24];
+    for (int i = 0; i < 24; ++i) base[i] = (uint32_t*)(slot + Lo.u32n[i]);
     W.elem = base[0];
     W.pos = base[1];
     W.inlev = base[2];
@@ -1054,6 +1187,7 @@ __device__ __noinline__ SpResult sp_search(const BatchArgs& A, int g, uint8_t* s
     W.pre = base[20];
     W.fpos = base[21];
     W.bpos = base[22];
+    W.nsl = base[23];
     W.fcode = (int32_t*)(slot + Lo.fcode);
     W.ccode = (int32_t*)(slot + Lo.ccode);
     W.pool_owner = (int32_t*)(slot + Lo.pool_owner);
@@ -1076,6 +1210,31 @@ __device__ __noinline__ SpResult sp_search(const BatchArgs& A, int g, uint8_t* s
     W.nsw = (W.nw + 63) / 64 + 1;
     W.stride = Lo.stride;
     W.npend = 0;
+    if (smem && sp_smem_bytes(n) <= smem_bytes) {
+      // stage the per-step arrays in this warp's shared memory
+      const uint64_t a = (((uint64_t)n + 2) * 4u + 15) & ~15ull;
+      const uint32_t nw2 = W.nw, nsw2 = W.nsw;
+      uint8_t* q = smem;
+      W.elem = (uint32_t*)q;
+      q += a;
+      W.pos = (uint32_t*)q;
+      q += a;
+      W.inlev = (uint32_t*)q;
+      q += a;
+      W.nsl = (uint32_t*)q;
+      q += a;
+      W.stb = (uint64_t*)q;
+      q += 8 * nw2;
+      W.sts = (uint64_t*)q;
+      q += 8 * nsw2;
+      W.act = (uint64_t*)q;
+      q += 8 * nw2;
+      W.acts = (uint64_t*)q;
+      q += 8 * nsw2;
+      W.tcb = (uint64_t*)q;
+      q += 8 * nw2;
+      W.tcbs = (uint64_t*)q;
+    }
     W.pool_top = 0;
     W.pool_cap = pool;
     W.aut_cap = cap;

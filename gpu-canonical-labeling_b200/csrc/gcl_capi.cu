@@ -27,15 +27,24 @@ namespace gcl {
 
 constexpr uint32_t kW64AutCap = 256;  // ring slots per warp in the fast pass
 
+// Size buckets of the sparse kernel (n > 64): each bucket is one launch whose
+// warps stage their per-step arrays in shared memory sized for the bucket's
+// largest graph (the last bucket uses device memory only).
+constexpr int kSpBuckets = 4;
+constexpr uint32_t kSpBucketHi[kSpBuckets] = {256, 1024, 4096, 0xffffffffu};
+__host__ __device__ inline int sp_bucket(int64_t n) {
+  return n <= 256 ? 0 : n <= 1024 ? 1 : n <= 4096 ? 2 : 3;
+}
+
 // Device-side lists of deferred graphs.
 struct Deferred {
   int overflow_count;  // n <= 64 graphs that outgrew the ring
-  int large_count;     // n > 64 graphs
   int next_overflow;
-  int next_large;
   int next;            // work counter of the first pass
   int sp_fail_count;   // n > 64 graphs that outgrew pool or ring
   int next_sp_fail;
+  int large_count[kSpBuckets];  // n > 64 graphs per size bucket
+  int next_large[kSpBuckets];
 };
 
 // Largest graphs first: a counting sort of the graph ids by descending n
@@ -67,16 +76,19 @@ __global__ void __launch_bounds__(kOrderThreads)
   }
 }
 
+constexpr int kSpSmemPerBlock = 200 * 1024;  // dynamic shared memory cap of one sparse block
 constexpr uint32_t kSpPool = 8;     // per-level orbit arrays in the first sparse pass
 constexpr uint32_t kSpAutCap = 64;  // ring entries in the first sparse pass
 
 __global__ void __launch_bounds__(kSpThreads)
     sp_batch_kernel(BatchArgs A, const int* list, const int* count, int* next, int* fail_list,
                     int* fail_count, uint32_t n_max, uint64_t m2_max, uint32_t pool, uint32_t cap,
-                    uint64_t slot_bytes) {
+                    uint64_t slot_bytes, uint64_t smem_per_warp) {
+  extern __shared__ __align__(16) uint8_t sp_dyn[];
   const int warp = (int)(threadIdx.x >> 5);
   const uint32_t lane = lane_id();
   uint8_t* slot = A.work + ((uint64_t)blockIdx.x * kSpWarps + (uint64_t)warp) * slot_bytes;
+  uint8_t* smem = smem_per_warp ? sp_dyn + (uint64_t)warp * smem_per_warp : nullptr;
   const SpLayout Lo = sp_layout(n_max, m2_max, pool, cap);
   const int total = *(volatile const int*)count;
   while (true) {
@@ -91,7 +103,7 @@ __global__ void __launch_bounds__(kSpThreads)
       if (lane == 0) A.status[g] = kTooLarge;
       continue;
     }
-    const SpResult r = sp_search(A, g, slot, Lo, pool, cap);
+    const SpResult r = sp_search(A, g, slot, Lo, pool, cap, smem, smem_per_warp);
     if (lane == 0) {
       A.status[g] = r.status;
       if (A.out_stats) {
@@ -122,7 +134,8 @@ __global__ void __launch_bounds__(kW64Threads, 8)
     if (n > kW64MaxN) {
       if (lane == 0) {
         A.status[g] = kTooLarge;
-        large_list[atomicAdd(&D->large_count, 1)] = g;
+        const int bk = sp_bucket(n);
+        large_list[(int64_t)bk * A.count + atomicAdd(&D->large_count[bk], 1)] = g;
       }
       continue;
     }
@@ -172,8 +185,7 @@ struct gcl_context {
   DevBuf work_big;
   uint32_t work_big_aut = 0;
   int big_slots = 0;
-  DevBuf sp_work, sp_work_big;
-  int sp_grid = 0;
+  DevBuf sp_work[kSpBuckets], sp_work_big;
   DevBuf deferred, overflow_list, large_list, sp_fail_list, order;
   // staging for host-pointer calls
   DevBuf voff, eoff, rowptr, col, color, ooff, dense, roff, rows, label, stats, status;
@@ -249,10 +261,9 @@ int gcl_create(int device, gcl_context** out) {
     c->w64_grid = c->sms * std::max(per_sm, 1);
     e = c->deferred.ensure(sizeof(Deferred));
   }
-  int sp_per_sm = 0;
   if (e == cudaSuccess)
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sp_per_sm, sp_batch_kernel, kSpThreads, 0);
-  if (e == cudaSuccess) c->sp_grid = c->sms * std::max(sp_per_sm, 1);
+    e = cudaFuncSetAttribute(sp_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             kSpSmemPerBlock);
   if (e != cudaSuccess) {
     if (c->stream) cudaStreamDestroy(c->stream);
     c->deferred.release();
@@ -267,7 +278,8 @@ int gcl_destroy(gcl_context* c) {
   if (!c) return GCL_ERR_ARG;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
-  DevBuf* bufs[] = {&c->work, &c->work_big, &c->sp_work, &c->sp_work_big, &c->deferred,
+  for (DevBuf& b : c->sp_work) b.release();
+  DevBuf* bufs[] = {&c->work, &c->work_big, &c->sp_work_big, &c->deferred,
                     &c->overflow_list, &c->large_list, &c->sp_fail_list, &c->order, &c->voff, &c->eoff, &c->rowptr, &c->col, &c->color,
                     &c->ooff, &c->dense, &c->roff, &c->rows, &c->label, &c->stats,
                     &c->status};
@@ -304,7 +316,7 @@ int gcl_canon_batch_device_async(gcl_context* c, int count, const int64_t* d_vof
   const uint64_t slots = (uint64_t)c->w64_grid * kW64Warps;
   GCL_TRY(c->work.ensure(slots * slot_bytes));
   GCL_TRY(c->overflow_list.ensure((size_t)count * sizeof(int)));
-  GCL_TRY(c->large_list.ensure((size_t)count * sizeof(int)));
+  GCL_TRY(c->large_list.ensure((size_t)count * kSpBuckets * sizeof(int)));
   GCL_TRY(c->order.ensure((size_t)count * sizeof(int)));
   GCL_TRY(cudaMemsetAsync(c->deferred.p, 0, sizeof(Deferred), c->stream));
   order_by_size_kernel<<<1, kOrderThreads, 0, c->stream>>>(count, d_voff, (int*)c->order.p);
@@ -354,34 +366,49 @@ int gcl_canon_batch_device_async(gcl_context* c, int count, const int64_t* d_vof
   }
 
   if (max_n > kW64MaxN) {
-    // graphs with n > 64: the sparse kernel over the deferred list
-    const uint32_t nmax = (uint32_t)max_n;
+    // graphs with n > 64: one sparse pass per size bucket, then a rerun of
+    // the graphs that outgrew the first passes' orbit pool or ring
     const uint64_t m2max = (uint64_t)std::max<int64_t>(max_m2, 1);
     const uint32_t cap1 = std::min<uint32_t>(maut, kSpAutCap);
-    const uint64_t sb1 = sp_layout(nmax, m2max, kSpPool, cap1).bytes;
     const uint64_t budget = workspace_budget();
-    int64_t slots = std::min<int64_t>((int64_t)c->sp_grid * kSpWarps,
-                                      std::max<int64_t>(kSpWarps, (int64_t)(budget / sb1)));
-    slots = std::min<int64_t>(slots, ((int64_t)count + kSpWarps - 1) / kSpWarps * kSpWarps);
-    slots = std::max<int64_t>(kSpWarps, slots / kSpWarps * kSpWarps);
-    GCL_TRY(c->sp_work.ensure((size_t)(slots * sb1)));
     GCL_TRY(c->sp_fail_list.ensure((size_t)count * sizeof(int)));
-    BatchArgs Sa = A;
-    Sa.work = (uint8_t*)c->sp_work.p;
-    sp_batch_kernel<<<(int)(slots / kSpWarps), kSpThreads, 0, c->stream>>>(
-        Sa, (const int*)c->large_list.p, &D->large_count, &D->next_large,
-        (int*)c->sp_fail_list.p, &D->sp_fail_count, nmax, m2max, kSpPool, cap1, sb1);
-    GCL_TRY(cudaGetLastError());
+    for (int bk = 0; bk < kSpBuckets; ++bk) {
+      const uint32_t lo = bk == 0 ? (uint32_t)kW64MaxN + 1 : kSpBucketHi[bk - 1] + 1;
+      if ((uint32_t)max_n < lo) break;
+      const uint32_t nmax = std::min<uint32_t>((uint32_t)max_n, kSpBucketHi[bk]);
+      const uint64_t sb1 = sp_layout(nmax, m2max, kSpPool, cap1).bytes;
+      uint64_t smw = sp_smem_bytes(nmax);
+      if (smw * kSpWarps > (uint64_t)kSpSmemPerBlock) smw = 0;  // device memory only
+      int per_sm = 0;
+      GCL_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sp_batch_kernel, kSpThreads,
+                                                            (size_t)(smw * kSpWarps)));
+      int64_t slots = std::min<int64_t>((int64_t)c->sms * std::max(per_sm, 1) * kSpWarps,
+                                        std::max<int64_t>(kSpWarps, (int64_t)(budget / sb1)));
+      slots = std::min<int64_t>(slots, ((int64_t)count + kSpWarps - 1) / kSpWarps * kSpWarps);
+      slots = std::max<int64_t>(kSpWarps, slots / kSpWarps * kSpWarps);
+      DevBuf& wb = c->sp_work[bk];
+      GCL_TRY(wb.ensure((size_t)(slots * sb1)));
+      BatchArgs Sa = A;
+      Sa.work = (uint8_t*)wb.p;
+      sp_batch_kernel<<<(int)(slots / kSpWarps), kSpThreads, (size_t)(smw * kSpWarps),
+                        c->stream>>>(Sa, (const int*)c->large_list.p + (int64_t)bk * count,
+                                     &D->large_count[bk], &D->next_large[bk],
+                                     (int*)c->sp_fail_list.p, &D->sp_fail_count, nmax, m2max,
+                                     kSpPool, cap1, sb1, smw);
+      GCL_TRY(cudaGetLastError());
+    }
     // rerun with a representative array per level and the full ring
+    const uint32_t nmax = (uint32_t)max_n;
     const uint32_t pool2 = nmax + 2;
     const uint64_t sb2 = sp_layout(nmax, m2max, pool2, maut).bytes;
     int64_t slots2 = std::max<int64_t>(1, std::min<int64_t>((int64_t)c->sms,
                                                           (int64_t)(budget / (sb2 * kSpWarps))));
     GCL_TRY(c->sp_work_big.ensure((size_t)(slots2 * kSpWarps * sb2)));
-    Sa.work = (uint8_t*)c->sp_work_big.p;
+    BatchArgs Sb = A;
+    Sb.work = (uint8_t*)c->sp_work_big.p;
     sp_batch_kernel<<<(int)slots2, kSpThreads, 0, c->stream>>>(
-        Sa, (const int*)c->sp_fail_list.p, &D->sp_fail_count, &D->next_sp_fail, nullptr, nullptr,
-        nmax, m2max, pool2, maut, sb2);
+        Sb, (const int*)c->sp_fail_list.p, &D->sp_fail_count, &D->next_sp_fail, nullptr, nullptr,
+        nmax, m2max, pool2, maut, sb2, 0);
     GCL_TRY(cudaGetLastError());
   }
   return GCL_OK;

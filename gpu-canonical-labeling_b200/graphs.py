@@ -176,11 +176,14 @@ def move_one_edge(g: Graph, rng: np.random.Generator) -> Graph:
 
 def random_regular(n: int, d: int, rng: np.random.Generator,
                    max_tries: int = 10000) -> Graph:
-    """Configuration model, rejected until simple."""
+    """Random simple d-regular graph: configuration model rejected until
+    simple, falling back (when the whole-pairing acceptance rate is tiny,
+    e.g. d = 6) to pairing stubs one edge at a time among the pairs that keep
+    the graph simple, restarting on a dead end (Steger-Wormald)."""
     if (n * d) % 2:
         raise ValueError("n*d must be even")
     stubs = np.repeat(np.arange(n), d)
-    for _ in range(max_tries):
+    for _ in range(min(max_tries, 200)):
         p = rng.permutation(stubs).reshape(-1, 2)
         if np.any(p[:, 0] == p[:, 1]):
             continue
@@ -189,7 +192,26 @@ def random_regular(n: int, d: int, rng: np.random.Generator,
         if len(np.unique(key)) != len(key):
             continue
         return from_edges(n, a)
-    raise RuntimeError("configuration model did not produce a simple graph")
+    for _ in range(max_tries):
+        free = list(stubs)
+        edges = set()
+        ok = True
+        while free:
+            for _attempt in range(100):
+                i, j = rng.choice(len(free), 2, replace=False)
+                u, v = free[i], free[j]
+                if u != v and (min(u, v), max(u, v)) not in edges:
+                    break
+            else:
+                ok = False
+                break
+            edges.add((min(u, v), max(u, v)))
+            for k in sorted((i, j), reverse=True):
+                free[k] = free[-1]
+                free.pop()
+        if ok:
+            return from_edges(n, np.array(sorted(edges)))
+    raise RuntimeError("no simple regular graph found")
 
 
 def torus(k1: int, k2: Optional[int] = None) -> Graph:
@@ -285,7 +307,7 @@ def mixed_batch(count: int = 2000, seed: int = 4000, n_lo: int = 64,
                 n_hi: int = 4096) -> List[Graph]:
     """Mixed-size workload: n log-uniform in [n_lo, n_hi], four families in
     equal shares (ER mean degree 8, random d-regular d in {3,4,6}, toroidal
-    grids, disjoint unions of identical random regular components)."""
+    grids, disjoint unions of 2-4 copies of one random regular component)."""
     rng = np.random.default_rng(seed)
     out: List[Graph] = []
     for i in range(count):
@@ -303,10 +325,14 @@ def mixed_batch(count: int = 2000, seed: int = 4000, n_lo: int = 64,
             k2 = max(3, int(round(n / k1)))
             out.append(torus(k1, k2))
         else:
-            c = int(rng.choice([8, 10, 12, 16]))
-            d = 3
+            # a few copies of one larger component: the reference's search
+            # (first-leaf and per-level orbit pruning only) grows exponentially
+            # in the number of identical components
+            k = int(rng.choice([2, 3, 4]))
+            c = max(8, n // k)
+            d = 3 if c % 2 == 0 else 4
             comp = random_regular(c, d, rng)
-            out.append(disjoint_union(comp, max(1, n // c)))
+            out.append(disjoint_union(comp, k))
     return out
 
 
