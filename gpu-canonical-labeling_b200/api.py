@@ -37,8 +37,11 @@ ERRORS = {
 EXPORTS = [
     "gcl_status_string", "gcl_version", "gcl_create", "gcl_destroy", "gcl_stream",
     "gcl_canon_one", "gcl_canon_batch", "gcl_canon_batch_device_async", "gcl_sync", "gcl_iso",
-    "gcl_canon_batch_noalloc",
+    "gcl_canon_batch_noalloc", "gcl_set_option", "gcl_canon_wide_device_async",
 ]
+
+GCL_OPT_WIDE_MIN_N = 1
+GCL_MAX_N = 65536
 
 
 class GclError(RuntimeError):
@@ -78,8 +81,12 @@ def load_library(path: str = LIB_PATH):
                             ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     lib.gcl_canon_batch_noalloc.argtypes = [_P, ctypes.c_int, _P, _P, _P, _P, _P, ctypes.c_int,
                                             ctypes.c_int, _P, _P, _P, _P, _P]
+    lib.gcl_set_option.argtypes = [_P, ctypes.c_int, ctypes.c_int64]
+    lib.gcl_canon_wide_device_async.argtypes = [_P, _P, _P, _P, ctypes.c_int, ctypes.c_int64,
+                                                ctypes.c_int, _P, _P, _P, _P, _P]
     for name in ("gcl_create", "gcl_destroy", "gcl_sync", "gcl_canon_one", "gcl_canon_batch",
-                 "gcl_canon_batch_device_async", "gcl_iso", "gcl_canon_batch_noalloc"):
+                 "gcl_canon_batch_device_async", "gcl_iso", "gcl_canon_batch_noalloc",
+                 "gcl_set_option", "gcl_canon_wide_device_async"):
         getattr(lib, name).restype = ctypes.c_int
     _lib = lib
     return lib
@@ -97,12 +104,20 @@ def _ptr(a: Optional[np.ndarray]):
 class Context:
     """A device context (workspace, stream, staging buffers) on one GPU."""
 
-    def __init__(self, device: int = 0):
+    def __init__(self, device: int = 0, wide_min_n: Optional[int] = None):
         self.lib = load_library()
         h = _P()
         _check(self.lib.gcl_create(device, ctypes.byref(h)), "gcl_create")
         self.handle = h
         self.device = device
+        if wide_min_n is not None:
+            self.set_wide_min_n(wide_min_n)
+
+    def set_wide_min_n(self, n: int):
+        """Single graphs with at least n vertices use the wide search
+        (GCL_OPT_WIDE_MIN_N); GCL_MAX_N + 1 keeps the sequential traversal."""
+        _check(self.lib.gcl_set_option(self.handle, GCL_OPT_WIDE_MIN_N, int(n)),
+               "gcl_set_option")
 
     def close(self):
         if getattr(self, "handle", None):

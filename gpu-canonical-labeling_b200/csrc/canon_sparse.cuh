@@ -46,7 +46,7 @@ struct SpTc {
 // Byte layout of one slot for graphs with at most n vertices and m2 CSR
 // entries, `pool` per-level representative arrays and `cap` ring slots.
 struct SpLayout {
-  uint64_t u32n[24];  // offsets of the n-sized u32 arrays
+  uint64_t u32n[25];  // offsets of the n-sized u32 arrays
   uint64_t fcode, ccode, pool_owner;
   uint64_t stb, sts, act, acts, tcb, tcbs;
   uint64_t fcert, bcert, ccert;
@@ -67,7 +67,7 @@ __host__ __device__ inline SpLayout sp_layout(uint32_t n, uint64_t m2, uint32_t 
   };
   const uint64_t N1 = (uint64_t)n + 2;
   L.stride = (uint32_t)N1;
-  for (int i = 0; i < 24; ++i) L.u32n[i] = take(4 * N1);
+  for (int i = 0; i < 25; ++i) L.u32n[i] = take(4 * N1);
   L.fcode = take(4 * (N1 + 1));
   L.ccode = take(4 * (N1 + 1));
   L.pool_owner = take(4 * ((uint64_t)pool + 1));
@@ -102,7 +102,7 @@ __host__ __device__ inline uint64_t sp_smem_bytes(uint32_t n) {
 struct SpWarp {
   uint32_t *elem, *pos, *inlev, *cnt, *T, *Tc, *cellcnt, *off, *fill, *G, *tmp, *lst1, *lst2;
   uint32_t *seq, *fseq, *bseq, *flabel, *blabel, *dsu, *hist, *pre, *fpos, *bpos, *nsl;
-  int32_t *fcode, *ccode, *pool_owner;
+  int32_t *fcode, *ccode, *pool_owner, *pathcode;
   uint64_t *stb, *sts, *act, *acts, *tcb, *tcbs;
   uint32_t *fcert, *bcert, *ccert, *reps;
   SpTc* tc;
@@ -117,6 +117,15 @@ struct SpWarp {
 };
 
 __shared__ SpWarp g_sp[kSpWarps];
+
+// Loads of data that warps on other SMs write during the same launch (the
+// shared automorphism store and best leaf of the many-warp search) go
+// through L2 only; everything else uses ordinary loads.
+template <bool kCg, typename T>
+__device__ __forceinline__ T ldx(const T* p) {
+  if constexpr (kCg) return __ldcg(p);
+  else return *p;
+}
 __device__ __forceinline__ SpWarp& sp_w() { return g_sp[threadIdx.x >> 5]; }
 
 // ---- bitmaps with a summary word per 64 words ----------------------------
@@ -813,6 +822,7 @@ __device__ __noinline__ void sp_leaf_cert(uint32_t* cert) {
 // with a stored leaf (vertex order label[], rows in cert2) in canonical
 // row order.  upper: compare_adj_upper (entries right of the diagonal,
 // sequential.cpp:114-124); otherwise full-row equality.  Returns -1/0/+1.
+template <bool kCg = false>
 __device__ __noinline__ int sp_cmp_leaf(const uint32_t* cur, const uint32_t* label,
                                         const uint32_t* cert2, bool upper) {
   SpWarp& W = sp_w();
@@ -822,11 +832,11 @@ __device__ __noinline__ int sp_cmp_leaf(const uint32_t* cur, const uint32_t* lab
     const uint32_t i = i0 + lane;
     int r = 0;
     if (i < n) {
-      const uint32_t va = W.elem[i], vb = label[i];
+      const uint32_t va = W.elem[i], vb = ldx<kCg>(label + i);
       int32_t a = W.rp[va], ae = W.rp[va + 1], b = W.rp[vb], be = W.rp[vb + 1];
       if (upper) {
         while (a < ae && cur[a] <= i) ++a;
-        while (b < be && cert2[b] <= i) ++b;
+        while (b < be && ldx<kCg>(cert2 + b) <= i) ++b;
       }
       while (true) {
         const bool ea = a >= ae, eb = b >= be;
@@ -839,7 +849,7 @@ __device__ __noinline__ int sp_cmp_leaf(const uint32_t* cur, const uint32_t* lab
           r = 1;
           break;
         }
-        const uint32_t x = cur[a], y = cert2[b];
+        const uint32_t x = cur[a], y = ldx<kCg>(cert2 + b);
         if (x != y) {
           r = x < y ? 1 : -1;
           break;
@@ -926,7 +936,36 @@ __device__ __forceinline__ uint32_t sp_find(volatile uint32_t* d, uint32_t x, ui
   return x;
 }
 
+// Merge the cycles of permutation pm into the min-root union-find W.dsu:
+// hook the larger root under the smaller one, then shortcut every vertex to
+// its root, until a round changes nothing (compute_orbits_fast's DSU,
+// perm_group.cpp:60-116).  False if the rounds do not converge.
+template <bool kCg>
+__device__ __noinline__ bool sp_dsu_apply(const uint16_t* pm, uint32_t n) {
+  SpWarp& W = sp_w();
+  const uint32_t lane = lane_id();
+  volatile uint32_t* dsu = W.dsu;
+  for (uint32_t round = 0;; ++round) {
+    if (round > n + 1) return false;
+    bool changed = false;
+    for (uint32_t v = lane; v < n; v += 32) {
+      const uint32_t img = ldx<kCg>(pm + v);
+      if (img == v) continue;
+      const uint32_t a = sp_find(dsu, v, n), b = sp_find(dsu, img, n);
+      if (a != b) {
+        atomicMin((uint32_t*)&dsu[max(a, b)], min(a, b));
+        changed = true;
+      }
+    }
+    __syncwarp();
+    for (uint32_t v = lane; v < n; v += 32) atomicMin((uint32_t*)&dsu[v], sp_find(dsu, v, n));
+    __syncwarp();
+    if (!__any_sync(GCL_FULL, changed)) return true;
+  }
+}
+
 // subgroup_fixing_sequence + compute_orbits_fast (perm_group.cpp:5-116)
+template <bool kCg = false>
 __device__ __noinline__ bool sp_orbits(int idx, int num_aut, uint32_t seqlen) {
   SpWarp& W = sp_w();
   const uint32_t lane = lane_id();
@@ -950,27 +989,11 @@ __device__ __noinline__ bool sp_orbits(int idx, int num_aut, uint32_t seqlen) {
     bool bad = false;
     for (uint32_t j = lane; j < seqlen; j += 32) {
       const uint32_t sv = W.seq[j];
-      if (pm[sv] != sv) bad = true;
+      if (ldx<kCg>(pm + sv) != sv) bad = true;
     }
     if (__any_sync(GCL_FULL, bad)) continue;
     any = true;
-    for (uint32_t round = 0;; ++round) {
-      if (round > n + 1) return false;
-      bool changed = false;
-      for (uint32_t v = lane; v < n; v += 32) {
-        const uint32_t img = pm[v];
-        if (img == v) continue;
-        const uint32_t a = sp_find(dsu, v, n), b = sp_find(dsu, img, n);
-        if (a != b) {
-          atomicMin((uint32_t*)&dsu[max(a, b)], min(a, b));
-          changed = true;
-        }
-      }
-      __syncwarp();
-      for (uint32_t v = lane; v < n; v += 32) atomicMin((uint32_t*)&dsu[v], sp_find(dsu, v, n));
-      __syncwarp();
-      if (!__any_sync(GCL_FULL, changed)) break;
-    }
+    if (!sp_dsu_apply<kCg>(pm, n)) return false;
   }
   if (!any) return true;
   if (t.rslot < 0) {
@@ -1149,6 +1172,96 @@ struct SpResult {
   int64_t nodes;
 };
 
+// Point the warp's arrays into its slot (and its shared-memory region when
+// the per-step arrays fit there).  Lane 0 writes; the caller syncs the warp.
+__device__ __noinline__ void sp_bind(uint8_t* slot, const SpLayout& Lo, uint32_t n,
+                                     const int32_t* rp, const int32_t* col, uint8_t* smem,
+                                     uint64_t smem_bytes, uint32_t pool, uint32_t cap,
+                                     uint32_t max_aut) {
+  SpWarp& W = sp_w();
+  if (lane_id() != 0) return;
+  // the n-sized u32 arrays
+  uint32_t* base[25];
+  for (int i = 0; i < 25; ++i) base[i] = (uint32_t*)(slot + Lo.u32n[i]);
+  W.elem = base[0];
+  W.pos = base[1];
+  W.inlev = base[2];
+  W.cnt = base[3];
+  W.T = base[4];
+  W.Tc = base[5];
+  W.cellcnt = base[6];
+  W.off = base[7];
+  W.fill = base[8];
+  W.G = base[9];
+  W.tmp = base[10];
+  W.lst1 = base[11];
+  W.lst2 = base[12];
+  W.seq = base[13];
+  W.fseq = base[14];
+  W.bseq = base[15];
+  W.flabel = base[16];
+  W.blabel = base[17];
+  W.dsu = base[18];
+  W.hist = base[19];
+  W.pre = base[20];
+  W.fpos = base[21];
+  W.bpos = base[22];
+  W.nsl = base[23];
+  W.pathcode = (int32_t*)base[24];
+  W.fcode = (int32_t*)(slot + Lo.fcode);
+  W.ccode = (int32_t*)(slot + Lo.ccode);
+  W.pool_owner = (int32_t*)(slot + Lo.pool_owner);
+  W.stb = (uint64_t*)(slot + Lo.stb);
+  W.sts = (uint64_t*)(slot + Lo.sts);
+  W.act = (uint64_t*)(slot + Lo.act);
+  W.acts = (uint64_t*)(slot + Lo.acts);
+  W.tcb = (uint64_t*)(slot + Lo.tcb);
+  W.tcbs = (uint64_t*)(slot + Lo.tcbs);
+  W.fcert = (uint32_t*)(slot + Lo.fcert);
+  W.bcert = (uint32_t*)(slot + Lo.bcert);
+  W.ccert = (uint32_t*)(slot + Lo.ccert);
+  W.tc = (SpTc*)(slot + Lo.tc);
+  W.reps = (uint32_t*)(slot + Lo.reps);
+  W.auts = (uint16_t*)(slot + Lo.auts);
+  W.rp = rp;
+  W.col = col;
+  W.n = n;
+  W.nw = (n + 63) / 64 + 1;
+  W.nsw = (W.nw + 63) / 64 + 1;
+  W.stride = Lo.stride;
+  W.npend = 0;
+  if (smem && sp_smem_bytes(n) <= smem_bytes) {
+    // stage the per-step arrays in this warp's shared memory
+    const uint64_t a = (((uint64_t)n + 2) * 4u + 15) & ~15ull;
+    const uint32_t nw2 = W.nw, nsw2 = W.nsw;
+    uint8_t* q = smem;
+    W.elem = (uint32_t*)q;
+    q += a;
+    W.pos = (uint32_t*)q;
+    q += a;
+    W.inlev = (uint32_t*)q;
+    q += a;
+    W.nsl = (uint32_t*)q;
+    q += a;
+    W.stb = (uint64_t*)q;
+    q += 8 * nw2;
+    W.sts = (uint64_t*)q;
+    q += 8 * nsw2;
+    W.act = (uint64_t*)q;
+    q += 8 * nw2;
+    W.acts = (uint64_t*)q;
+    q += 8 * nsw2;
+    W.tcb = (uint64_t*)q;
+    q += 8 * nw2;
+    W.tcbs = (uint64_t*)q;
+  }
+  W.pool_top = 0;
+  W.pool_cap = pool;
+  W.aut_cap = cap;
+  W.max_aut = max_aut;
+  W.ntouched = 0;
+}
+
 __device__ __noinline__ SpResult sp_search(const BatchArgs& A, int g, uint8_t* slot,
                                            const SpLayout& Lo, uint32_t pool, uint32_t cap,
                                            uint8_t* smem, uint64_t smem_bytes) {
@@ -1160,87 +1273,7 @@ __device__ __noinline__ SpResult sp_search(const BatchArgs& A, int g, uint8_t* s
   const int64_t m = A.eoff[g + 1] - eo;
   SpResult res{kOk, 0, 1};
   if (n == 0) return res;
-  if (lane == 0) {
-    // the n-sized u32 arrays
-    uint32_t* base[24];
-    for (int i = 0; i < 24; ++i) base[i] = (uint32_t*)(slot + Lo.u32n[i]);
-    W.elem = base[0];
-    W.pos = base[1];
-    W.inlev = base[2];
-    W.cnt = base[3];
-    W.T = base[4];
-    W.Tc = base[5];
-    W.cellcnt = base[6];
-    W.off = base[7];
-    W.fill = base[8];
-    W.G = base[9];
-    W.tmp = base[10];
-    W.lst1 = base[11];
-    W.lst2 = base[12];
-    W.seq = base[13];
-    W.fseq = base[14];
-    W.bseq = base[15];
-    W.flabel = base[16];
-    W.blabel = base[17];
-    W.dsu = base[18];
-    W.hist = base[19];
-    W.pre = base[20];
-    W.fpos = base[21];
-    W.bpos = base[22];
-    W.nsl = base[23];
-    W.fcode = (int32_t*)(slot + Lo.fcode);
-    W.ccode = (int32_t*)(slot + Lo.ccode);
-    W.pool_owner = (int32_t*)(slot + Lo.pool_owner);
-    W.stb = (uint64_t*)(slot + Lo.stb);
-    W.sts = (uint64_t*)(slot + Lo.sts);
-    W.act = (uint64_t*)(slot + Lo.act);
-    W.acts = (uint64_t*)(slot + Lo.acts);
-    W.tcb = (uint64_t*)(slot + Lo.tcb);
-    W.tcbs = (uint64_t*)(slot + Lo.tcbs);
-    W.fcert = (uint32_t*)(slot + Lo.fcert);
-    W.bcert = (uint32_t*)(slot + Lo.bcert);
-    W.ccert = (uint32_t*)(slot + Lo.ccert);
-    W.tc = (SpTc*)(slot + Lo.tc);
-    W.reps = (uint32_t*)(slot + Lo.reps);
-    W.auts = (uint16_t*)(slot + Lo.auts);
-    W.rp = A.rowptr + vo + g;
-    W.col = A.col + eo;
-    W.n = n;
-    W.nw = (n + 63) / 64 + 1;
-    W.nsw = (W.nw + 63) / 64 + 1;
-    W.stride = Lo.stride;
-    W.npend = 0;
-    if (smem && sp_smem_bytes(n) <= smem_bytes) {
-      // stage the per-step arrays in this warp's shared memory
-      const uint64_t a = (((uint64_t)n + 2) * 4u + 15) & ~15ull;
-      const uint32_t nw2 = W.nw, nsw2 = W.nsw;
-      uint8_t* q = smem;
-      W.elem = (uint32_t*)q;
-      q += a;
-      W.pos = (uint32_t*)q;
-      q += a;
-      W.inlev = (uint32_t*)q;
-      q += a;
-      W.nsl = (uint32_t*)q;
-      q += a;
-      W.stb = (uint64_t*)q;
-      q += 8 * nw2;
-      W.sts = (uint64_t*)q;
-      q += 8 * nsw2;
-      W.act = (uint64_t*)q;
-      q += 8 * nw2;
-      W.acts = (uint64_t*)q;
-      q += 8 * nsw2;
-      W.tcb = (uint64_t*)q;
-      q += 8 * nw2;
-      W.tcbs = (uint64_t*)q;
-    }
-    W.pool_top = 0;
-    W.pool_cap = pool;
-    W.aut_cap = cap;
-    W.max_aut = A.max_aut;
-    W.ntouched = 0;
-  }
+  sp_bind(slot, Lo, n, A.rowptr + vo + g, A.col + eo, smem, smem_bytes, pool, cap, A.max_aut);
   __syncwarp();
   if (!sp_check_input(m)) {
     res.status = kBadInput;

@@ -1,0 +1,835 @@
+// canon_wide.cuh -- many warps search the tree of one graph.
+//
+// The reference's GPU path (nauty_parallel.cu, BWDWorkList.cuh) spreads one
+// graph's search tree over thread blocks that share the automorphism store
+// and the best leaf.  This is the B200 form of that idea, built on the
+// sparse warp machinery of canon_sparse.cuh:
+//
+//   1. one warp walks the first path (first_path_node, sequential.cpp:216-257)
+//      to the first leaf and records, per level, the target cell's position
+//      range, the path's codes and the leaf's partition;
+//   2. the siblings of the first path -- every member of every level's target
+//      cell except the first-path vertex -- become work items, deepest level
+//      first.  A persistent grid of warps takes items from an atomic counter;
+//      a warp rebuilds the item's parent node by backtracking a copy of the
+//      first leaf's partition (cells never move vertices across their
+//      boundaries, so reconstruct_at_level gives the node back), drops the
+//      item if the vertex is not the least of its orbit under the stored
+//      automorphisms that fix the path prefix, and otherwise runs the
+//      reference's DFS (other_path_node / classify_node, sequential.cpp:304-624)
+//      over the item's subtree;
+//   3. automorphisms go to one device-wide append-only store, the best leaf
+//      to one device-wide record guarded by a lock; each warp prunes against
+//      its private copy of the best leaf, which is never better than the
+//      shared one, and publishes under the lock when it finds a better leaf.
+//
+// The reference's leaf order is total -- the trail of codes, then a sentinel,
+// then the upper-triangle matrix -- and every pruning rule discards only
+// leaves that are worse than, or equivalent to, a leaf that some warp still
+// covers, so the best leaf's matrix is the sequential one.  Two rules change
+// to keep that true when subtrees finish out of order: a leaf equivalent to
+// a best leaf found outside the current item only records the automorphism
+// and steps back one level (the sequential jump to the common ancestor
+// assumes that ancestor's other subtree is already complete), and a node
+// found worse than a newly adopted best is pruned at once.  The stored
+// automorphism count and node count are the wide search's own, like the
+// reference GPU path's.
+#pragma once
+#include <cstdint>
+
+#include "canon_sparse.cuh"
+
+namespace gcl {
+
+constexpr uint32_t kWideSpinLimit = 1u << 24;  // lock attempts (~1 s with back-off)
+
+struct WideHdr {
+  uint32_t D;          // level of the first leaf
+  uint32_t nitems;     // work items (first-path siblings)
+  uint32_t next_item;  // work counter
+  uint32_t naut;       // automorphism slots claimed
+  uint32_t lock;       // guards the best leaf
+  uint32_t version;    // best-leaf version (0 = the first leaf)
+  uint32_t best_level;
+  uint32_t best_seqlen;
+  int32_t status;
+  uint32_t pad;
+  unsigned long long nodes;
+  unsigned long long t0;  // start time (globaltimer ns)
+};
+
+// Byte layout of the device-wide region of one wide search.
+struct WideLayout {
+  uint64_t hdr, fcode, fseq, flabel, fcert, lelem, linlev, lstb, tcfirst, tclen, cum;
+  uint64_t bcode, bseq, blabel, bcert, auts, ready, fixlev, bytes;
+  uint32_t cap, stride;
+};
+
+__host__ __device__ inline WideLayout wide_layout(uint32_t n, uint64_t m2, uint32_t cap) {
+  WideLayout L{};
+  uint64_t o = 0;
+  auto take = [&](uint64_t bytes) {
+    const uint64_t at = o;
+    o = (o + bytes + 255u) & ~255ull;
+    return at;
+  };
+  const uint64_t N1 = (uint64_t)n + 2;
+  const uint64_t nw = (n + 63) / 64 + 1;
+  L.stride = (uint32_t)N1;
+  L.cap = cap;
+  L.hdr = take(sizeof(WideHdr));
+  L.fcode = take(4 * (N1 + 1));
+  L.fseq = take(4 * N1);
+  L.flabel = take(4 * N1);
+  L.fcert = take(4 * (m2 + 1));
+  L.lelem = take(4 * N1);
+  L.linlev = take(4 * N1);
+  L.lstb = take(8 * nw);
+  L.tcfirst = take(4 * N1);
+  L.tclen = take(4 * N1);
+  L.cum = take(4 * (N1 + 1));
+  L.bcode = take(4 * (N1 + 1));
+  L.bseq = take(4 * N1);
+  L.blabel = take(4 * N1);
+  L.bcert = take(4 * (m2 + 1));
+  L.auts = take(2ull * cap * N1);
+  L.ready = take(4ull * cap);
+  L.fixlev = take(4ull * cap);
+  L.bytes = o;
+  return L;
+}
+
+struct WideArgs {
+  const int32_t* rp;
+  const int32_t* col;
+  const int32_t* color;
+  uint32_t n;
+  int64_t m;  // CSR entries
+  uint8_t* sh;
+  WideLayout WL;
+  uint8_t* slots;  // per-warp workspace
+  SpLayout Lo;
+  uint64_t slot_bytes;
+  uint32_t pool;
+  uint64_t smem_per_warp;
+  uint64_t budget_ns;
+  uint8_t* out_dense;    // n*n, or null
+  uint64_t* out_rows;    // n * ceil(n/64) words, or null
+  int32_t* out_label;    // n, or null
+  int64_t* out_stats;    // {num_aut, nodes}, or null
+  int32_t* out_status;   // 1
+};
+
+struct WidePtrs {
+  WideHdr* H;
+  int32_t *fcode, *bcode;
+  uint32_t *fseq, *flabel, *fcert, *lelem, *linlev, *tcfirst, *tclen, *cum;
+  uint32_t *bseq, *blabel, *bcert, *ready, *fixlev;
+  uint64_t* lstb;
+  uint16_t* auts;
+};
+
+__device__ inline WidePtrs wide_ptrs(const WideArgs& A) {
+  uint8_t* b = A.sh;
+  const WideLayout& L = A.WL;
+  WidePtrs P;
+  P.H = (WideHdr*)(b + L.hdr);
+  P.fcode = (int32_t*)(b + L.fcode);
+  P.bcode = (int32_t*)(b + L.bcode);
+  P.fseq = (uint32_t*)(b + L.fseq);
+  P.flabel = (uint32_t*)(b + L.flabel);
+  P.fcert = (uint32_t*)(b + L.fcert);
+  P.lelem = (uint32_t*)(b + L.lelem);
+  P.linlev = (uint32_t*)(b + L.linlev);
+  P.tcfirst = (uint32_t*)(b + L.tcfirst);
+  P.tclen = (uint32_t*)(b + L.tclen);
+  P.cum = (uint32_t*)(b + L.cum);
+  P.bseq = (uint32_t*)(b + L.bseq);
+  P.blabel = (uint32_t*)(b + L.blabel);
+  P.bcert = (uint32_t*)(b + L.bcert);
+  P.ready = (uint32_t*)(b + L.ready);
+  P.fixlev = (uint32_t*)(b + L.fixlev);
+  P.lstb = (uint64_t*)(b + L.lstb);
+  P.auts = (uint16_t*)(b + L.auts);
+  return P;
+}
+
+__device__ __forceinline__ void wide_fail(WideHdr* H, int32_t status) {
+  if (lane_id() == 0) atomicCAS((int*)&H->status, (int)kOk, (int)status);
+}
+
+// ---------------------------------------------------------------------------
+// 1. First path (one warp).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(32) wide_first_kernel(WideArgs A) {
+  const uint32_t lane = lane_id();
+  const WidePtrs P = wide_ptrs(A);
+  WideHdr* H = P.H;
+  SpWarp& W = sp_w();
+  const uint32_t n = A.n;
+  if (lane == 0) {
+    H->D = 0;
+    H->nitems = 0;
+    H->next_item = 0;
+    H->naut = 0;
+    H->lock = 0;
+    H->version = 0;
+    H->best_level = 0;
+    H->best_seqlen = 0;
+    H->status = kOk;
+    H->nodes = 1;
+    H->t0 = global_ns();
+  }
+  sp_bind(A.slots, A.Lo, n, A.rp, A.col, nullptr, 0, A.pool, 0, 1);
+  __syncwarp();
+  if (!sp_check_input(A.m)) {
+    wide_fail(H, kBadInput);
+    return;
+  }
+  sp_init_partition(A.color);
+  int code = sp_refine(0);
+  if (code < 0) {
+    wide_fail(H, kInternal);
+    return;
+  }
+  uint32_t level = 1, seqlen = 0;
+  unsigned long long nodes = 1;
+  if (lane == 0) P.fcode[0] = code;
+  __syncwarp();
+  while (W.ncells < n) {
+    const uint32_t t = level <= n ? sp_first_nonsingleton() : kNone;
+    if (t == kNone) {
+      wide_fail(H, kInternal);
+      return;
+    }
+    const uint32_t len = sp_cell_end(W, t) - t;
+    uint32_t v = kNone;
+    for (uint32_t q = t + lane; q < t + len; q += 32) v = min(v, W.elem[q]);
+    v = __reduce_min_sync(GCL_FULL, v);  // first representative: the least member
+    __syncwarp();
+    if (lane == 0) {
+      P.tcfirst[level - 1] = t;
+      P.tclen[level - 1] = len;
+      W.seq[seqlen] = v;
+    }
+    __syncwarp();
+    ++seqlen;
+    ++nodes;
+    if (!sp_individualize(level, v, t)) {
+      wide_fail(H, kInternal);
+      return;
+    }
+    code = sp_refine(level);
+    if (code < 0) {
+      wide_fail(H, kInternal);
+      return;
+    }
+    ++level;
+    __syncwarp();
+    if (lane == 0) P.fcode[level - 1] = code;
+    __syncwarp();
+  }
+  // the first leaf: certificate, labeling, partition, and the initial best
+  const uint32_t D = level;
+  sp_leaf_cert(P.fcert);
+  for (uint32_t i = lane; i < n; i += 32) {
+    const uint32_t e = W.elem[i];
+    P.flabel[i] = e;
+    P.blabel[i] = e;
+    P.lelem[i] = e;
+    P.linlev[i] = W.inlev[i];
+  }
+  for (uint32_t i = lane; i < seqlen; i += 32) {
+    P.fseq[i] = W.seq[i];
+    P.bseq[i] = W.seq[i];
+  }
+  for (uint32_t w = lane; w < W.nw; w += 32) P.lstb[w] = W.stb[w];
+  for (int64_t i = lane; i < A.m; i += 32) P.bcert[i] = P.fcert[i];
+  for (uint32_t i = lane; i < D; i += 32) P.bcode[i] = P.fcode[i];
+  __syncwarp();
+  if (lane == 0) {
+    P.fcode[D] = kSentinel;
+    P.bcode[D] = kSentinel;
+    // items of node level L = D-1 .. 1: its target cell minus the first-path
+    // vertex, which the first path left at the cell's first position
+    uint32_t run = 0;
+    P.cum[0] = 0;
+    for (uint32_t i = 0; i + 1 < D; ++i) {
+      const uint32_t L = D - 1 - i;
+      run += P.tclen[L - 1] - 1;
+      P.cum[i + 1] = run;
+    }
+    H->D = D;
+    H->best_level = D;
+    H->best_seqlen = seqlen;
+    H->nodes = nodes;
+    __threadfence();
+    H->nitems = run;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 2. Items (persistent grid, one item per warp at a time).
+// ---------------------------------------------------------------------------
+
+// Number of leading automorphism-store entries whose contents are complete.
+__device__ __noinline__ uint32_t wide_ready_prefix(const WidePtrs& P, uint32_t known,
+                                                   uint32_t cap) {
+  uint32_t k = known;
+  if (lane_id() == 0) {
+    const uint32_t claimed = min(*(volatile uint32_t*)&P.H->naut, cap);
+    while (k < claimed && *(volatile uint32_t*)&P.ready[k]) ++k;
+    __threadfence();
+  }
+  return __shfl_sync(GCL_FULL, k, 0);
+}
+
+// Least vertex of v's orbit under the stored automorphisms that fix the
+// first path's first `k` vertices (subgroup_fixing_sequence +
+// compute_orbits_fast, perm_group.cpp:5-116).
+__device__ __noinline__ uint32_t wide_orbit_min(const WidePtrs& P, uint32_t v, uint32_t k,
+                                                uint32_t known, uint32_t stride, bool* ok) {
+  SpWarp& W = sp_w();
+  const uint32_t lane = lane_id();
+  const uint32_t n = W.n;
+  bool init = false;
+  for (uint32_t a = 0; a < known; ++a) {
+    if (__ldcg(P.fixlev + a) < k) continue;
+    if (!init) {
+      for (uint32_t x = lane; x < n; x += 32) W.dsu[x] = x;
+      __syncwarp();
+      init = true;
+    }
+    if (!sp_dsu_apply<true>(P.auts + (uint64_t)a * stride, n)) {
+      *ok = false;
+      return v;
+    }
+  }
+  if (!init) return v;
+  return sp_find(W.dsu, v, n);
+}
+
+// Append aut[label[j]] = elem[j] to the store with its fixed-prefix length.
+template <bool kCgLabel>
+__device__ __noinline__ void wide_store_aut(const WidePtrs& P, const uint32_t* label, uint32_t cap,
+                                            uint32_t stride, uint32_t D) {
+  SpWarp& W = sp_w();
+  const uint32_t lane = lane_id();
+  uint32_t slot = 0;
+  if (lane == 0) slot = atomicAdd(&P.H->naut, 1u);
+  slot = __shfl_sync(GCL_FULL, slot, 0);
+  if (slot >= cap) return;  // store full: fewer prunes, same result
+  uint16_t* pm = P.auts + (uint64_t)slot * stride;
+  for (uint32_t j = lane; j < W.n; j += 32) pm[ldx<kCgLabel>(label + j)] = (uint16_t)W.elem[j];
+  __syncwarp();
+  // leading first-path vertices it fixes
+  const uint32_t np = D - 1;
+  uint32_t fl = np;
+  for (uint32_t i0 = 0; i0 < np; i0 += 32) {
+    const uint32_t i = i0 + lane;
+    const uint32_t b = __ballot_sync(GCL_FULL, i < np && pm[P.fseq[i]] != P.fseq[i]);
+    if (b) {
+      fl = i0 + (uint32_t)(__ffs(b) - 1);
+      break;
+    }
+  }
+  __threadfence();
+  __syncwarp();
+  if (lane == 0) {
+    P.fixlev[slot] = fl;
+    __threadfence();
+    *(volatile uint32_t*)&P.ready[slot] = 1u;
+  }
+  __syncwarp();
+}
+
+__device__ __noinline__ bool wide_lock(WideHdr* H) {
+  uint32_t got = 0;
+  if (lane_id() == 0) {
+    for (uint32_t i = 0; i < kWideSpinLimit; ++i) {
+      if (atomicCAS(&H->lock, 0u, 1u) == 0u) {
+        got = 1;
+        break;
+      }
+      __nanosleep(64);
+    }
+    __threadfence();
+  }
+  return __shfl_sync(GCL_FULL, got, 0) != 0;
+}
+
+__device__ __noinline__ void wide_unlock(WideHdr* H) {
+  __threadfence();
+  __syncwarp();
+  if (lane_id() == 0) atomicExch(&H->lock, 0u);
+  __syncwarp();
+}
+
+struct WideBest {
+  int canon_level;
+  uint32_t best_seqlen;
+  uint32_t version;
+};
+
+// Copy the shared best leaf into the warp's private copy (lock held).
+__device__ __noinline__ WideBest wide_adopt(const WidePtrs& P, int64_t m) {
+  SpWarp& W = sp_w();
+  const uint32_t lane = lane_id();
+  WideBest b;
+  b.canon_level = (int)*(volatile uint32_t*)&P.H->best_level;
+  b.best_seqlen = *(volatile uint32_t*)&P.H->best_seqlen;
+  b.version = *(volatile uint32_t*)&P.H->version;
+  for (uint32_t i = lane; i <= (uint32_t)b.canon_level; i += 32) W.ccode[i] = __ldcg(P.bcode + i);
+  for (uint32_t i = lane; i < W.n; i += 32) W.blabel[i] = __ldcg(P.blabel + i);
+  for (uint32_t i = lane; i < b.best_seqlen; i += 32) W.bseq[i] = __ldcg(P.bseq + i);
+  for (int64_t i = lane; i < m; i += 32) W.bcert[i] = __ldcg(P.bcert + i);
+  __syncwarp();
+  return b;
+}
+
+// The path's comparison state against the private best: the first level
+// whose code differs (eqlevcanon) and the sign there (comp_canon); a better
+// path overwrites the private trail from there on, as classify_node does.
+__device__ __noinline__ void wide_recompare(uint32_t Lp, int canon_level, int* eqlevcanon,
+                                            int* comp_canon) {
+  SpWarp& W = sp_w();
+  const uint32_t lane = lane_id();
+  const uint32_t lim = min(Lp, (uint32_t)canon_level);
+  uint32_t i = lim;
+  for (uint32_t j0 = 0; j0 < lim; j0 += 32) {
+    const uint32_t j = j0 + lane;
+    const uint32_t b = __ballot_sync(GCL_FULL, j < lim && W.pathcode[j] != W.ccode[j]);
+    if (b) {
+      i = j0 + (uint32_t)(__ffs(b) - 1);
+      break;
+    }
+  }
+  if (i == Lp) {
+    *eqlevcanon = (int)Lp;
+    *comp_canon = 0;
+    return;
+  }
+  *eqlevcanon = (int)i;
+  const int bc = (int)i < canon_level ? W.ccode[i] : kSentinel;
+  *comp_canon = W.pathcode[i] < bc ? -1 : 1;
+  if (*comp_canon > 0) {
+    __syncwarp();
+    for (uint32_t j = i + lane; j < Lp; j += 32) W.ccode[j] = W.pathcode[j];
+  }
+  __syncwarp();
+}
+
+// Publish a leaf that beats the private best (lock held by the caller).
+// Returns 1 if it became the shared best, 0 if the shared best was kept
+// (and adopted; an equal shared leaf also yields an automorphism).
+__device__ __noinline__ int wide_publish(const WidePtrs& P, const WideArgs& A, uint32_t Lv,
+                                         uint32_t seqlen, WideBest* nb) {
+  SpWarp& W = sp_w();
+  const uint32_t lane = lane_id();
+  const uint32_t gl = *(volatile uint32_t*)&P.H->best_level;
+  const uint32_t lim = min(Lv, gl);
+  int cmp = 0;
+  for (uint32_t j0 = 0; j0 < lim; j0 += 32) {
+    const uint32_t j = j0 + lane;
+    const int32_t pc = j < lim ? W.pathcode[j] : 0;
+    const int32_t gc = j < lim ? __ldcg(P.bcode + j) : 0;
+    const uint32_t b = __ballot_sync(GCL_FULL, j < lim && pc != gc);
+    if (b) {
+      const int src = __ffs(b) - 1;
+      const int32_t a = __shfl_sync(GCL_FULL, pc, src), c = __shfl_sync(GCL_FULL, gc, src);
+      cmp = a < c ? -1 : 1;
+      break;
+    }
+  }
+  if (cmp == 0) {
+    if (Lv < gl)
+      cmp = 1;
+    else if (Lv > gl)
+      cmp = -1;
+    else
+      cmp = sp_cmp_leaf<true>(W.ccert, P.blabel, P.bcert, true);
+  }
+  if (cmp > 0) {
+    for (uint32_t i = lane; i < Lv; i += 32) P.bcode[i] = W.pathcode[i];
+    for (uint32_t i = lane; i < W.n; i += 32) P.blabel[i] = W.elem[i];
+    for (uint32_t i = lane; i < seqlen; i += 32) P.bseq[i] = W.seq[i];
+    for (int64_t i = lane; i < A.m; i += 32) P.bcert[i] = W.ccert[i];
+    __syncwarp();
+    uint32_t ver = 0;
+    if (lane == 0) {
+      P.bcode[Lv] = kSentinel;
+      P.H->best_level = Lv;
+      P.H->best_seqlen = seqlen;
+      ver = P.H->version + 1;
+      P.H->version = ver;
+    }
+    nb->version = __shfl_sync(GCL_FULL, ver, 0);
+    nb->canon_level = (int)Lv;
+    nb->best_seqlen = seqlen;
+    return 1;
+  }
+  if (cmp == 0) wide_store_aut<true>(P, P.blabel, A.WL.cap, A.WL.stride, P.H->D);
+  *nb = wide_adopt(P, A.m);
+  return 0;
+}
+
+__global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
+  extern __shared__ __align__(16) uint8_t sp_dyn[];
+  const int warp = (int)(threadIdx.x >> 5);
+  const uint32_t lane = lane_id();
+  const WidePtrs P = wide_ptrs(A);
+  WideHdr* H = P.H;
+  if (H->status != kOk || H->nitems == 0) return;
+  SpWarp& W = sp_w();
+  const uint32_t n = A.n, D = H->D, nitems = H->nitems, cap = A.WL.cap;
+  uint8_t* slot = A.slots + ((uint64_t)blockIdx.x * kSpWarps + (uint64_t)warp) * A.slot_bytes;
+  uint8_t* smem = A.smem_per_warp ? sp_dyn + (uint64_t)warp * A.smem_per_warp : nullptr;
+  sp_bind(slot, A.Lo, n, A.rp, A.col, smem, A.smem_per_warp, A.pool, 0, cap);
+  __syncwarp();
+  if (lane == 0) {
+    // the first path is shared and read-only; automorphisms go to the store
+    W.fcode = P.fcode;
+    W.fseq = P.fseq;
+    W.flabel = P.flabel;
+    W.fcert = P.fcert;
+    W.auts = P.auts;
+    W.stride = A.WL.stride;
+    W.nact = 0;
+    W.ntouched = 0;
+  }
+  __syncwarp();
+  for (uint32_t i = lane; i < n; i += 32) {
+    W.cnt[i] = 0;
+    W.cellcnt[i] = 0;
+    W.fill[i] = 0;
+  }
+  for (uint32_t w = lane; w < W.nw; w += 32) {
+    W.act[w] = 0;
+    W.tcb[w] = 0;
+  }
+  for (uint32_t w = lane; w < W.nsw; w += 32) {
+    W.acts[w] = 0;
+    W.tcbs[w] = 0;
+  }
+  __syncwarp();
+  const uint64_t deadline = A.budget_ns ? H->t0 + A.budget_ns : 0;
+  WideBest best{0, 0, 0xffffffffu};
+  uint32_t known = 0;
+  unsigned long long my_nodes = 0;
+  int32_t status = kOk;
+  uint64_t iter = 0;
+  while (status == kOk) {
+    uint32_t it = 0;
+    if (lane == 0) it = atomicAdd(&H->next_item, 1u);
+    it = __shfl_sync(GCL_FULL, it, 0);
+    if (it >= nitems) break;
+    if (*(volatile int32_t*)&H->status != kOk) break;
+    // item -> level (cum is ascending over levels taken deepest first)
+    uint32_t lo = 0, hi = D - 1;  // cum[lo] <= it < cum[hi]
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (P.cum[mid] <= it)
+        lo = mid;
+      else
+        hi = mid;
+    }
+    const uint32_t k = D - 2 - lo;  // parent node level k+1, its target cell index k
+    const uint32_t tf = P.tcfirst[k], tl = P.tclen[k];
+    const uint32_t v = P.lelem[tf + 1 + (it - P.cum[lo])];
+    (void)tl;
+    known = wide_ready_prefix(P, known, cap);
+    if (known) {
+      bool ok = true;
+      const uint32_t r = wide_orbit_min(P, v, k, known, A.WL.stride, &ok);
+      if (!ok) {
+        status = kInternal;
+        break;
+      }
+      if (r != v) continue;  // an equivalent sibling is covered by its orbit's least vertex
+    }
+    // the parent node: the first leaf backtracked to level k+1
+    for (uint32_t i = lane; i < n; i += 32) {
+      const uint32_t e = P.lelem[i];
+      W.elem[i] = e;
+      W.pos[e] = i;
+      W.inlev[i] = P.linlev[i];
+    }
+    for (uint32_t w = lane; w < W.nw; w += 32) W.stb[w] = P.lstb[w];
+    __syncwarp();
+    bm_resummarize(W.stb, W.sts, W.nw, W.nsw);
+    if (lane == 0) W.ncells = n;
+    __syncwarp();
+    if (!sp_backtrack(k + 1) || sp_cell_end(W, tf) - tf != tl) {
+      status = kInternal;
+      break;
+    }
+    for (uint32_t i = lane; i < k; i += 32) W.seq[i] = P.fseq[i];
+    for (uint32_t i = lane; i <= k; i += 32) W.pathcode[i] = P.fcode[i];
+    __syncwarp();
+    if (lane == 0) {
+      SpTc h;
+      h.first = tf;
+      h.len = tl;
+      h.counter = n;  // this warp takes no other child of the parent
+      h.last = 0;
+      h.rslot = -1;
+      h.pad = 0;
+      W.tc[k] = h;
+      W.pool_top = 0;
+    }
+    __syncwarp();
+    // private best: refresh when the shared one has changed
+    if (*(volatile uint32_t*)&H->version != best.version) {
+      if (!wide_lock(H)) {
+        status = kTimeout;
+        break;
+      }
+      best = wide_adopt(P, A.m);
+      wide_unlock(H);
+    }
+    bool best_local = best.version == 0;  // the first leaf anchors gca jumps
+    uint32_t eqlevfirst = k + 1, seqlen = k, level = k + 1;
+    int eqlevcanon = 0, comp_canon = 0, tcl = (int)k + 1;
+    wide_recompare(k + 1, best.canon_level, &eqlevcanon, &comp_canon);
+    // the item's node
+    __syncwarp();
+    if (lane == 0) W.seq[seqlen] = v;
+    __syncwarp();
+    ++seqlen;
+    ++my_nodes;
+    if (!sp_individualize(level, v, tf)) {
+      status = kInternal;
+      break;
+    }
+    int code = sp_refine(level);
+    if (code < 0) {
+      status = kInternal;
+      break;
+    }
+    ++level;
+    bool have_node = true;
+    // DFS of the item's subtree (other_path_node / classify_node)
+    while (true) {
+      if ((++iter & 15) == 0 && deadline &&
+          __shfl_sync(GCL_FULL, lane == 0 ? global_ns() : 0ull, 0) > deadline) {
+        status = kTimeout;
+        break;
+      }
+      int bt = -1;
+      bool recompare = false;
+      if (have_node) {
+        have_node = false;
+        const uint32_t Lv = level;
+        __syncwarp();
+        if (lane == 0) W.pathcode[Lv - 1] = code;
+        __syncwarp();
+        if (eqlevfirst == Lv - 1 && code == W.fcode[Lv - 1]) eqlevfirst = Lv;
+        if (eqlevcanon == (int)Lv - 1) {
+          const int cc = W.ccode[Lv - 1];
+          if (code < cc) {
+            comp_canon = -1;
+          } else if (code > cc) {
+            comp_canon = 1;
+          } else {
+            comp_canon = 0;
+            eqlevcanon = (int)Lv;
+          }
+        }
+        if (comp_canon > 0) {
+          __syncwarp();
+          if (lane == 0) W.ccode[Lv - 1] = code;
+          __syncwarp();
+        }
+        int dec = 0;
+        if (eqlevfirst != Lv && comp_canon < 0) {
+          dec = 4;
+        } else if (W.ncells == n) {
+          sp_leaf_cert(W.ccert);
+          if (eqlevfirst == Lv && sp_cmp_leaf(W.ccert, W.flabel, W.fcert, false) == 0) dec = 1;
+          if (dec == 0) {
+            if (comp_canon == 0) {
+              if ((int)Lv < best.canon_level)
+                comp_canon = 1;
+              else
+                comp_canon = sp_cmp_leaf(W.ccert, W.blabel, W.bcert, true);
+            }
+            dec = comp_canon == 0 ? 2 : (comp_canon > 0 ? 3 : 4);
+          }
+        }
+        if (dec == 1) {
+          wide_store_aut<false>(P, W.flabel, cap, A.WL.stride, D);
+          const int gg = sp_gca(W.fseq, D - 1, seqlen);
+          bt = gg >= 0 ? gg : (int)Lv - 1;
+        } else if (dec == 2) {
+          wide_store_aut<false>(P, W.blabel, cap, A.WL.stride, D);
+          const int gg = best_local ? sp_gca(W.bseq, best.best_seqlen, seqlen) : -1;
+          bt = gg >= 0 ? gg : (int)Lv - 1;
+        } else if (dec == 3) {
+          if (!wide_lock(H)) {
+            status = kTimeout;
+            break;
+          }
+          WideBest nb;
+          const int r = wide_publish(P, A, Lv, seqlen, &nb);
+          wide_unlock(H);
+          if (r == 1) {
+            // the leaf is the new shared best and the private one
+            sp_copy_u32(W.bcert, W.ccert, (uint32_t)A.m);
+            sp_copy_u32(W.blabel, W.elem, n);
+            sp_copy_u32(W.bseq, W.seq, seqlen);
+            if (lane == 0) W.ccode[Lv] = kSentinel;
+            __syncwarp();
+            best = nb;
+            best_local = true;
+            eqlevcanon = (int)Lv;
+            comp_canon = 0;
+          } else {
+            best = nb;
+            best_local = false;
+            recompare = true;
+          }
+          bt = (int)Lv - 1;
+        } else if (dec == 4) {
+          bt = (int)Lv - 1;
+        }
+      } else {
+        const bool disc = W.ncells == n;
+        if (!disc && (eqlevfirst == level || comp_canon >= 0)) {
+          if (tcl < (int)level) {
+            const uint32_t t = sp_first_nonsingleton();
+            if (t == kNone) {
+              status = kInternal;
+              break;
+            }
+            if (lane == 0) {
+              SpTc h;
+              h.first = t;
+              h.len = sp_cell_end(W, t) - t;
+              h.counter = 0;
+              h.last = 0;
+              h.rslot = -1;
+              h.pad = 0;
+              W.tc[tcl] = h;
+            }
+            __syncwarp();
+            ++tcl;
+          }
+          const int idx = (int)level - 1;
+          if (W.tc[idx].counter >= n) {
+            bt = (int)level - 1;
+          } else {
+            known = wide_ready_prefix(P, known, cap);
+            if (known > (uint32_t)W.tc[idx].last) {
+              if (!sp_orbits<true>(idx, (int)known, seqlen)) {
+                status = W.pool_top >= W.pool_cap ? kAutOverflow : kInternal;
+                break;
+              }
+              __syncwarp();
+              if (lane == 0) W.tc[idx].last = (int32_t)known;
+              __syncwarp();
+            }
+            const SpTc t = W.tc[idx];
+            const uint32_t u = sp_next_rep(t);
+            __syncwarp();
+            if (u == kNone) {
+              if (lane == 0) W.tc[idx].counter = n;
+              __syncwarp();
+              bt = (int)level - 1;
+            } else {
+              if (lane == 0) {
+                W.tc[idx].counter = u + 1;
+                W.seq[seqlen] = u;
+              }
+              __syncwarp();
+              ++seqlen;
+              ++my_nodes;
+              if (!sp_individualize(level, u, t.first)) {
+                status = kInternal;
+                break;
+              }
+              code = sp_refine(level);
+              if (code < 0) {
+                status = kInternal;
+                break;
+              }
+              ++level;
+              have_node = true;
+            }
+          }
+        } else {
+          // worse than the private best and off the first path's trail
+          bt = (int)level - 1;
+          recompare = true;
+        }
+      }
+      if (bt >= 0) {
+        const uint32_t Lv = (uint32_t)bt;
+        if (Lv <= k + 1) break;  // the item's subtree is done
+        if (!sp_backtrack(Lv)) {
+          status = kInternal;
+          break;
+        }
+        if (Lv < eqlevfirst) eqlevfirst = Lv;
+        if ((int)Lv <= eqlevcanon) {
+          eqlevcanon = (int)Lv;
+          comp_canon = 0;
+        }
+        seqlen = Lv - 1;
+        tcl = (int)Lv;
+        level = Lv;
+        __syncwarp();
+        if (lane == 0)
+          while (W.pool_top > 0 && W.pool_owner[W.pool_top - 1] >= (int32_t)Lv) W.pool_top -= 1;
+        __syncwarp();
+        if (recompare) wide_recompare(level, best.canon_level, &eqlevcanon, &comp_canon);
+      }
+    }
+  }
+  if (status != kOk) wide_fail(H, status);
+  if (lane == 0) atomicAdd(&H->nodes, my_nodes);
+}
+
+// ---------------------------------------------------------------------------
+// 3. Outputs from the shared best leaf (one warp).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(32) wide_finish_kernel(WideArgs A) {
+  const uint32_t lane = lane_id();
+  const WidePtrs P = wide_ptrs(A);
+  const WideHdr* H = P.H;
+  const uint32_t n = A.n;
+  const int32_t status = H->status;
+  if (lane == 0) {
+    A.out_status[0] = status;
+    if (A.out_stats) {
+      A.out_stats[0] = (int64_t)H->naut;
+      A.out_stats[1] = (int64_t)H->nodes;
+    }
+  }
+  if (status != kOk) return;
+  if (A.out_label)
+    for (uint32_t j = lane; j < n; j += 32) A.out_label[j] = (int32_t)P.blabel[j];
+  if (A.out_rows) {
+    const uint32_t words = (n + 63) / 64;
+    for (uint32_t i = lane; i < n; i += 32) {
+      uint64_t* row = A.out_rows + (uint64_t)i * words;
+      for (uint32_t w = 0; w < words; ++w) row[w] = 0;
+      const uint32_t v = P.blabel[i];
+      for (int32_t j = A.rp[v]; j < A.rp[v + 1]; ++j) {
+        const uint32_t c = P.bcert[j];
+        row[c >> 6] |= bit64(c & 63);
+      }
+    }
+  }
+  if (A.out_dense) {
+    const uint64_t nn = (uint64_t)n * n;
+    for (uint64_t i = lane; i < nn; i += 32) A.out_dense[i] = 0;
+    __syncwarp();
+    for (uint32_t i = 0; i < n; ++i) {
+      const uint32_t v = P.blabel[i];
+      for (int32_t j = A.rp[v] + (int32_t)lane; j < A.rp[v + 1]; j += 32)
+        A.out_dense[(uint64_t)i * n + P.bcert[j]] = 1;
+    }
+  }
+}
+
+}  // namespace gcl

@@ -22,6 +22,7 @@
 #include "../../include/gcl.h"
 #include "canon_sparse.cuh"
 #include "canon_warp64.cuh"
+#include "canon_wide.cuh"
 
 namespace gcl {
 
@@ -77,6 +78,8 @@ __global__ void __launch_bounds__(kOrderThreads)
 }
 
 constexpr int kSpSmemPerBlock = 200 * 1024;  // dynamic shared memory cap of one sparse block
+constexpr uint32_t kWidePool = 32;  // per-level orbit arrays of a wide-search warp
+constexpr uint64_t kWideStoreBytes = 1ull << 30;  // automorphism store of a wide search
 constexpr uint32_t kSpPool = 8;     // per-level orbit arrays in the first sparse pass
 constexpr uint32_t kSpAutCap = 64;  // ring entries in the first sparse pass
 
@@ -186,6 +189,9 @@ struct gcl_context {
   uint32_t work_big_aut = 0;
   int big_slots = 0;
   DevBuf sp_work[kSpBuckets], sp_work_big;
+  // wide search of one graph: shared region and per-warp slots
+  DevBuf wide_sh, wide_slots;
+  int64_t wide_min_n = kW64MaxN + 1;
   DevBuf deferred, overflow_list, large_list, sp_fail_list, order;
   // staging for host-pointer calls
   DevBuf voff, eoff, rowptr, col, color, ooff, dense, roff, rows, label, stats, status;
@@ -264,6 +270,9 @@ int gcl_create(int device, gcl_context** out) {
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(sp_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              kSpSmemPerBlock);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(wide_items_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             kSpSmemPerBlock);
   if (e != cudaSuccess) {
     if (c->stream) cudaStreamDestroy(c->stream);
     c->deferred.release();
@@ -279,7 +288,8 @@ int gcl_destroy(gcl_context* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   for (DevBuf& b : c->sp_work) b.release();
-  DevBuf* bufs[] = {&c->work, &c->work_big, &c->sp_work_big, &c->deferred,
+  DevBuf* bufs[] = {&c->work, &c->work_big, &c->sp_work_big, &c->deferred, &c->wide_sh,
+                    &c->wide_slots,
                     &c->overflow_list, &c->large_list, &c->sp_fail_list, &c->order, &c->voff, &c->eoff, &c->rowptr, &c->col, &c->color,
                     &c->ooff, &c->dense, &c->roff, &c->rows, &c->label, &c->stats,
                     &c->status};
@@ -414,6 +424,78 @@ int gcl_canon_batch_device_async(gcl_context* c, int count, const int64_t* d_vof
   return GCL_OK;
 }
 
+int gcl_set_option(gcl_context* c, int option, int64_t value) {
+  if (!c) return GCL_ERR_ARG;
+  switch (option) {
+    case GCL_OPT_WIDE_MIN_N:
+      if (value < 1) return GCL_ERR_ARG;
+      c->wide_min_n = value;
+      return GCL_OK;
+    default:
+      return GCL_ERR_ARG;
+  }
+}
+
+int gcl_canon_wide_device_async(gcl_context* c, const int32_t* d_rowptr, const int32_t* d_col,
+                                const int32_t* d_color, int n, int64_t m, int max_aut,
+                                uint8_t* d_out_dense, uint64_t* d_out_rows,
+                                int32_t* d_out_label, int64_t* d_out_stats,
+                                int32_t* d_out_status) {
+  if (!c || n < 1 || m < 0 || max_aut <= 0 || !d_rowptr || (m > 0 && !d_col) || !d_out_status)
+    return GCL_ERR_ARG;
+  if (n > GCL_MAX_N) return GCL_ERR_TOO_LARGE;
+  GCL_TRY(cudaSetDevice(c->device));
+  const uint32_t un = (uint32_t)n;
+  const uint64_t m2 = (uint64_t)std::max<int64_t>(m, 1);
+  // automorphism store: up to max_aut entries within kWideStoreBytes
+  const uint64_t per_aut = 2ull * ((uint64_t)un + 2);
+  const uint32_t cap = (uint32_t)std::max<uint64_t>(
+      1, std::min<uint64_t>((uint64_t)max_aut, kWideStoreBytes / per_aut));
+  const WideLayout WL = wide_layout(un, m2, cap);
+  const SpLayout Lo = sp_layout(un, m2, kWidePool, 0);
+  uint64_t smw = sp_smem_bytes(un);
+  if (smw * kSpWarps > (uint64_t)kSpSmemPerBlock) smw = 0;
+  int per_sm = 0;
+  GCL_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, wide_items_kernel, kSpThreads,
+                                                        (size_t)(smw * kSpWarps)));
+  const uint64_t budget = workspace_budget();
+  int64_t warps = std::min<int64_t>((int64_t)c->sms * std::max(per_sm, 1) * kSpWarps,
+                                    std::max<int64_t>(kSpWarps, (int64_t)(budget / Lo.bytes)));
+  // no more warps than the largest possible number of work items
+  warps = std::min<int64_t>(warps, ((int64_t)n * 2 + kSpWarps - 1) / kSpWarps * kSpWarps);
+  warps = std::max<int64_t>(kSpWarps, warps / kSpWarps * kSpWarps);
+  GCL_TRY(c->wide_sh.ensure(WL.bytes));
+  GCL_TRY(c->wide_slots.ensure((size_t)(warps * Lo.bytes)));
+  WideArgs WA;
+  std::memset(&WA, 0, sizeof WA);
+  WA.rp = d_rowptr;
+  WA.col = d_col;
+  WA.color = d_color;
+  WA.n = un;
+  WA.m = m;
+  WA.sh = (uint8_t*)c->wide_sh.p;
+  WA.WL = WL;
+  WA.slots = (uint8_t*)c->wide_slots.p;
+  WA.Lo = Lo;
+  WA.slot_bytes = Lo.bytes;
+  WA.pool = kWidePool;
+  WA.smem_per_warp = smw;
+  WA.budget_ns = graph_budget_ns();
+  WA.out_dense = d_out_dense;
+  WA.out_rows = d_out_rows;
+  WA.out_label = d_out_label;
+  WA.out_stats = d_out_stats;
+  WA.out_status = d_out_status;
+  cudaStream_t s = c->stream;
+  wide_first_kernel<<<1, 32, 0, s>>>(WA);
+  GCL_TRY(cudaGetLastError());
+  wide_items_kernel<<<(int)(warps / kSpWarps), kSpThreads, (size_t)(smw * kSpWarps), s>>>(WA);
+  GCL_TRY(cudaGetLastError());
+  wide_finish_kernel<<<1, 32, 0, s>>>(WA);
+  GCL_TRY(cudaGetLastError());
+  return GCL_OK;
+}
+
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
@@ -439,6 +521,45 @@ int graph_status_to_rc(int32_t s) {
     case kTimeout: return GCL_ERR_TIMEOUT;
     default: return GCL_ERR_INTERNAL;
   }
+}
+
+// Wide search of one graph given in host memory; the dense matrix and the
+// statistics come back to the host.  GCL_ERR_INTERNAL: no result (workspace
+// outgrown or an internal check), the caller falls back.
+int canon_wide_host(gcl_context* c, const int32_t* rowptr, const int32_t* col,
+                    const int32_t* color, int n, int max_aut, uint8_t* out_nxn, int64_t* st) {
+  const int64_t m = rowptr[n];
+  if (rowptr[0] != 0 || m < 0) return GCL_ERR_BAD_INPUT;
+  if (m > 0 && !col) return GCL_ERR_ARG;
+  GCL_TRY(cudaSetDevice(c->device));
+  cudaStream_t s = c->stream;
+  GCL_TRY(c->rowptr.ensure(((size_t)n + 1) * sizeof(int32_t)));
+  GCL_TRY(c->col.ensure(std::max<size_t>((size_t)m, 1) * sizeof(int32_t)));
+  GCL_TRY(c->dense.ensure(std::max<size_t>((size_t)n * n, 1)));
+  GCL_TRY(c->stats.ensure(2 * sizeof(int64_t)));
+  GCL_TRY(c->status.ensure(sizeof(int32_t)));
+  GCL_TRY(cudaMemcpyAsync(c->rowptr.p, rowptr, ((size_t)n + 1) * sizeof(int32_t),
+                          cudaMemcpyHostToDevice, s));
+  if (m) GCL_TRY(cudaMemcpyAsync(c->col.p, col, (size_t)m * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+  int32_t* d_color = nullptr;
+  if (color) {
+    GCL_TRY(c->color.ensure((size_t)n * sizeof(int32_t)));
+    GCL_TRY(cudaMemcpyAsync(c->color.p, color, (size_t)n * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    d_color = (int32_t*)c->color.p;
+  }
+  int rc = gcl_canon_wide_device_async(c, (int32_t*)c->rowptr.p, (int32_t*)c->col.p, d_color, n,
+                                       m, max_aut, (uint8_t*)c->dense.p, nullptr, nullptr,
+                                       (int64_t*)c->stats.p, (int32_t*)c->status.p);
+  if (rc != GCL_OK) return rc == GCL_ERR_NOMEM ? GCL_ERR_INTERNAL : rc;
+  int32_t status = 0;
+  GCL_TRY(cudaMemcpyAsync(&status, c->status.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  GCL_TRY(cudaMemcpyAsync(st, c->stats.p, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+  GCL_TRY(cudaStreamSynchronize(s));
+  if (status == kAutOverflow) return GCL_ERR_INTERNAL;
+  if (status != kOk) return graph_status_to_rc(status);
+  GCL_TRY(cudaMemcpyAsync(out_nxn, c->dense.p, (size_t)n * n, cudaMemcpyDeviceToHost, s));
+  GCL_TRY(cudaStreamSynchronize(s));
+  return GCL_OK;
 }
 
 }  // namespace
@@ -550,10 +671,20 @@ int gcl_canon_one(gcl_context* c, const int32_t* rowptr, const int32_t* col, con
     if (num_aut) *num_aut = 0;
     return GCL_OK;
   }
+  int64_t st[2] = {0, 0};
+  if ((int64_t)n >= c->wide_min_n && n <= GCL_MAX_N) {
+    const int rcw = canon_wide_host(c, rowptr, col, color, n, max_aut, out_nxn, st);
+    if (rcw != GCL_ERR_INTERNAL) {  // no result for want of workspace: sequential search
+      if (rcw == GCL_OK) {
+        if (num_aut) *num_aut = st[0];
+        if (node_count) *node_count = st[1];
+      }
+      return rcw;
+    }
+  }
   const int64_t voff[2] = {0, n};
   const int64_t eoff[2] = {0, rowptr[n]};
   const int64_t ooff[2] = {0, (int64_t)n * n};
-  int64_t st[2] = {0, 0};
   int32_t status = 0;
   int rc = gcl_canon_batch(c, 1, voff, eoff, rowptr, col, color, max_aut, out_nxn, ooff, nullptr,
                            nullptr, nullptr, st, &status);

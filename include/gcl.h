@@ -19,7 +19,9 @@
  * edges are rejected with GCL_ERR_BAD_INPUT (the reference's refinement is
  * undefined on parallel edges).  Results are bit-identical to the reference's sequential
  * path: the canonical matrix, its best-leaf labeling, the number of stored
- * automorphisms and the number of search-tree nodes.
+ * automorphisms and the number of search-tree nodes (the wide search of one
+ * large graph keeps the matrix and has statistics of its own, see
+ * GCL_OPT_WIDE_MIN_N).
  *
  * Errors are returned as negative status codes; nothing calls exit().  All
  * calls are synchronous unless named *_async.
@@ -63,6 +65,21 @@ int gcl_create(int device, gcl_context** out);
 int gcl_destroy(gcl_context* ctx);
 /* The CUDA stream (cudaStream_t) the context launches on. */
 void* gcl_stream(gcl_context* ctx);
+
+/* ---- options -------------------------------------------------------------
+ * GCL_OPT_WIDE_MIN_N: single-graph calls (gcl_canon_one, gcl_iso) on graphs
+ *   with at least this many vertices use the wide search -- the search tree
+ *   spread over every SM, like the reference's GPU path (a persistent grid of
+ *   warps sharing one automorphism store and one best leaf).  Its canonical
+ *   matrix is the sequential path's; its labeling is one of the equivalent
+ *   best leaves and its statistics (stored automorphisms, nodes) are its own,
+ *   as the reference GPU path's node count is.  Default 65 (the graphs the
+ *   warp-per-graph kernel for n <= 64 does not take); GCL_MAX_N + 1 keeps the
+ *   sequential traversal and its exact statistics for every size.  A wide
+ *   search that fails for want of workspace falls back to the sequential one.
+ * Returns GCL_ERR_ARG for an unknown option or value. */
+#define GCL_OPT_WIDE_MIN_N 1
+int gcl_set_option(gcl_context* ctx, int option, int64_t value);
 
 /* ---- one graph (drop-in for Nauty_Parallel, src/nauty_parallel.h:9-13) ---
  * out_nxn receives the n*n canonical adjacency matrix (row-major, 0/1 bytes,
@@ -111,6 +128,17 @@ int gcl_canon_batch_device_async(gcl_context* ctx, int count,
                                  int32_t* d_out_label, int64_t* d_out_stats,
                                  int32_t* d_out_status);
 int gcl_sync(gcl_context* ctx);
+
+/* ---- one graph, wide search, device pointers --------------------------------
+ * The wide search (see GCL_OPT_WIDE_MIN_N) of one graph already on the
+ * device: rowptr[n+1], col[m], color[n] or NULL.  Outputs as in the batched
+ * layout for a batch of one (each may be NULL except out_status[1]).  Work is
+ * enqueued on the context stream; call gcl_sync before reading results. */
+int gcl_canon_wide_device_async(gcl_context* ctx, const int32_t* d_rowptr,
+                                const int32_t* d_col, const int32_t* d_color, int n,
+                                int64_t m, int max_aut, uint8_t* d_out_dense,
+                                uint64_t* d_out_rows, int32_t* d_out_label,
+                                int64_t* d_out_stats, int32_t* d_out_status);
 
 /* ---- batched, allocation-free (n <= 64) ---------------------------------
  * No counterpart in the reference.  For callers that cannot call cudaMalloc

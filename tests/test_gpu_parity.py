@@ -15,7 +15,8 @@ pytestmark = pytest.mark.gpu
 
 @pytest.fixture(scope="module")
 def ctx(pkg):
-    return pkg.Context(0)
+    # sequential traversal for every size: statistics comparable with the oracle
+    return pkg.Context(0, wide_min_n=pkg.api.GCL_MAX_N + 1)
 
 
 def _check_batch(pkg, G, oracle_mod, graphs, ctx, max_aut=10000):
