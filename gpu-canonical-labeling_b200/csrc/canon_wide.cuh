@@ -41,7 +41,8 @@
 
 namespace gcl {
 
-constexpr uint32_t kWideSpinLimit = 1u << 24;  // lock attempts (~1 s with back-off)
+constexpr uint32_t kWideSpinLimit = 1u << 24;      // lock attempts (~1 s with back-off)
+constexpr uint32_t kWideGateSpinLimit = 1u << 30;  // gate polls, 1 us apart
 
 struct WideHdr {
   uint32_t D;          // level of the first leaf
@@ -53,6 +54,10 @@ struct WideHdr {
   uint32_t best_level;
   uint32_t best_seqlen;
   int32_t status;
+  uint32_t done;       // items finished (the gate of the next level)
+  uint32_t orb_lock;   // guards the orbit cache
+  int32_t orb_level;   // level index the orbit cache belongs to (-1 = none)
+  uint32_t orb_known;  // store entries merged into the orbit cache
   uint32_t pad;
   unsigned long long nodes;
   unsigned long long t0;  // start time (globaltimer ns)
@@ -61,7 +66,7 @@ struct WideHdr {
 // Byte layout of the device-wide region of one wide search.
 struct WideLayout {
   uint64_t hdr, fcode, fseq, flabel, fcert, lelem, linlev, lstb, tcfirst, tclen, cum;
-  uint64_t bcode, bseq, blabel, bcert, auts, ready, fixlev, bytes;
+  uint64_t bcode, bseq, blabel, bcert, auts, ready, fixlev, orb, bytes;
   uint32_t cap, stride;
 };
 
@@ -95,6 +100,7 @@ __host__ __device__ inline WideLayout wide_layout(uint32_t n, uint64_t m2, uint3
   L.auts = take(2ull * cap * N1);
   L.ready = take(4ull * cap);
   L.fixlev = take(4ull * cap);
+  L.orb = take(4 * N1);
   L.bytes = o;
   return L;
 }
@@ -124,7 +130,7 @@ struct WidePtrs {
   WideHdr* H;
   int32_t *fcode, *bcode;
   uint32_t *fseq, *flabel, *fcert, *lelem, *linlev, *tcfirst, *tclen, *cum;
-  uint32_t *bseq, *blabel, *bcert, *ready, *fixlev;
+  uint32_t *bseq, *blabel, *bcert, *ready, *fixlev, *orb;
   uint64_t* lstb;
   uint16_t* auts;
 };
@@ -149,6 +155,7 @@ __device__ inline WidePtrs wide_ptrs(const WideArgs& A) {
   P.bcert = (uint32_t*)(b + L.bcert);
   P.ready = (uint32_t*)(b + L.ready);
   P.fixlev = (uint32_t*)(b + L.fixlev);
+  P.orb = (uint32_t*)(b + L.orb);
   P.lstb = (uint64_t*)(b + L.lstb);
   P.auts = (uint16_t*)(b + L.auts);
   return P;
@@ -177,6 +184,10 @@ __global__ void __launch_bounds__(32) wide_first_kernel(WideArgs A) {
     H->best_level = 0;
     H->best_seqlen = 0;
     H->status = kOk;
+    H->done = 0;
+    H->orb_lock = 0;
+    H->orb_level = -1;
+    H->orb_known = 0;
     H->nodes = 1;
     H->t0 = global_ns();
   }
@@ -284,29 +295,99 @@ __device__ __noinline__ uint32_t wide_ready_prefix(const WidePtrs& P, uint32_t k
   return __shfl_sync(GCL_FULL, k, 0);
 }
 
+__device__ __noinline__ bool wide_lock(uint32_t* lk) {
+  uint32_t got = 0;
+  if (lane_id() == 0) {
+    for (uint32_t i = 0; i < kWideSpinLimit; ++i) {
+      if (atomicCAS(lk, 0u, 1u) == 0u) {
+        got = 1;
+        break;
+      }
+      __nanosleep(64);
+    }
+    __threadfence();
+  }
+  return __shfl_sync(GCL_FULL, got, 0) != 0;
+}
+
+__device__ __noinline__ void wide_unlock(uint32_t* lk) {
+  __threadfence();
+  __syncwarp();
+  if (lane_id() == 0) atomicExch(lk, 0u);
+  __syncwarp();
+}
+
+__device__ __forceinline__ uint32_t wide_find(const uint32_t* d, uint32_t x, uint32_t n) {
+  uint32_t p = __ldcg(d + x);
+  for (uint32_t step = 0; p < x && step <= n; ++step) {
+    x = p;
+    p = __ldcg(d + x);
+  }
+  return x;
+}
+
 // Least vertex of v's orbit under the stored automorphisms that fix the
-// first path's first `k` vertices (subgroup_fixing_sequence +
-// compute_orbits_fast, perm_group.cpp:5-116).
-__device__ __noinline__ uint32_t wide_orbit_min(const WidePtrs& P, uint32_t v, uint32_t k,
-                                                uint32_t known, uint32_t stride, bool* ok) {
+// first path's first k vertices (subgroup_fixing_sequence +
+// compute_orbits_fast, perm_group.cpp:5-116).  Only one level's items run at
+// a time, so one device-wide union-find serves them all: the first warp of a
+// level resets it, every warp merges the store entries that arrived since
+// the last merge, under the cache lock.  A root below v without the lock is
+// already a proof that v is not the least of its orbit (roots only move
+// down).  Sets *ok = false when a wait or a merge gives up.
+__device__ __noinline__ uint32_t wide_orbit_min(const WidePtrs& P, uint32_t v, uint32_t li,
+                                                uint32_t k, uint32_t known, uint32_t stride,
+                                                bool* ok) {
   SpWarp& W = sp_w();
   const uint32_t lane = lane_id();
   const uint32_t n = W.n;
-  bool init = false;
-  for (uint32_t a = 0; a < known; ++a) {
-    if (__ldcg(P.fixlev + a) < k) continue;
-    if (!init) {
-      for (uint32_t x = lane; x < n; x += 32) W.dsu[x] = x;
-      __syncwarp();
-      init = true;
+  WideHdr* H = P.H;
+  uint32_t r = kNone;
+  if (lane == 0 && *(volatile int32_t*)&H->orb_level == (int32_t)li) {
+    const uint32_t merged = *(volatile uint32_t*)&H->orb_known;
+    __threadfence();
+    const uint32_t x = wide_find(P.orb, v, n);
+    if (x < v || merged >= known) r = x;
+  }
+  r = __shfl_sync(GCL_FULL, r, 0);
+  if (r != kNone) return r;
+  if (!wide_lock(&H->orb_lock)) {
+    *ok = false;
+    return v;
+  }
+  if (*(volatile int32_t*)&H->orb_level != (int32_t)li) {
+    for (uint32_t x = lane; x < n; x += 32) P.orb[x] = x;
+    __threadfence();
+    __syncwarp();
+    if (lane == 0) {
+      H->orb_known = 0;
+      __threadfence();
+      *(volatile int32_t*)&H->orb_level = (int32_t)li;
     }
+    __syncwarp();
+  }
+  uint32_t from = *(volatile uint32_t*)&H->orb_known;
+  uint32_t* own = W.dsu;
+  __syncwarp();
+  if (lane == 0) W.dsu = P.orb;
+  __syncwarp();
+  for (uint32_t a = from; a < known; ++a) {
+    if (__ldcg(P.fixlev + a) < k) continue;
     if (!sp_dsu_apply<true>(P.auts + (uint64_t)a * stride, n)) {
       *ok = false;
-      return v;
+      break;
     }
   }
-  if (!init) return v;
-  return sp_find(W.dsu, v, n);
+  __syncwarp();
+  if (lane == 0) W.dsu = own;
+  __threadfence();
+  __syncwarp();
+  if (lane == 0) {
+    if (*ok && known > from) H->orb_known = known;
+    r = wide_find(P.orb, v, n);
+  }
+  r = __shfl_sync(GCL_FULL, r, 0);
+  wide_unlock(&H->orb_lock);
+  return r;
 }
 
 // Append aut[label[j]] = elem[j] to the store with its fixed-prefix length.
@@ -343,48 +424,57 @@ __device__ __noinline__ void wide_store_aut(const WidePtrs& P, const uint32_t* l
   __syncwarp();
 }
 
-__device__ __noinline__ bool wide_lock(WideHdr* H) {
-  uint32_t got = 0;
-  if (lane_id() == 0) {
-    for (uint32_t i = 0; i < kWideSpinLimit; ++i) {
-      if (atomicCAS(&H->lock, 0u, 1u) == 0u) {
-        got = 1;
-        break;
-      }
-      __nanosleep(64);
-    }
-    __threadfence();
-  }
-  return __shfl_sync(GCL_FULL, got, 0) != 0;
-}
-
-__device__ __noinline__ void wide_unlock(WideHdr* H) {
-  __threadfence();
-  __syncwarp();
-  if (lane_id() == 0) atomicExch(&H->lock, 0u);
-  __syncwarp();
-}
-
 struct WideBest {
   int canon_level;
   uint32_t best_seqlen;
-  uint32_t version;
+  uint32_t version;  // even; 0 = the first leaf
 };
 
-// Copy the shared best leaf into the warp's private copy (lock held).
-__device__ __noinline__ WideBest wide_adopt(const WidePtrs& P, int64_t m) {
+// Copy the shared best leaf into the warp's private copy.  The shared record
+// is a sequence lock: its version is odd while a writer (holding the best
+// lock) rewrites it, so a copy taken between two equal even versions is
+// whole.  After repeated collisions the copy is taken under the lock.
+__device__ __noinline__ bool wide_adopt(const WidePtrs& P, int64_t m, WideBest* out) {
   SpWarp& W = sp_w();
   const uint32_t lane = lane_id();
-  WideBest b;
-  b.canon_level = (int)*(volatile uint32_t*)&P.H->best_level;
-  b.best_seqlen = *(volatile uint32_t*)&P.H->best_seqlen;
-  b.version = *(volatile uint32_t*)&P.H->version;
-  for (uint32_t i = lane; i <= (uint32_t)b.canon_level; i += 32) W.ccode[i] = __ldcg(P.bcode + i);
-  for (uint32_t i = lane; i < W.n; i += 32) W.blabel[i] = __ldcg(P.blabel + i);
-  for (uint32_t i = lane; i < b.best_seqlen; i += 32) W.bseq[i] = __ldcg(P.bseq + i);
-  for (int64_t i = lane; i < m; i += 32) W.bcert[i] = __ldcg(P.bcert + i);
-  __syncwarp();
-  return b;
+  WideHdr* H = P.H;
+  for (int attempt = 0; attempt < 66; ++attempt) {
+    const bool locked = attempt == 65;
+    if (locked && !wide_lock(&H->lock)) return false;
+    uint32_t v1 = 0, lvl = 0, sl = 0;
+    if (lane == 0) {
+      v1 = *(volatile uint32_t*)&H->version;
+      __threadfence();
+      lvl = *(volatile uint32_t*)&H->best_level;
+      sl = *(volatile uint32_t*)&H->best_seqlen;
+      __threadfence();
+    }
+    v1 = __shfl_sync(GCL_FULL, v1, 0);
+    lvl = __shfl_sync(GCL_FULL, lvl, 0);
+    sl = __shfl_sync(GCL_FULL, sl, 0);
+    if ((v1 & 1u) && !locked) {
+      if (lane == 0) __nanosleep(256);
+      __syncwarp();
+      continue;
+    }
+    for (uint32_t i = lane; i <= lvl; i += 32) W.ccode[i] = __ldcg(P.bcode + i);
+    for (uint32_t i = lane; i < W.n; i += 32) W.blabel[i] = __ldcg(P.blabel + i);
+    for (uint32_t i = lane; i < sl; i += 32) W.bseq[i] = __ldcg(P.bseq + i);
+    for (int64_t i = lane; i < m; i += 32) W.bcert[i] = __ldcg(P.bcert + i);
+    __threadfence();
+    __syncwarp();
+    uint32_t v2 = 0;
+    if (lane == 0) v2 = *(volatile uint32_t*)&H->version;
+    v2 = __shfl_sync(GCL_FULL, v2, 0);
+    if (locked) wide_unlock(&H->lock);
+    if (v1 == v2 || locked) {
+      out->canon_level = (int)lvl;
+      out->best_seqlen = sl;
+      out->version = v1;
+      return true;
+    }
+  }
+  return false;
 }
 
 // The path's comparison state against the private best: the first level
@@ -419,58 +509,94 @@ __device__ __noinline__ void wide_recompare(uint32_t Lp, int canon_level, int* e
   __syncwarp();
 }
 
-// Publish a leaf that beats the private best (lock held by the caller).
-// Returns 1 if it became the shared best, 0 if the shared best was kept
-// (and adopted; an equal shared leaf also yields an automorphism).
-__device__ __noinline__ int wide_publish(const WidePtrs& P, const WideArgs& A, uint32_t Lv,
-                                         uint32_t seqlen, WideBest* nb) {
+// The current leaf (level Lv) against the private best: trail of codes, then
+// the level (a shorter trail ends in the sentinel and wins), then the upper
+// triangle.
+__device__ __noinline__ int wide_cmp_private(uint32_t Lv, int canon_level) {
   SpWarp& W = sp_w();
   const uint32_t lane = lane_id();
-  const uint32_t gl = *(volatile uint32_t*)&P.H->best_level;
-  const uint32_t lim = min(Lv, gl);
-  int cmp = 0;
+  const uint32_t lim = min(Lv, (uint32_t)canon_level);
   for (uint32_t j0 = 0; j0 < lim; j0 += 32) {
     const uint32_t j = j0 + lane;
-    const int32_t pc = j < lim ? W.pathcode[j] : 0;
-    const int32_t gc = j < lim ? __ldcg(P.bcode + j) : 0;
-    const uint32_t b = __ballot_sync(GCL_FULL, j < lim && pc != gc);
+    const int32_t pc = j < lim ? W.pathcode[j] : 0, bc = j < lim ? W.ccode[j] : 0;
+    const uint32_t b = __ballot_sync(GCL_FULL, j < lim && pc != bc);
     if (b) {
       const int src = __ffs(b) - 1;
-      const int32_t a = __shfl_sync(GCL_FULL, pc, src), c = __shfl_sync(GCL_FULL, gc, src);
-      cmp = a < c ? -1 : 1;
-      break;
+      const int32_t x = __shfl_sync(GCL_FULL, pc, src), y = __shfl_sync(GCL_FULL, bc, src);
+      return x < y ? -1 : 1;
     }
   }
-  if (cmp == 0) {
-    if (Lv < gl)
-      cmp = 1;
-    else if (Lv > gl)
-      cmp = -1;
-    else
-      cmp = sp_cmp_leaf<true>(W.ccert, P.blabel, P.bcert, true);
+  if ((int)Lv < canon_level) return 1;
+  if ((int)Lv > canon_level) return -1;
+  return sp_cmp_leaf(W.ccert, W.blabel, W.bcert, true);
+}
+
+// Make the current leaf, which beats the private best of version
+// `best.version`, the shared best.  Returns 1 when it was written, 0 when
+// the shared best had moved on (it is then adopted: the caller compares the
+// leaf again), -1 when the lock could not be taken.
+__device__ __noinline__ int wide_try_publish(const WidePtrs& P, const WideArgs& A, uint32_t Lv,
+                                             uint32_t seqlen, WideBest* best) {
+  SpWarp& W = sp_w();
+  const uint32_t lane = lane_id();
+  WideHdr* H = P.H;
+  if (!wide_lock(&H->lock)) return -1;
+  uint32_t cur = 0;
+  if (lane == 0) cur = *(volatile uint32_t*)&H->version;
+  cur = __shfl_sync(GCL_FULL, cur, 0);
+  if (cur != best->version) {
+    wide_unlock(&H->lock);
+    return wide_adopt(P, A.m, best) ? 0 : -1;
   }
-  if (cmp > 0) {
-    for (uint32_t i = lane; i < Lv; i += 32) P.bcode[i] = W.pathcode[i];
-    for (uint32_t i = lane; i < W.n; i += 32) P.blabel[i] = W.elem[i];
-    for (uint32_t i = lane; i < seqlen; i += 32) P.bseq[i] = W.seq[i];
-    for (int64_t i = lane; i < A.m; i += 32) P.bcert[i] = W.ccert[i];
-    __syncwarp();
-    uint32_t ver = 0;
-    if (lane == 0) {
-      P.bcode[Lv] = kSentinel;
-      P.H->best_level = Lv;
-      P.H->best_seqlen = seqlen;
-      ver = P.H->version + 1;
-      P.H->version = ver;
+  if (lane == 0) {
+    *(volatile uint32_t*)&H->version = cur + 1;  // odd: being rewritten
+    __threadfence();
+  }
+  __syncwarp();
+  for (uint32_t i = lane; i < Lv; i += 32) P.bcode[i] = W.pathcode[i];
+  for (uint32_t i = lane; i < W.n; i += 32) P.blabel[i] = W.elem[i];
+  for (uint32_t i = lane; i < seqlen; i += 32) P.bseq[i] = W.seq[i];
+  for (int64_t i = lane; i < A.m; i += 32) P.bcert[i] = W.ccert[i];
+  __threadfence();
+  __syncwarp();
+  if (lane == 0) {
+    P.bcode[Lv] = kSentinel;
+    H->best_level = Lv;
+    H->best_seqlen = seqlen;
+    __threadfence();
+    *(volatile uint32_t*)&H->version = cur + 2;
+  }
+  wide_unlock(&H->lock);
+  best->version = cur + 2;
+  best->canon_level = (int)Lv;
+  best->best_seqlen = seqlen;
+  return 1;
+}
+
+// Wait until `need` items have finished: a level's items start once every
+// item of the deeper levels is done, so their automorphisms prune the level
+// as they do in the sequential order.  The items being waited for are held
+// by running warps of the same grid; the wait ends with the time budget or a
+// recorded error at the latest.
+__device__ __noinline__ int32_t wide_gate(WideHdr* H, uint32_t need, uint64_t deadline) {
+  int32_t st = kOk;
+  if (lane_id() == 0) {
+    for (uint32_t i = 0;; ++i) {
+      if (*(volatile uint32_t*)&H->done >= need) break;
+      const int32_t hs = *(volatile int32_t*)&H->status;
+      if (hs != kOk) {
+        st = hs;
+        break;
+      }
+      if (i >= kWideGateSpinLimit || (deadline && (i & 63u) == 0 && global_ns() > deadline)) {
+        st = kTimeout;
+        break;
+      }
+      __nanosleep(1000);
     }
-    nb->version = __shfl_sync(GCL_FULL, ver, 0);
-    nb->canon_level = (int)Lv;
-    nb->best_seqlen = seqlen;
-    return 1;
+    __threadfence();
   }
-  if (cmp == 0) wide_store_aut<true>(P, P.blabel, A.WL.cap, A.WL.stride, P.H->D);
-  *nb = wide_adopt(P, A.m);
-  return 0;
+  return __shfl_sync(GCL_FULL, st, 0);
 }
 
 __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
@@ -536,17 +662,26 @@ __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
     const uint32_t k = D - 2 - lo;  // parent node level k+1, its target cell index k
     const uint32_t tf = P.tcfirst[k], tl = P.tclen[k];
     const uint32_t v = P.lelem[tf + 1 + (it - P.cum[lo])];
-    (void)tl;
-    known = wide_ready_prefix(P, known, cap);
-    if (known) {
-      bool ok = true;
-      const uint32_t r = wide_orbit_min(P, v, k, known, A.WL.stride, &ok);
-      if (!ok) {
-        status = kInternal;
+    {
+      const int32_t gs = wide_gate(H, P.cum[lo], deadline);
+      if (gs != kOk) {
+        status = gs;
         break;
       }
-      if (r != v) continue;  // an equivalent sibling is covered by its orbit's least vertex
     }
+    known = wide_ready_prefix(P, known, cap);
+    bool skip = false;
+    if (known) {
+      bool ok = true;
+      const uint32_t r = wide_orbit_min(P, v, lo, k, known, A.WL.stride, &ok);
+      if (!ok) {
+        status = kTimeout;
+        break;
+      }
+      skip = r != v;  // an equivalent sibling is covered by its orbit's least vertex
+    }
+    do {
+    if (skip) break;
     // the parent node: the first leaf backtracked to level k+1
     for (uint32_t i = lane; i < n; i += 32) {
       const uint32_t e = P.lelem[i];
@@ -579,13 +714,9 @@ __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
     }
     __syncwarp();
     // private best: refresh when the shared one has changed
-    if (*(volatile uint32_t*)&H->version != best.version) {
-      if (!wide_lock(H)) {
-        status = kTimeout;
-        break;
-      }
-      best = wide_adopt(P, A.m);
-      wide_unlock(H);
+    if (*(volatile uint32_t*)&H->version != best.version && !wide_adopt(P, A.m, &best)) {
+      status = kTimeout;
+      break;
     }
     bool best_local = best.version == 0;  // the first leaf anchors gca jumps
     uint32_t eqlevfirst = k + 1, seqlen = k, level = k + 1;
@@ -665,28 +796,39 @@ __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
           const int gg = best_local ? sp_gca(W.bseq, best.best_seqlen, seqlen) : -1;
           bt = gg >= 0 ? gg : (int)Lv - 1;
         } else if (dec == 3) {
-          if (!wide_lock(H)) {
-            status = kTimeout;
-            break;
+          // the leaf beats the private best: it becomes the shared best
+          // unless the shared best has moved on, in which case that one is
+          // adopted and the leaf compared again
+          int res = 0;
+          for (int tries = 0; tries < 64 && res == 0; ++tries) {
+            const int r = wide_try_publish(P, A, Lv, seqlen, &best);
+            if (r != 0) {
+              res = r;
+              break;
+            }
+            const int c = wide_cmp_private(Lv, best.canon_level);
+            if (c < 0) res = 4;
+            if (c == 0) res = 2;
           }
-          WideBest nb;
-          const int r = wide_publish(P, A, Lv, seqlen, &nb);
-          wide_unlock(H);
-          if (r == 1) {
+          if (res == 1) {
             // the leaf is the new shared best and the private one
             sp_copy_u32(W.bcert, W.ccert, (uint32_t)A.m);
             sp_copy_u32(W.blabel, W.elem, n);
             sp_copy_u32(W.bseq, W.seq, seqlen);
+            sp_copy_u32((uint32_t*)W.ccode, (const uint32_t*)W.pathcode, Lv);
             if (lane == 0) W.ccode[Lv] = kSentinel;
             __syncwarp();
-            best = nb;
             best_local = true;
             eqlevcanon = (int)Lv;
             comp_canon = 0;
-          } else {
-            best = nb;
+          } else if (res == 2 || res == 4) {
+            // equivalent to, or worse than, the adopted best
+            if (res == 2) wide_store_aut<false>(P, W.blabel, cap, A.WL.stride, D);
             best_local = false;
             recompare = true;
+          } else {
+            status = kTimeout;
+            break;
           }
           bt = (int)Lv - 1;
         } else if (dec == 4) {
@@ -784,6 +926,11 @@ __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
         if (recompare) wide_recompare(level, best.canon_level, &eqlevcanon, &comp_canon);
       }
     }
+    } while (0);
+    if (status != kOk) break;
+    __syncwarp();
+    if (lane == 0) atomicAdd(&H->done, 1u);  // opens the next level's gate when it is the last
+    __syncwarp();
   }
   if (status != kOk) wide_fail(H, status);
   if (lane == 0) atomicAdd(&H->nodes, my_nodes);
