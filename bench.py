@@ -60,6 +60,14 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-serving", action="store_true")
+    p.add_argument("--serve-requests", type=int, default=6000)
+    p.add_argument("--serve-rate", type=float, default=2000.0,
+                   help="Poisson arrival rate of the serving run, requests/s")
+    p.add_argument("--serve-nmax", type=int, default=20000)
+    p.add_argument("--no-single", action="store_true")
+    p.add_argument("--no-mixed", action="store_true")
+    p.add_argument("--mixed-graphs", type=int, default=2000)
     return p.parse_args()
 
 
@@ -469,12 +477,134 @@ def gpu_arm(args):
                                 "kind": kind,
                                 "sample": f"{g_done} graphs (the {count}-graph batch repeated) "
                                           f"in {t_done:.1f} s on {pool.cores} processes"}
+    if rank == 0 and not args.no_serving:
+        line["serving"] = serving_block(args, pkg, local)
+    if rank == 0 and not args.no_single:
+        line["single_graph"] = single_graph_block(args, pkg, local, not args.no_cpu_baseline)
+    if rank == 0 and not args.no_mixed:
+        line["mixed_batch"] = mixed_block(args, pkg, local)
     if rank == 0:
         print(json.dumps(line))
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
     ctx.close()
+
+
+# --------------------------------------------------------------------------
+# Secondary workloads, reported beside the headline
+# --------------------------------------------------------------------------
+def serving_block(args, pkg, local):
+    """Open-loop Poisson stream through the serving loop (gcl_serve_replay),
+    then the plain form: the same requests one at a time, one launch each."""
+    G = pkg.graphs
+    W = G.serving_workload(args.serve_requests, args.serve_rate, seed=5000,
+                           n_max=args.serve_nmax)
+    arena = G.pack(W.graphs)
+    srv = pkg.Server(local)
+    # warm-up: a short replay of the first requests
+    k0 = min(300, len(W.kind))
+    srv.replay(arena, W.kind[:k0], W.g1[:k0], W.g2[:k0], W.arrival[:k0], timeout_s=600)
+    srv.close()
+    srv = pkg.Server(local)
+    t0 = time.perf_counter()
+    res = srv.replay(arena, W.kind, W.g1, W.g2, W.arrival, timeout_s=1800)
+    wall = time.perf_counter() - t0
+    st = srv.stats()
+    srv.close()
+    lat = np.array([r.latency_s for r in res]) * 1e3
+    ok = all(r.status == 0 for r in res)
+    ns = np.array([max(W.graphs[W.g1[i]].n, W.graphs[W.g2[i]].n) for i in range(len(res))])
+    big = ns > 2048
+    iso = W.kind == 1
+    block = {
+        "workload": (f"open-loop Poisson stream, {len(res)} requests at {args.serve_rate:.0f}/s; "
+                     f"sizes 90% n<=128, 9% 128<n<=2048, 1% 2048<n<={args.serve_nmax}; tree "
+                     f"(max deg 4) + 0-6 edges; 30% iso pairs (half relabelings), 20% of "
+                     f"canonizations relabeled repeats"),
+        "requests": len(res), "all_ok": ok, "wall_s": wall,
+        "throughput_req_s": len(res) / wall,
+        "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+        "p999_ms": float(np.percentile(lat, 99.9)), "max_ms": float(lat.max()),
+        "p50_ms_n_le_2048": float(np.percentile(lat[~big], 50)),
+        "p99_ms_n_le_2048": float(np.percentile(lat[~big], 99)),
+        "p50_ms_iso": float(np.percentile(lat[iso], 50)) if iso.any() else None,
+        "large_requests": int(big.sum()),
+        "batches": st["batches"], "graphs": st["graphs"], "memo_hits": st["memo_hits"],
+        "class_repeats": st["class_repeats"],
+    }
+    # plain form: one request at a time, gcl_canon_one per graph (a sample)
+    ctx = pkg.Context(local, wide_min_n=pkg.api.GCL_MAX_N + 1)
+    idx = [i for i in range(len(res)) if ns[i] <= 2048][:400]
+    ts = []
+    for i in idx[:20]:
+        pkg.canon(W.graphs[W.g1[i]], ctx=ctx)
+    for i in idx:
+        t = time.perf_counter()
+        pkg.canon(W.graphs[W.g1[i]], ctx=ctx)
+        if W.kind[i] == 1:
+            pkg.canon(W.graphs[W.g2[i]], ctx=ctx)
+        ts.append(time.perf_counter() - t)
+    ctx.close()
+    ts = np.array(ts) * 1e3
+    block["plain_one_per_launch"] = {
+        "sample": f"{len(idx)} requests with n <= 2048, one gcl_canon_one per graph, serially",
+        "p50_ms": float(np.percentile(ts, 50)), "p99_ms": float(np.percentile(ts, 99)),
+        "throughput_req_s": len(ts) / (ts.sum() / 1e3)}
+    return block
+
+
+def single_graph_block(args, pkg, local, with_cpu):
+    """Search-heavy single graphs through gcl_canon_one (the wide search),
+    each also under a random relabeling; the reference CPU path beside the
+    ones it finishes in seconds."""
+    G = pkg.graphs
+    rng = np.random.default_rng(2000)
+    cases = [("reg3_n1024", G.random_regular(1024, 3, rng), True),
+             ("reg3_n4096", G.random_regular(4096, 3, rng), False),
+             ("torus_32x32", G.torus(32), True), ("torus_64x64", G.torus(64), True)]
+    ctx = pkg.Context(local)
+    pkg.canon(G.from_edges(3, [(0, 1)]), ctx=ctx)
+    out = {}
+    O = None
+    if with_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O  # the reference's CPU path (checker / baseline)
+    for name, g, cpu in cases:
+        rel = G.random_relabel(g, rng)
+        pkg.canon(g, ctx=ctx)  # warm-up (workspace)
+        t = time.perf_counter()
+        a = pkg.canon(g, ctx=ctx)
+        t1 = time.perf_counter()
+        b = pkg.canon(rel, ctx=ctx)
+        t2 = time.perf_counter()
+        row = {"n": g.n, "gpu_ms": (t1 - t) * 1e3, "gpu_ms_relabeled": (t2 - t1) * 1e3,
+               "nodes": a.nodes, "relabel_invariant": bool(np.array_equal(a.matrix, b.matrix))}
+        if cpu and O is not None and O.available("reference"):
+            t = time.perf_counter()
+            m = O.canon(g, kind="reference")[0]
+            row["cpu_ref_ms"] = (time.perf_counter() - t) * 1e3
+            row["equal_to_cpu_ref"] = bool(np.array_equal(m, a.matrix))
+        out[name] = row
+    ctx.close()
+    return out
+
+
+def mixed_block(args, pkg, local):
+    """Mixed-size batch: n log-uniform in [64, 4096], four families."""
+    G = pkg.graphs
+    gs = G.mixed_batch(args.mixed_graphs, seed=4000)
+    arena = G.pack(gs)
+    ctx = pkg.Context(local)
+    pkg.canon_batch(arena, ctx=ctx, dense=False, rows=True)
+    t = time.perf_counter()
+    r = pkg.canon_batch(arena, ctx=ctx, dense=False, rows=True)
+    dt = time.perf_counter() - t
+    ctx.close()
+    return {"workload": f"{arena.count} graphs, n log-uniform [64,4096], ER(deg 8) / "
+                        f"d-regular / tori / 2-4 copies of a regular component",
+            "seconds": dt, "graphs_per_s": arena.count / dt,
+            "all_ok": bool((r.status == 0).all()), "max_nodes": int(r.stats[:, 1].max())}
 
 
 def main():

@@ -6,6 +6,6 @@ the CUDA library's C ABI (``api``).
 """
 from . import graphs  # noqa: F401
 from .api import (  # noqa: F401
-    BatchResult, CanonResult, Context, GclError, Nauty_Parallel, canon, canon_batch,
+    BatchResult, CanonResult, Context, GclError, Nauty_Parallel, Server, canon, canon_batch,
     default_context, is_isomorphic, load_library,
 )

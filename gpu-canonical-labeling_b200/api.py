@@ -38,6 +38,8 @@ EXPORTS = [
     "gcl_status_string", "gcl_version", "gcl_create", "gcl_destroy", "gcl_stream",
     "gcl_canon_one", "gcl_canon_batch", "gcl_canon_batch_device_async", "gcl_sync", "gcl_iso",
     "gcl_canon_batch_noalloc", "gcl_set_option", "gcl_canon_wide_device_async",
+    "gcl_serve_create", "gcl_serve_destroy", "gcl_serve_submit", "gcl_serve_poll",
+    "gcl_serve_stats_get", "gcl_serve_replay",
 ]
 
 GCL_OPT_WIDE_MIN_N = 1
@@ -254,3 +256,131 @@ def is_isomorphic(g1: Graph, g2: Graph, max_aut: int = 10000,
                          _ptr(b[1]), _ptr(b[2]), g2.n, max_aut, ctypes.byref(v))
     _check(rc, "gcl_iso")
     return bool(v.value)
+
+
+# ---------------------------------------------------------------------------
+# Serving (gcl_serve_*): continuous batching over several device contexts.
+# ---------------------------------------------------------------------------
+
+REQ_CANON = 0
+REQ_ISO = 1
+
+
+class ServeConfig(ctypes.Structure):
+    _fields_ = [("lanes", ctypes.c_int), ("mid_lanes", ctypes.c_int),
+                ("large_lanes", ctypes.c_int), ("max_batch", ctypes.c_int),
+                ("mid_n", ctypes.c_int), ("large_n", ctypes.c_int), ("max_aut", ctypes.c_int),
+                ("lane_bytes", ctypes.c_int64), ("table_slots", ctypes.c_int64),
+                ("store_bytes", ctypes.c_int64), ("memo_bytes", ctypes.c_int64)]
+
+
+class ServeResult(ctypes.Structure):
+    _fields_ = [("id", ctypes.c_int64), ("status", ctypes.c_int32), ("verdict", ctypes.c_int32),
+                ("repeat", ctypes.c_int32), ("batch", ctypes.c_int32),
+                ("class_id", ctypes.c_int64), ("canon_hash", ctypes.c_uint64),
+                ("latency_s", ctypes.c_double)]
+
+
+class ServeStats(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_int64) for k in ("submitted", "completed", "batches", "graphs",
+                                              "memo_hits", "class_repeats", "classes",
+                                              "large_graphs")]
+
+
+def _serve_sigs(lib):
+    if getattr(lib, "_serve_sigs", False):
+        return
+    lib.gcl_serve_create.argtypes = [ctypes.c_int, ctypes.POINTER(ServeConfig), ctypes.POINTER(_P)]
+    lib.gcl_serve_destroy.argtypes = [_P]
+    lib.gcl_serve_submit.argtypes = [_P, ctypes.c_int64, ctypes.c_int, _P, _P, _P, ctypes.c_int,
+                                     _P, _P, _P, ctypes.c_int, _P, _P]
+    lib.gcl_serve_poll.argtypes = [_P, ctypes.POINTER(ServeResult), ctypes.c_int, ctypes.c_int]
+    lib.gcl_serve_stats_get.argtypes = [_P, ctypes.POINTER(ServeStats)]
+    lib.gcl_serve_replay.argtypes = [_P, ctypes.c_int, _P, _P, _P, _P, ctypes.c_int, _P, _P, _P,
+                                     _P, _P, ctypes.c_double, ctypes.POINTER(ServeResult)]
+    for name in ("gcl_serve_create", "gcl_serve_destroy", "gcl_serve_submit", "gcl_serve_poll",
+                 "gcl_serve_stats_get", "gcl_serve_replay"):
+        getattr(lib, name).restype = ctypes.c_int
+    lib._serve_sigs = True
+
+
+class Server:
+    """A request loop on one GPU (gcl_serve_create): submit canonization and
+    isomorphism requests as they arrive, poll finished results."""
+
+    def __init__(self, device: int = 0, **cfg):
+        self.lib = load_library()
+        _serve_sigs(self.lib)
+        c = ServeConfig()
+        for k, v in cfg.items():
+            setattr(c, k, v)
+        h = _P()
+        _check(self.lib.gcl_serve_create(device, ctypes.byref(c), ctypes.byref(h)),
+               "gcl_serve_create")
+        self.handle = h
+        self._keep = {}  # output buffers of requests in flight, by id
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.gcl_serve_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit_canon(self, rid: int, g: Graph, want_form: bool = True):
+        rp, cl, co = _csr(g)
+        rows = np.zeros(max(g.n * ((g.n + 63) // 64), 1), np.uint64) if want_form else None
+        lab = np.zeros(max(g.n, 1), np.int32) if want_form else None
+        self._keep[rid] = (rows, lab, g.n)
+        rc = self.lib.gcl_serve_submit(self.handle, rid, REQ_CANON, _ptr(rp), _ptr(cl), _ptr(co),
+                                       g.n, None, None, None, 0, _ptr(rows), _ptr(lab))
+        _check(rc, "gcl_serve_submit")
+
+    def submit_iso(self, rid: int, g1: Graph, g2: Graph):
+        a, b = _csr(g1), _csr(g2)
+        rc = self.lib.gcl_serve_submit(self.handle, rid, REQ_ISO, _ptr(a[0]), _ptr(a[1]),
+                                       _ptr(a[2]), g1.n, _ptr(b[0]), _ptr(b[1]), _ptr(b[2]),
+                                       g2.n, None, None)
+        _check(rc, "gcl_serve_submit")
+
+    def poll(self, max_results: int = 1024, timeout_ms: int = 10):
+        """[(result, rows, label)] for finished requests; rows/label are the
+        packed canonical form and labeling of canonization requests."""
+        buf = (ServeResult * max_results)()
+        k = self.lib.gcl_serve_poll(self.handle, buf, max_results, timeout_ms)
+        if k < 0:
+            _check(k, "gcl_serve_poll")
+        out = []
+        for i in range(k):
+            r = buf[i]
+            rows, lab, n = self._keep.pop(r.id, (None, None, 0))
+            out.append((r, None if rows is None else rows[: n * ((n + 63) // 64)],
+                        None if lab is None else lab[:n]))
+        return out
+
+    def stats(self) -> dict:
+        s = ServeStats()
+        _check(self.lib.gcl_serve_stats_get(self.handle, ctypes.byref(s)), "gcl_serve_stats_get")
+        return {k: int(getattr(s, k)) for k, _ in ServeStats._fields_}
+
+    def replay(self, arena: Arena, kind, g1, g2, arrival_s, timeout_s: float = 600.0):
+        """Open-loop load (gcl_serve_replay): request i is submitted at
+        arrival_s[i]; returns the results in request order (latency from the
+        scheduled arrival)."""
+        nreq = len(kind)
+        kind = np.ascontiguousarray(kind, np.int32)
+        g1 = np.ascontiguousarray(g1, np.int32)
+        g2 = np.ascontiguousarray(g2, np.int32)
+        arr = np.ascontiguousarray(arrival_s, np.float64)
+        res = (ServeResult * max(nreq, 1))()
+        col = arena.col if arena.col.size else np.zeros(1, np.int32)
+        color = arena.color if arena.color.any() else None
+        rc = self.lib.gcl_serve_replay(self.handle, nreq, _ptr(arr), _ptr(kind), _ptr(g1),
+                                       _ptr(g2), arena.count, _ptr(arena.voff), _ptr(arena.eoff),
+                                       _ptr(arena.rowptr), _ptr(col), _ptr(color), timeout_s, res)
+        _check(rc, "gcl_serve_replay")
+        return [res[i] for i in range(nreq)]

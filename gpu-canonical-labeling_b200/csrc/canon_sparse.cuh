@@ -46,11 +46,12 @@ struct SpTc {
 // Byte layout of one slot for graphs with at most n vertices and m2 CSR
 // entries, `pool` per-level representative arrays and `cap` ring slots.
 struct SpLayout {
-  uint64_t u32n[25];  // offsets of the n-sized u32 arrays
+  uint64_t u32n[26];  // offsets of the n-sized u32 arrays
   uint64_t fcode, ccode, pool_owner;
   uint64_t stb, sts, act, acts, tcb, tcbs;
   uint64_t fcert, bcert, ccert;
-  uint64_t tc, reps, auts;
+  uint64_t tc, reps, auts, ulog;
+  uint32_t ulog_cap;
   uint64_t bytes;
   uint32_t nw, nsw;
   uint32_t stride;  // elements per representative array / ring entry
@@ -67,7 +68,7 @@ __host__ __device__ inline SpLayout sp_layout(uint32_t n, uint64_t m2, uint32_t 
   };
   const uint64_t N1 = (uint64_t)n + 2;
   L.stride = (uint32_t)N1;
-  for (int i = 0; i < 25; ++i) L.u32n[i] = take(4 * N1);
+  for (int i = 0; i < 26; ++i) L.u32n[i] = take(4 * N1);
   L.fcode = take(4 * (N1 + 1));
   L.ccode = take(4 * (N1 + 1));
   L.pool_owner = take(4 * ((uint64_t)pool + 1));
@@ -85,6 +86,8 @@ __host__ __device__ inline SpLayout sp_layout(uint32_t n, uint64_t m2, uint32_t 
   L.tc = take(sizeof(SpTc) * N1);
   L.reps = take(4ull * pool * N1);
   L.auts = take(2ull * cap * N1);
+  L.ulog_cap = 5 * n + 64;
+  L.ulog = take(8ull * L.ulog_cap);
   L.bytes = o;
   return L;
 }
@@ -103,6 +106,8 @@ struct SpWarp {
   uint32_t *elem, *pos, *inlev, *cnt, *T, *Tc, *cellcnt, *off, *fill, *G, *tmp, *lst1, *lst2;
   uint32_t *seq, *fseq, *bseq, *flabel, *blabel, *dsu, *hist, *pre, *fpos, *bpos, *nsl;
   int32_t *fcode, *ccode, *pool_owner, *pathcode;
+  uint32_t *umark;  // per level: undo-log size when the level's child was made
+  uint2* ulog;      // undo log: {position | kStartFlag, previous in_level}
   uint64_t *stb, *sts, *act, *acts, *tcb, *tcbs;
   uint32_t *fcert, *bcert, *ccert, *reps;
   SpTc* tc;
@@ -112,6 +117,7 @@ struct SpWarp {
   uint32_t n, nw, nsw, stride;  // stride: elements per pool / ring entry
   uint32_t ncells, nact, ntouched, nl1, nl2, npend;
   uint32_t pool_top, pool_cap, aut_cap, max_aut;
+  uint32_t utop, ulog_cap, ulog_bad;
   // values the serial fold hands to the whole warp
   uint32_t lc, hint;
 };
@@ -204,6 +210,29 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
   uint32_t m;
   asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
   return m;
+}
+
+// ---- undo log of the partition's cell structure ----------------------------
+// Every change of a cell start or an in_level after the root refinement is
+// logged (by lane 0, in order), so backtracking undoes exactly the changes
+// made below the target level instead of rescanning the whole partition.
+// Vertex order inside cells is not restored: only cells as sets matter.
+constexpr uint32_t kStartFlag = 0x80000000u;
+
+__device__ __forceinline__ void ulog_push(SpWarp& W, uint32_t x, uint32_t old) {
+  if (W.utop < W.ulog_cap)
+    W.ulog[W.utop++] = make_uint2(x, old);
+  else
+    W.ulog_bad = 1;  // full: backtracks rescan the partition
+}
+// lane 0: in_level write / new cell start, logged
+__device__ __forceinline__ void set_inlev(SpWarp& W, uint32_t p, uint32_t v) {
+  ulog_push(W, p, W.inlev[p]);
+  W.inlev[p] = v;
+}
+__device__ __forceinline__ void add_start(SpWarp& W, uint32_t p) {
+  ulog_push(W, p | kStartFlag, 0u);
+  bm_set1(W.stb, W.sts, p);
 }
 
 // ---------------------------------------------------------------------------
@@ -392,9 +421,9 @@ __device__ __noinline__ int sp_refine(uint32_t level) {
         const bool was = bm_test(W.act, cmin);
         __syncwarp();
         if (lane == 0) {
-          W.inlev[pp] = W.inlev[cmin];
-          W.inlev[cmin] = lvl1;
-          bm_set1(W.stb, W.sts, pp);
+          set_inlev(W, pp, W.inlev[cmin]);
+          set_inlev(W, cmin, lvl1);
+          add_start(W, pp);
           W.ncells += 1;
           const uint32_t nb = kk, nn = LL - kk;
           if (was || nb >= nn) {
@@ -480,9 +509,9 @@ __device__ __noinline__ int sp_refine(uint32_t level) {
           lc = mash(lc, p - 1);
           const bool was = bm_test(W.act, c);
           if (lane == 0) {
-            W.inlev[p] = W.inlev[c];
-            W.inlev[c] = lvl1;
-            bm_set1(W.stb, W.sts, p);
+            set_inlev(W, p, W.inlev[c]);
+            set_inlev(W, c, lvl1);
+            add_start(W, p);
             W.ncells += 1;
             const uint32_t nb = k, nn = L - k;
             if (was || nb >= nn) {
@@ -564,7 +593,7 @@ __device__ __noinline__ int sp_refine(uint32_t level) {
             uint32_t maxsz = 0, maxf = c, lastf = c, nfr = 0;
             if (L > k) {  // untouched fragment first
               lc = mash(lc, 0u + c);
-              W.inlev[c] = lvl1;
+              set_inlev(W, c, lvl1);
               maxsz = L - k;
               nfr = 1;
             }
@@ -573,7 +602,7 @@ __device__ __noinline__ int sp_refine(uint32_t level) {
               const uint32_t sz = W.hist[i];
               if (!sz) continue;
               lc = mash(lc, mn + i + f);
-              W.inlev[f] = lvl1;
+              set_inlev(W, f, lvl1);
               if (f != c) {
                 W.fpos[W.npend++] = f;  // set after the fold: the fold walks the old starts
                 W.ncells += 1;
@@ -601,7 +630,7 @@ __device__ __noinline__ int sp_refine(uint32_t level) {
                 W.nact -= 1;
               }
             }
-            W.inlev[lastf] = oldlev;
+            set_inlev(W, lastf, oldlev);
             W.lc = lc;
             W.hint = hint;
           }
@@ -614,7 +643,7 @@ __device__ __noinline__ int sp_refine(uint32_t level) {
     // new starts of the non-singleton fold
     __syncwarp();
     if (lane == 0) {
-      for (uint32_t i = 0; i < W.npend; ++i) bm_set1(W.stb, W.sts, W.fpos[i]);
+      for (uint32_t i = 0; i < W.npend; ++i) add_start(W, W.fpos[i]);
       W.npend = 0;
     }
     // reset per-step scratch
@@ -647,15 +676,16 @@ __device__ __noinline__ bool sp_individualize(uint32_t level, uint32_t v, uint32
   if (e - t <= 1) return false;
   __syncwarp();
   if (lane == 0) {
+    W.umark[level] = W.utop;  // backtracking to `level` undoes from here
     const uint32_t p = W.pos[v], x = W.elem[t];
     W.elem[p] = x;
     W.pos[x] = p;
     W.elem[t] = v;
     W.pos[v] = t;
-    bm_set1(W.stb, W.sts, t + 1);
+    add_start(W, t + 1);
     W.ncells += 1;
-    W.inlev[t + 1] = W.inlev[t];
-    W.inlev[t] = level + 1;
+    set_inlev(W, t + 1, W.inlev[t]);
+    set_inlev(W, t, level + 1);
     bm_set1(W.act, W.acts, t);
     W.nact = 1;
   }
@@ -793,6 +823,61 @@ __device__ __noinline__ bool sp_backtrack(uint32_t Lv) {
   __syncwarp();
   bm_resummarize(W.stb, W.sts, nw, W.nsw);
   if (lane == 0) W.ncells -= removed;
+  __syncwarp();
+  return true;
+}
+
+// Backtrack to node level Lv by undoing the logged changes made since that
+// node's child was created: the same cells as reconstruct_at_level.  Every
+// start created below Lv is cleared, and every in_level changed below Lv
+// returns to the value before its first change (entries are processed in
+// parallel: per position the earliest entry wins).
+__device__ __noinline__ bool sp_backtrack_log(uint32_t Lv) {
+  SpWarp& W = sp_w();
+  const uint32_t lane = lane_id();
+  if (W.ulog_bad) {
+    const bool ok = sp_backtrack(Lv);
+    __syncwarp();
+    return ok;
+  }
+  const uint32_t lo = W.umark[Lv], hi = W.utop;
+  if (lo > hi) return false;
+  for (uint32_t i = lo + lane; i < hi; i += 32) {
+    const uint2 e = W.ulog[i];
+    if (!(e.x & kStartFlag)) W.tmp[e.x] = 0xffffffffu;
+  }
+  __syncwarp();
+  for (uint32_t i = lo + lane; i < hi; i += 32) {
+    const uint2 e = W.ulog[i];
+    if (!(e.x & kStartFlag)) atomicMin(&W.tmp[e.x], i);
+  }
+  __syncwarp();
+  uint32_t removed = 0;
+  for (uint32_t i = lo + lane; i < hi; i += 32) {
+    const uint2 e = W.ulog[i];
+    if (e.x & kStartFlag) {
+      const uint32_t p = e.x & ~kStartFlag;
+      atomicAnd((unsigned long long*)&W.stb[p >> 6], (unsigned long long)~bit64(p & 63));
+      ++removed;
+    } else if (W.tmp[e.x] == i) {
+      W.inlev[e.x] = e.y;
+    }
+  }
+  __syncwarp();
+  for (uint32_t i = lo + lane; i < hi; i += 32) {
+    const uint2 e = W.ulog[i];
+    if (e.x & kStartFlag) {
+      const uint32_t w = (e.x & ~kStartFlag) >> 6;
+      if (W.stb[w] == 0)
+        atomicAnd((unsigned long long*)&W.sts[w >> 6], (unsigned long long)~bit64(w & 63));
+    }
+  }
+  removed = __reduce_add_sync(GCL_FULL, removed);
+  __syncwarp();
+  if (lane == 0) {
+    W.ncells -= removed;
+    W.utop = lo;
+  }
   __syncwarp();
   return true;
 }
@@ -936,19 +1021,22 @@ __device__ __forceinline__ uint32_t sp_find(volatile uint32_t* d, uint32_t x, ui
   return x;
 }
 
-// Merge the cycles of permutation pm into the min-root union-find W.dsu:
-// hook the larger root under the smaller one, then shortcut every vertex to
-// its root, until a round changes nothing (compute_orbits_fast's DSU,
-// perm_group.cpp:60-116).  False if the rounds do not converge.
+// Merge the cycles of permutation pm on the `count` vertices members[] into
+// the min-root union-find W.dsu: hook the larger root under the smaller
+// one, then shortcut every member to its root, until a round changes
+// nothing (compute_orbits_fast's DSU, perm_group.cpp:60-116).  pm must map
+// the member set onto itself.  False if the rounds do not converge.
 template <bool kCg>
-__device__ __noinline__ bool sp_dsu_apply(const uint16_t* pm, uint32_t n) {
+__device__ __noinline__ bool sp_dsu_apply(const uint16_t* pm, const uint32_t* members,
+                                          uint32_t count, uint32_t n) {
   SpWarp& W = sp_w();
   const uint32_t lane = lane_id();
   volatile uint32_t* dsu = W.dsu;
   for (uint32_t round = 0;; ++round) {
-    if (round > n + 1) return false;
+    if (round > count + 1) return false;
     bool changed = false;
-    for (uint32_t v = lane; v < n; v += 32) {
+    for (uint32_t i = lane; i < count; i += 32) {
+      const uint32_t v = members[i];
       const uint32_t img = ldx<kCg>(pm + v);
       if (img == v) continue;
       const uint32_t a = sp_find(dsu, v, n), b = sp_find(dsu, img, n);
@@ -958,13 +1046,21 @@ __device__ __noinline__ bool sp_dsu_apply(const uint16_t* pm, uint32_t n) {
       }
     }
     __syncwarp();
-    for (uint32_t v = lane; v < n; v += 32) atomicMin((uint32_t*)&dsu[v], sp_find(dsu, v, n));
+    for (uint32_t i = lane; i < count; i += 32) {
+      const uint32_t v = members[i];
+      atomicMin((uint32_t*)&dsu[v], sp_find(dsu, v, n));
+    }
     __syncwarp();
     if (!__any_sync(GCL_FULL, changed)) return true;
   }
 }
 
-// subgroup_fixing_sequence + compute_orbits_fast (perm_group.cpp:5-116)
+// subgroup_fixing_sequence + compute_orbits_fast (perm_group.cpp:5-116).
+// The reference unites v with aut[v] over all vertices; an automorphism that
+// fixes the sequence maps the node's partition onto itself, cell by cell, so
+// the orbits that meet the target cell lie inside it and are found by
+// uniting over the cell's members alone (O(cell) per automorphism instead of
+// O(n)); the least vertex of each orbit -- the representative -- is the same.
 template <bool kCg = false>
 __device__ __noinline__ bool sp_orbits(int idx, int num_aut, uint32_t seqlen) {
   SpWarp& W = sp_w();
@@ -972,28 +1068,68 @@ __device__ __noinline__ bool sp_orbits(int idx, int num_aut, uint32_t seqlen) {
   const uint32_t n = W.n;
   SpTc t = W.tc[idx];
   const int limit = num_aut < (int)W.max_aut ? num_aut : (int)W.max_aut;
-  int from = t.last == -1 ? 0 : t.last;
+  const int from = t.last == -1 ? 0 : t.last;
   volatile uint32_t* dsu = W.dsu;
   const uint32_t* reps = t.rslot >= 0 ? W.reps + (uint64_t)t.rslot * W.stride : nullptr;
-  for (uint32_t v = lane; v < n; v += 32) dsu[v] = v;
-  __syncwarp();
-  if (reps)
-    for (uint32_t q = t.first + lane; q < t.first + t.len; q += 32) {
-      const uint32_t v = W.elem[q];
-      dsu[v] = reps[v];
-    }
+  const uint32_t* mem = W.elem + t.first;
+  for (uint32_t i = lane; i < t.len; i += 32) {
+    const uint32_t v = mem[i];
+    dsu[v] = reps ? reps[v] : v;
+  }
   __syncwarp();
   bool any = false;
-  for (int i = from; i < limit; ++i) {
-    const uint16_t* pm = W.auts + (uint64_t)i * W.stride;
-    bool bad = false;
-    for (uint32_t j = lane; j < seqlen; j += 32) {
-      const uint32_t sv = W.seq[j];
-      if (ldx<kCg>(pm + sv) != sv) bad = true;
+  // the store entries that fix the sequence, 32 at a time (one per lane),
+  // each batch merged in one union-find pass over (entry, member) pairs
+  for (int base = from; base < limit; base += 32) {
+    const int a = base + (int)lane;
+    bool fix = a < limit;
+    const uint16_t* pa = W.auts + (uint64_t)(fix ? a : 0) * W.stride;
+    // eight independent loads per round: one memory latency per eight entries
+    for (uint32_t j0 = 0; fix && j0 < seqlen; j0 += 8) {
+      uint32_t sv[8], im[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) sv[u] = j0 + u < seqlen ? W.seq[j0 + u] : 0u;
+#pragma unroll
+      for (int u = 0; u < 8; ++u) im[u] = j0 + u < seqlen ? ldx<kCg>(pa + sv[u]) : sv[u];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) fix = fix && im[u] == sv[u];
     }
-    if (__any_sync(GCL_FULL, bad)) continue;
+    const uint32_t fm = __ballot_sync(GCL_FULL, fix);
+    if (!fm) continue;
     any = true;
-    if (!sp_dsu_apply<kCg>(pm, n)) return false;
+    const uint32_t nf = (uint32_t)__popc(fm);
+    // the cell must map onto itself (a failed check is an internal error)
+    bool out = false;
+    for (uint32_t x = lane; x < nf * t.len; x += 32) {
+      const uint32_t which = (uint32_t)__fns(fm, 0, (int)(x / t.len) + 1);
+      const uint16_t* pm = W.auts + (uint64_t)(base + (int)which) * W.stride;
+      const uint32_t q = W.pos[ldx<kCg>(pm + mem[x % t.len])];
+      out |= q < t.first || q >= t.first + t.len;
+    }
+    if (__any_sync(GCL_FULL, out)) return false;
+    for (uint32_t round = 0;; ++round) {
+      if (round > t.len + 1) return false;
+      bool changed = false;
+      for (uint32_t x = lane; x < nf * t.len; x += 32) {
+        const uint32_t which = (uint32_t)__fns(fm, 0, (int)(x / t.len) + 1);
+        const uint16_t* pm = W.auts + (uint64_t)(base + (int)which) * W.stride;
+        const uint32_t v = mem[x % t.len];
+        const uint32_t img = ldx<kCg>(pm + v);
+        if (img == v) continue;
+        const uint32_t ra = sp_find(dsu, v, n), rb = sp_find(dsu, img, n);
+        if (ra != rb) {
+          atomicMin((uint32_t*)&dsu[max(ra, rb)], min(ra, rb));
+          changed = true;
+        }
+      }
+      __syncwarp();
+      for (uint32_t i = lane; i < t.len; i += 32) {
+        const uint32_t v = mem[i];
+        atomicMin((uint32_t*)&dsu[v], sp_find(dsu, v, n));
+      }
+      __syncwarp();
+      if (!__any_sync(GCL_FULL, changed)) break;
+    }
   }
   if (!any) return true;
   if (t.rslot < 0) {
@@ -1008,8 +1144,8 @@ __device__ __noinline__ bool sp_orbits(int idx, int num_aut, uint32_t seqlen) {
     __syncwarp();
   }
   uint32_t* rw = W.reps + (uint64_t)t.rslot * W.stride;
-  for (uint32_t q = t.first + lane; q < t.first + t.len; q += 32) {
-    const uint32_t v = W.elem[q];
+  for (uint32_t i = lane; i < t.len; i += 32) {
+    const uint32_t v = mem[i];
     rw[v] = sp_find(dsu, v, n);
   }
   __syncwarp();
@@ -1181,8 +1317,8 @@ __device__ __noinline__ void sp_bind(uint8_t* slot, const SpLayout& Lo, uint32_t
   SpWarp& W = sp_w();
   if (lane_id() != 0) return;
   // the n-sized u32 arrays
-  uint32_t* base[25];
-  for (int i = 0; i < 25; ++i) base[i] = (uint32_t*)(slot + Lo.u32n[i]);
+  uint32_t* base[26];
+  for (int i = 0; i < 26; ++i) base[i] = (uint32_t*)(slot + Lo.u32n[i]);
   W.elem = base[0];
   W.pos = base[1];
   W.inlev = base[2];
@@ -1208,6 +1344,11 @@ __device__ __noinline__ void sp_bind(uint8_t* slot, const SpLayout& Lo, uint32_t
   W.bpos = base[22];
   W.nsl = base[23];
   W.pathcode = (int32_t*)base[24];
+  W.umark = base[25];
+  W.ulog = (uint2*)(slot + Lo.ulog);
+  W.ulog_cap = Lo.ulog_cap;
+  W.utop = 0;
+  W.ulog_bad = 0;
   W.fcode = (int32_t*)(slot + Lo.fcode);
   W.ccode = (int32_t*)(slot + Lo.ccode);
   W.pool_owner = (int32_t*)(slot + Lo.pool_owner);
@@ -1301,7 +1442,10 @@ __device__ __noinline__ SpResult sp_search(const BatchArgs& A, int g, uint8_t* s
       }
       ++level;
       __syncwarp();
-      if (lane == 0) W.fcode[level - 1] = code;
+      if (lane == 0) {
+        W.fcode[level - 1] = code;
+        if (level == 1) W.utop = 0;  // the root partition is never undone
+      }
       __syncwarp();
       continue;
     }
@@ -1500,7 +1644,7 @@ __device__ __noinline__ SpResult sp_search(const BatchArgs& A, int g, uint8_t* s
         level = 0;
         continue;
       }
-      if (!sp_backtrack(Lv)) {
+      if (!sp_backtrack_log(Lv)) {
         status = kInternal;
         break;
       }

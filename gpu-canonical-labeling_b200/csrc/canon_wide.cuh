@@ -328,15 +328,17 @@ __device__ __forceinline__ uint32_t wide_find(const uint32_t* d, uint32_t x, uin
 
 // Least vertex of v's orbit under the stored automorphisms that fix the
 // first path's first k vertices (subgroup_fixing_sequence +
-// compute_orbits_fast, perm_group.cpp:5-116).  Only one level's items run at
+// compute_orbits_fast, perm_group.cpp:5-116), uniting over the members of
+// the level's target cell only (positions [tf, tf+tl) of the first leaf;
+// such automorphisms map the cell onto itself).  Only one level's items run at
 // a time, so one device-wide union-find serves them all: the first warp of a
 // level resets it, every warp merges the store entries that arrived since
 // the last merge, under the cache lock.  A root below v without the lock is
 // already a proof that v is not the least of its orbit (roots only move
 // down).  Sets *ok = false when a wait or a merge gives up.
 __device__ __noinline__ uint32_t wide_orbit_min(const WidePtrs& P, uint32_t v, uint32_t li,
-                                                uint32_t k, uint32_t known, uint32_t stride,
-                                                bool* ok) {
+                                                uint32_t k, uint32_t tf, uint32_t tl,
+                                                uint32_t known, uint32_t stride, bool* ok) {
   SpWarp& W = sp_w();
   const uint32_t lane = lane_id();
   const uint32_t n = W.n;
@@ -372,7 +374,7 @@ __device__ __noinline__ uint32_t wide_orbit_min(const WidePtrs& P, uint32_t v, u
   __syncwarp();
   for (uint32_t a = from; a < known; ++a) {
     if (__ldcg(P.fixlev + a) < k) continue;
-    if (!sp_dsu_apply<true>(P.auts + (uint64_t)a * stride, n)) {
+    if (!sp_dsu_apply<true>(P.auts + (uint64_t)a * stride, P.lelem + tf, tl, n)) {
       *ok = false;
       break;
     }
@@ -673,7 +675,7 @@ __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
     bool skip = false;
     if (known) {
       bool ok = true;
-      const uint32_t r = wide_orbit_min(P, v, lo, k, known, A.WL.stride, &ok);
+      const uint32_t r = wide_orbit_min(P, v, lo, k, tf, tl, known, A.WL.stride, &ok);
       if (!ok) {
         status = kTimeout;
         break;
@@ -698,6 +700,12 @@ __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
       status = kInternal;
       break;
     }
+    __syncwarp();
+    if (lane == 0) {  // the item's DFS logs its changes from here
+      W.utop = 0;
+      W.ulog_bad = 0;
+    }
+    __syncwarp();
     for (uint32_t i = lane; i < k; i += 32) W.seq[i] = P.fseq[i];
     for (uint32_t i = lane; i <= k; i += 32) W.pathcode[i] = P.fcode[i];
     __syncwarp();
@@ -907,7 +915,7 @@ __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
       if (bt >= 0) {
         const uint32_t Lv = (uint32_t)bt;
         if (Lv <= k + 1) break;  // the item's subtree is done
-        if (!sp_backtrack(Lv)) {
+        if (!sp_backtrack_log(Lv)) {
           status = kInternal;
           break;
         }

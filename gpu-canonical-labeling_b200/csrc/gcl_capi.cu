@@ -78,7 +78,7 @@ __global__ void __launch_bounds__(kOrderThreads)
 }
 
 constexpr int kSpSmemPerBlock = 200 * 1024;  // dynamic shared memory cap of one sparse block
-constexpr uint32_t kWidePool = 32;  // per-level orbit arrays of a wide-search warp
+constexpr uint32_t kWidePool = 64;  // per-level orbit arrays of a wide-search warp
 constexpr uint64_t kWideStoreBytes = 1ull << 30;  // automorphism store of a wide search
 constexpr uint32_t kSpPool = 8;     // per-level orbit arrays in the first sparse pass
 constexpr uint32_t kSpAutCap = 64;  // ring entries in the first sparse pass
@@ -192,6 +192,8 @@ struct gcl_context {
   // wide search of one graph: shared region and per-warp slots
   DevBuf wide_sh, wide_slots;
   int64_t wide_min_n = kW64MaxN + 1;
+  uint64_t workspace_bytes = 0;  // per-pass workspace cap, 0 = GCL_WORKSPACE_GB
+  int64_t wide_max_warps = 0;    // 0 = as many as fit
   DevBuf deferred, overflow_list, large_list, sp_fail_list, order;
   // staging for host-pointer calls
   DevBuf voff, eoff, rowptr, col, color, ooff, dense, roff, rows, label, stats, status;
@@ -214,6 +216,10 @@ static uint64_t workspace_budget() {
   double g = e ? std::atof(e) : 4.0;
   if (!(g > 0)) g = 4.0;
   return (uint64_t)(g * (1ull << 30));
+}
+
+static uint64_t ctx_workspace(const gcl_context* c) {
+  return c->workspace_bytes ? c->workspace_bytes : workspace_budget();
 }
 
 static int cuda_status(cudaError_t e) {
@@ -380,7 +386,7 @@ int gcl_canon_batch_device_async(gcl_context* c, int count, const int64_t* d_vof
     // the graphs that outgrew the first passes' orbit pool or ring
     const uint64_t m2max = (uint64_t)std::max<int64_t>(max_m2, 1);
     const uint32_t cap1 = std::min<uint32_t>(maut, kSpAutCap);
-    const uint64_t budget = workspace_budget();
+    const uint64_t budget = ctx_workspace(c);
     GCL_TRY(c->sp_fail_list.ensure((size_t)count * sizeof(int)));
     for (int bk = 0; bk < kSpBuckets; ++bk) {
       const uint32_t lo = bk == 0 ? (uint32_t)kW64MaxN + 1 : kSpBucketHi[bk - 1] + 1;
@@ -431,6 +437,14 @@ int gcl_set_option(gcl_context* c, int option, int64_t value) {
       if (value < 1) return GCL_ERR_ARG;
       c->wide_min_n = value;
       return GCL_OK;
+    case GCL_OPT_WORKSPACE_BYTES:
+      if (value < 0) return GCL_ERR_ARG;
+      c->workspace_bytes = (uint64_t)value;
+      return GCL_OK;
+    case GCL_OPT_WIDE_MAX_WARPS:
+      if (value < 0) return GCL_ERR_ARG;
+      c->wide_max_warps = value;
+      return GCL_OK;
     default:
       return GCL_ERR_ARG;
   }
@@ -458,11 +472,12 @@ int gcl_canon_wide_device_async(gcl_context* c, const int32_t* d_rowptr, const i
   int per_sm = 0;
   GCL_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, wide_items_kernel, kSpThreads,
                                                         (size_t)(smw * kSpWarps)));
-  const uint64_t budget = workspace_budget();
+  const uint64_t budget = ctx_workspace(c);
   int64_t warps = std::min<int64_t>((int64_t)c->sms * std::max(per_sm, 1) * kSpWarps,
                                     std::max<int64_t>(kSpWarps, (int64_t)(budget / Lo.bytes)));
   // no more warps than the largest possible number of work items
   warps = std::min<int64_t>(warps, ((int64_t)n * 2 + kSpWarps - 1) / kSpWarps * kSpWarps);
+  if (c->wide_max_warps > 0) warps = std::min<int64_t>(warps, c->wide_max_warps);
   warps = std::max<int64_t>(kSpWarps, warps / kSpWarps * kSpWarps);
   GCL_TRY(c->wide_sh.ensure(WL.bytes));
   GCL_TRY(c->wide_slots.ensure((size_t)(warps * Lo.bytes)));

@@ -261,25 +261,74 @@ def prufer_tree(n: int, rng: np.random.Generator, max_deg: int = 4) -> List[Tupl
     return edges
 
 
+def recursive_tree(n: int, rng: np.random.Generator, max_deg: int = 4) -> List[Tuple[int, int]]:
+    """Random tree with max degree <= max_deg for sizes where rejecting
+    Pruefer sequences is hopeless (the chance that a uniform tree on n
+    vertices has max degree <= 4 falls like exp(-0.019 n)): vertices arrive in
+    a random order and each attaches to a uniformly chosen earlier vertex of
+    degree < max_deg."""
+    if n <= 1:
+        return []
+    order = rng.permutation(n)
+    deg = np.zeros(n, dtype=np.int64)
+    open_ = [int(order[0])]  # vertices with spare degree
+    edges = []
+    for i in range(1, n):
+        v = int(order[i])
+        j = int(rng.integers(len(open_)))
+        u = open_[j]
+        edges.append((u, v))
+        deg[u] += 1
+        deg[v] += 1
+        if deg[u] >= max_deg:
+            open_[j] = open_[-1]
+            open_.pop()
+        open_.append(v)
+    return edges
+
+
 def tree_plus_edges(n: int, rng: np.random.Generator, max_deg: int = 4,
                     max_extra: int = 6) -> Graph:
     """Pruefer tree (max degree 4) plus U{0..max_extra} ring-closing edges
-    drawn uniformly among non-edges that keep the max degree <= max_deg."""
-    edges = [(min(a, b), max(a, b)) for a, b in prufer_tree(n, rng, max_deg)]
+    drawn uniformly among non-edges that keep the max degree <= max_deg.
+    Above 128 vertices the tree comes from ``recursive_tree`` and the extra
+    edges from rejection sampling (same distribution of extra edges)."""
+    tree = prufer_tree(n, rng, max_deg) if n <= 128 else recursive_tree(n, rng, max_deg)
+    edges = [(min(a, b), max(a, b)) for a, b in tree]
     deg = np.zeros(n, dtype=np.int64)
     adj = set(edges)
     for a, b in edges:
         deg[a] += 1
         deg[b] += 1
     extra = int(rng.integers(0, max_extra + 1))
+    adjm = None
+    if n <= 128:
+        adjm = np.zeros((n, n), dtype=bool)
+        for a, b in edges:
+            adjm[a, b] = True
     for _ in range(extra):
         free = np.nonzero(deg < max_deg)[0]
-        cand = [(int(a), int(b)) for i, a in enumerate(free) for b in free[i + 1:]
-                if (int(a), int(b)) not in adj]
-        if not cand:
-            break
-        a, b = cand[int(rng.integers(len(cand)))]
+        if n <= 128:
+            # every non-adjacent pair of free vertices, in (i, j) row order
+            iu, ju = np.triu_indices(len(free), 1)
+            ca, cb = free[iu], free[ju]
+            keep = ~adjm[ca, cb]
+            ca, cb = ca[keep], cb[keep]
+            if ca.size == 0:
+                break
+            k = int(rng.integers(ca.size))
+            a, b = int(ca[k]), int(cb[k])
+        else:
+            if len(free) < 2:
+                break
+            while True:  # uniform over non-adjacent pairs of free vertices
+                i, j = rng.choice(len(free), 2, replace=False)
+                a, b = int(min(free[i], free[j])), int(max(free[i], free[j]))
+                if (a, b) not in adj:
+                    break
         adj.add((a, b))
+        if adjm is not None:
+            adjm[a, b] = True
         edges.append((a, b))
         deg[a] += 1
         deg[b] += 1
@@ -334,6 +383,64 @@ def mixed_batch(count: int = 2000, seed: int = 4000, n_lo: int = 64,
             comp = random_regular(c, d, rng)
             out.append(disjoint_union(comp, k))
     return out
+
+
+@dataclass
+class ServingWorkload:
+    """An open-loop request stream over a pool of graphs: request i arrives
+    at ``arrival[i]`` seconds and is a canonization of ``graphs[g1[i]]``
+    (kind 0) or an isomorphism query between ``graphs[g1[i]]`` and
+    ``graphs[g2[i]]`` (kind 1)."""
+
+    graphs: List[Graph]
+    kind: np.ndarray
+    g1: np.ndarray
+    g2: np.ndarray
+    arrival: np.ndarray
+
+
+def serving_size(rng: np.random.Generator, n_lo: int = 10, n_mid: int = 128,
+                 n_big: int = 2048, n_max: int = 20000) -> int:
+    """Heavy-tailed request size: 90% uniform on [n_lo, n_mid], 9%
+    log-uniform on (n_mid, n_big], 1% log-uniform on (n_big, n_max]."""
+    u = rng.random()
+    if u < 0.90:
+        return int(rng.integers(n_lo, n_mid + 1))
+    lo, hi = (n_mid, n_big) if u < 0.99 else (n_big, n_max)
+    return int(min(hi, max(lo + 1, round(math.exp(rng.uniform(math.log(lo + 1), math.log(hi)))))))
+
+
+def serving_workload(count: int, rate: float, seed: int = 5000, iso_frac: float = 0.3,
+                     repeat_frac: float = 0.2, n_max: int = 20000) -> ServingWorkload:
+    """Poisson arrivals at ``rate`` requests/s.  Graphs are the batched
+    workload's family (tree of max degree 4 plus 0-6 extra edges) with the
+    heavy-tailed sizes of ``serving_size``.  ``iso_frac`` of the requests are
+    isomorphism pairs, half of them a random relabeling (isomorphic) and half
+    a copy with one edge moved (almost always not); ``repeat_frac`` of the
+    canonization requests re-ask an earlier graph under a random relabeling
+    (the canonical-hash table's repeats)."""
+    rng = np.random.default_rng(seed)
+    graphs: List[Graph] = []
+    kind = np.zeros(count, np.int32)
+    g1 = np.zeros(count, np.int32)
+    g2 = np.zeros(count, np.int32)
+    canon_ids: List[int] = []
+    for i in range(count):
+        if rng.random() < iso_frac:
+            a = tree_plus_edges(serving_size(rng, n_max=n_max), rng)
+            b = random_relabel(a, rng) if rng.random() < 0.5 else move_one_edge(a, rng)
+            graphs += [a, b]
+            kind[i], g1[i], g2[i] = 1, len(graphs) - 2, len(graphs) - 1
+            continue
+        if canon_ids and rng.random() < repeat_frac:
+            src = graphs[canon_ids[int(rng.integers(len(canon_ids)))]]
+            graphs.append(random_relabel(src, rng))
+        else:
+            graphs.append(tree_plus_edges(serving_size(rng, n_max=n_max), rng))
+        g1[i] = g2[i] = len(graphs) - 1
+        canon_ids.append(len(graphs) - 1)
+    arrival = np.cumsum(rng.exponential(1.0 / rate, count))
+    return ServingWorkload(graphs, kind, g1, g2, arrival - arrival[0])
 
 
 # --------------------------------------------------------------------------

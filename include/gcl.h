@@ -77,8 +77,15 @@ void* gcl_stream(gcl_context* ctx);
  *   warp-per-graph kernel for n <= 64 does not take); GCL_MAX_N + 1 keeps the
  *   sequential traversal and its exact statistics for every size.  A wide
  *   search that fails for want of workspace falls back to the sequential one.
+ * GCL_OPT_WORKSPACE_BYTES: device memory one pass of per-warp workspace may
+ *   take (fewer resident warps when it binds); 0 = the GCL_WORKSPACE_GB
+ *   environment variable, default 4 GiB.
+ * GCL_OPT_WIDE_MAX_WARPS: upper bound on the warps of a wide search (0 = as
+ *   many as fit on the GPU), to leave SMs to concurrent work.
  * Returns GCL_ERR_ARG for an unknown option or value. */
 #define GCL_OPT_WIDE_MIN_N 1
+#define GCL_OPT_WORKSPACE_BYTES 2
+#define GCL_OPT_WIDE_MAX_WARPS 3
 int gcl_set_option(gcl_context* ctx, int option, int64_t value);
 
 /* ---- one graph (drop-in for Nauty_Parallel, src/nauty_parallel.h:9-13) ---
@@ -177,6 +184,95 @@ int gcl_iso(gcl_context* ctx, const int32_t* rowptr1, const int32_t* col1,
             const int32_t* color1, int n1, const int32_t* rowptr2,
             const int32_t* col2, const int32_t* color2, int n2, int max_aut,
             int* verdict);
+
+/* ---- serving: a request loop with continuous batching -------------------
+ * No counterpart in the reference (its CLI canonizes one or two graphs per
+ * process).  A server owns `lanes` device contexts, each with its own stream
+ * and workspace; one dispatcher thread keeps every lane busy: whenever a lane
+ * is free it takes the queued requests that fit the lane's device-memory
+ * budget (graphs, outputs and search workspace -- admission by HBM
+ * footprint) and launches them as one batch, so requests that arrive while
+ * others are on the GPU run in the next batch on another lane, overlapping
+ * on the device.  Requests are split in three classes by their largest
+ * graph -- small (n < mid_n), mid, and large (n >= large_n: the wide search,
+ * one request at a time, one block per SM) -- each with its own queue and
+ * lanes, so a batch never waits for a slower class.  Results are those of
+ * gcl_canon_batch (gcl_canon_wide_device_async for large) on the same graph.
+ *
+ * After each batch a kernel hashes every canonical form into a device table
+ * (open addressing, 64-bit keys, forms kept in a device store and compared in
+ * full on a key match): equal class ids mean isomorphic graphs, and a
+ * request whose class was seen before is reported as a repeat.  Exact
+ * repeats of an earlier input are answered from a host-side memo of recent
+ * results without a launch.
+ *
+ * Thread safety: submit, poll and stats may be called from any threads. */
+typedef struct gcl_server gcl_server;
+
+typedef struct {
+  int lanes;           /* lanes for requests whose graphs have n < mid_n, default 3 */
+  int mid_lanes;       /* lanes for mid_n <= n < large_n, default 3            */
+  int large_lanes;     /* lanes for n >= large_n (wide search), default 1      */
+  int max_batch;       /* graphs per batch, default 8192                      */
+  int mid_n;           /* default 65                                          */
+  int large_n;         /* default 2049                                        */
+  int max_aut;         /* default 10000                                       */
+  int64_t lane_bytes;  /* device-memory budget of one small or mid lane's
+                          batch (inputs, outputs, search workspace), 256 MiB  */
+  int64_t table_slots; /* canonical-hash table slots (power of two), 1 << 20  */
+  int64_t store_bytes; /* device store of canonical forms, default 256 MiB    */
+  int64_t memo_bytes;  /* host memo of exact repeats, default 64 MiB, < 0 = off */
+} gcl_serve_config;
+
+#define GCL_REQ_CANON 0
+#define GCL_REQ_ISO 1
+
+typedef struct {
+  int64_t id;          /* the id given to gcl_serve_submit                      */
+  int32_t status;      /* GCL_OK or a GCL_ERR_* code                           */
+  int32_t verdict;     /* GCL_REQ_ISO: 1 isomorphic, 0 not; else -1            */
+  int32_t repeat;      /* 1: an isomorphic graph was canonized before (the
+                          class was in the table); 2: an identical input was
+                          answered from the memo                               */
+  int32_t batch;       /* graphs in the batch that carried the request (0 = memo) */
+  int64_t class_id;    /* isomorphism class of (the first) graph, -1 unknown   */
+  uint64_t canon_hash; /* 64-bit hash of the canonical form                    */
+  double latency_s;    /* submit -> result ready (host steady clock)           */
+} gcl_serve_result;
+
+typedef struct {
+  int64_t submitted, completed, batches, graphs, memo_hits, class_repeats, classes;
+  int64_t large_graphs;
+} gcl_serve_stats;
+
+/* cfg may be NULL (all defaults); zero fields take their default. */
+int gcl_serve_create(int device, const gcl_serve_config* cfg, gcl_server** out);
+/* Waits for work in flight, then frees everything. */
+int gcl_serve_destroy(gcl_server* srv);
+/* Queue a request.  The graphs are copied before the call returns.  For
+ * GCL_REQ_CANON the second graph is ignored and out_rows (n * ceil(n/64)
+ * words, the packed layout of gcl_canon_batch) and out_label (n) may be
+ * NULL or caller buffers that stay valid until the request's result has been
+ * polled.  For GCL_REQ_ISO both outputs are ignored. */
+int gcl_serve_submit(gcl_server* srv, int64_t id, int kind, const int32_t* rowptr,
+                     const int32_t* col, const int32_t* color, int n,
+                     const int32_t* rowptr2, const int32_t* col2, const int32_t* color2,
+                     int n2, uint64_t* out_rows, int32_t* out_label);
+/* Up to max finished results; waits up to timeout_ms (0 = do not wait, -1 =
+ * until at least one is ready).  Returns the number written or an error. */
+int gcl_serve_poll(gcl_server* srv, gcl_serve_result* out, int max, int timeout_ms);
+int gcl_serve_stats_get(gcl_server* srv, gcl_serve_stats* out);
+
+/* Open-loop load: request i (kind[i], graphs g1[i] and g2[i] of the arena in
+ * the batched layout) is submitted at arrival_s[i] seconds after the call
+ * starts, from a generator thread, whatever the server's progress; the call
+ * returns when every result is in (results[i] for request i, latency
+ * measured from the scheduled arrival) or timeout_s has passed
+ * (GCL_ERR_TIMEOUT). */
+int gcl_serve_replay(gcl_server* srv, int nreq, const double* arrival_s, const int32_t* kind,
+                     const int32_t* g1, const int32_t* g2, int count, const int64_t* voff,
+                     const int64_t* eoff, const int32_t* rowptr, const int32_t* col,
+                     const int32_t* color, double timeout_s, gcl_serve_result* results);
 
 #ifdef __cplusplus
 }
