@@ -61,13 +61,18 @@ def parse():
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-serving", action="store_true")
-    p.add_argument("--serve-requests", type=int, default=6000)
-    p.add_argument("--serve-rate", type=float, default=2000.0,
+    p.add_argument("--serve-requests", type=int, default=4000)
+    p.add_argument("--serve-rate", type=float, default=500.0,
                    help="Poisson arrival rate of the serving run, requests/s")
-    p.add_argument("--serve-nmax", type=int, default=20000)
+    p.add_argument("--serve-nmax", type=int, default=4096,
+                   help="largest request size (the 1%% tail is log-uniform on (2048, nmax])")
+    p.add_argument("--serve-plain", type=int, default=800,
+                   help="requests replayed through the plain one-graph-per-launch form")
     p.add_argument("--no-single", action="store_true")
-    p.add_argument("--no-mixed", action="store_true")
-    p.add_argument("--mixed-graphs", type=int, default=2000)
+    p.add_argument("--mixed", action="store_true",
+                   help="also time the mixed-size batch (n log-uniform [64,4096]); off by default: "
+                        "its union graphs take the reference's search minutes each")
+    p.add_argument("--mixed-graphs", type=int, default=300)
     return p.parse_args()
 
 
@@ -481,7 +486,7 @@ def gpu_arm(args):
         line["serving"] = serving_block(args, pkg, local)
     if rank == 0 and not args.no_single:
         line["single_graph"] = single_graph_block(args, pkg, local, not args.no_cpu_baseline)
-    if rank == 0 and not args.no_mixed:
+    if rank == 0 and args.mixed:
         line["mixed_batch"] = mixed_block(args, pkg, local)
     if rank == 0:
         print(json.dumps(line))
@@ -533,24 +538,36 @@ def serving_block(args, pkg, local):
         "batches": st["batches"], "graphs": st["graphs"], "memo_hits": st["memo_hits"],
         "class_repeats": st["class_repeats"],
     }
-    # plain form: one request at a time, gcl_canon_one per graph (a sample)
-    ctx = pkg.Context(local, wide_min_n=pkg.api.GCL_MAX_N + 1)
-    idx = [i for i in range(len(res)) if ns[i] <= 2048][:400]
-    ts = []
-    for i in idx[:20]:
+    # the plain form under the same arrivals: the first requests served one
+    # at a time in arrival order, each graph through its own gcl_canon_one
+    # call; service times are measured, queueing (FIFO, one server) follows
+    # from the arrival times
+    ctx = pkg.Context(local)
+    k = min(len(res), args.serve_plain)
+    for i in range(min(20, k)):
         pkg.canon(W.graphs[W.g1[i]], ctx=ctx)
-    for i in idx:
+    svc = np.zeros(k)
+    for i in range(k):
         t = time.perf_counter()
         pkg.canon(W.graphs[W.g1[i]], ctx=ctx)
         if W.kind[i] == 1:
             pkg.canon(W.graphs[W.g2[i]], ctx=ctx)
-        ts.append(time.perf_counter() - t)
+        svc[i] = time.perf_counter() - t
     ctx.close()
-    ts = np.array(ts) * 1e3
+    done, plat = 0.0, np.zeros(k)
+    for i in range(k):
+        start = max(W.arrival[i], done)
+        done = start + svc[i]
+        plat[i] = done - W.arrival[i]
+    plat *= 1e3
     block["plain_one_per_launch"] = {
-        "sample": f"{len(idx)} requests with n <= 2048, one gcl_canon_one per graph, serially",
-        "p50_ms": float(np.percentile(ts, 50)), "p99_ms": float(np.percentile(ts, 99)),
-        "throughput_req_s": len(ts) / (ts.sum() / 1e3)}
+        "sample": f"the first {k} requests in arrival order, one gcl_canon_one per graph, "
+                  f"FIFO single server at the same arrival times",
+        "p50_ms": float(np.percentile(plat, 50)), "p99_ms": float(np.percentile(plat, 99)),
+        "service_p50_ms": float(np.percentile(svc, 50) * 1e3),
+        "capacity_req_s": k / float(svc.sum()),
+        "served_p50_ms_same_requests": float(np.percentile(lat[:k], 50)),
+        "served_p99_ms_same_requests": float(np.percentile(lat[:k], 99))}
     return block
 
 

@@ -267,9 +267,10 @@ REQ_ISO = 1
 
 
 class ServeConfig(ctypes.Structure):
-    _fields_ = [("lanes", ctypes.c_int), ("mid_lanes", ctypes.c_int),
+    _fields_ = [("lanes", ctypes.c_int), ("mid_lanes", ctypes.c_int), ("big_lanes", ctypes.c_int),
                 ("large_lanes", ctypes.c_int), ("max_batch", ctypes.c_int),
-                ("mid_n", ctypes.c_int), ("large_n", ctypes.c_int), ("max_aut", ctypes.c_int),
+                ("mid_batch", ctypes.c_int), ("big_batch", ctypes.c_int), ("mid_n", ctypes.c_int),
+                ("big_n", ctypes.c_int), ("large_n", ctypes.c_int), ("max_aut", ctypes.c_int),
                 ("lane_bytes", ctypes.c_int64), ("table_slots", ctypes.c_int64),
                 ("store_bytes", ctypes.c_int64), ("memo_bytes", ctypes.c_int64)]
 

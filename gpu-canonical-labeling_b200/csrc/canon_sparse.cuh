@@ -50,15 +50,16 @@ struct SpLayout {
   uint64_t fcode, ccode, pool_owner;
   uint64_t stb, sts, act, acts, tcb, tcbs;
   uint64_t fcert, bcert, ccert;
-  uint64_t tc, reps, auts, ulog;
-  uint32_t ulog_cap;
+  uint64_t tc, reps, auts, ulog, fixst;
+  uint32_t ulog_cap, fixcap;
   uint64_t bytes;
   uint32_t nw, nsw;
   uint32_t stride;  // elements per representative array / ring entry
 };
 
 __host__ __device__ inline SpLayout sp_layout(uint32_t n, uint64_t m2, uint32_t pool,
-                                              uint32_t cap) {
+                                              uint32_t cap, uint32_t fixcap = 0xffffffffu) {
+  if (fixcap == 0xffffffffu) fixcap = cap;
   SpLayout L{};
   uint64_t o = 0;
   auto take = [&](uint64_t bytes) {
@@ -88,6 +89,8 @@ __host__ __device__ inline SpLayout sp_layout(uint32_t n, uint64_t m2, uint32_t 
   L.auts = take(2ull * cap * N1);
   L.ulog_cap = 5 * n + 64;
   L.ulog = take(8ull * L.ulog_cap);
+  L.fixcap = fixcap;
+  L.fixst = take(8ull * fixcap);
   L.bytes = o;
   return L;
 }
@@ -108,6 +111,8 @@ struct SpWarp {
   int32_t *fcode, *ccode, *pool_owner, *pathcode;
   uint32_t *umark;  // per level: undo-log size when the level's child was made
   uint2* ulog;      // undo log: {position | kStartFlag, previous in_level}
+  uint2* fixst;     // per stored automorphism: {prefix of seq it fixes, first
+                    // position of seq it moves or kNone}, valid for the path
   uint64_t *stb, *sts, *act, *acts, *tcb, *tcbs;
   uint32_t *fcert, *bcert, *ccert, *reps;
   SpTc* tc;
@@ -1083,16 +1088,25 @@ __device__ __noinline__ bool sp_orbits(int idx, int num_aut, uint32_t seqlen) {
   for (int base = from; base < limit; base += 32) {
     const int a = base + (int)lane;
     bool fix = a < limit;
-    const uint16_t* pa = W.auts + (uint64_t)(fix ? a : 0) * W.stride;
-    // eight independent loads per round: one memory latency per eight entries
-    for (uint32_t j0 = 0; fix && j0 < seqlen; j0 += 8) {
-      uint32_t sv[8], im[8];
-#pragma unroll
-      for (int u = 0; u < 8; ++u) sv[u] = j0 + u < seqlen ? W.seq[j0 + u] : 0u;
-#pragma unroll
-      for (int u = 0; u < 8; ++u) im[u] = j0 + u < seqlen ? ldx<kCg>(pa + sv[u]) : sv[u];
-#pragma unroll
-      for (int u = 0; u < 8; ++u) fix = fix && im[u] == sv[u];
+    if (fix) {
+      // extend what is known about entry a along the current sequence: the
+      // prefix it fixes and the first position it moves stay valid until a
+      // backtrack shortens the sequence below them (sp_fix_clamp)
+      uint2 st = W.fixst[a];
+      if (st.y != kNone && st.y < seqlen) {
+        fix = false;
+      } else {
+        const uint16_t* pa = W.auts + (uint64_t)a * W.stride;
+        uint32_t j = st.x;
+        for (; j < seqlen; ++j) {
+          const uint32_t sv = W.seq[j];
+          if (ldx<kCg>(pa + sv) != sv) break;
+        }
+        fix = j >= seqlen;
+        st.x = j;
+        st.y = fix ? kNone : j;
+        W.fixst[a] = st;
+      }
     }
     const uint32_t fm = __ballot_sync(GCL_FULL, fix);
     if (!fm) continue;
@@ -1150,6 +1164,21 @@ __device__ __noinline__ bool sp_orbits(int idx, int num_aut, uint32_t seqlen) {
   }
   __syncwarp();
   return true;
+}
+
+// After a backtrack to sequence length s: positions >= s of the sequence
+// change, so what entries [0, count) knew about them is dropped.
+__device__ __noinline__ void sp_fix_clamp(uint32_t s, uint32_t count) {
+  SpWarp& W = sp_w();
+  for (uint32_t a = lane_id(); a < count; a += 32) {
+    uint2 st = W.fixst[a];
+    if (st.x > s || (st.y != kNone && st.y >= s)) {
+      st.x = min(st.x, s);
+      if (st.y != kNone && st.y >= s) st.y = kNone;
+      W.fixst[a] = st;
+    }
+  }
+  __syncwarp();
 }
 
 // aut[label[j]] = elem[j] (sequential.cpp:505-520, 544-555)
@@ -1346,6 +1375,7 @@ __device__ __noinline__ void sp_bind(uint8_t* slot, const SpLayout& Lo, uint32_t
   W.pathcode = (int32_t*)base[24];
   W.umark = base[25];
   W.ulog = (uint2*)(slot + Lo.ulog);
+  W.fixst = (uint2*)(slot + Lo.fixst);
   W.ulog_cap = Lo.ulog_cap;
   W.utop = 0;
   W.ulog_bad = 0;
@@ -1619,6 +1649,8 @@ __device__ __noinline__ SpResult sp_search(const BatchArgs& A, int g, uint8_t* s
           break;
         }
         sp_store_aut(dec == 1 ? W.flabel : W.blabel, W.auts + (uint64_t)si * W.stride);
+        if (lane == 0) W.fixst[si] = make_uint2(0u, kNone);
+        __syncwarp();
         ++num_aut;
         const int gg = dec == 1 ? sp_gca(W.fseq, first_seqlen, seqlen)
                                 : sp_gca(W.bseq, best_seqlen, seqlen);
@@ -1656,6 +1688,7 @@ __device__ __noinline__ SpResult sp_search(const BatchArgs& A, int g, uint8_t* s
       seqlen = Lv - 1;
       tcl = (int)Lv;
       level = Lv;
+      sp_fix_clamp(seqlen, (uint32_t)min(num_aut, (int)W.max_aut));
       // representative arrays of levels deeper than Lv are free again
       __syncwarp();
       if (lane == 0)

@@ -601,6 +601,14 @@ __device__ __noinline__ int32_t wide_gate(WideHdr* H, uint32_t need, uint64_t de
   return __shfl_sync(GCL_FULL, st, 0);
 }
 
+// Store entries [from, to) become known to this warp: nothing is known yet
+// about how they act on its sequence.
+__device__ __noinline__ void wide_fix_init(uint32_t from, uint32_t to) {
+  SpWarp& W = sp_w();
+  for (uint32_t a = from + lane_id(); a < to; a += 32) W.fixst[a] = make_uint2(0u, kNone);
+  __syncwarp();
+}
+
 __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
   extern __shared__ __align__(16) uint8_t sp_dyn[];
   const int warp = (int)(threadIdx.x >> 5);
@@ -642,7 +650,7 @@ __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
   __syncwarp();
   const uint64_t deadline = A.budget_ns ? H->t0 + A.budget_ns : 0;
   WideBest best{0, 0, 0xffffffffu};
-  uint32_t known = 0;
+  uint32_t known = 0, fix_init = 0, prev_k = 0;
   unsigned long long my_nodes = 0;
   int32_t status = kOk;
   uint64_t iter = 0;
@@ -709,6 +717,10 @@ __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
     for (uint32_t i = lane; i < k; i += 32) W.seq[i] = P.fseq[i];
     for (uint32_t i = lane; i <= k; i += 32) W.pathcode[i] = P.fcode[i];
     __syncwarp();
+    // the previous item's sequence shares the first path's first
+    // min(k, prev_k) vertices with this one
+    sp_fix_clamp(min(k, prev_k), fix_init);
+    prev_k = k;
     if (lane == 0) {
       SpTc h;
       h.first = tf;
@@ -869,6 +881,10 @@ __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
             bt = (int)level - 1;
           } else {
             known = wide_ready_prefix(P, known, cap);
+            if (known > fix_init) {
+              wide_fix_init(fix_init, known);
+              fix_init = known;
+            }
             if (known > (uint32_t)W.tc[idx].last) {
               if (!sp_orbits<true>(idx, (int)known, seqlen)) {
                 status = W.pool_top >= W.pool_cap ? kAutOverflow : kInternal;
@@ -927,6 +943,7 @@ __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
         seqlen = Lv - 1;
         tcl = (int)Lv;
         level = Lv;
+        sp_fix_clamp(seqlen, fix_init);
         __syncwarp();
         if (lane == 0)
           while (W.pool_top > 0 && W.pool_owner[W.pool_top - 1] >= (int32_t)Lv) W.pool_top -= 1;

@@ -466,7 +466,7 @@ int gcl_canon_wide_device_async(gcl_context* c, const int32_t* d_rowptr, const i
   const uint32_t cap = (uint32_t)std::max<uint64_t>(
       1, std::min<uint64_t>((uint64_t)max_aut, kWideStoreBytes / per_aut));
   const WideLayout WL = wide_layout(un, m2, cap);
-  const SpLayout Lo = sp_layout(un, m2, kWidePool, 0);
+  const SpLayout Lo = sp_layout(un, m2, kWidePool, 0, cap);
   uint64_t smw = sp_smem_bytes(un);
   if (smw * kSpWarps > (uint64_t)kSpSmemPerBlock) smw = 0;
   int per_sm = 0;

@@ -236,10 +236,11 @@ struct MemoEntry {
 };
 
 // Request classes by the larger graph's n: small (the warp kernel for
-// n <= 64, microseconds), mid (the sparse warp kernel), large (the wide
-// search).  Each class has its own queue and lanes, so a batch never waits
-// for a graph of a slower class.
-enum { kSmall = 0, kMid = 1, kLarge = 2 };
+// n <= 64, microseconds), mid and big (the sparse warp kernel: milliseconds,
+// tenths of seconds), large (the wide search).  Each class has its own
+// queue, lanes and batch-size cap, so a batch never waits for a graph of a
+// slower class.
+enum { kSmall = 0, kMid = 1, kBig = 2, kLarge = 3, kClasses = 4 };
 
 struct Lane {
   gcl_context* ctx = nullptr;
@@ -298,7 +299,8 @@ struct gcl_server {
   std::vector<Lane*> lanes;
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
-  std::deque<Req*> q[3];
+  std::deque<Req*> q[kClasses];
+  int max_batch[kClasses] = {0, 0, 0, 1};
   std::deque<gcl_serve_result> done;
   std::thread th;
   bool stop = false;
@@ -382,7 +384,9 @@ std::vector<Req*> take_batch(gcl_server* S, Lane* L) {
     Req* r = q.front();
     int64_t b = 0;
     for (int i = 0; i < r->ng; ++i) b += footprint(r->g[i]);
-    if (!out.empty() && (graphs + r->ng > S->cfg.max_batch || bytes + b > S->cfg.lane_bytes)) break;
+    if (!out.empty() &&
+        (graphs + r->ng > S->max_batch[L->cls] || bytes + b > S->cfg.lane_bytes))
+      break;
     q.pop_front();
     out.push_back(r);
     graphs += r->ng;
@@ -539,13 +543,13 @@ void complete(gcl_server* S, Lane* L) {
     const int g = L->first[k];
     if (L->large && L->err == GCL_OK) {
       // a wide search that ran out of per-warp orbit storage (or failed an
-      // internal check) has no result: the request goes to the mid lanes,
+      // internal check) has no result: the request goes to the big lanes,
       // whose sequential search reruns with full storage
       bool retry = false;
       for (int i = 0; i < r->ng; ++i) retry |= status[g + i] == 1 || status[g + i] == 4;
       if (retry) {
         std::lock_guard<std::mutex> lk(S->mu);
-        S->q[kMid].push_back(r);
+        S->q[kBig].push_back(r);
         continue;
       }
     }
@@ -665,7 +669,9 @@ void dispatcher(gcl_server* S) {
       any_busy |= L->busy;
       any_ready |= L->busy && L->ready.load();
     }
-    if (S->stop && !any_busy && S->q[0].empty() && S->q[1].empty() && S->q[2].empty()) break;
+    bool queued = false;
+    for (auto& q : S->q) queued |= !q.empty();
+    if (S->stop && !any_busy && !queued) break;
     if (progress || any_ready) continue;
     bool can_launch = false;
     for (Lane* L : S->lanes)
@@ -710,9 +716,13 @@ int gcl_serve_create(int device, const gcl_serve_config* cfg, gcl_server** out) 
   if (cfg) c = *cfg;
   if (c.lanes <= 0) c.lanes = 3;
   if (c.mid_lanes <= 0) c.mid_lanes = 3;
-  if (c.large_lanes <= 0) c.large_lanes = 1;
+  if (c.big_lanes <= 0) c.big_lanes = 2;
+  if (c.large_lanes <= 0) c.large_lanes = 4;
   if (c.max_batch <= 0) c.max_batch = 8192;
+  if (c.mid_batch <= 0) c.mid_batch = 512;
+  if (c.big_batch <= 0) c.big_batch = 64;
   if (c.mid_n <= 0) c.mid_n = 65;
+  if (c.big_n <= 0) c.big_n = 257;
   if (c.large_n <= 0) c.large_n = 2049;
   if (c.max_aut <= 0) c.max_aut = 10000;
   if (c.lane_bytes <= 0) c.lane_bytes = 256ll << 20;
@@ -720,23 +730,29 @@ int gcl_serve_create(int device, const gcl_serve_config* cfg, gcl_server** out) 
   if (c.store_bytes <= 0) c.store_bytes = 256ll << 20;
   if (c.memo_bytes == 0) c.memo_bytes = 64ll << 20;
   if (c.memo_bytes < 0) c.memo_bytes = 0;  // off
-  if ((c.table_slots & (c.table_slots - 1)) != 0 || c.large_n < c.mid_n) return GCL_ERR_ARG;
+  if ((c.table_slots & (c.table_slots - 1)) != 0 || c.big_n < c.mid_n || c.large_n < c.big_n)
+    return GCL_ERR_ARG;
   cudaError_t e = cudaSetDevice(device);
   if (e != cudaSuccess) return rc_of(e);
   gcl_server* S = new (std::nothrow) gcl_server();
   if (!S) return GCL_ERR_NOMEM;
   S->device = device;
   S->cfg = c;
+  S->max_batch[kSmall] = c.max_batch;
+  S->max_batch[kMid] = c.mid_batch;
+  S->max_batch[kBig] = c.big_batch;
+  S->max_batch[kLarge] = 1;
   int rc = GCL_OK;
   int dev_sms = 0;
   cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, device);
-  for (int i = 0; i < c.lanes + c.mid_lanes + c.large_lanes && rc == GCL_OK; ++i) {
+  const int nl[kClasses] = {c.lanes, c.mid_lanes, c.big_lanes, c.large_lanes};
+  for (int i = 0; i < nl[0] + nl[1] + nl[2] + nl[3] && rc == GCL_OK; ++i) {
     Lane* L = new (std::nothrow) Lane();
     if (!L) {
       rc = GCL_ERR_NOMEM;
       break;
     }
-    L->cls = i < c.lanes ? kSmall : i < c.lanes + c.mid_lanes ? kMid : kLarge;
+    L->cls = i < nl[0] ? kSmall : i < nl[0] + nl[1] ? kMid : i < nl[0] + nl[1] + nl[2] ? kBig : kLarge;
     L->large = L->cls == kLarge;
     S->lanes.push_back(L);
     rc = gcl_create(device, &L->ctx);
@@ -850,7 +866,10 @@ int gcl_serve_submit(gcl_server* S, int64_t id, int kind, const int32_t* rowptr,
     return GCL_OK;
   }
   const int nmax = std::max(r->g[0].n, r->ng == 2 ? r->g[1].n : 0);
-  const int cls = nmax >= S->cfg.large_n ? kLarge : nmax >= S->cfg.mid_n ? kMid : kSmall;
+  const int cls = nmax >= S->cfg.large_n ? kLarge
+                  : nmax >= S->cfg.big_n ? kBig
+                  : nmax >= S->cfg.mid_n ? kMid
+                                         : kSmall;
   {
     std::lock_guard<std::mutex> lk(S->mu);
     S->q[cls].push_back(r);

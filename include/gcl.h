@@ -193,10 +193,11 @@ int gcl_iso(gcl_context* ctx, const int32_t* rowptr1, const int32_t* col1,
  * budget (graphs, outputs and search workspace -- admission by HBM
  * footprint) and launches them as one batch, so requests that arrive while
  * others are on the GPU run in the next batch on another lane, overlapping
- * on the device.  Requests are split in three classes by their largest
- * graph -- small (n < mid_n), mid, and large (n >= large_n: the wide search,
- * one request at a time, one block per SM) -- each with its own queue and
- * lanes, so a batch never waits for a slower class.  Results are those of
+ * on the device.  Requests are split in four classes by their largest
+ * graph -- small (n < mid_n: the warp kernel for n <= 64), mid, big, and
+ * large (n >= large_n: the wide search, one request at a time, one block per
+ * SM) -- each with its own queue, lanes and batch-size cap, so a batch
+ * never waits for a slower class.  Results are those of
  * gcl_canon_batch (gcl_canon_wide_device_async for large) on the same graph.
  *
  * After each batch a kernel hashes every canonical form into a device table
@@ -211,14 +212,18 @@ typedef struct gcl_server gcl_server;
 
 typedef struct {
   int lanes;           /* lanes for requests whose graphs have n < mid_n, default 3 */
-  int mid_lanes;       /* lanes for mid_n <= n < large_n, default 3            */
-  int large_lanes;     /* lanes for n >= large_n (wide search), default 1      */
-  int max_batch;       /* graphs per batch, default 8192                      */
+  int mid_lanes;       /* lanes for mid_n <= n < big_n, default 3              */
+  int big_lanes;       /* lanes for big_n <= n < large_n, default 2            */
+  int large_lanes;     /* lanes for n >= large_n (wide search), default 4      */
+  int max_batch;       /* graphs per small batch, default 8192                */
+  int mid_batch;       /* graphs per mid batch, default 512                   */
+  int big_batch;       /* graphs per big batch, default 64                    */
   int mid_n;           /* default 65                                          */
+  int big_n;           /* default 257                                         */
   int large_n;         /* default 2049                                        */
   int max_aut;         /* default 10000                                       */
-  int64_t lane_bytes;  /* device-memory budget of one small or mid lane's
-                          batch (inputs, outputs, search workspace), 256 MiB  */
+  int64_t lane_bytes;  /* device-memory budget of one batch (inputs, outputs,
+                          search workspace) on the batched lanes, 256 MiB      */
   int64_t table_slots; /* canonical-hash table slots (power of two), 1 << 20  */
   int64_t store_bytes; /* device store of canonical forms, default 256 MiB    */
   int64_t memo_bytes;  /* host memo of exact repeats, default 64 MiB, < 0 = off */
