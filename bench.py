@@ -35,6 +35,12 @@ import time
 
 import numpy as np
 
+# The serving loop runs a dozen streams at once; with the default of 8
+# hardware work queues, streams share queues and a short batch can wait
+# behind a long search queued on another stream.  Must be set before CUDA
+# starts in this process.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 PKG = "gpu-canonical-labeling_b200"
@@ -66,6 +72,8 @@ def parse():
                    help="Poisson arrival rate of the serving run, requests/s")
     p.add_argument("--serve-nmax", type=int, default=4096,
                    help="largest request size (the 1%% tail is log-uniform on (2048, nmax])")
+    p.add_argument("--serve-large-n", type=int, default=0,
+                   help="server large_n (0 = the library default)")
     p.add_argument("--serve-plain", type=int, default=800,
                    help="requests replayed through the plain one-graph-per-launch form")
     p.add_argument("--no-single", action="store_true")
@@ -506,16 +514,19 @@ def serving_block(args, pkg, local):
     W = G.serving_workload(args.serve_requests, args.serve_rate, seed=5000,
                            n_max=args.serve_nmax)
     arena = G.pack(W.graphs)
-    srv = pkg.Server(local)
-    # warm-up: a short replay of the first requests
-    k0 = min(300, len(W.kind))
-    srv.replay(arena, W.kind[:k0], W.g1[:k0], W.g2[:k0], W.arrival[:k0], timeout_s=600)
-    srv.close()
-    srv = pkg.Server(local)
+    scfg = {"large_n": args.serve_large_n} if args.serve_large_n else {}
+    srv = pkg.Server(local, **scfg)
+    # warm-up on the same server (its lanes size their buffers): a short
+    # replay of the first requests
+    Ww = G.serving_workload(300, args.serve_rate, seed=5001, n_max=min(args.serve_nmax, 2048))
+    srv.replay(G.pack(Ww.graphs), Ww.kind, Ww.g1, Ww.g2, Ww.arrival, timeout_s=600)
+    st0 = srv.stats()
     t0 = time.perf_counter()
     res = srv.replay(arena, W.kind, W.g1, W.g2, W.arrival, timeout_s=1800)
     wall = time.perf_counter() - t0
-    st = srv.stats()
+    st1 = srv.stats()
+    st = {k: ([a - b for a, b in zip(v, st0[k])] if isinstance(v, list) else v - st0[k])
+          for k, v in st1.items()}
     srv.close()
     lat = np.array([r.latency_s for r in res]) * 1e3
     ok = all(r.status == 0 for r in res)
@@ -535,7 +546,16 @@ def serving_block(args, pkg, local):
         "p99_ms_n_le_2048": float(np.percentile(lat[~big], 99)),
         "p50_ms_iso": float(np.percentile(lat[iso], 50)) if iso.any() else None,
         "large_requests": int(big.sum()),
+        "p50_p99_ms_by_size": {
+            name: [float(np.percentile(lat[m], 50)), float(np.percentile(lat[m], 99)), int(m.sum())]
+            for name, m in (("n<=64", ns <= 64), ("65-256", (ns > 64) & (ns <= 256)),
+                            ("257-2048", (ns > 256) & (ns <= 2048)), (">2048", ns > 2048))
+            if m.any()},
         "batches": st["batches"], "graphs": st["graphs"], "memo_hits": st["memo_hits"],
+        "per_class": {name: {"batches": st["class_batches"][c],
+                             "mean_batch_ms": st["class_batch_ns"][c] / 1e6 / max(st["class_batches"][c], 1),
+                             "mean_queue_ms": st["class_queue_ns"][c] / 1e6 / max(st["class_batches"][c], 1)}
+                      for c, name in enumerate(("small", "mid", "big", "large"))},
         "class_repeats": st["class_repeats"],
     }
     # the plain form under the same arrivals: the first requests served one

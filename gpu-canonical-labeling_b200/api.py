@@ -43,6 +43,9 @@ EXPORTS = [
 ]
 
 GCL_OPT_WIDE_MIN_N = 1
+GCL_OPT_WORKSPACE_BYTES = 2
+GCL_OPT_WIDE_MAX_WARPS = 3
+GCL_OPT_SMEM_STAGE = 4
 GCL_MAX_N = 65536
 
 
@@ -285,7 +288,9 @@ class ServeResult(ctypes.Structure):
 class ServeStats(ctypes.Structure):
     _fields_ = [(k, ctypes.c_int64) for k in ("submitted", "completed", "batches", "graphs",
                                               "memo_hits", "class_repeats", "classes",
-                                              "large_graphs")]
+                                              "large_graphs")] + [
+        ("class_batches", ctypes.c_int64 * 4), ("class_batch_ns", ctypes.c_int64 * 4),
+        ("class_queue_ns", ctypes.c_int64 * 4)]
 
 
 def _serve_sigs(lib):
@@ -366,7 +371,11 @@ class Server:
     def stats(self) -> dict:
         s = ServeStats()
         _check(self.lib.gcl_serve_stats_get(self.handle, ctypes.byref(s)), "gcl_serve_stats_get")
-        return {k: int(getattr(s, k)) for k, _ in ServeStats._fields_}
+        out = {}
+        for k, _ in ServeStats._fields_:
+            v = getattr(s, k)
+            out[k] = [int(x) for x in v] if hasattr(v, "__len__") else int(v)
+        return out
 
     def replay(self, arena: Arena, kind, g1, g2, arrival_s, timeout_s: float = 600.0):
         """Open-loop load (gcl_serve_replay): request i is submitted at

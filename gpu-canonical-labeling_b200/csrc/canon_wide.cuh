@@ -42,7 +42,7 @@
 namespace gcl {
 
 constexpr uint32_t kWideSpinLimit = 1u << 24;      // lock attempts (~1 s with back-off)
-constexpr uint32_t kWideGateSpinLimit = 1u << 30;  // gate polls, 1 us apart
+constexpr uint32_t kWideGateSpinLimit = 1u << 26;  // gate polls, up to 32 us apart
 
 struct WideHdr {
   uint32_t D;          // level of the first leaf
@@ -583,6 +583,9 @@ __device__ __noinline__ int wide_try_publish(const WidePtrs& P, const WideArgs& 
 __device__ __noinline__ int32_t wide_gate(WideHdr* H, uint32_t need, uint64_t deadline) {
   int32_t st = kOk;
   if (lane_id() == 0) {
+    // back off from 0.5 us to 32 us between polls: many warps may wait on
+    // the same counter, and a level lasts far longer than the poll period
+    uint32_t sleep_ns = 512;
     for (uint32_t i = 0;; ++i) {
       if (*(volatile uint32_t*)&H->done >= need) break;
       const int32_t hs = *(volatile int32_t*)&H->status;
@@ -590,11 +593,12 @@ __device__ __noinline__ int32_t wide_gate(WideHdr* H, uint32_t need, uint64_t de
         st = hs;
         break;
       }
-      if (i >= kWideGateSpinLimit || (deadline && (i & 63u) == 0 && global_ns() > deadline)) {
+      if (i >= kWideGateSpinLimit || (deadline && (i & 15u) == 0 && global_ns() > deadline)) {
         st = kTimeout;
         break;
       }
-      __nanosleep(1000);
+      __nanosleep(sleep_ns);
+      if (sleep_ns < 32768) sleep_ns <<= 1;
     }
     __threadfence();
   }

@@ -155,21 +155,27 @@ using namespace gcl;
 
 namespace {
 
+// Device buffer allocated in stream order on its context's stream: growing
+// or freeing it never waits for the rest of the device (a cudaFree would,
+// stalling every other context's work -- the serving loop runs several).
 struct DevBuf {
   void* p = nullptr;
   size_t cap = 0;
+  cudaStream_t stream = nullptr;
   cudaError_t ensure(size_t bytes) {
     if (bytes <= cap && p) return cudaSuccess;
-    if (p) cudaFree(p);
+    // grow by half again at least, so that a growing buffer is replaced
+    // only a logarithmic number of times
+    const size_t want = std::max<size_t>(std::max<size_t>(bytes, 256), cap + cap / 2);
+    if (p) cudaFreeAsync(p, stream);
     p = nullptr;
     cap = 0;
-    size_t want = std::max<size_t>(bytes, 256);
-    cudaError_t e = cudaMalloc(&p, want);
+    cudaError_t e = cudaMallocAsync(&p, want, stream);
     if (e == cudaSuccess) cap = want;
     return e;
   }
   void release() {
-    if (p) cudaFree(p);
+    if (p) cudaFreeAsync(p, stream);
     p = nullptr;
     cap = 0;
   }
@@ -191,9 +197,19 @@ struct gcl_context {
   DevBuf sp_work[kSpBuckets], sp_work_big;
   // wide search of one graph: shared region and per-warp slots
   DevBuf wide_sh, wide_slots;
+  template <typename F>
+  void each_buf(F f) {
+    for (DevBuf& b : sp_work) f(b);
+    DevBuf* bufs[] = {&work, &work_big, &sp_work_big, &deferred, &wide_sh, &wide_slots,
+                      &overflow_list, &large_list, &sp_fail_list, &order, &voff, &eoff,
+                      &rowptr, &col, &color, &ooff, &dense, &roff, &rows, &label, &stats,
+                      &status};
+    for (DevBuf* b : bufs) f(*b);
+  }
   int64_t wide_min_n = kW64MaxN + 1;
   uint64_t workspace_bytes = 0;  // per-pass workspace cap, 0 = GCL_WORKSPACE_GB
   int64_t wide_max_warps = 0;    // 0 = as many as fit
+  bool smem_stage = true;        // sparse and wide kernels stage per-step arrays in shared memory
   DevBuf deferred, overflow_list, large_list, sp_fail_list, order;
   // staging for host-pointer calls
   DevBuf voff, eoff, rowptr, col, color, ooff, dense, roff, rows, label, stats, status;
@@ -262,6 +278,17 @@ int gcl_create(int device, gcl_context** out) {
   c->device = device;
   cudaError_t e = cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) {
+    c->each_buf([&](DevBuf& b) { b.stream = c->stream; });
+    // keep freed stream-ordered memory in the device's default pool instead
+    // of returning it at every synchronization (it is reused by the next
+    // allocation of this process)
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+      uint64_t keep = ~0ull;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+  }
   int per_sm = 0;
   if (e == cudaSuccess)
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, w64_batch_kernel, kW64Threads, 0);
@@ -280,8 +307,11 @@ int gcl_create(int device, gcl_context** out) {
     e = cudaFuncSetAttribute(wide_items_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              kSpSmemPerBlock);
   if (e != cudaSuccess) {
-    if (c->stream) cudaStreamDestroy(c->stream);
     c->deferred.release();
+    if (c->stream) {
+      cudaStreamSynchronize(c->stream);
+      cudaStreamDestroy(c->stream);
+    }
     delete c;
     return cuda_status(e);
   }
@@ -293,14 +323,11 @@ int gcl_destroy(gcl_context* c) {
   if (!c) return GCL_ERR_ARG;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
-  for (DevBuf& b : c->sp_work) b.release();
-  DevBuf* bufs[] = {&c->work, &c->work_big, &c->sp_work_big, &c->deferred, &c->wide_sh,
-                    &c->wide_slots,
-                    &c->overflow_list, &c->large_list, &c->sp_fail_list, &c->order, &c->voff, &c->eoff, &c->rowptr, &c->col, &c->color,
-                    &c->ooff, &c->dense, &c->roff, &c->rows, &c->label, &c->stats,
-                    &c->status};
-  for (DevBuf* b : bufs) b->release();
-  if (c->stream) cudaStreamDestroy(c->stream);
+  c->each_buf([](DevBuf& b) { b.release(); });
+  if (c->stream) {
+    cudaStreamSynchronize(c->stream);
+    cudaStreamDestroy(c->stream);
+  }
   delete c;
   return GCL_OK;
 }
@@ -393,7 +420,7 @@ int gcl_canon_batch_device_async(gcl_context* c, int count, const int64_t* d_vof
       if ((uint32_t)max_n < lo) break;
       const uint32_t nmax = std::min<uint32_t>((uint32_t)max_n, kSpBucketHi[bk]);
       const uint64_t sb1 = sp_layout(nmax, m2max, kSpPool, cap1).bytes;
-      uint64_t smw = sp_smem_bytes(nmax);
+      uint64_t smw = c->smem_stage ? sp_smem_bytes(nmax) : 0;
       if (smw * kSpWarps > (uint64_t)kSpSmemPerBlock) smw = 0;  // device memory only
       int per_sm = 0;
       GCL_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sp_batch_kernel, kSpThreads,
@@ -445,6 +472,10 @@ int gcl_set_option(gcl_context* c, int option, int64_t value) {
       if (value < 0) return GCL_ERR_ARG;
       c->wide_max_warps = value;
       return GCL_OK;
+    case GCL_OPT_SMEM_STAGE:
+      if (value != 0 && value != 1) return GCL_ERR_ARG;
+      c->smem_stage = value != 0;
+      return GCL_OK;
     default:
       return GCL_ERR_ARG;
   }
@@ -467,7 +498,7 @@ int gcl_canon_wide_device_async(gcl_context* c, const int32_t* d_rowptr, const i
       1, std::min<uint64_t>((uint64_t)max_aut, kWideStoreBytes / per_aut));
   const WideLayout WL = wide_layout(un, m2, cap);
   const SpLayout Lo = sp_layout(un, m2, kWidePool, 0, cap);
-  uint64_t smw = sp_smem_bytes(un);
+  uint64_t smw = c->smem_stage ? sp_smem_bytes(un) : 0;
   if (smw * kSpWarps > (uint64_t)kSpSmemPerBlock) smw = 0;
   int per_sm = 0;
   GCL_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, wide_items_kernel, kSpThreads,

@@ -145,20 +145,28 @@ namespace {
 
 using Clock = std::chrono::steady_clock;
 
+// Pinned host buffer.  Freeing pinned memory waits for the whole device, so
+// a buffer that grows keeps its old allocation until the server is
+// destroyed (growth is geometric, so the retired ones add up to less than
+// twice the final size).
 struct HostBuf {
   void* p = nullptr;
   size_t cap = 0;
+  std::vector<void*> retired;
   cudaError_t ensure(size_t bytes) {
     if (bytes <= cap && p) return cudaSuccess;
-    if (p) cudaFreeHost(p);
-    p = nullptr;
-    cap = 0;
-    const size_t want = std::max<size_t>(bytes + bytes / 2, 4096);
-    cudaError_t e = cudaHostAlloc(&p, want, cudaHostAllocDefault);
-    if (e == cudaSuccess) cap = want;
-    return e;
+    const size_t want = std::max<size_t>(std::max<size_t>(bytes, 4096), 2 * cap);
+    void* q = nullptr;
+    cudaError_t e = cudaHostAlloc(&q, want, cudaHostAllocDefault);
+    if (e != cudaSuccess) return e;
+    if (p) retired.push_back(p);
+    p = q;
+    cap = want;
+    return cudaSuccess;
   }
   void release() {
+    for (void* q : retired) cudaFreeHost(q);
+    retired.clear();
     if (p) cudaFreeHost(p);
     p = nullptr;
     cap = 0;
@@ -169,21 +177,24 @@ struct HostBuf {
   }
 };
 
+// Device buffer allocated in stream order on its lane's stream (no wait for
+// the other lanes when it grows).
 struct DevMem {
   void* p = nullptr;
   size_t cap = 0;
+  cudaStream_t stream = nullptr;
   cudaError_t ensure(size_t bytes) {
     if (bytes <= cap && p) return cudaSuccess;
-    if (p) cudaFree(p);
+    const size_t want = std::max<size_t>(std::max<size_t>(bytes, 4096), 2 * cap);
+    if (p) cudaFreeAsync(p, stream);
     p = nullptr;
     cap = 0;
-    const size_t want = std::max<size_t>(bytes + bytes / 2, 4096);
-    cudaError_t e = cudaMalloc(&p, want);
+    cudaError_t e = cudaMallocAsync(&p, want, stream);
     if (e == cudaSuccess) cap = want;
     return e;
   }
   void release() {
-    if (p) cudaFree(p);
+    if (p) cudaFreeAsync(p, stream);
     p = nullptr;
     cap = 0;
   }
@@ -243,6 +254,7 @@ struct MemoEntry {
 enum { kSmall = 0, kMid = 1, kBig = 2, kLarge = 3, kClasses = 4 };
 
 struct Lane {
+  Clock::time_point t_launch;
   gcl_context* ctx = nullptr;
   cudaStream_t s = nullptr;
   int cls = kSmall;
@@ -591,6 +603,9 @@ void complete(gcl_server* S, Lane* L) {
   {
     std::lock_guard<std::mutex> lk(S->mu);
     S->st.batches += 1;
+    S->st.class_batches[L->cls] += 1;
+    S->st.class_batch_ns[L->cls] +=
+        std::chrono::duration_cast<std::chrono::nanoseconds>(now - L->t_launch).count();
     S->st.graphs += L->count;
     S->st.class_repeats += repeats;
     S->st.classes += classes;
@@ -651,6 +666,14 @@ void dispatcher(gcl_server* S) {
       }
       if (L->reqs.empty()) continue;
       L->busy = true;
+      L->t_launch = Clock::now();
+      {
+        int64_t q = 0;
+        for (Req* r : L->reqs)
+          q += std::chrono::duration_cast<std::chrono::nanoseconds>(L->t_launch - r->t0).count();
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->st.class_queue_ns[L->cls] += q / (int64_t)L->reqs.size();
+      }
       L->ready.store(false);
       int rc = launch(S, L);
       if (rc == GCL_OK) {
@@ -758,10 +781,18 @@ int gcl_serve_create(int device, const gcl_serve_config* cfg, gcl_server** out) 
     rc = gcl_create(device, &L->ctx);
     if (rc == GCL_OK) {
       L->s = (cudaStream_t)gcl_stream(L->ctx);
+      DevMem* db[] = {&L->d_voff, &L->d_eoff, &L->d_rp, &L->d_col, &L->d_color, &L->d_roff,
+                      &L->d_rows, &L->d_label, &L->d_status, &L->d_hash, &L->d_class, &L->d_seen};
+      for (DevMem* b : db) b->stream = L->s;
       if (!L->large) rc = gcl_set_option(L->ctx, GCL_OPT_WORKSPACE_BYTES, c.lane_bytes);
       // a wide search takes one block per SM, leaving room on every SM for
       // the batches of the other lanes
       else rc = gcl_set_option(L->ctx, GCL_OPT_WIDE_MAX_WARPS, (int64_t)std::max(dev_sms, 1) * 4);
+      // searches of big and large graphs run for long: their blocks keep
+      // their per-step arrays in device memory so that they never fill an
+      // SM's shared memory and lock the small lanes' kernels out
+      if (rc == GCL_OK && (L->cls == kBig || L->large))
+        rc = gcl_set_option(L->ctx, GCL_OPT_SMEM_STAGE, 0);
     }
   }
   if (rc == GCL_OK) rc = rc_of(S->keys.ensure((size_t)c.table_slots * 8));
@@ -774,14 +805,15 @@ int gcl_serve_create(int device, const gcl_serve_config* cfg, gcl_server** out) 
   if (rc == GCL_OK) rc = rc_of(cudaDeviceSynchronize());
   if (rc != GCL_OK) {
     for (Lane* L : S->lanes) {
+      L->release();  // frees on the lane's stream, before the context goes
       if (L->ctx) gcl_destroy(L->ctx);
-      L->release();
       delete L;
     }
     S->keys.release();
     S->vals.release();
     S->store.release();
     S->top.release();
+    cudaDeviceSynchronize();
     delete S;
     return rc;
   }
@@ -801,14 +833,15 @@ int gcl_serve_destroy(gcl_server* S) {
   cudaSetDevice(S->device);
   for (Lane* L : S->lanes) {
     if (L->s) cudaStreamSynchronize(L->s);
+    L->release();  // frees on the lane's stream, before the context goes
     if (L->ctx) gcl_destroy(L->ctx);
-    L->release();
     delete L;
   }
   S->keys.release();
   S->vals.release();
   S->store.release();
   S->top.release();
+  cudaDeviceSynchronize();
   for (auto& q : S->q)
     for (Req* r : q) delete r;
   delete S;

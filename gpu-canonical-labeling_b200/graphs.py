@@ -406,7 +406,9 @@ def serving_size(rng: np.random.Generator, n_lo: int = 10, n_mid: int = 128,
     u = rng.random()
     if u < 0.90:
         return int(rng.integers(n_lo, n_mid + 1))
-    lo, hi = (n_mid, n_big) if u < 0.99 else (n_big, n_max)
+    lo, hi = (n_mid, min(n_big, n_max)) if u < 0.99 else (min(n_big, n_max), n_max)
+    if hi <= lo + 1:
+        return int(hi)
     return int(min(hi, max(lo + 1, round(math.exp(rng.uniform(math.log(lo + 1), math.log(hi)))))))
 
 

@@ -82,10 +82,15 @@ void* gcl_stream(gcl_context* ctx);
  *   environment variable, default 4 GiB.
  * GCL_OPT_WIDE_MAX_WARPS: upper bound on the warps of a wide search (0 = as
  *   many as fit on the GPU), to leave SMs to concurrent work.
+ * GCL_OPT_SMEM_STAGE: 1 (default) lets the kernels for n > 64 keep their
+ *   per-step arrays in shared memory (up to 200 KiB per block, which leaves
+ *   little room on an SM for other kernels); 0 keeps them in device memory,
+ *   for contexts whose long searches share the GPU with latency-bound work.
  * Returns GCL_ERR_ARG for an unknown option or value. */
 #define GCL_OPT_WIDE_MIN_N 1
 #define GCL_OPT_WORKSPACE_BYTES 2
 #define GCL_OPT_WIDE_MAX_WARPS 3
+#define GCL_OPT_SMEM_STAGE 4
 int gcl_set_option(gcl_context* ctx, int option, int64_t value);
 
 /* ---- one graph (drop-in for Nauty_Parallel, src/nauty_parallel.h:9-13) ---
@@ -207,7 +212,13 @@ int gcl_iso(gcl_context* ctx, const int32_t* rowptr1, const int32_t* col1,
  * repeats of an earlier input are answered from a host-side memo of recent
  * results without a launch.
  *
- * Thread safety: submit, poll and stats may be called from any threads. */
+ * Thread safety: submit, poll and stats may be called from any threads.
+ *
+ * Each lane is a CUDA stream.  Streams beyond CUDA_DEVICE_MAX_CONNECTIONS
+ * (default 8) share hardware work queues, and a short batch then waits
+ * behind a long search that happens to share its queue: set the variable to
+ * at least the number of lanes (32 is the maximum) before the process
+ * first uses CUDA. */
 typedef struct gcl_server gcl_server;
 
 typedef struct {
@@ -248,6 +259,9 @@ typedef struct {
 typedef struct {
   int64_t submitted, completed, batches, graphs, memo_hits, class_repeats, classes;
   int64_t large_graphs;
+  /* per request class (small, mid, big, large): batches launched, their
+     summed launch-to-result time and summed time queued before launch (ns) */
+  int64_t class_batches[4], class_batch_ns[4], class_queue_ns[4];
 } gcl_serve_stats;
 
 /* cfg may be NULL (all defaults); zero fields take their default. */

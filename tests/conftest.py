@@ -15,6 +15,8 @@ PKG_NAME = "gpu-canonical-labeling_b200"
 # Bound every graph's device search in tests: a regression that loops stops
 # with GCL_ERR_TIMEOUT instead of holding the GPU.
 os.environ.setdefault("GCL_GRAPH_BUDGET_S", "30")
+# one hardware work queue per stream for the serving tests' many lanes
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 
 def pytest_configure(config):
