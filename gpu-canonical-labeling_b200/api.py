@@ -46,6 +46,7 @@ GCL_OPT_WIDE_MIN_N = 1
 GCL_OPT_WORKSPACE_BYTES = 2
 GCL_OPT_WIDE_MAX_WARPS = 3
 GCL_OPT_SMEM_STAGE = 4
+GCL_OPT_STREAM_PRIORITY = 5
 GCL_MAX_N = 65536
 
 

@@ -44,6 +44,8 @@ struct Deferred {
   int next;            // work counter of the first pass
   int sp_fail_count;   // n > 64 graphs that outgrew pool or ring
   int next_sp_fail;
+  int sp_fail2_count;  // ... and the middle rerun's pool or ring
+  int next_sp_fail2;
   int large_count[kSpBuckets];  // n > 64 graphs per size bucket
   int next_large[kSpBuckets];
 };
@@ -80,8 +82,14 @@ __global__ void __launch_bounds__(kOrderThreads)
 constexpr int kSpSmemPerBlock = 200 * 1024;  // dynamic shared memory cap of one sparse block
 constexpr uint32_t kWidePool = 64;  // per-level orbit arrays of a wide-search warp
 constexpr uint64_t kWideStoreBytes = 1ull << 30;  // automorphism store of a wide search
-constexpr uint32_t kSpPool = 8;     // per-level orbit arrays in the first sparse pass
-constexpr uint32_t kSpAutCap = 64;  // ring entries in the first sparse pass
+// Per-level orbit arrays and automorphism-ring entries of the sparse passes:
+// the first pass (n <= 4096 / larger), then a middle rerun of the graphs
+// that outgrew them, then a rerun with a full-size pool and ring.  Each
+// tier's slots are smaller than the next one's, so more warps fit in the
+// workspace budget.
+constexpr uint32_t kSpPool = 32, kSpPoolHuge = 8;
+constexpr uint32_t kSpAutCap = 256, kSpAutCapHuge = 64;
+constexpr uint32_t kSpPoolMid = 256, kSpAutCapMid = 2048;
 
 __global__ void __launch_bounds__(kSpThreads)
     sp_batch_kernel(BatchArgs A, const int* list, const int* count, int* next, int* fail_list,
@@ -194,14 +202,16 @@ struct gcl_context {
   DevBuf work_big;
   uint32_t work_big_aut = 0;
   int big_slots = 0;
-  DevBuf sp_work[kSpBuckets], sp_work_big;
+  DevBuf sp_work[kSpBuckets], sp_work_mid, sp_work_big;
   // wide search of one graph: shared region and per-warp slots
   DevBuf wide_sh, wide_slots;
   template <typename F>
   void each_buf(F f) {
     for (DevBuf& b : sp_work) f(b);
-    DevBuf* bufs[] = {&work, &work_big, &sp_work_big, &deferred, &wide_sh, &wide_slots,
-                      &overflow_list, &large_list, &sp_fail_list, &order, &voff, &eoff,
+    DevBuf* bufs[] = {&work, &work_big, &sp_work_mid, &sp_work_big, &deferred, &wide_sh,
+                      &wide_slots,
+                      &overflow_list, &large_list, &sp_fail_list, &sp_fail_list2, &order,
+                      &voff, &eoff,
                       &rowptr, &col, &color, &ooff, &dense, &roff, &rows, &label, &stats,
                       &status};
     for (DevBuf* b : bufs) f(*b);
@@ -210,7 +220,7 @@ struct gcl_context {
   uint64_t workspace_bytes = 0;  // per-pass workspace cap, 0 = GCL_WORKSPACE_GB
   int64_t wide_max_warps = 0;    // 0 = as many as fit
   bool smem_stage = true;        // sparse and wide kernels stage per-step arrays in shared memory
-  DevBuf deferred, overflow_list, large_list, sp_fail_list, order;
+  DevBuf deferred, overflow_list, large_list, sp_fail_list, sp_fail_list2, order;
   // staging for host-pointer calls
   DevBuf voff, eoff, rowptr, col, color, ooff, dense, roff, rows, label, stats, status;
 };
@@ -412,14 +422,16 @@ int gcl_canon_batch_device_async(gcl_context* c, int count, const int64_t* d_vof
     // graphs with n > 64: one sparse pass per size bucket, then a rerun of
     // the graphs that outgrew the first passes' orbit pool or ring
     const uint64_t m2max = (uint64_t)std::max<int64_t>(max_m2, 1);
-    const uint32_t cap1 = std::min<uint32_t>(maut, kSpAutCap);
+    const uint32_t cap1 = std::min<uint32_t>(maut, max_n <= 4096 ? kSpAutCap : kSpAutCapHuge);
+    const uint32_t pool1 = max_n <= 4096 ? kSpPool : kSpPoolHuge;
     const uint64_t budget = ctx_workspace(c);
     GCL_TRY(c->sp_fail_list.ensure((size_t)count * sizeof(int)));
+    GCL_TRY(c->sp_fail_list2.ensure((size_t)count * sizeof(int)));
     for (int bk = 0; bk < kSpBuckets; ++bk) {
       const uint32_t lo = bk == 0 ? (uint32_t)kW64MaxN + 1 : kSpBucketHi[bk - 1] + 1;
       if ((uint32_t)max_n < lo) break;
       const uint32_t nmax = std::min<uint32_t>((uint32_t)max_n, kSpBucketHi[bk]);
-      const uint64_t sb1 = sp_layout(nmax, m2max, kSpPool, cap1).bytes;
+      const uint64_t sb1 = sp_layout(nmax, m2max, pool1, cap1).bytes;
       uint64_t smw = c->smem_stage ? sp_smem_bytes(nmax) : 0;
       if (smw * kSpWarps > (uint64_t)kSpSmemPerBlock) smw = 0;  // device memory only
       int per_sm = 0;
@@ -437,11 +449,30 @@ int gcl_canon_batch_device_async(gcl_context* c, int count, const int64_t* d_vof
                         c->stream>>>(Sa, (const int*)c->large_list.p + (int64_t)bk * count,
                                      &D->large_count[bk], &D->next_large[bk],
                                      (int*)c->sp_fail_list.p, &D->sp_fail_count, nmax, m2max,
-                                     kSpPool, cap1, sb1, smw);
+                                     pool1, cap1, sb1, smw);
       GCL_TRY(cudaGetLastError());
     }
-    // rerun with a representative array per level and the full ring
+    // middle rerun: a larger pool and ring, still many warps
     const uint32_t nmax = (uint32_t)max_n;
+    {
+      const uint32_t poolm = std::min<uint32_t>(nmax + 2, kSpPoolMid);
+      const uint32_t capm = std::min<uint32_t>(maut, kSpAutCapMid);
+      const uint64_t sbm = sp_layout(nmax, m2max, poolm, capm).bytes;
+      int per_sm = 0;
+      GCL_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sp_batch_kernel, kSpThreads, 0));
+      int64_t slotsm = std::min<int64_t>((int64_t)c->sms * std::max(per_sm, 1) * kSpWarps,
+                                         (int64_t)(budget / sbm));
+      slotsm = std::min<int64_t>(slotsm, ((int64_t)count + kSpWarps - 1) / kSpWarps * kSpWarps);
+      slotsm = std::max<int64_t>(kSpWarps, slotsm / kSpWarps * kSpWarps);
+      GCL_TRY(c->sp_work_mid.ensure((size_t)(slotsm * sbm)));
+      BatchArgs Sm = A;
+      Sm.work = (uint8_t*)c->sp_work_mid.p;
+      sp_batch_kernel<<<(int)(slotsm / kSpWarps), kSpThreads, 0, c->stream>>>(
+          Sm, (const int*)c->sp_fail_list.p, &D->sp_fail_count, &D->next_sp_fail,
+          (int*)c->sp_fail_list2.p, &D->sp_fail2_count, nmax, m2max, poolm, capm, sbm, 0);
+      GCL_TRY(cudaGetLastError());
+    }
+    // last rerun with a representative array per level and the full ring
     const uint32_t pool2 = nmax + 2;
     const uint64_t sb2 = sp_layout(nmax, m2max, pool2, maut).bytes;
     int64_t slots2 = std::max<int64_t>(1, std::min<int64_t>((int64_t)c->sms,
@@ -450,7 +481,8 @@ int gcl_canon_batch_device_async(gcl_context* c, int count, const int64_t* d_vof
     BatchArgs Sb = A;
     Sb.work = (uint8_t*)c->sp_work_big.p;
     sp_batch_kernel<<<(int)slots2, kSpThreads, 0, c->stream>>>(
-        Sb, (const int*)c->sp_fail_list.p, &D->sp_fail_count, &D->next_sp_fail, nullptr, nullptr,
+        Sb, (const int*)c->sp_fail_list2.p, &D->sp_fail2_count, &D->next_sp_fail2, nullptr,
+        nullptr,
         nmax, m2max, pool2, maut, sb2, 0);
     GCL_TRY(cudaGetLastError());
   }
@@ -476,6 +508,20 @@ int gcl_set_option(gcl_context* c, int option, int64_t value) {
       if (value != 0 && value != 1) return GCL_ERR_ARG;
       c->smem_stage = value != 0;
       return GCL_OK;
+    case GCL_OPT_STREAM_PRIORITY: {
+      if (value != 0 && value != 1) return GCL_ERR_ARG;
+      int lo = 0, hi = 0;
+      GCL_TRY(cudaSetDevice(c->device));
+      GCL_TRY(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+      cudaStream_t s2 = nullptr;
+      GCL_TRY(cudaStreamCreateWithPriority(&s2, cudaStreamNonBlocking, value ? hi : lo));
+      // work and stream-ordered frees issued so far finish on the old stream
+      cudaStreamSynchronize(c->stream);
+      cudaStreamDestroy(c->stream);
+      c->stream = s2;
+      c->each_buf([&](DevBuf& b) { b.stream = s2; });
+      return GCL_OK;
+    }
     default:
       return GCL_ERR_ARG;
   }

@@ -739,11 +739,11 @@ int gcl_serve_create(int device, const gcl_serve_config* cfg, gcl_server** out) 
   if (cfg) c = *cfg;
   if (c.lanes <= 0) c.lanes = 3;
   if (c.mid_lanes <= 0) c.mid_lanes = 3;
-  if (c.big_lanes <= 0) c.big_lanes = 2;
+  if (c.big_lanes <= 0) c.big_lanes = 8;
   if (c.large_lanes <= 0) c.large_lanes = 4;
   if (c.max_batch <= 0) c.max_batch = 8192;
   if (c.mid_batch <= 0) c.mid_batch = 512;
-  if (c.big_batch <= 0) c.big_batch = 64;
+  if (c.big_batch <= 0) c.big_batch = 8;
   if (c.mid_n <= 0) c.mid_n = 65;
   if (c.big_n <= 0) c.big_n = 257;
   if (c.large_n <= 0) c.large_n = 2049;
@@ -779,6 +779,10 @@ int gcl_serve_create(int device, const gcl_serve_config* cfg, gcl_server** out) 
     L->large = L->cls == kLarge;
     S->lanes.push_back(L);
     rc = gcl_create(device, &L->ctx);
+    // short work first: small and mid lanes get high-priority streams
+    if (rc == GCL_OK)
+      rc = gcl_set_option(L->ctx, GCL_OPT_STREAM_PRIORITY,
+                          L->cls == kSmall || L->cls == kMid ? 1 : 0);
     if (rc == GCL_OK) {
       L->s = (cudaStream_t)gcl_stream(L->ctx);
       DevMem* db[] = {&L->d_voff, &L->d_eoff, &L->d_rp, &L->d_col, &L->d_color, &L->d_roff,

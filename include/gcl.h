@@ -86,11 +86,16 @@ void* gcl_stream(gcl_context* ctx);
  *   per-step arrays in shared memory (up to 200 KiB per block, which leaves
  *   little room on an SM for other kernels); 0 keeps them in device memory,
  *   for contexts whose long searches share the GPU with latency-bound work.
+ * GCL_OPT_STREAM_PRIORITY: 1 replaces the context's stream by one of the
+ *   highest priority (the block scheduler then starts its blocks before those
+ *   of lower-priority streams), 0 by one of the lowest.  Waits for the
+ *   context's work first; the stream gcl_stream returned before is gone.
  * Returns GCL_ERR_ARG for an unknown option or value. */
 #define GCL_OPT_WIDE_MIN_N 1
 #define GCL_OPT_WORKSPACE_BYTES 2
 #define GCL_OPT_WIDE_MAX_WARPS 3
 #define GCL_OPT_SMEM_STAGE 4
+#define GCL_OPT_STREAM_PRIORITY 5
 int gcl_set_option(gcl_context* ctx, int option, int64_t value);
 
 /* ---- one graph (drop-in for Nauty_Parallel, src/nauty_parallel.h:9-13) ---
@@ -224,11 +229,11 @@ typedef struct gcl_server gcl_server;
 typedef struct {
   int lanes;           /* lanes for requests whose graphs have n < mid_n, default 3 */
   int mid_lanes;       /* lanes for mid_n <= n < big_n, default 3              */
-  int big_lanes;       /* lanes for big_n <= n < large_n, default 2            */
+  int big_lanes;       /* lanes for big_n <= n < large_n, default 8            */
   int large_lanes;     /* lanes for n >= large_n (wide search), default 4      */
   int max_batch;       /* graphs per small batch, default 8192                */
   int mid_batch;       /* graphs per mid batch, default 512                   */
-  int big_batch;       /* graphs per big batch, default 64                    */
+  int big_batch;       /* graphs per big batch, default 8                     */
   int mid_n;           /* default 65                                          */
   int big_n;           /* default 257                                         */
   int large_n;         /* default 2049                                        */
