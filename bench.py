@@ -17,6 +17,14 @@ Reported JSON line (rank 0):
   cpu_baseline  the reference's own sequential path (oracle/_ref), on all
          host cores, over the same graphs
   plain_per_launch  the same library launched once per graph (the plain form)
+  serving  an open-loop Poisson request stream through the serving loop
+         (gcl_serve_replay): p50 / p99 latency from the scheduled arrival,
+         throughput, per-size and per-lane-class figures, and the plain form
+         (one gcl_canon_one per graph, FIFO) under the same arrivals
+  single_graph  search-heavy single graphs (random 3-regular n = 1024, 4096;
+         tori 32x32, 64x64) through gcl_canon_one (the wide search), each also
+         relabeled, with the reference's CPU path beside the ones it finishes
+         in seconds
 
 --impl reference: the reference's CPU implementation of the path (its own
 sequential sources compiled into oracle/_ref, else the C restatement) on all
