@@ -201,6 +201,28 @@ def reference_arm(args):
 
 
 # --------------------------------------------------------------------------
+# Multi-rank timing: every rank canonizes its own batch (graphs are
+# independent: no data-path collective); the job's time is the slowest rank's
+# --------------------------------------------------------------------------
+def max_over_ranks(seconds_or_ms: float, world: int, device=None) -> float:
+    """The largest value over all ranks (an all-reduce MAX; the value itself
+    when there is one rank).  Every rank must call it at the same point."""
+    if world <= 1:
+        return seconds_or_ms
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([seconds_or_ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(graphs_per_rank: int, world: int, steps: int, seconds: float) -> float:
+    """Whole-job graphs/s: the graphs all ranks processed over the slowest
+    rank's time (weak scaling: the per-rank batch is fixed)."""
+    return world * graphs_per_rank * steps / seconds
+
+
+# --------------------------------------------------------------------------
 # GPU side
 # --------------------------------------------------------------------------
 class Clocks:
@@ -360,12 +382,8 @@ def gpu_arm(args):
     clocks.mark(tw0, time.perf_counter())
     clk = clocks.stop()
     per = np.array([a.elapsed_time(b) for a, b in evs])  # ms
-    dev_ms = float(per.sum())
-    if world > 1:
-        t = torch.tensor([dev_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dev_ms = float(t.item())
-    value = world * count * args.steps / (dev_ms / 1e3)
+    dev_ms = max_over_ranks(float(per.sum()), world, dev)
+    value = job_rate(count, world, args.steps, dev_ms / 1e3)
 
     # end to end through the C ABI: pinned host buffers, copies inside
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
@@ -397,12 +415,7 @@ def gpu_arm(args):
             e2e_call(dense)
             ts.append(time.perf_counter() - t0)
         barrier()
-        s = float(np.sum(ts)) if ts else float("nan")
-        if world > 1:
-            t = torch.tensor([s], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            s = float(t.item())
-        return s
+        return max_over_ranks(float(np.sum(ts)) if ts else float("nan"), world, dev)
 
     e2e_s = e2e_run(False)
     e2e_dense_s = e2e_run(True)
@@ -428,10 +441,10 @@ def gpu_arm(args):
                        "parallelism": f"graph-sharded x{world} (no collective)",
                        "l2": "flushed between steps (256 MiB write outside the timed events)",
                        "output": "bit-packed canonical rows, stats and status per graph"},
-            "e2e": {"value": world * count * args.steps / e2e_s, "unit": UNIT,
+            "e2e": {"value": job_rate(count, world, args.steps, e2e_s), "unit": UNIT,
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                     "output": "bit-packed canonical rows (n x ceil(n/64) words per graph)"},
-            "e2e_dense": {"value": world * count * args.steps / e2e_dense_s, "unit": UNIT,
+            "e2e_dense": {"value": job_rate(count, world, args.steps, e2e_dense_s), "unit": UNIT,
                           "h2d_bytes_per_step": int(h2d_dense),
                           "d2h_bytes_per_step": int(d2h_dense),
                           "output": "n*n byte matrices (the reference's Nauty_Parallel form)"},

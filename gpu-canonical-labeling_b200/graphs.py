@@ -484,6 +484,21 @@ class Arena:
         return o
 
 
+def shard_ranges(sizes: Sequence[int], world: int) -> List[Tuple[int, int]]:
+    """Split graphs 0..len(sizes) into `world` contiguous ranges of nearly
+    equal cost, the cost of a graph taken as n^2 + 1 (its canonical matrix and
+    a search that grows with n).  Each rank canonizes its range on its own
+    GPU; the only exchange is gathering the results."""
+    cost = np.asarray(sizes, dtype=np.float64) ** 2 + 1.0
+    cum = np.concatenate([[0.0], np.cumsum(cost)])
+    cuts = [0]
+    for r in range(1, world):
+        cuts.append(int(np.searchsorted(cum, cum[-1] * r / world, side="left")))
+    cuts.append(len(sizes))
+    cuts = np.maximum.accumulate(np.asarray(cuts))
+    return [(int(cuts[r]), int(cuts[r + 1])) for r in range(world)]
+
+
 def pack(graphs: Sequence[Graph]) -> Arena:
     count = len(graphs)
     ns = np.array([g.n for g in graphs], dtype=np.int64)
