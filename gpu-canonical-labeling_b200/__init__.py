@@ -15,5 +15,5 @@ _os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 from . import graphs  # noqa: E402,F401
 from .api import (  # noqa: E402,F401
     BatchResult, CanonResult, Context, GclError, Nauty_Parallel, Server, canon, canon_batch,
-    default_context, is_isomorphic, load_library,
+    default_context, group_order, is_isomorphic, load_library, perm_group_order,
 )

@@ -39,7 +39,7 @@ EXPORTS = [
     "gcl_canon_one", "gcl_canon_batch", "gcl_canon_batch_device_async", "gcl_sync", "gcl_iso",
     "gcl_canon_batch_noalloc", "gcl_set_option", "gcl_canon_wide_device_async",
     "gcl_serve_create", "gcl_serve_destroy", "gcl_serve_submit", "gcl_serve_poll",
-    "gcl_serve_stats_get", "gcl_serve_replay",
+    "gcl_serve_stats_get", "gcl_serve_replay", "gcl_group_order", "gcl_perm_group_order",
 ]
 
 GCL_OPT_WIDE_MIN_N = 1
@@ -88,11 +88,17 @@ def load_library(path: str = LIB_PATH):
     lib.gcl_canon_batch_noalloc.argtypes = [_P, ctypes.c_int, _P, _P, _P, _P, _P, ctypes.c_int,
                                             ctypes.c_int, _P, _P, _P, _P, _P]
     lib.gcl_set_option.argtypes = [_P, ctypes.c_int, ctypes.c_int64]
+    lib.gcl_group_order.argtypes = [_P, _P, _P, _P, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                    ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int64)]
+    lib.gcl_perm_group_order.argtypes = [ctypes.c_int, _P, ctypes.c_int64,
+                                         ctypes.POINTER(ctypes.c_double), ctypes.c_char_p,
+                                         ctypes.c_int]
     lib.gcl_canon_wide_device_async.argtypes = [_P, _P, _P, _P, ctypes.c_int, ctypes.c_int64,
                                                 ctypes.c_int, _P, _P, _P, _P, _P]
     for name in ("gcl_create", "gcl_destroy", "gcl_sync", "gcl_canon_one", "gcl_canon_batch",
                  "gcl_canon_batch_device_async", "gcl_iso", "gcl_canon_batch_noalloc",
-                 "gcl_set_option", "gcl_canon_wide_device_async"):
+                 "gcl_set_option", "gcl_canon_wide_device_async", "gcl_group_order",
+                 "gcl_perm_group_order"):
         getattr(lib, name).restype = ctypes.c_int
     _lib = lib
     return lib
@@ -182,6 +188,35 @@ def canon(g: Graph, max_aut: int = 10000, ctx: Optional[Context] = None) -> Cano
                                ctypes.byref(nodes), ctypes.byref(naut))
     _check(rc, "gcl_canon_one")
     return CanonResult(out, int(nodes.value), int(naut.value))
+
+
+def group_order(g: Graph, ctx: Optional[Context] = None) -> int:
+    """|Aut(g)| (colour-preserving), exact, from the automorphisms the wide
+    search finds (gcl_group_order)."""
+    ctx = ctx or default_context()
+    rp, cl, co = _csr(g)
+    lg = ctypes.c_double()
+    ngen = ctypes.c_int64()
+    buf = ctypes.create_string_buffer(1 << 20)
+    rc = ctx.lib.gcl_group_order(ctx.handle, _ptr(rp), _ptr(cl), _ptr(co), g.n, ctypes.byref(lg),
+                                 buf, len(buf), ctypes.byref(ngen))
+    _check(rc, "gcl_group_order")
+    return int(buf.value.decode())
+
+
+def perm_group_order(perms) -> int:
+    """Order of the group generated by the rows of `perms` (count x n
+    permutations of 0..n-1), host Schreier-Sims (gcl_perm_group_order)."""
+    lib = load_library()
+    p = np.ascontiguousarray(perms, dtype=np.uint16)
+    if p.ndim != 2:
+        raise ValueError("perms must be count x n")
+    lg = ctypes.c_double()
+    buf = ctypes.create_string_buffer(1 << 20)
+    rc = lib.gcl_perm_group_order(p.shape[1], _ptr(p) if p.size else None, p.shape[0],
+                                  ctypes.byref(lg), buf, len(buf))
+    _check(rc, "gcl_perm_group_order")
+    return int(buf.value.decode())
 
 
 def Nauty_Parallel(g: Graph, max_aut: int = 10000) -> bytes:  # noqa: N802 (reference name)

@@ -23,6 +23,7 @@
 #include "canon_sparse.cuh"
 #include "canon_warp64.cuh"
 #include "canon_wide.cuh"
+#include "gcl_group.h"
 
 namespace gcl {
 
@@ -82,6 +83,14 @@ __global__ void __launch_bounds__(kOrderThreads)
 constexpr int kSpSmemPerBlock = 200 * 1024;  // dynamic shared memory cap of one sparse block
 constexpr uint32_t kWidePool = 64;  // per-level orbit arrays of a wide-search warp
 constexpr uint64_t kWideStoreBytes = 1ull << 30;  // automorphism store of a wide search
+constexpr uint64_t kGroupWorkCap = 40000000000ull;  // Schreier-Sims operations (~20 s)
+
+// entries of a wide search's automorphism store: max_aut, within kWideStoreBytes
+static uint32_t wide_store_cap(uint32_t n, int max_aut) {
+  const uint64_t per_aut = 2ull * ((uint64_t)n + 2);
+  return (uint32_t)std::max<uint64_t>(
+      1, std::min<uint64_t>((uint64_t)max_aut, kWideStoreBytes / per_aut));
+}
 // Per-level orbit arrays and automorphism-ring entries of the sparse passes:
 // the first pass (n <= 4096 / larger), then a middle rerun of the graphs
 // that outgrew them, then a rerun with a full-size pool and ring.  Each
@@ -538,10 +547,7 @@ int gcl_canon_wide_device_async(gcl_context* c, const int32_t* d_rowptr, const i
   GCL_TRY(cudaSetDevice(c->device));
   const uint32_t un = (uint32_t)n;
   const uint64_t m2 = (uint64_t)std::max<int64_t>(m, 1);
-  // automorphism store: up to max_aut entries within kWideStoreBytes
-  const uint64_t per_aut = 2ull * ((uint64_t)un + 2);
-  const uint32_t cap = (uint32_t)std::max<uint64_t>(
-      1, std::min<uint64_t>((uint64_t)max_aut, kWideStoreBytes / per_aut));
+  const uint32_t cap = wide_store_cap(un, max_aut);
   const WideLayout WL = wide_layout(un, m2, cap);
   const SpLayout Lo = sp_layout(un, m2, kWidePool, 0, cap);
   uint64_t smw = c->smem_stage ? sp_smem_bytes(un) : 0;
@@ -806,6 +812,99 @@ int gcl_iso(gcl_context* c, const int32_t* rp1, const int32_t* col1, const int32
         break;
       }
   *verdict = same;
+  return GCL_OK;
+}
+
+int gcl_group_order(gcl_context* c, const int32_t* rowptr, const int32_t* col,
+                    const int32_t* color, int n, double* log10_order, char* digits,
+                    int digits_cap, int64_t* generators) {
+  if (n < 0 || !rowptr || !log10_order || (digits && digits_cap < 2)) return GCL_ERR_ARG;
+  if (n > GCL_MAX_N) return GCL_ERR_TOO_LARGE;
+  if (!c) {
+    int rc = default_context(&c);
+    if (rc != GCL_OK) return rc;
+  }
+  auto put = [&](const std::string& d, double lg, int64_t ng) {
+    *log10_order = lg;
+    if (generators) *generators = ng;
+    if (!digits) return GCL_OK;
+    if ((int)d.size() + 1 > digits_cap) return GCL_ERR_ARG;
+    std::memcpy(digits, d.c_str(), d.size() + 1);
+    return GCL_OK;
+  };
+  if (n <= 1) return put("1", 0.0, 0);
+  // a wide search whose store takes every automorphism it finds
+  const int64_t m = rowptr[n];
+  if (rowptr[0] != 0 || m < 0) return GCL_ERR_BAD_INPUT;
+  if (m > 0 && !col) return GCL_ERR_ARG;
+  GCL_TRY(cudaSetDevice(c->device));
+  cudaStream_t s = c->stream;
+  GCL_TRY(c->rowptr.ensure(((size_t)n + 1) * sizeof(int32_t)));
+  GCL_TRY(c->col.ensure(std::max<size_t>((size_t)m, 1) * sizeof(int32_t)));
+  GCL_TRY(c->stats.ensure(2 * sizeof(int64_t)));
+  GCL_TRY(c->status.ensure(sizeof(int32_t)));
+  GCL_TRY(cudaMemcpyAsync(c->rowptr.p, rowptr, ((size_t)n + 1) * sizeof(int32_t),
+                          cudaMemcpyHostToDevice, s));
+  if (m) GCL_TRY(cudaMemcpyAsync(c->col.p, col, (size_t)m * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+  int32_t* d_color = nullptr;
+  if (color) {
+    GCL_TRY(c->color.ensure((size_t)n * sizeof(int32_t)));
+    GCL_TRY(cudaMemcpyAsync(c->color.p, color, (size_t)n * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    d_color = (int32_t*)c->color.p;
+  }
+  const int max_aut = 0x7fffffff;
+  int rc = gcl_canon_wide_device_async(c, (int32_t*)c->rowptr.p, (int32_t*)c->col.p, d_color, n,
+                                       m, max_aut, nullptr, nullptr, nullptr,
+                                       (int64_t*)c->stats.p, (int32_t*)c->status.p);
+  if (rc != GCL_OK) return rc;
+  int32_t status = 0;
+  int64_t st[2] = {0, 0};
+  GCL_TRY(cudaMemcpyAsync(&status, c->status.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  GCL_TRY(cudaMemcpyAsync(st, c->stats.p, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+  GCL_TRY(cudaStreamSynchronize(s));
+  if (status != kOk) return graph_status_to_rc(status);
+  const uint32_t un = (uint32_t)n;
+  const uint32_t cap = wide_store_cap(un, max_aut);
+  if ((uint64_t)st[0] > cap) return GCL_ERR_TOO_LARGE;  // the store lost generators
+  const WideLayout WL = wide_layout(un, (uint64_t)std::max<int64_t>(m, 1), cap);
+  std::vector<uint16_t> auts((size_t)st[0] * WL.stride + 1);
+  if (st[0])
+    GCL_TRY(cudaMemcpyAsync(auts.data(), (const uint8_t*)c->wide_sh.p + WL.auts,
+                            (size_t)st[0] * WL.stride * sizeof(uint16_t),
+                            cudaMemcpyDeviceToHost, s));
+  GCL_TRY(cudaStreamSynchronize(s));
+  double lg = 0;
+  std::string d;
+  uint64_t base_len = 0;
+  if (!group_order(un, auts.data(), (uint64_t)st[0], WL.stride, kGroupWorkCap, &lg, &d, &base_len))
+    return GCL_ERR_TIMEOUT;
+  return put(d, lg, st[0]);
+}
+
+int gcl_perm_group_order(int n, const uint16_t* perms, int64_t count, double* log10_order,
+                         char* digits, int digits_cap) {
+  if (n < 0 || n > GCL_MAX_N || count < 0 || (count > 0 && !perms) || !log10_order ||
+      (digits && digits_cap < 2))
+    return GCL_ERR_ARG;
+  for (int64_t a = 0; a < count; ++a) {  // each row must be a permutation
+    std::vector<char> seen((size_t)n, 0);
+    for (int x = 0; x < n; ++x) {
+      const uint16_t y = perms[a * n + x];
+      if (y >= n || seen[y]) return GCL_ERR_ARG;
+      seen[y] = 1;
+    }
+  }
+  double lg = 0;
+  std::string d = "1";
+  uint64_t base_len = 0;
+  if (n > 1 && !group_order((uint32_t)n, perms, (uint64_t)count, (uint64_t)n, kGroupWorkCap, &lg,
+                            &d, &base_len))
+    return GCL_ERR_TIMEOUT;
+  *log10_order = lg;
+  if (digits) {
+    if ((int)d.size() + 1 > digits_cap) return GCL_ERR_ARG;
+    std::memcpy(digits, d.c_str(), d.size() + 1);
+  }
   return GCL_OK;
 }
 

@@ -186,6 +186,24 @@ int gcl_canon_batch_noalloc(void* stream, int count, const int64_t* d_voff,
                             const int64_t* d_ooff, int32_t* d_out_label,
                             int64_t* d_out_stats, int32_t* d_out_status);
 
+/* ---- automorphism group order --------------------------------------------
+ * The reference never computes |Aut(G)|; it prints how many automorphisms it
+ * stored (sequential.cpp:83), which depends on the traversal and max_aut.
+ * gcl_group_order runs the wide search with a store that keeps every
+ * automorphism found (they generate the group) and builds a base and strong
+ * generating set (Schreier-Sims) on the host: *log10_order = log10 |Aut|,
+ * digits (if not NULL) the order in decimal, *generators the automorphisms
+ * the search stored.  GCL_ERR_TOO_LARGE if the search found more
+ * automorphisms than its 1 GiB store holds, GCL_ERR_TIMEOUT if Schreier-Sims
+ * exceeds its work cap, GCL_ERR_ARG if digits_cap is too small.
+ * gcl_perm_group_order is the host part alone: the order of the group
+ * generated by `count` permutations of {0..n-1} (row a at perms + a*n). */
+int gcl_group_order(gcl_context* ctx, const int32_t* rowptr, const int32_t* col,
+                    const int32_t* color, int n, double* log10_order, char* digits,
+                    int digits_cap, int64_t* generators);
+int gcl_perm_group_order(int n, const uint16_t* perms, int64_t count, double* log10_order,
+                         char* digits, int digits_cap);
+
 /* ---- isomorphism (main.cpp:172-197) --------------------------------------
  * *verdict = 1 when the canonical upper triangles are equal (ISOMORPHIC),
  * 0 otherwise.  Graphs with different vertex counts are NOT ISOMORPHIC (the
