@@ -654,6 +654,7 @@ def mixed_block(args, pkg, local):
     gs = G.mixed_batch(args.mixed_graphs, seed=4000)
     arena = G.pack(gs)
     ctx = pkg.Context(local)
+    tuning = ctx.autotune(gs[: min(len(gs), 120)], repeats=1)  # launch shapes per size bucket
     pkg.canon_batch(arena, ctx=ctx, dense=False, rows=True)
     t = time.perf_counter()
     r = pkg.canon_batch(arena, ctx=ctx, dense=False, rows=True)
@@ -662,7 +663,8 @@ def mixed_block(args, pkg, local):
     return {"workload": f"{arena.count} graphs, n log-uniform [64,4096], ER(deg 8) / "
                         f"d-regular / tori / 2-4 copies of a regular component",
             "seconds": dt, "graphs_per_s": arena.count / dt,
-            "all_ok": bool((r.status == 0).all()), "max_nodes": int(r.stats[:, 1].max())}
+            "all_ok": bool((r.status == 0).all()), "max_nodes": int(r.stats[:, 1].max()),
+            "tuning": tuning}
 
 
 def main():

@@ -40,6 +40,7 @@ EXPORTS = [
     "gcl_canon_batch_noalloc", "gcl_set_option", "gcl_canon_wide_device_async",
     "gcl_serve_create", "gcl_serve_destroy", "gcl_serve_submit", "gcl_serve_poll",
     "gcl_serve_stats_get", "gcl_serve_replay", "gcl_group_order", "gcl_perm_group_order",
+    "gcl_autotune", "gcl_set_tuning",
 ]
 
 GCL_OPT_WIDE_MIN_N = 1
@@ -48,6 +49,19 @@ GCL_OPT_WIDE_MAX_WARPS = 3
 GCL_OPT_SMEM_STAGE = 4
 GCL_OPT_STREAM_PRIORITY = 5
 GCL_MAX_N = 65536
+
+
+class Tuning(ctypes.Structure):
+    """Launch shapes of the batched path per size bucket (gcl_tuning)."""
+    _fields_ = [("w64_blocks_per_sm", ctypes.c_int), ("sp_blocks_per_sm", ctypes.c_int * 4),
+                ("sp_stage", ctypes.c_int * 4), ("w64_ms", ctypes.c_float),
+                ("sp_ms", ctypes.c_float * 4)]
+
+    def as_dict(self) -> dict:
+        return {"w64_blocks_per_sm": self.w64_blocks_per_sm,
+                "sp_blocks_per_sm": list(self.sp_blocks_per_sm),
+                "sp_stage": list(self.sp_stage), "w64_ms": self.w64_ms,
+                "sp_ms": list(self.sp_ms)}
 
 
 class GclError(RuntimeError):
@@ -88,6 +102,9 @@ def load_library(path: str = LIB_PATH):
     lib.gcl_canon_batch_noalloc.argtypes = [_P, ctypes.c_int, _P, _P, _P, _P, _P, ctypes.c_int,
                                             ctypes.c_int, _P, _P, _P, _P, _P]
     lib.gcl_set_option.argtypes = [_P, ctypes.c_int, ctypes.c_int64]
+    lib.gcl_autotune.argtypes = [_P, ctypes.c_int, _P, _P, _P, _P, _P, ctypes.c_int, ctypes.c_int,
+                                 ctypes.POINTER(Tuning)]
+    lib.gcl_set_tuning.argtypes = [_P, ctypes.POINTER(Tuning)]
     lib.gcl_group_order.argtypes = [_P, _P, _P, _P, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
                                     ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int64)]
     lib.gcl_perm_group_order.argtypes = [ctypes.c_int, _P, ctypes.c_int64,
@@ -98,7 +115,7 @@ def load_library(path: str = LIB_PATH):
     for name in ("gcl_create", "gcl_destroy", "gcl_sync", "gcl_canon_one", "gcl_canon_batch",
                  "gcl_canon_batch_device_async", "gcl_iso", "gcl_canon_batch_noalloc",
                  "gcl_set_option", "gcl_canon_wide_device_async", "gcl_group_order",
-                 "gcl_perm_group_order"):
+                 "gcl_perm_group_order", "gcl_autotune", "gcl_set_tuning"):
         getattr(lib, name).restype = ctypes.c_int
     _lib = lib
     return lib
@@ -124,6 +141,28 @@ class Context:
         self.device = device
         if wide_min_n is not None:
             self.set_wide_min_n(wide_min_n)
+
+    def autotune(self, graphs, max_aut: int = 10000, repeats: int = 2) -> dict:
+        """Time the batched path's launch shapes on a sample (an Arena or a
+        list of graphs), keep the fastest per size bucket for this context
+        and return the choice (gcl_autotune)."""
+        arena = graphs if isinstance(graphs, Arena) else pack(graphs)
+        t = Tuning()
+        col = arena.col if arena.col.size else np.zeros(1, np.int32)
+        color = arena.color if arena.color.any() else None
+        _check(self.lib.gcl_autotune(self.handle, arena.count, _ptr(arena.voff), _ptr(arena.eoff),
+                                     _ptr(arena.rowptr), _ptr(col), _ptr(color), max_aut, repeats,
+                                     ctypes.byref(t)), "gcl_autotune")
+        return t.as_dict()
+
+    def set_tuning(self, d: dict):
+        """Apply a choice returned by autotune (gcl_set_tuning)."""
+        t = Tuning()
+        t.w64_blocks_per_sm = int(d.get("w64_blocks_per_sm", 0))
+        for k in range(4):
+            t.sp_blocks_per_sm[k] = int(d.get("sp_blocks_per_sm", [0] * 4)[k])
+            t.sp_stage[k] = int(d.get("sp_stage", [-1] * 4)[k])
+        _check(self.lib.gcl_set_tuning(self.handle, ctypes.byref(t)), "gcl_set_tuning")
 
     def set_wide_min_n(self, n: int):
         """Single graphs with at least n vertices use the wide search

@@ -229,6 +229,15 @@ struct gcl_context {
   uint64_t workspace_bytes = 0;  // per-pass workspace cap, 0 = GCL_WORKSPACE_GB
   int64_t wide_max_warps = 0;    // 0 = as many as fit
   bool smem_stage = true;        // sparse and wide kernels stage per-step arrays in shared memory
+  // launch shape per size bucket (gcl_autotune / gcl_set_tuning): 0 / -1 = default
+  int w64_per_sm = 0;            // resident blocks the warp kernel's occupancy allows
+  int tune_w64_bps = 0;
+  int tune_sp_bps[kSpBuckets] = {0, 0, 0, 0};
+  int tune_sp_stage[kSpBuckets] = {-1, -1, -1, -1};
+  // timing of the passes of one batch (autotuner)
+  bool timing = false;
+  cudaEvent_t tev[2][1 + kSpBuckets] = {};
+  bool tev_used[1 + kSpBuckets] = {};
   DevBuf deferred, overflow_list, large_list, sp_fail_list, sp_fail_list2, order;
   // staging for host-pointer calls
   DevBuf voff, eoff, rowptr, col, color, ooff, dense, roff, rows, label, stats, status;
@@ -316,6 +325,7 @@ int gcl_create(int device, gcl_context** out) {
     // warps per SM run each graph faster; more hide more latency)
     const char* cap_env = std::getenv("GCL_W64_BLOCKS_PER_SM");
     if (cap_env && std::atoi(cap_env) > 0) per_sm = std::min(per_sm, std::atoi(cap_env));
+    c->w64_per_sm = std::max(per_sm, 1);
     c->w64_grid = c->sms * std::max(per_sm, 1);
     e = c->deferred.ensure(sizeof(Deferred));
   }
@@ -342,6 +352,9 @@ int gcl_destroy(gcl_context* c) {
   if (!c) return GCL_ERR_ARG;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  for (auto& row : c->tev)
+    for (cudaEvent_t& ev : row)
+      if (ev) cudaEventDestroy(ev);
   c->each_buf([](DevBuf& b) { b.release(); });
   if (c->stream) {
     cudaStreamSynchronize(c->stream);
@@ -406,10 +419,21 @@ int gcl_canon_batch_device_async(gcl_context* c, int count, const int64_t* d_vof
   A.slot_bytes = slot_bytes;
   A.budget_ns = graph_budget_ns();
   Deferred* D = (Deferred*)c->deferred.p;
-  const int grid1 = (int)std::min<int64_t>(c->w64_grid, ((int64_t)count + kW64Warps - 1) / kW64Warps);
+  const int64_t w64_grid = c->tune_w64_bps > 0
+                               ? (int64_t)c->sms * std::min(c->tune_w64_bps, c->w64_per_sm)
+                               : (int64_t)c->w64_grid;
+  const int grid1 = (int)std::min<int64_t>(w64_grid, ((int64_t)count + kW64Warps - 1) / kW64Warps);
+  if (c->timing) {
+    for (int k = 0; k <= kSpBuckets; ++k) c->tev_used[k] = false;
+    GCL_TRY(cudaEventRecord(c->tev[0][0], c->stream));
+  }
   w64_batch_kernel<<<grid1, kW64Threads, 0, c->stream>>>(A, D, (int*)c->overflow_list.p,
                                                          (int*)c->large_list.p, 0);
   GCL_TRY(cudaGetLastError());
+  if (c->timing) {
+    GCL_TRY(cudaEventRecord(c->tev[1][0], c->stream));
+    c->tev_used[0] = true;
+  }
 
   if (cap < maut) {
     // graphs whose ring outgrew `cap`: rerun with the full ring
@@ -441,11 +465,13 @@ int gcl_canon_batch_device_async(gcl_context* c, int count, const int64_t* d_vof
       if ((uint32_t)max_n < lo) break;
       const uint32_t nmax = std::min<uint32_t>((uint32_t)max_n, kSpBucketHi[bk]);
       const uint64_t sb1 = sp_layout(nmax, m2max, pool1, cap1).bytes;
-      uint64_t smw = c->smem_stage ? sp_smem_bytes(nmax) : 0;
+      const bool stage = c->tune_sp_stage[bk] >= 0 ? c->tune_sp_stage[bk] != 0 : c->smem_stage;
+      uint64_t smw = stage ? sp_smem_bytes(nmax) : 0;
       if (smw * kSpWarps > (uint64_t)kSpSmemPerBlock) smw = 0;  // device memory only
       int per_sm = 0;
       GCL_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sp_batch_kernel, kSpThreads,
                                                             (size_t)(smw * kSpWarps)));
+      if (c->tune_sp_bps[bk] > 0) per_sm = std::min(per_sm, c->tune_sp_bps[bk]);
       int64_t slots = std::min<int64_t>((int64_t)c->sms * std::max(per_sm, 1) * kSpWarps,
                                         std::max<int64_t>(kSpWarps, (int64_t)(budget / sb1)));
       slots = std::min<int64_t>(slots, ((int64_t)count + kSpWarps - 1) / kSpWarps * kSpWarps);
@@ -454,12 +480,17 @@ int gcl_canon_batch_device_async(gcl_context* c, int count, const int64_t* d_vof
       GCL_TRY(wb.ensure((size_t)(slots * sb1)));
       BatchArgs Sa = A;
       Sa.work = (uint8_t*)wb.p;
+      if (c->timing) GCL_TRY(cudaEventRecord(c->tev[0][1 + bk], c->stream));
       sp_batch_kernel<<<(int)(slots / kSpWarps), kSpThreads, (size_t)(smw * kSpWarps),
                         c->stream>>>(Sa, (const int*)c->large_list.p + (int64_t)bk * count,
                                      &D->large_count[bk], &D->next_large[bk],
                                      (int*)c->sp_fail_list.p, &D->sp_fail_count, nmax, m2max,
                                      pool1, cap1, sb1, smw);
       GCL_TRY(cudaGetLastError());
+      if (c->timing) {
+        GCL_TRY(cudaEventRecord(c->tev[1][1 + bk], c->stream));
+        c->tev_used[1 + bk] = true;
+      }
     }
     // middle rerun: a larger pool and ring, still many warps
     const uint32_t nmax = (uint32_t)max_n;
@@ -906,6 +937,119 @@ int gcl_perm_group_order(int n, const uint16_t* perms, int64_t count, double* lo
     std::memcpy(digits, d.c_str(), d.size() + 1);
   }
   return GCL_OK;
+}
+
+int gcl_set_tuning(gcl_context* c, const gcl_tuning* t) {
+  if (!c || !t) return GCL_ERR_ARG;
+  c->tune_w64_bps = std::max(t->w64_blocks_per_sm, 0);
+  for (int bk = 0; bk < kSpBuckets; ++bk) {
+    c->tune_sp_bps[bk] = std::max(t->sp_blocks_per_sm[bk], 0);
+    c->tune_sp_stage[bk] = t->sp_stage[bk] < 0 ? -1 : (t->sp_stage[bk] ? 1 : 0);
+  }
+  return GCL_OK;
+}
+
+int gcl_autotune(gcl_context* c, int count, const int64_t* voff, const int64_t* eoff,
+                 const int32_t* rowptr, const int32_t* col, const int32_t* color, int max_aut,
+                 int repeats, gcl_tuning* out) {
+  if (!c || count <= 0 || !voff || !eoff || !rowptr || !out || max_aut <= 0) return GCL_ERR_ARG;
+  if (repeats < 1) repeats = 2;
+  GCL_TRY(cudaSetDevice(c->device));
+  for (auto& row : c->tev)
+    for (cudaEvent_t& ev : row)
+      if (!ev) GCL_TRY(cudaEventCreate(&ev));
+  std::vector<int64_t> roff(count + 1, 0);
+  for (int g = 0; g < count; ++g) {
+    const int64_t n = voff[g + 1] - voff[g];
+    roff[g + 1] = roff[g] + n * ((n + 63) / 64);
+  }
+  std::vector<uint64_t> rows((size_t)std::max<int64_t>(roff[count], 1));
+  std::vector<int32_t> status(count);
+  // one timed batch per candidate and repeat: the best pass time per bucket
+  auto run = [&](float* ms) -> int {
+    for (int k = 0; k <= kSpBuckets; ++k) ms[k] = -1.f;
+    c->timing = true;
+    int rc = gcl_canon_batch(c, count, voff, eoff, rowptr, col, color, max_aut, nullptr, nullptr,
+                             rows.data(), roff.data(), nullptr, nullptr, status.data());
+    c->timing = false;
+    if (rc != GCL_OK) return rc;
+    for (int k = 0; k <= kSpBuckets; ++k)
+      if (c->tev_used[k]) GCL_TRY(cudaEventElapsedTime(&ms[k], c->tev[0][k], c->tev[1][k]));
+    return GCL_OK;
+  };
+  const int saved_w64 = c->tune_w64_bps;
+  int saved_bps[kSpBuckets], saved_stage[kSpBuckets];
+  for (int bk = 0; bk < kSpBuckets; ++bk) {
+    saved_bps[bk] = c->tune_sp_bps[bk];
+    saved_stage[bk] = c->tune_sp_stage[bk];
+  }
+  float ms[1 + kSpBuckets];
+  int rc = run(ms);  // warm-up (workspace allocation, first launches)
+  // the warp kernel: resident blocks per SM
+  float best_w64 = 1e30f;
+  int w64_choice = 0;
+  const int w64_cands[] = {1, 2, 3, 4, 6, 8, 12, 16};
+  for (int ci = 0; rc == GCL_OK && ci < 8; ++ci) {
+    if (w64_cands[ci] > c->w64_per_sm) break;
+    c->tune_w64_bps = w64_cands[ci];
+    float best = 1e30f;
+    for (int r = 0; r < repeats && rc == GCL_OK; ++r) {
+      rc = run(ms);
+      if (ms[0] >= 0) best = std::min(best, ms[0]);
+    }
+    if (best < best_w64) {
+      best_w64 = best;
+      w64_choice = w64_cands[ci];
+    }
+  }
+  c->tune_w64_bps = w64_choice;
+  // the sparse buckets: shared-memory staging and resident blocks per SM,
+  // one candidate for every bucket per batch (the passes are independent)
+  float best_sp[kSpBuckets];
+  int bps_choice[kSpBuckets], stage_choice[kSpBuckets];
+  for (int bk = 0; bk < kSpBuckets; ++bk) {
+    best_sp[bk] = 1e30f;
+    bps_choice[bk] = 0;
+    stage_choice[bk] = -1;
+  }
+  const int sp_bps[] = {1, 2, 4, 0};
+  for (int stage = 1; stage >= 0 && rc == GCL_OK; --stage)
+    for (int bi = 0; bi < 4 && rc == GCL_OK; ++bi) {
+      for (int bk = 0; bk < kSpBuckets; ++bk) {
+        c->tune_sp_stage[bk] = stage;
+        c->tune_sp_bps[bk] = sp_bps[bi];
+      }
+      float best[kSpBuckets];
+      for (int bk = 0; bk < kSpBuckets; ++bk) best[bk] = 1e30f;
+      for (int r = 0; r < repeats && rc == GCL_OK; ++r) {
+        rc = run(ms);
+        for (int bk = 0; bk < kSpBuckets; ++bk)
+          if (ms[1 + bk] >= 0) best[bk] = std::min(best[bk], ms[1 + bk]);
+      }
+      for (int bk = 0; bk < kSpBuckets; ++bk)
+        if (best[bk] < best_sp[bk]) {
+          best_sp[bk] = best[bk];
+          bps_choice[bk] = sp_bps[bi];
+          stage_choice[bk] = stage;
+        }
+    }
+  if (rc != GCL_OK) {  // leave the context as it was
+    c->tune_w64_bps = saved_w64;
+    for (int bk = 0; bk < kSpBuckets; ++bk) {
+      c->tune_sp_bps[bk] = saved_bps[bk];
+      c->tune_sp_stage[bk] = saved_stage[bk];
+    }
+    return rc;
+  }
+  out->w64_blocks_per_sm = w64_choice;
+  out->w64_ms = best_w64 < 1e30f ? best_w64 : -1.f;
+  for (int bk = 0; bk < kSpBuckets; ++bk) {
+    const bool seen = best_sp[bk] < 1e30f;
+    out->sp_blocks_per_sm[bk] = seen ? bps_choice[bk] : 0;
+    out->sp_stage[bk] = seen ? stage_choice[bk] : -1;
+    out->sp_ms[bk] = seen ? best_sp[bk] : -1.f;
+  }
+  return gcl_set_tuning(c, out);
 }
 
 }  // extern "C"

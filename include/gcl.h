@@ -186,6 +186,28 @@ int gcl_canon_batch_noalloc(void* stream, int count, const int64_t* d_voff,
                             const int64_t* d_ooff, int32_t* d_out_label,
                             int64_t* d_out_stats, int32_t* d_out_status);
 
+/* ---- autotuning of the batched launches ----------------------------------
+ * The batched path runs the warp kernel (n <= 64) and one sparse-kernel pass
+ * per size bucket (n <= 256, <= 1024, <= 4096, larger).  gcl_autotune times
+ * them on a sample batch (host arrays in the batched layout) under candidate
+ * launch shapes -- resident blocks per SM of the warp kernel; per sparse
+ * bucket, shared-memory staging on or off and resident blocks per SM --
+ * keeps for each the fastest, applies the choice to the context and returns
+ * it.  A bucket without graphs in the sample keeps its default (its sp_ms is
+ * -1).  Results are unchanged by any choice: only the launch shape moves.
+ * gcl_set_tuning applies a saved choice (0 / -1 fields = default). */
+typedef struct {
+  int w64_blocks_per_sm;    /* 0 = as many as fit                           */
+  int sp_blocks_per_sm[4];  /* 0 = as many as fit                           */
+  int sp_stage[4];          /* 1 = stage in shared memory, 0 = not, -1 = default */
+  float w64_ms;             /* best pass time found (ms), -1 = not timed    */
+  float sp_ms[4];
+} gcl_tuning;
+int gcl_autotune(gcl_context* ctx, int count, const int64_t* voff, const int64_t* eoff,
+                 const int32_t* rowptr, const int32_t* col, const int32_t* color,
+                 int max_aut, int repeats, gcl_tuning* out);
+int gcl_set_tuning(gcl_context* ctx, const gcl_tuning* tuning);
+
 /* ---- automorphism group order --------------------------------------------
  * The reference never computes |Aut(G)|; it prints how many automorphisms it
  * stored (sequential.cpp:83), which depends on the traversal and max_aut.
