@@ -40,7 +40,7 @@ EXPORTS = [
     "gcl_canon_batch_noalloc", "gcl_set_option", "gcl_canon_wide_device_async",
     "gcl_serve_create", "gcl_serve_destroy", "gcl_serve_submit", "gcl_serve_poll",
     "gcl_serve_stats_get", "gcl_serve_replay", "gcl_group_order", "gcl_perm_group_order",
-    "gcl_autotune", "gcl_set_tuning",
+    "gcl_autotune", "gcl_set_tuning", "gcl_canon_files",
 ]
 
 GCL_OPT_WIDE_MIN_N = 1
@@ -72,6 +72,9 @@ class GclError(RuntimeError):
 
 _P = ctypes.c_void_p
 _lib = None
+_FILE_CB = ctypes.CFUNCTYPE(None, _P, ctypes.c_int64, ctypes.c_int32, ctypes.c_int,
+                            ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_int32),
+                            ctypes.c_int64, ctypes.c_int64)
 
 
 def load_library(path: str = LIB_PATH):
@@ -102,6 +105,8 @@ def load_library(path: str = LIB_PATH):
     lib.gcl_canon_batch_noalloc.argtypes = [_P, ctypes.c_int, _P, _P, _P, _P, _P, ctypes.c_int,
                                             ctypes.c_int, _P, _P, _P, _P, _P]
     lib.gcl_set_option.argtypes = [_P, ctypes.c_int, ctypes.c_int64]
+    lib.gcl_canon_files.argtypes = [_P, ctypes.c_int64, ctypes.POINTER(ctypes.c_char_p),
+                                    ctypes.c_int, ctypes.c_int, ctypes.c_int, _FILE_CB, _P]
     lib.gcl_autotune.argtypes = [_P, ctypes.c_int, _P, _P, _P, _P, _P, ctypes.c_int, ctypes.c_int,
                                  ctypes.POINTER(Tuning)]
     lib.gcl_set_tuning.argtypes = [_P, ctypes.POINTER(Tuning)]
@@ -115,7 +120,8 @@ def load_library(path: str = LIB_PATH):
     for name in ("gcl_create", "gcl_destroy", "gcl_sync", "gcl_canon_one", "gcl_canon_batch",
                  "gcl_canon_batch_device_async", "gcl_iso", "gcl_canon_batch_noalloc",
                  "gcl_set_option", "gcl_canon_wide_device_async", "gcl_group_order",
-                 "gcl_perm_group_order", "gcl_autotune", "gcl_set_tuning"):
+                 "gcl_perm_group_order", "gcl_autotune", "gcl_set_tuning",
+                 "gcl_canon_files"):
         getattr(lib, name).restype = ctypes.c_int
     _lib = lib
     return lib
@@ -227,6 +233,38 @@ def canon(g: Graph, max_aut: int = 10000, ctx: Optional[Context] = None) -> Cano
                                ctypes.byref(nodes), ctypes.byref(naut))
     _check(rc, "gcl_canon_one")
     return CanonResult(out, int(nodes.value), int(naut.value))
+
+
+@dataclass
+class FileResult:
+    status: int
+    n: int
+    rows: Optional[np.ndarray]   # packed canonical rows (n * ceil(n/64) words)
+    label: Optional[np.ndarray]
+    num_aut: int
+    nodes: int
+
+
+def canon_files(paths: Sequence[str], max_aut: int = 10000, ctx: Optional[Context] = None,
+                chunk: int = 4096, threads: int = 0) -> List[FileResult]:
+    """Canonize DIMACS files, parsing on host threads while the GPU works
+    (gcl_canon_files); one FileResult per path, in order."""
+    ctx = ctx or default_context()
+    out: List[Optional[FileResult]] = [None] * len(paths)
+
+    def cb(_user, index, status, n, rows, label, num_aut, nodes):
+        r = l = None
+        if status == 0:
+            w = n * ((n + 63) // 64)
+            r = np.ctypeslib.as_array(rows, shape=(max(w, 1),))[:w].copy() if w else np.zeros(0, np.uint64)
+            l = np.ctypeslib.as_array(label, shape=(max(n, 1),))[:n].copy() if n else np.zeros(0, np.int32)
+        out[index] = FileResult(int(status), int(n), r, l, int(num_aut), int(nodes))
+
+    arr = (ctypes.c_char_p * max(len(paths), 1))(*[os.fsencode(p) for p in paths])
+    fn = _FILE_CB(cb)
+    _check(ctx.lib.gcl_canon_files(ctx.handle, len(paths), arr, max_aut, chunk, threads, fn, None),
+           "gcl_canon_files")
+    return out
 
 
 def group_order(g: Graph, ctx: Optional[Context] = None) -> int:

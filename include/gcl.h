@@ -186,6 +186,23 @@ int gcl_canon_batch_noalloc(void* stream, int count, const int64_t* d_voff,
                             const int64_t* d_ooff, int32_t* d_out_label,
                             int64_t* d_out_stats, int32_t* d_out_status);
 
+/* ---- files: DIMACS parsing overlapped with the GPU -------------------------
+ * Canonize `count` DIMACS files (the reference's graph.txt format,
+ * CSRGraph::fromDIMACS, src/CSRGraph.cpp:40-119) in chunks of `chunk` files
+ * (0 = 4096): `threads` host threads (0 = all cores) parse chunk k while the
+ * GPU canonizes chunk k-1 through the batched path.  For every file, in
+ * order and on the calling thread, cb receives its index, a GCL_GRAPH_*
+ * status (an unreadable file, an endpoint out of range or a duplicate edge
+ * is GCL_GRAPH_BAD_INPUT), n, the packed canonical rows (n * ceil(n/64)
+ * words) and the labeling -- both NULL unless the status is GCL_GRAPH_OK,
+ * valid only during the call -- and the statistics.  Returns GCL_OK once
+ * every file has been delivered, else the first launch or copy error. */
+typedef void (*gcl_file_result_fn)(void* user, int64_t index, int32_t status, int n,
+                                   const uint64_t* rows, const int32_t* label,
+                                   int64_t num_aut, int64_t nodes);
+int gcl_canon_files(gcl_context* ctx, int64_t count, const char* const* paths, int max_aut,
+                    int chunk, int threads, gcl_file_result_fn cb, void* user);
+
 /* ---- autotuning of the batched launches ----------------------------------
  * The batched path runs the warp kernel (n <= 64) and one sparse-kernel pass
  * per size bucket (n <= 256, <= 1024, <= 4096, larger).  gcl_autotune times
