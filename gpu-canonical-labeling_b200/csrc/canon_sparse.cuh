@@ -205,11 +205,6 @@ __device__ void bm_resummarize(const uint64_t* B, uint64_t* Sm, uint32_t nw, uin
   __syncwarp();
 }
 
-__device__ __forceinline__ uint32_t sp_cell_end_p(const uint64_t* stb, const uint64_t* sts,
-                                                  uint32_t n, uint32_t nw, uint32_t nsw,
-                                                  uint32_t c) {
-  return bm_next(stb, sts, c + 1, n, nw, nsw);
-}
 __device__ __forceinline__ uint32_t sp_cell_end(const SpWarp& W, uint32_t c) {
   return bm_next(W.stb, W.sts, c + 1, W.n, W.nw, W.nsw);
 }
@@ -344,31 +339,6 @@ __device__ __noinline__ int sp_refine(uint32_t level) {
   SpWarp& W = sp_w();
   const uint32_t lane = lane_id();
   const uint32_t n = W.n, nw = W.nw, nsw = W.nsw;
-  // the warp's arrays do not move during a refinement: keep their addresses
-  // in registers instead of reloading them from the shared warp record
-  uint32_t* const elem_ = W.elem;
-  uint32_t* const pos_ = W.pos;
-  uint32_t* const inlev_ = W.inlev;
-  uint32_t* const cnt_ = W.cnt;
-  uint32_t* const cellcnt_ = W.cellcnt;
-  uint32_t* const off_ = W.off;
-  uint32_t* const fill_ = W.fill;
-  uint32_t* const hist_ = W.hist;
-  uint32_t* const pre_ = W.pre;
-  uint32_t* const tmp_ = W.tmp;
-  uint32_t* const fpos_ = W.fpos;
-  uint32_t* const nsl_ = W.nsl;
-  uint64_t* const act_ = W.act;
-  uint64_t* const acts_ = W.acts;
-  uint64_t* const tcb_ = W.tcb;
-  uint64_t* const tcbs_ = W.tcbs;
-  const int32_t* const rp_ = W.rp;
-  const int32_t* const col_ = W.col;
-  uint32_t* const T_ = W.T;
-  uint32_t* const Tc_ = W.Tc;
-  uint32_t* const G_ = W.G;
-  uint64_t* const stb_ = W.stb;
-  uint64_t* const sts_ = W.sts;
   const uint32_t lvl1 = level + 1;
   uint32_t lc = W.ncells, hint = 0;
   uint64_t iters = 0;
@@ -379,11 +349,11 @@ __device__ __noinline__ int sp_refine(uint32_t level) {
       break;
     }
     uint32_t s;
-    if (bm_test(act_, hint)) {
+    if (bm_test(W.act, hint)) {
       s = hint;
     } else {
-      s = bm_next(act_, acts_, hint + 1, n, nw, nsw);
-      if (s >= n) s = bm_next(act_, acts_, 0, n, nw, nsw);
+      s = bm_next(W.act, W.acts, hint + 1, n, nw, nsw);
+      if (s >= n) s = bm_next(W.act, W.acts, 0, n, nw, nsw);
     }
     if (s >= n) {
       ok = 0;
@@ -391,12 +361,12 @@ __device__ __noinline__ int sp_refine(uint32_t level) {
     }
     __syncwarp();
     if (lane == 0) {
-      bm_clear1(act_, acts_, s);
+      bm_clear1(W.act, W.acts, s);
       W.nact -= 1;
       W.ntouched = 0;
     }
     __syncwarp();
-    const uint32_t e = sp_cell_end_p(stb_, sts_, n, nw, nsw, s);
+    const uint32_t e = sp_cell_end(W, s);
     const uint32_t len = e - s;
     lc = mash(lc, s + e - 1);
     if (len > 1) lc = mash(lc, len);
@@ -407,16 +377,16 @@ __device__ __noinline__ int sp_refine(uint32_t level) {
     // [neighbours, non-neighbours]: its misplaced neighbours swap with the
     // non-neighbours inside its first k positions, then the split cells are
     // folded in position order (:296-309, 399-435).
-    if (len == 1 && rp_[elem_[s] + 1] - rp_[elem_[s]] <= 32) {
-      const uint32_t w = elem_[s];
-      const int32_t b = rp_[w], d = rp_[w + 1] - b;
+    if (len == 1 && W.rp[W.elem[s] + 1] - W.rp[W.elem[s]] <= 32) {
+      const uint32_t w = W.elem[s];
+      const int32_t b = W.rp[w], d = W.rp[w + 1] - b;
       const bool have = (int32_t)lane < d;
       uint32_t u = 0, p = 0, c = kNone, L = 0;
       if (have) {
-        u = (uint32_t)col_[b + (int32_t)lane];
-        p = pos_[u];
-        c = bm_prev(stb_, sts_, p);
-        L = sp_cell_end_p(stb_, sts_, n, nw, nsw, c) - c;
+        u = (uint32_t)W.col[b + (int32_t)lane];
+        p = W.pos[u];
+        c = sp_cell_of(W, p);
+        L = sp_cell_end(W, c) - c;
       }
       const bool act_l = have && L > 1;
       const uint32_t grp = __match_any_sync(GCL_FULL, act_l ? c : kNone);
@@ -432,16 +402,16 @@ __device__ __noinline__ int sp_refine(uint32_t level) {
           const uint32_t j = (uint32_t)__popc(outs & lanemask_lt());
           const uint32_t holes = ~inner & (k >= 32 ? 0xffffffffu : ((1u << k) - 1u));
           h = c + (uint32_t)__fns(holes, 0, (int)j + 1);
-          x = elem_[h];
+          x = W.elem[h];
           mv = true;
         }
       }
       __syncwarp();
       if (mv) {
-        elem_[h] = u;
-        pos_[u] = h;
-        elem_[p] = x;
-        pos_[x] = p;
+        W.elem[h] = u;
+        W.pos[u] = h;
+        W.elem[p] = x;
+        W.pos[x] = p;
       }
       __syncwarp();
       uint32_t leaders = __ballot_sync(GCL_FULL, spl_l && lane == (uint32_t)(__ffs(grp) - 1));
@@ -453,20 +423,20 @@ __device__ __noinline__ int sp_refine(uint32_t level) {
         leaders &= ~(1u << src);
         const uint32_t pp = cmin + kk;
         lc = mash(lc, pp - 1);  // cell.first + neighbors_size - 1
-        const bool was = bm_test(act_, cmin);
+        const bool was = bm_test(W.act, cmin);
         __syncwarp();
         if (lane == 0) {
-          set_inlev(W, pp, inlev_[cmin]);
+          set_inlev(W, pp, W.inlev[cmin]);
           set_inlev(W, cmin, lvl1);
           add_start(W, pp);
           W.ncells += 1;
           const uint32_t nb = kk, nn = LL - kk;
           if (was || nb >= nn) {
-            bm_set1(act_, acts_, pp);
+            bm_set1(W.act, W.acts, pp);
             W.nact += 1;
             if (nn == 1) hint = pp;
           } else {
-            bm_set1(act_, acts_, cmin);
+            bm_set1(W.act, W.acts, cmin);
             W.nact += 1;
             if (nb == 1) hint = cmin;
           }
@@ -481,32 +451,32 @@ __device__ __noinline__ int sp_refine(uint32_t level) {
     // count neighbours in the splitter, record touched vertices and cells
     // (cells that are singletons never split and are skipped, :257-259)
     if (len == 1) {
-      const uint32_t w = elem_[s];
-      const int32_t b = rp_[w], d = rp_[w + 1] - b;
+      const uint32_t w = W.elem[s];
+      const int32_t b = W.rp[w], d = W.rp[w + 1] - b;
       for (int32_t i = (int32_t)lane; i < d; i += 32) {
-        const uint32_t u = (uint32_t)col_[b + i];
-        const uint32_t c = bm_prev(stb_, sts_, pos_[u]);
-        if (sp_cell_end_p(stb_, sts_, n, nw, nsw, c) - c == 1) continue;
-        if (atomicAdd(&cnt_[u], 1u) == 0) {
+        const uint32_t u = (uint32_t)W.col[b + i];
+        const uint32_t c = sp_cell_of(W, W.pos[u]);
+        if (sp_cell_end(W, c) - c == 1) continue;
+        if (atomicAdd(&W.cnt[u], 1u) == 0) {
           const uint32_t t = atomicAdd(&W.ntouched, 1u);
-          T_[t] = u;
-          Tc_[t] = c;
-          if (atomicAdd(&cellcnt_[c], 1u) == 0) bm_set_atomic(tcb_, tcbs_, c);
+          W.T[t] = u;
+          W.Tc[t] = c;
+          if (atomicAdd(&W.cellcnt[c], 1u) == 0) bm_set_atomic(W.tcb, W.tcbs, c);
         }
       }
     } else {
       for (uint32_t q = s + lane; q < e; q += 32) {
-        const uint32_t w = elem_[q];
-        const int32_t b = rp_[w], f = rp_[w + 1];
+        const uint32_t w = W.elem[q];
+        const int32_t b = W.rp[w], f = W.rp[w + 1];
         for (int32_t i = b; i < f; ++i) {
-          const uint32_t u = (uint32_t)col_[i];
-          const uint32_t c = bm_prev(stb_, sts_, pos_[u]);
-          if (sp_cell_end_p(stb_, sts_, n, nw, nsw, c) - c == 1) continue;
-          if (atomicAdd(&cnt_[u], 1u) == 0) {
+          const uint32_t u = (uint32_t)W.col[i];
+          const uint32_t c = sp_cell_of(W, W.pos[u]);
+          if (sp_cell_end(W, c) - c == 1) continue;
+          if (atomicAdd(&W.cnt[u], 1u) == 0) {
             const uint32_t t = atomicAdd(&W.ntouched, 1u);
-            T_[t] = u;
-            Tc_[t] = c;
-            if (atomicAdd(&cellcnt_[c], 1u) == 0) bm_set_atomic(tcb_, tcbs_, c);
+            W.T[t] = u;
+            W.Tc[t] = c;
+            if (atomicAdd(&W.cellcnt[c], 1u) == 0) bm_set_atomic(W.tcb, W.tcbs, c);
           }
         }
       }
@@ -516,17 +486,17 @@ __device__ __noinline__ int sp_refine(uint32_t level) {
     // group the touched vertices by cell (counting sort, cells in order)
     {
       uint32_t run = 0;
-      uint32_t c = bm_next(tcb_, tcbs_, 0, n, nw, nsw);
+      uint32_t c = bm_next(W.tcb, W.tcbs, 0, n, nw, nsw);
       while (c < n) {
-        const uint32_t k = cellcnt_[c];
-        if (lane == 0) off_[c] = run;
+        const uint32_t k = W.cellcnt[c];
+        if (lane == 0) W.off[c] = run;
         run += k;
-        c = bm_next(tcb_, tcbs_, c + 1, n, nw, nsw);
+        c = bm_next(W.tcb, W.tcbs, c + 1, n, nw, nsw);
       }
       __syncwarp();
       for (uint32_t i = lane; i < nt; i += 32) {
-        const uint32_t c2 = Tc_[i];
-        G_[off_[c2] + atomicAdd(&fill_[c2], 1u)] = T_[i];
+        const uint32_t c2 = W.Tc[i];
+        W.G[W.off[c2] + atomicAdd(&W.fill[c2], 1u)] = W.T[i];
       }
       __syncwarp();
     }
@@ -534,28 +504,28 @@ __device__ __noinline__ int sp_refine(uint32_t level) {
     if (len == 1) {
       // every touched cell that is not all neighbours splits into
       // [neighbours, non-neighbours] (:296-309, 399-435)
-      uint32_t c = bm_next(tcb_, tcbs_, 0, n, nw, nsw);
+      uint32_t c = bm_next(W.tcb, W.tcbs, 0, n, nw, nsw);
       while (c < n) {
-        const uint32_t k = cellcnt_[c], ce = sp_cell_end_p(stb_, sts_, n, nw, nsw, c), L = ce - c;
-        const uint32_t cnext = bm_next(tcb_, tcbs_, c + 1, n, nw, nsw);
+        const uint32_t k = W.cellcnt[c], ce = sp_cell_end(W, c), L = ce - c;
+        const uint32_t cnext = bm_next(W.tcb, W.tcbs, c + 1, n, nw, nsw);
         if (k < L) {
-          sp_regroup(G_ + off_[c], k, c, nullptr);
+          sp_regroup(W.G + W.off[c], k, c, nullptr);
           const uint32_t p = c + k;
           lc = mash(lc, p - 1);
-          const bool was = bm_test(act_, c);
+          const bool was = bm_test(W.act, c);
           if (lane == 0) {
-            set_inlev(W, p, inlev_[c]);
+            set_inlev(W, p, W.inlev[c]);
             set_inlev(W, c, lvl1);
             add_start(W, p);
             W.ncells += 1;
             const uint32_t nb = k, nn = L - k;
             if (was || nb >= nn) {
-              bm_set1(act_, acts_, p);
+              bm_set1(W.act, W.acts, p);
               W.nact += 1;
               if (nn == 1) hint = p;
             } else {
               if (!was) {
-                bm_set1(act_, acts_, c);
+                bm_set1(W.act, W.acts, c);
                 W.nact += 1;
               }
               if (nb == 1) hint = c;
@@ -574,8 +544,8 @@ __device__ __noinline__ int sp_refine(uint32_t level) {
       const uint32_t K = sp_list_nonsingleton();
       for (uint32_t i0 = 0; i0 < K; i0 += 32) {
         const uint32_t il = i0 + lane;
-        const uint32_t cl = il < K ? nsl_[il] : 0u;
-        const uint32_t tmask = __ballot_sync(GCL_FULL, il < K && bm_test(tcb_, cl));
+        const uint32_t cl = il < K ? W.nsl[il] : 0u;
+        const uint32_t tmask = __ballot_sync(GCL_FULL, il < K && bm_test(W.tcb, cl));
         const uint32_t cnt32 = min(32u, K - i0);
         for (uint32_t jj = 0; jj < cnt32; ++jj) {
           const uint32_t c = __shfl_sync(GCL_FULL, cl, (int)jj);
@@ -583,12 +553,12 @@ __device__ __noinline__ int sp_refine(uint32_t level) {
             lc = mash(lc, c);  // every member has count 0
             continue;
           }
-          const uint32_t ce = sp_cell_end_p(stb_, sts_, n, nw, nsw, c), L = ce - c;
-          const uint32_t k = cellcnt_[c];
-          const uint32_t* seg = G_ + off_[c];
+          const uint32_t ce = sp_cell_end(W, c), L = ce - c;
+          const uint32_t k = W.cellcnt[c];
+          const uint32_t* seg = W.G + W.off[c];
           uint32_t mn = 0xffffffffu, mx = 0;
           for (uint32_t i = lane; i < k; i += 32) {
-            const uint32_t x = cnt_[seg[i]];
+            const uint32_t x = W.cnt[seg[i]];
             mn = min(mn, x);
             mx = max(mx, x);
           }
@@ -600,29 +570,29 @@ __device__ __noinline__ int sp_refine(uint32_t level) {
           }
           // counting sort of the touched vertices by count
           const uint32_t range = mx - mn + 1;
-          for (uint32_t i = lane; i < range; i += 32) hist_[i] = 0;
+          for (uint32_t i = lane; i < range; i += 32) W.hist[i] = 0;
           __syncwarp();
-          for (uint32_t i = lane; i < k; i += 32) atomicAdd(&hist_[cnt_[seg[i]] - mn], 1u);
+          for (uint32_t i = lane; i < k; i += 32) atomicAdd(&W.hist[W.cnt[seg[i]] - mn], 1u);
           __syncwarp();
           if (lane == 0) {
             uint32_t run = 0;
             for (uint32_t i = 0; i < range; ++i) {
-              pre_[i] = run;
-              run += hist_[i];
+              W.pre[i] = run;
+              run += W.hist[i];
             }
           }
           __syncwarp();
           for (uint32_t i = lane; i < k; i += 32) {
             const uint32_t u = seg[i];
-            const uint32_t d = cnt_[u] - mn;
-            tmp_[atomicAdd(&pre_[d], 1u)] = u;  // pre[d] ends at the fragment end
+            const uint32_t d = W.cnt[u] - mn;
+            W.tmp[atomicAdd(&W.pre[d], 1u)] = u;  // pre[d] ends at the fragment end
           }
           __syncwarp();
           const uint32_t r0 = c + (L - k);
-          sp_regroup(seg, k, r0, tmp_);
+          sp_regroup(seg, k, r0, W.tmp);
           // fragments: hash, starts, in_level, active (:326-465)
-          const bool was = bm_test(act_, c);
-          const uint32_t oldlev = inlev_[c];
+          const bool was = bm_test(W.act, c);
+          const uint32_t oldlev = W.inlev[c];
           __syncwarp();
           if (lane == 0) {
             uint32_t maxsz = 0, maxf = c, lastf = c, nfr = 0;
@@ -634,15 +604,15 @@ __device__ __noinline__ int sp_refine(uint32_t level) {
             }
             uint32_t f = r0;
             for (uint32_t i = 0; i < range; ++i) {
-              const uint32_t sz = hist_[i];
+              const uint32_t sz = W.hist[i];
               if (!sz) continue;
               lc = mash(lc, mn + i + f);
               set_inlev(W, f, lvl1);
               if (f != c) {
-                fpos_[W.npend++] = f;  // set after the fold: the fold walks the old starts
+                W.fpos[W.npend++] = f;  // set after the fold: the fold walks the old starts
                 W.ncells += 1;
-                if (!bm_test(act_, f)) {
-                  bm_set1(act_, acts_, f);
+                if (!bm_test(W.act, f)) {
+                  bm_set1(W.act, W.acts, f);
                   W.nact += 1;
                 }
                 if (sz == 1) hint = f;
@@ -656,12 +626,12 @@ __device__ __noinline__ int sp_refine(uint32_t level) {
               ++nfr;
             }
             if (!was) {
-              if (!bm_test(act_, c)) {
-                bm_set1(act_, acts_, c);
+              if (!bm_test(W.act, c)) {
+                bm_set1(W.act, W.acts, c);
                 W.nact += 1;
               }
-              if (bm_test(act_, maxf)) {
-                bm_clear1(act_, acts_, maxf);
+              if (bm_test(W.act, maxf)) {
+                bm_clear1(W.act, W.acts, maxf);
                 W.nact -= 1;
               }
             }
@@ -678,25 +648,25 @@ __device__ __noinline__ int sp_refine(uint32_t level) {
     // new starts of the non-singleton fold
     __syncwarp();
     if (lane == 0) {
-      for (uint32_t i = 0; i < W.npend; ++i) add_start(W, fpos_[i]);
+      for (uint32_t i = 0; i < W.npend; ++i) add_start(W, W.fpos[i]);
       W.npend = 0;
     }
     // reset per-step scratch
     __syncwarp();
     for (uint32_t i = lane; i < nt; i += 32) {
-      const uint32_t u = T_[i], c = Tc_[i];
-      cnt_[u] = 0;
-      cellcnt_[c] = 0;
-      fill_[c] = 0;
-      tcb_[c >> 6] = 0;
-      tcbs_[c >> 12] = 0;
+      const uint32_t u = W.T[i], c = W.Tc[i];
+      W.cnt[u] = 0;
+      W.cellcnt[c] = 0;
+      W.fill[c] = 0;
+      W.tcb[c >> 6] = 0;
+      W.tcbs[c >> 12] = 0;
     }
     __syncwarp();
   }
   // clear what is left of the active set
   __syncwarp();
-  for (uint32_t w = lane; w < nw; w += 32) act_[w] = 0;
-  for (uint32_t w = lane; w < nsw; w += 32) acts_[w] = 0;
+  for (uint32_t w = lane; w < nw; w += 32) W.act[w] = 0;
+  for (uint32_t w = lane; w < nsw; w += 32) W.acts[w] = 0;
   if (lane == 0) W.nact = 0;
   __syncwarp();
   if (!ok) return -1;
