@@ -76,7 +76,7 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-serving", action="store_true")
     p.add_argument("--serve-requests", type=int, default=4000)
-    p.add_argument("--serve-rate", type=float, default=500.0,
+    p.add_argument("--serve-rate", type=float, default=350.0,
                    help="Poisson arrival rate of the serving run, requests/s")
     p.add_argument("--serve-nmax", type=int, default=4096,
                    help="largest request size (the 1%% tail is log-uniform on (2048, nmax])")
