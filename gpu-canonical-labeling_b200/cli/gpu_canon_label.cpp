@@ -7,7 +7,8 @@
 //       "Result: ISOMORPHIC" / "Result: NOT ISOMORPHIC"
 //
 // Both --parallel and --sequential run the GPU library, whose result is the
-// reference's sequential canonical form bit for bit.
+// reference's sequential canonical form bit for bit; --sequential also keeps
+// the reference's traversal and prints its statistics.
 #include <algorithm>
 #include <cstdint>
 #include <fstream>
@@ -94,8 +95,10 @@ void print_help(const char* prog) {
             << "Options:\n"
             << "  --max-aut=N            Maximum number of automorphisms stored.\n"
             << "                         Default: 10000\n"
-            << "  --sequential           Accepted for compatibility (same GPU result).\n"
+            << "  --sequential           The reference's sequential traversal on the GPU:\n"
+            << "                         same canonical form, exact statistics printed.\n"
             << "  --parallel             Use the GPU canonical labeling. Default.\n"
+            << "  --group-order          Also print the order of the automorphism group.\n"
             << "  -h, --help             Print this help message.\n";
 }
 
@@ -125,15 +128,53 @@ void print_adjacency_list(const std::vector<unsigned char>& A, int n, std::ostre
   }
 }
 
-std::vector<unsigned char> canonicalize(const Graph& g, int max_aut) {
+struct Options {
+  unsigned max_aut = 10000;
+  bool sequential = false;   // the reference's traversal: exact statistics, printed
+  bool group_order = false;  // print |Aut(G)|
+};
+
+// --sequential keeps the reference's sequential traversal for every size and
+// prints its two statistics lines (sequential.cpp:83-85); the default
+// (--parallel) lets large graphs use the wide search, like the reference's
+// GPU path.
+gcl_context* context(bool sequential) {
+  static gcl_context* ctx[2] = {nullptr, nullptr};
+  gcl_context*& c = ctx[sequential ? 1 : 0];
+  if (!c) {
+    if (gcl_create(0, &c) != GCL_OK) return nullptr;
+    if (sequential) gcl_set_option(c, GCL_OPT_WIDE_MIN_N, (int64_t)GCL_MAX_N + 1);
+  }
+  return c;
+}
+
+std::vector<unsigned char> canonicalize(const Graph& g, const Options& o) {
   std::vector<unsigned char> out((size_t)g.n * g.n);
   bool colored = std::any_of(g.color.begin(), g.color.end(), [](int c) { return c != 0; });
-  int rc = gcl_canon_one(nullptr, g.rowptr.data(), g.col.empty() ? nullptr : g.col.data(),
-                         colored ? g.color.data() : nullptr, g.n, max_aut,
-                         out.empty() ? nullptr : out.data(), nullptr, nullptr);
+  int64_t nodes = 0, num_aut = 0;
+  gcl_context* c = context(o.sequential);
+  int rc = c ? gcl_canon_one(c, g.rowptr.data(), g.col.empty() ? nullptr : g.col.data(),
+                             colored ? g.color.data() : nullptr, g.n, (int)o.max_aut,
+                             out.empty() ? nullptr : out.data(), &nodes, &num_aut)
+             : GCL_ERR_CUDA;
   if (rc != GCL_OK) {
     std::cerr << "[ERROR] " << gcl_status_string(rc) << "\n";
     return {};
+  }
+  if (o.sequential) {
+    std::cout << "Total automorphisms discovered (sequential): " << num_aut << std::endl;
+    std::cout << "Total search tree nodes created (sequential): " << nodes << std::endl;
+  }
+  if (o.group_order) {
+    double lg = 0;
+    std::vector<char> digits(1 << 20);
+    int rg = gcl_group_order(c, g.rowptr.data(), g.col.empty() ? nullptr : g.col.data(),
+                             colored ? g.color.data() : nullptr, g.n, &lg, digits.data(),
+                             (int)digits.size(), nullptr);
+    if (rg != GCL_OK)
+      std::cerr << "[ERROR] group order: " << gcl_status_string(rg) << "\n";
+    else
+      std::cout << "Automorphism group order: " << digits.data() << std::endl;
   }
   return out;
 }
@@ -141,7 +182,8 @@ std::vector<unsigned char> canonicalize(const Graph& g, int max_aut) {
 }  // namespace
 
 int main(int argc, char* argv[]) {
-  unsigned max_aut = 10000;
+  Options opt;
+  unsigned& max_aut = opt.max_aut;
   std::vector<std::string> files;
   for (int i = 1; i < argc; ++i) {
     const std::string a = argv[i];
@@ -155,8 +197,12 @@ int main(int argc, char* argv[]) {
         std::cerr << "[ERROR] " << e.what() << "\n";
         return 1;
       }
-    } else if (a == "--parallel" || a == "--sequential") {
-      // both run the GPU library
+    } else if (a == "--parallel") {
+      opt.sequential = false;
+    } else if (a == "--sequential") {
+      opt.sequential = true;
+    } else if (a == "--group-order") {
+      opt.group_order = true;
     } else if (!a.empty() && a[0] == '-') {
       std::cerr << "[ERROR] Unknown option: " << a << "\n";
       return 1;
@@ -176,7 +222,7 @@ int main(int argc, char* argv[]) {
   try {
     if (files.size() == 1) {
       const Graph g = read_dimacs(files[0]);
-      const std::vector<unsigned char> canon = canonicalize(g, (int)max_aut);
+      const std::vector<unsigned char> canon = canonicalize(g, opt);
       if (canon.empty() && g.n > 0) {
         std::cerr << "[ERROR] Canonical labeling failed.\n";
         return 1;
@@ -193,10 +239,10 @@ int main(int argc, char* argv[]) {
     const Graph g2 = read_dimacs(files[1]);
     std::cout << "\nGraph 1: " << files[0] << "\n";
     std::cout << "Computing canonical form...\n";
-    const std::vector<unsigned char> c1 = canonicalize(g1, (int)max_aut);
+    const std::vector<unsigned char> c1 = canonicalize(g1, opt);
     std::cout << "\nGraph 2: " << files[1] << "\n";
     std::cout << "Computing canonical form...\n";
-    const std::vector<unsigned char> c2 = canonicalize(g2, (int)max_aut);
+    const std::vector<unsigned char> c2 = canonicalize(g2, opt);
     if ((c1.empty() && g1.n > 0) || (c2.empty() && g2.n > 0)) {
       std::cerr << "[ERROR] Canonical labeling failed.\n";
       return 1;

@@ -82,3 +82,23 @@ def test_two_graph_verdicts(G, tmp_path):
     assert r.returncode == 0 and "Result: ISOMORPHIC" in r.stdout
     r = run(["a.txt", "c.txt", "--sequential"], tmp_path)
     assert r.returncode == 0 and "Result: NOT ISOMORPHIC" in r.stdout
+
+
+@pytest.mark.gpu
+def test_sequential_statistics_and_group_order(G, oracle_mod, tmp_path):
+    # --sequential prints the reference's two statistics lines with its exact
+    # counts (sequential.cpp:83-85); --group-order prints |Aut(G)|
+    rng = np.random.default_rng(8)
+    for k, (g, order) in enumerate([(G.torus(6), 8 * 36), (G.erdos_renyi(120, 0.05, rng), None)]):
+        p = tmp_path / f"s{k}.txt"
+        G.write_dimacs(g, str(p))
+        r = run([p.name, "--sequential", "--group-order"], tmp_path)
+        assert r.returncode == 0, r.stderr
+        mat, _, na, nd = oracle_mod.canon(g)
+        assert f"Total automorphisms discovered (sequential): {na}\n" in r.stdout
+        assert f"Total search tree nodes created (sequential): {nd}\n" in r.stdout
+        assert (tmp_path / "output").read_text() == reference_listing(mat)
+        line = [x for x in r.stdout.splitlines() if x.startswith("Automorphism group order: ")]
+        assert len(line) == 1
+        if order is not None:
+            assert int(line[0].split(": ")[1]) == order
