@@ -42,3 +42,45 @@ def test_generators(G):
         assert 10 <= g.n <= 64
         assert np.diff(g.rowptr).max() <= 4
         assert g.m >= g.n - 1
+
+
+def _is_tree(n, edges):
+    if len(edges) != n - 1:
+        return False
+    parent = list(range(n))
+
+    def find(x):
+        while parent[x] != x:
+            parent[x] = parent[parent[x]]
+            x = parent[x]
+        return x
+
+    for a, b in edges:
+        ra, rb = find(a), find(b)
+        if ra == rb:
+            return False
+        parent[ra] = rb
+    return True
+
+
+def test_large_trees_keep_degree_bound(G):
+    rng = np.random.default_rng(17)
+    for n in (129, 500, 3000):
+        t = G.recursive_tree(n, rng)
+        assert _is_tree(n, t)
+        g = G.tree_plus_edges(n, rng)
+        deg = np.diff(g.rowptr)
+        assert deg.max() <= 4 and n - 1 <= g.col.size // 2 <= n + 5
+
+
+def test_serving_workload_mix(G):
+    W = G.serving_workload(3000, rate=1000.0, seed=3, n_max=4096)
+    ns = np.array([max(W.graphs[a].n, W.graphs[b].n) for a, b in zip(W.g1, W.g2)])
+    assert abs((ns <= 128).mean() - 0.90) < 0.03
+    assert abs(((ns > 128) & (ns <= 2048)).mean() - 0.09) < 0.03
+    assert 0 < (ns > 2048).mean() < 0.03 and ns.max() <= 4096
+    assert abs(W.kind.mean() - 0.30) < 0.04
+    assert (np.diff(W.arrival) >= 0).all() and W.arrival[0] == 0
+    assert abs(len(W.kind) / W.arrival[-1] - 1000.0) < 100.0
+    iso = np.nonzero(W.kind == 1)[0]
+    assert all(W.graphs[W.g1[i]].n == W.graphs[W.g2[i]].n for i in iso)
