@@ -123,6 +123,7 @@ struct SpWarp {
   uint32_t ncells, nact, ntouched, nl1, nl2, npend;
   uint32_t pool_top, pool_cap, aut_cap, max_aut;
   uint32_t utop, ulog_cap, ulog_bad;
+  uint32_t fixcap;  // store entries whose fix state is kept (later ones are checked in full)
   // values the serial fold hands to the whole warp
   uint32_t lc, hint;
 };
@@ -1092,7 +1093,8 @@ __device__ __noinline__ bool sp_orbits(int idx, int num_aut, uint32_t seqlen) {
       // extend what is known about entry a along the current sequence: the
       // prefix it fixes and the first position it moves stay valid until a
       // backtrack shortens the sequence below them (sp_fix_clamp)
-      uint2 st = W.fixst[a];
+      const bool kept = (uint32_t)a < W.fixcap;
+      uint2 st = kept ? W.fixst[a] : make_uint2(0u, kNone);
       if (st.y != kNone && st.y < seqlen) {
         fix = false;
       } else {
@@ -1105,7 +1107,7 @@ __device__ __noinline__ bool sp_orbits(int idx, int num_aut, uint32_t seqlen) {
         fix = j >= seqlen;
         st.x = j;
         st.y = fix ? kNone : j;
-        W.fixst[a] = st;
+        if (kept) W.fixst[a] = st;
       }
     }
     const uint32_t fm = __ballot_sync(GCL_FULL, fix);
@@ -1170,6 +1172,7 @@ __device__ __noinline__ bool sp_orbits(int idx, int num_aut, uint32_t seqlen) {
 // change, so what entries [0, count) knew about them is dropped.
 __device__ __noinline__ void sp_fix_clamp(uint32_t s, uint32_t count) {
   SpWarp& W = sp_w();
+  count = min(count, W.fixcap);
   for (uint32_t a = lane_id(); a < count; a += 32) {
     uint2 st = W.fixst[a];
     if (st.x > s || (st.y != kNone && st.y >= s)) {
@@ -1376,6 +1379,7 @@ __device__ __noinline__ void sp_bind(uint8_t* slot, const SpLayout& Lo, uint32_t
   W.umark = base[25];
   W.ulog = (uint2*)(slot + Lo.ulog);
   W.fixst = (uint2*)(slot + Lo.fixst);
+  W.fixcap = Lo.fixcap;
   W.ulog_cap = Lo.ulog_cap;
   W.utop = 0;
   W.ulog_bad = 0;
@@ -1649,7 +1653,7 @@ __device__ __noinline__ SpResult sp_search(const BatchArgs& A, int g, uint8_t* s
           break;
         }
         sp_store_aut(dec == 1 ? W.flabel : W.blabel, W.auts + (uint64_t)si * W.stride);
-        if (lane == 0) W.fixst[si] = make_uint2(0u, kNone);
+        if (lane == 0 && si < W.fixcap) W.fixst[si] = make_uint2(0u, kNone);
         __syncwarp();
         ++num_aut;
         const int gg = dec == 1 ? sp_gca(W.fseq, first_seqlen, seqlen)

@@ -609,6 +609,7 @@ __device__ __noinline__ int32_t wide_gate(WideHdr* H, uint32_t need, uint64_t de
 // about how they act on its sequence.
 __device__ __noinline__ void wide_fix_init(uint32_t from, uint32_t to) {
   SpWarp& W = sp_w();
+  to = min(to, W.fixcap);
   for (uint32_t a = from + lane_id(); a < to; a += 32) W.fixst[a] = make_uint2(0u, kNone);
   __syncwarp();
 }

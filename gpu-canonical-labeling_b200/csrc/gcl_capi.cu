@@ -83,13 +83,16 @@ __global__ void __launch_bounds__(kOrderThreads)
 constexpr int kSpSmemPerBlock = 200 * 1024;  // dynamic shared memory cap of one sparse block
 constexpr uint32_t kWidePool = 64;  // per-level orbit arrays of a wide-search warp
 constexpr uint64_t kWideStoreBytes = 1ull << 30;  // automorphism store of a wide search
+constexpr uint64_t kWideStoreEntries = 1ull << 22;  // ... and at most this many entries
+constexpr uint32_t kWideFixCap = 4096;  // entries whose fix state a wide-search warp keeps
 constexpr uint64_t kGroupWorkCap = 40000000000ull;  // Schreier-Sims operations (~20 s)
 
 // entries of a wide search's automorphism store: max_aut, within kWideStoreBytes
 static uint32_t wide_store_cap(uint32_t n, int max_aut) {
   const uint64_t per_aut = 2ull * ((uint64_t)n + 2);
   return (uint32_t)std::max<uint64_t>(
-      1, std::min<uint64_t>((uint64_t)max_aut, kWideStoreBytes / per_aut));
+      1, std::min<uint64_t>(std::min<uint64_t>((uint64_t)max_aut, kWideStoreBytes / per_aut),
+                            kWideStoreEntries));
 }
 // Per-level orbit arrays and automorphism-ring entries of the sparse passes:
 // the first pass (n <= 4096 / larger), then a middle rerun of the graphs
@@ -580,7 +583,7 @@ int gcl_canon_wide_device_async(gcl_context* c, const int32_t* d_rowptr, const i
   const uint64_t m2 = (uint64_t)std::max<int64_t>(m, 1);
   const uint32_t cap = wide_store_cap(un, max_aut);
   const WideLayout WL = wide_layout(un, m2, cap);
-  const SpLayout Lo = sp_layout(un, m2, kWidePool, 0, cap);
+  const SpLayout Lo = sp_layout(un, m2, kWidePool, 0, std::min<uint32_t>(cap, kWideFixCap));
   uint64_t smw = c->smem_stage ? sp_smem_bytes(un) : 0;
   if (smw * kSpWarps > (uint64_t)kSpSmemPerBlock) smw = 0;
   int per_sm = 0;
