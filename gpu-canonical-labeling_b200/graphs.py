@@ -235,6 +235,42 @@ def disjoint_union(g: Graph, k: int) -> Graph:
     return from_edges(g.n * k, np.concatenate(parts) if len(e) else e, col)
 
 
+def cfi_graph(base_n: int, rng: np.random.Generator, twist: bool = False) -> Graph:
+    """Cai-Fuerer-Immerman gadget graph over a random cubic base graph of
+    `base_n` vertices (10 * base_n vertices).  Each base vertex becomes four
+    middle vertices (the even subsets of its three edges) and a pair of end
+    vertices per edge; a middle vertex joins end 1 of the edges in its subset
+    and end 0 of the others; the ends of a base edge are joined 0-0 and 1-1
+    (0-1 and 1-0 on the first edge when `twist`).  Colour refinement leaves
+    these graphs nearly undivided, so their search trees are deep with many
+    inequivalent leaves."""
+    base = random_regular(base_n, 3, rng)
+    be = [tuple(int(x) for x in e) for e in base.edges()]
+    inc: List[List[int]] = [[] for _ in range(base_n)]
+    for k, (u, v) in enumerate(be):
+        inc[u].append(k)
+        inc[v].append(k)
+    ends = {}
+    nid = 4 * base_n
+    for v in range(base_n):
+        for k in inc[v]:
+            for bit in (0, 1):
+                ends[(v, k, bit)] = nid
+                nid += 1
+    edges = []
+    subsets = [(), (0, 1), (0, 2), (1, 2)]
+    for v in range(base_n):
+        for si, sub in enumerate(subsets):
+            m = 4 * v + si
+            for t, k in enumerate(inc[v]):
+                edges.append((m, ends[(v, k, 1 if t in sub else 0)]))
+    for k, (u, v) in enumerate(be):
+        flip = 1 if (twist and k == 0) else 0
+        for bit in (0, 1):
+            edges.append((ends[(u, k, bit)], ends[(v, k, bit ^ flip)]))
+    return from_edges(nid, edges)
+
+
 def prufer_tree(n: int, rng: np.random.Generator, max_deg: int = 4) -> List[Tuple[int, int]]:
     """Uniform labelled tree (Pruefer sequence) rejected until max degree <= max_deg."""
     if n <= 2:

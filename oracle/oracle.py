@@ -123,3 +123,64 @@ def root_refine(g) -> Tuple[int, np.ndarray, np.ndarray]:
     code = lib.gcl_oracle_root_refine(n, _ptr(rp), _ptr(cl if cl.size else np.zeros(1, np.int32)),
                                       _ptr(co), _ptr(el), _ptr(cs))
     return code, el, cs
+
+
+WIDE_SO = os.path.join(HERE, "libgcl_wide_model.so")
+
+
+def _load_wide():
+    if "wide" in _libs:
+        return _libs["wide"]
+    if not os.path.exists(WIDE_SO):
+        raise FileNotFoundError(f"oracle library missing: {WIDE_SO} (run make -C oracle)")
+    lib = ctypes.CDLL(WIDE_SO)
+    lib.gcl_wide_model.argtypes = [ctypes.c_int, _P, _P, _P, ctypes.c_int, ctypes.c_uint,
+                                   ctypes.c_int, _P, ctypes.POINTER(ctypes.c_long),
+                                   ctypes.POINTER(ctypes.c_int), _P]
+    lib.gcl_wide_model.restype = ctypes.c_int
+    lib.gcl_exhaustive_canon.argtypes = [ctypes.c_int, _P, _P, _P, ctypes.c_long, _P,
+                                         ctypes.POINTER(ctypes.c_long)]
+    lib.gcl_exhaustive_canon.restype = ctypes.c_int
+    _libs["wide"] = lib
+    return lib
+
+
+def _csr(g):
+    rp = np.ascontiguousarray(g.rowptr, dtype=np.int32)
+    cl = np.ascontiguousarray(g.col, dtype=np.int32)
+    co = None if g.color is None else np.ascontiguousarray(g.color, dtype=np.int32)
+    return rp, (cl if cl.size else np.zeros(1, np.int32)), co
+
+
+def wide_model(g, workers: int, seed: int = 0, cap: int = 10000):
+    """CPU model of the many-worker search (wide_model.c): `workers` simulated
+    workers over the first path's sibling items, stepped round-robin (seed 0)
+    or in a seeded random order.  Returns (canonical matrix, nodes, automorphisms
+    stored, events) where events counts [leaves equivalent to a best found
+    outside their item, nodes pruned as worse than the private best, leaves
+    that beat the private best but not a newer shared one]."""
+    lib = _load_wide()
+    rp, cl, co = _csr(g)
+    out = np.zeros((g.n, g.n), dtype=np.uint8)
+    nodes = ctypes.c_long(0)
+    naut = ctypes.c_int(0)
+    ev = np.zeros(3, dtype=np.int64)
+    rc = lib.gcl_wide_model(g.n, _ptr(rp), _ptr(cl), _ptr(co), workers, seed, cap, _ptr(out),
+                            ctypes.byref(nodes), ctypes.byref(naut), _ptr(ev))
+    if rc != 0:
+        raise RuntimeError(f"wide model failed rc={rc}")
+    return out, int(nodes.value), int(naut.value), ev
+
+
+def exhaustive(g, max_leaves: int = 200000) -> Optional[np.ndarray]:
+    """The maximum leaf over the whole search tree (no pruning), or None when
+    the tree has more than `max_leaves` leaves."""
+    lib = _load_wide()
+    rp, cl, co = _csr(g)
+    out = np.zeros((g.n, g.n), dtype=np.uint8)
+    leaves = ctypes.c_long(0)
+    rc = lib.gcl_exhaustive_canon(g.n, _ptr(rp), _ptr(cl), _ptr(co), max_leaves, _ptr(out),
+                                  ctypes.byref(leaves))
+    if rc < 0:
+        raise RuntimeError("exhaustive search failed")
+    return None if rc else out
