@@ -24,6 +24,7 @@
 #include "canon_warp64.cuh"
 #include "canon_wide.cuh"
 #include "gcl_group.h"
+#include "gcl_guard.h"
 
 namespace gcl {
 
@@ -297,7 +298,7 @@ const char* gcl_status_string(int s) {
 
 int gcl_version(void) { return 100; }
 
-int gcl_create(int device, gcl_context** out) {
+int gcl_create(int device, gcl_context** out) try {
   if (!out) return GCL_ERR_ARG;
   *out = nullptr;
   int ndev = 0;
@@ -349,7 +350,7 @@ int gcl_create(int device, gcl_context** out) {
   }
   *out = c;
   return GCL_OK;
-}
+} GCL_CATCH_ALL
 
 int gcl_destroy(gcl_context* c) {
   if (!c) return GCL_ERR_ARG;
@@ -382,7 +383,7 @@ int gcl_canon_batch_device_async(gcl_context* c, int count, const int64_t* d_vof
                                  const int64_t* d_ooff, uint64_t* d_out_rows,
                                  const int64_t* d_roff,
                                  int32_t* d_out_label, int64_t* d_out_stats,
-                                 int32_t* d_out_status) {
+                                 int32_t* d_out_status) try {
   if (!c || count < 0 || max_aut <= 0 || !d_voff || !d_eoff || !d_rowptr || !d_out_status ||
       (d_out_dense && !d_ooff) || (d_out_rows && !d_roff) || max_n < 0 || max_n > GCL_MAX_N)
     return GCL_ERR_ARG;
@@ -530,7 +531,7 @@ int gcl_canon_batch_device_async(gcl_context* c, int count, const int64_t* d_vof
     GCL_TRY(cudaGetLastError());
   }
   return GCL_OK;
-}
+} GCL_CATCH_ALL
 
 int gcl_set_option(gcl_context* c, int option, int64_t value) {
   if (!c) return GCL_ERR_ARG;
@@ -574,7 +575,7 @@ int gcl_canon_wide_device_async(gcl_context* c, const int32_t* d_rowptr, const i
                                 const int32_t* d_color, int n, int64_t m, int max_aut,
                                 uint8_t* d_out_dense, uint64_t* d_out_rows,
                                 int32_t* d_out_label, int64_t* d_out_stats,
-                                int32_t* d_out_status) {
+                                int32_t* d_out_status) try {
   if (!c || n < 1 || m < 0 || max_aut <= 0 || !d_rowptr || (m > 0 && !d_col) || !d_out_status)
     return GCL_ERR_ARG;
   if (n > GCL_MAX_N) return GCL_ERR_TOO_LARGE;
@@ -626,7 +627,7 @@ int gcl_canon_wide_device_async(gcl_context* c, const int32_t* d_rowptr, const i
   wide_finish_kernel<<<1, 32, 0, s>>>(WA);
   GCL_TRY(cudaGetLastError());
   return GCL_OK;
-}
+} GCL_CATCH_ALL
 
 }  // extern "C"
 
@@ -702,7 +703,7 @@ int gcl_canon_batch(gcl_context* c, int count, const int64_t* voff, const int64_
                     const int32_t* rowptr, const int32_t* col, const int32_t* color, int max_aut,
                     uint8_t* out_dense, const int64_t* ooff, uint64_t* out_rows,
                     const int64_t* roff, int32_t* out_label, int64_t* out_stats,
-                    int32_t* out_status) {
+                    int32_t* out_status) try {
   if (!c || count < 0 || max_aut <= 0 || !voff || !eoff || !rowptr || !out_status ||
       (out_dense && !ooff) || (out_rows && !roff))
     return GCL_ERR_ARG;
@@ -789,10 +790,10 @@ int gcl_canon_batch(gcl_context* c, int count, const int64_t* voff, const int64_
   for (int g = 0; g < count; ++g)
     if (out_status[g] != kOk) return graph_status_to_rc(out_status[g]);
   return GCL_OK;
-}
+} GCL_CATCH_ALL
 
 int gcl_canon_one(gcl_context* c, const int32_t* rowptr, const int32_t* col, const int32_t* color,
-                  int n, int max_aut, uint8_t* out_nxn, int64_t* node_count, int64_t* num_aut) {
+                  int n, int max_aut, uint8_t* out_nxn, int64_t* node_count, int64_t* num_aut) try {
   if (n < 0 || !rowptr || max_aut <= 0 || (n > 0 && !out_nxn)) return GCL_ERR_ARG;
   if (!c) {
     int rc = default_context(&c);
@@ -824,11 +825,11 @@ int gcl_canon_one(gcl_context* c, const int32_t* rowptr, const int32_t* col, con
   if (num_aut) *num_aut = st[0];
   if (node_count) *node_count = st[1];
   return GCL_OK;
-}
+} GCL_CATCH_ALL
 
 int gcl_iso(gcl_context* c, const int32_t* rp1, const int32_t* col1, const int32_t* color1, int n1,
             const int32_t* rp2, const int32_t* col2, const int32_t* color2, int n2, int max_aut,
-            int* verdict) {
+            int* verdict) try {
   if (!verdict || n1 < 0 || n2 < 0 || !rp1 || !rp2 || max_aut <= 0) return GCL_ERR_ARG;
   if (!c) {
     int rc = default_context(&c);
@@ -847,11 +848,11 @@ int gcl_iso(gcl_context* c, const int32_t* rp1, const int32_t* col1, const int32
       }
   *verdict = same;
   return GCL_OK;
-}
+} GCL_CATCH_ALL
 
 int gcl_group_order(gcl_context* c, const int32_t* rowptr, const int32_t* col,
                     const int32_t* color, int n, double* log10_order, char* digits,
-                    int digits_cap, int64_t* generators) {
+                    int digits_cap, int64_t* generators) try {
   if (n < 0 || !rowptr || !log10_order || (digits && digits_cap < 2)) return GCL_ERR_ARG;
   if (n > GCL_MAX_N) return GCL_ERR_TOO_LARGE;
   if (!c) {
@@ -913,10 +914,10 @@ int gcl_group_order(gcl_context* c, const int32_t* rowptr, const int32_t* col,
   if (!group_order(un, auts.data(), (uint64_t)st[0], WL.stride, kGroupWorkCap, &lg, &d, &base_len))
     return GCL_ERR_TIMEOUT;
   return put(d, lg, st[0]);
-}
+} GCL_CATCH_ALL
 
 int gcl_perm_group_order(int n, const uint16_t* perms, int64_t count, double* log10_order,
-                         char* digits, int digits_cap) {
+                         char* digits, int digits_cap) try {
   if (n < 0 || n > GCL_MAX_N || count < 0 || (count > 0 && !perms) || !log10_order ||
       (digits && digits_cap < 2))
     return GCL_ERR_ARG;
@@ -940,7 +941,7 @@ int gcl_perm_group_order(int n, const uint16_t* perms, int64_t count, double* lo
     std::memcpy(digits, d.c_str(), d.size() + 1);
   }
   return GCL_OK;
-}
+} GCL_CATCH_ALL
 
 int gcl_set_tuning(gcl_context* c, const gcl_tuning* t) {
   if (!c || !t) return GCL_ERR_ARG;
@@ -954,7 +955,7 @@ int gcl_set_tuning(gcl_context* c, const gcl_tuning* t) {
 
 int gcl_autotune(gcl_context* c, int count, const int64_t* voff, const int64_t* eoff,
                  const int32_t* rowptr, const int32_t* col, const int32_t* color, int max_aut,
-                 int repeats, gcl_tuning* out) {
+                 int repeats, gcl_tuning* out) try {
   if (!c || count <= 0 || !voff || !eoff || !rowptr || !out || max_aut <= 0) return GCL_ERR_ARG;
   if (repeats < 1) repeats = 2;
   GCL_TRY(cudaSetDevice(c->device));
@@ -1053,6 +1054,6 @@ int gcl_autotune(gcl_context* c, int count, const int64_t* voff, const int64_t* 
     out->sp_ms[bk] = seen ? best_sp[bk] : -1.f;
   }
   return gcl_set_tuning(c, out);
-}
+} GCL_CATCH_ALL
 
 }  // extern "C"

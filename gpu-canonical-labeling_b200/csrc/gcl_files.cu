@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "../../include/gcl.h"
+#include "gcl_guard.h"
 
 namespace {
 
@@ -157,17 +158,32 @@ int rc_of(cudaError_t e) {
   return e == cudaErrorMemoryAllocation ? GCL_ERR_NOMEM : GCL_ERR_CUDA;
 }
 
-void parse_chunk(Slot& sl, const char* const* paths, int64_t first, int64_t cnt, int threads) {
+// Parses paths[first, first + cnt) into the slot with up to `threads` host
+// threads.  GCL_ERR_NOMEM when a parser ran out of host memory.
+int parse_chunk(Slot& sl, const char* const* paths, int64_t first, int64_t cnt, int threads) {
   sl.first = first;
   sl.graphs.assign((size_t)cnt, FGraph());
   std::atomic<int64_t> next{0};
+  std::atomic<bool> failed{false};
   auto work = [&] {
-    for (int64_t i = next++; i < cnt; i = next++) sl.graphs[i] = parse_dimacs(paths[first + i]);
+    for (int64_t i = next++; i < cnt && !failed.load(); i = next++) {
+      try {
+        sl.graphs[i] = parse_dimacs(paths[first + i]);
+      } catch (...) {
+        failed.store(true);
+      }
+    }
   };
   std::vector<std::thread> pool;
-  for (int t = 1; t < threads; ++t) pool.emplace_back(work);
+  try {
+    pool.reserve((size_t)std::max(threads - 1, 0));
+    for (int t = 1; t < threads; ++t) pool.emplace_back(work);
+  } catch (...) {
+    // fewer helper threads than asked for: the calling thread still parses
+  }
   work();
   for (auto& th : pool) th.join();
+  return failed.load() ? GCL_ERR_NOMEM : GCL_OK;
 }
 
 // pack the chunk's good graphs into the slot's pinned arena and enqueue copy
@@ -297,16 +313,21 @@ extern "C" int gcl_canon_files(gcl_context* c, int64_t count, const char* const*
     sl.bind(s);
     if (rc == GCL_OK) rc = rc_of(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming));
   }
-  int64_t k = 0;
-  for (int64_t first = 0; rc == GCL_OK && first < count; first += chunk, ++k) {
-    Slot& cur = slot[k & 1];
-    Slot& prev = slot[(k + 1) & 1];
-    // parse this chunk while the GPU works on the previous one
-    parse_chunk(cur, paths, first, std::min<int64_t>(chunk, count - first), threads);
-    if (k > 0) rc = deliver(prev, cb, user);
-    if (rc == GCL_OK) rc = launch_chunk(c, cur, max_aut);
+  try {
+    int64_t k = 0;
+    for (int64_t first = 0; rc == GCL_OK && first < count; first += chunk, ++k) {
+      Slot& cur = slot[k & 1];
+      Slot& prev = slot[(k + 1) & 1];
+      // parse this chunk while the GPU works on the previous one
+      rc = parse_chunk(cur, paths, first, std::min<int64_t>(chunk, count - first), threads);
+      if (rc == GCL_OK && k > 0) rc = deliver(prev, cb, user);
+      if (rc == GCL_OK) rc = launch_chunk(c, cur, max_aut);
+    }
+    if (rc == GCL_OK && k > 0) rc = deliver(slot[(k - 1) & 1], cb, user);
+  } catch (...) {
+    rc = gcl::exception_status();
   }
-  if (rc == GCL_OK && k > 0) rc = deliver(slot[(k - 1) & 1], cb, user);
+  // copies in flight read and write the slots' pinned buffers
   cudaStreamSynchronize(s);
   for (Slot& sl : slot) {
     sl.release();

@@ -19,6 +19,7 @@
 #include <cstdint>
 #include <cstring>
 #include <deque>
+#include <memory>
 #include <mutex>
 #include <new>
 #include <thread>
@@ -27,6 +28,7 @@
 
 #include "../../include/gcl.h"
 #include "gcl_device.cuh"
+#include "gcl_guard.h"
 
 namespace gcl {
 
@@ -728,11 +730,29 @@ bool copy_graph(Graph& g, const int32_t* rp, const int32_t* col, const int32_t* 
   return true;
 }
 
+// Frees the lanes (each on its own stream, before its context goes), the
+// device table and the server itself.  The dispatcher must not be running.
+void teardown(gcl_server* S) {
+  cudaSetDevice(S->device);
+  for (Lane* L : S->lanes) {
+    if (L->s) cudaStreamSynchronize(L->s);
+    L->release();
+    if (L->ctx) gcl_destroy(L->ctx);
+    delete L;
+  }
+  S->keys.release();
+  S->vals.release();
+  S->store.release();
+  S->top.release();
+  cudaDeviceSynchronize();
+  delete S;
+}
+
 }  // namespace
 
 extern "C" {
 
-int gcl_serve_create(int device, const gcl_serve_config* cfg, gcl_server** out) {
+int gcl_serve_create(int device, const gcl_serve_config* cfg, gcl_server** out) try {
   if (!out) return GCL_ERR_ARG;
   *out = nullptr;
   gcl_serve_config c{};
@@ -769,6 +789,12 @@ int gcl_serve_create(int device, const gcl_serve_config* cfg, gcl_server** out) 
   int dev_sms = 0;
   cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, device);
   const int nl[kClasses] = {c.lanes, c.mid_lanes, c.big_lanes, c.large_lanes};
+  try {
+    S->lanes.reserve((size_t)(nl[0] + nl[1] + nl[2] + nl[3]));
+  } catch (...) {
+    delete S;
+    throw;
+  }
   for (int i = 0; i < nl[0] + nl[1] + nl[2] + nl[3] && rc == GCL_OK; ++i) {
     Lane* L = new (std::nothrow) Lane();
     if (!L) {
@@ -808,23 +834,18 @@ int gcl_serve_create(int device, const gcl_serve_config* cfg, gcl_server** out) 
   if (rc == GCL_OK) rc = rc_of(cudaMemset(S->top.p, 0, 8));
   if (rc == GCL_OK) rc = rc_of(cudaDeviceSynchronize());
   if (rc != GCL_OK) {
-    for (Lane* L : S->lanes) {
-      L->release();  // frees on the lane's stream, before the context goes
-      if (L->ctx) gcl_destroy(L->ctx);
-      delete L;
-    }
-    S->keys.release();
-    S->vals.release();
-    S->store.release();
-    S->top.release();
-    cudaDeviceSynchronize();
-    delete S;
+    teardown(S);
     return rc;
   }
-  S->th = std::thread(dispatcher, S);
+  try {
+    S->th = std::thread(dispatcher, S);
+  } catch (...) {
+    teardown(S);
+    throw;
+  }
   *out = S;
   return GCL_OK;
-}
+} GCL_CATCH_ALL
 
 int gcl_serve_destroy(gcl_server* S) {
   if (!S) return GCL_ERR_ARG;
@@ -834,40 +855,26 @@ int gcl_serve_destroy(gcl_server* S) {
   }
   S->cv_work.notify_all();
   if (S->th.joinable()) S->th.join();
-  cudaSetDevice(S->device);
-  for (Lane* L : S->lanes) {
-    if (L->s) cudaStreamSynchronize(L->s);
-    L->release();  // frees on the lane's stream, before the context goes
-    if (L->ctx) gcl_destroy(L->ctx);
-    delete L;
-  }
-  S->keys.release();
-  S->vals.release();
-  S->store.release();
-  S->top.release();
-  cudaDeviceSynchronize();
   for (auto& q : S->q)
     for (Req* r : q) delete r;
-  delete S;
+  teardown(S);
   return GCL_OK;
 }
 
 int gcl_serve_submit(gcl_server* S, int64_t id, int kind, const int32_t* rowptr,
                      const int32_t* col, const int32_t* color, int n, const int32_t* rowptr2,
                      const int32_t* col2, const int32_t* color2, int n2, uint64_t* out_rows,
-                     int32_t* out_label) {
+                     int32_t* out_label) try {
   if (!S || (kind != GCL_REQ_CANON && kind != GCL_REQ_ISO)) return GCL_ERR_ARG;
-  Req* r = new (std::nothrow) Req();
+  std::unique_ptr<Req> r(new (std::nothrow) Req());
   if (!r) return GCL_ERR_NOMEM;
   r->t0 = Clock::now();
   r->id = id;
   r->kind = kind;
   r->ng = kind == GCL_REQ_ISO ? 2 : 1;
   if (!copy_graph(r->g[0], rowptr, col, color, n) ||
-      (r->ng == 2 && !copy_graph(r->g[1], rowptr2, col2, color2, n2))) {
-    delete r;
+      (r->ng == 2 && !copy_graph(r->g[1], rowptr2, col2, color2, n2)))
     return GCL_ERR_ARG;
-  }
   if (kind == GCL_REQ_CANON) {
     r->out_rows = out_rows;
     r->out_label = out_label;
@@ -898,8 +905,7 @@ int gcl_serve_submit(gcl_server* S, int64_t id, int kind, const int32_t* rowptr,
     } else {
       res.verdict = e[0].in.n == e[1].in.n && e[0].rows == e[1].rows;
     }
-    submit_done_now(S, r, res);
-    delete r;
+    submit_done_now(S, r.get(), res);
     return GCL_OK;
   }
   const int nmax = std::max(r->g[0].n, r->ng == 2 ? r->g[1].n : 0);
@@ -909,13 +915,14 @@ int gcl_serve_submit(gcl_server* S, int64_t id, int kind, const int32_t* rowptr,
                                          : kSmall;
   {
     std::lock_guard<std::mutex> lk(S->mu);
-    S->q[cls].push_back(r);
+    S->q[cls].push_back(r.get());
+    r.release();  // owned by the queue
   }
   S->cv_work.notify_one();
   return GCL_OK;
-}
+} GCL_CATCH_ALL
 
-int gcl_serve_poll(gcl_server* S, gcl_serve_result* out, int max, int timeout_ms) {
+int gcl_serve_poll(gcl_server* S, gcl_serve_result* out, int max, int timeout_ms) try {
   if (!S || !out || max < 0) return GCL_ERR_ARG;
   std::unique_lock<std::mutex> lk(S->mu);
   if (S->done.empty() && timeout_ms != 0) {
@@ -931,19 +938,19 @@ int gcl_serve_poll(gcl_server* S, gcl_serve_result* out, int max, int timeout_ms
     S->done.pop_front();
   }
   return k;
-}
+} GCL_CATCH_ALL
 
-int gcl_serve_stats_get(gcl_server* S, gcl_serve_stats* out) {
+int gcl_serve_stats_get(gcl_server* S, gcl_serve_stats* out) try {
   if (!S || !out) return GCL_ERR_ARG;
   std::lock_guard<std::mutex> lk(S->mu);
   *out = S->st;
   return GCL_OK;
-}
+} GCL_CATCH_ALL
 
 int gcl_serve_replay(gcl_server* S, int nreq, const double* arrival_s, const int32_t* kind,
                      const int32_t* g1, const int32_t* g2, int count, const int64_t* voff,
                      const int64_t* eoff, const int32_t* rowptr, const int32_t* col,
-                     const int32_t* color, double timeout_s, gcl_serve_result* results) {
+                     const int32_t* color, double timeout_s, gcl_serve_result* results) try {
   if (!S || nreq < 0 || !arrival_s || !kind || !g1 || !voff || !eoff || !rowptr || !results)
     return GCL_ERR_ARG;
   for (int i = 0; i < nreq; ++i) {
@@ -961,6 +968,7 @@ int gcl_serve_replay(gcl_server* S, int nreq, const double* arrival_s, const int
     *cl = col + eoff[g];
     *co = color ? color + voff[g] : nullptr;
   };
+  std::vector<gcl_serve_result> buf(256);  // allocated before the thread starts
   std::thread gen([&] {
     for (int i = 0; i < nreq; ++i) {
       const Clock::time_point due =
@@ -983,7 +991,6 @@ int gcl_serve_replay(gcl_server* S, int nreq, const double* arrival_s, const int
     }
   });
   int have = 0, rc = GCL_OK;
-  std::vector<gcl_serve_result> buf(256);
   while (have < nreq) {
     const int k = gcl_serve_poll(S, buf.data(), (int)buf.size(), 5);
     for (int j = 0; j < k; ++j) {
@@ -1006,6 +1013,6 @@ int gcl_serve_replay(gcl_server* S, int nreq, const double* arrival_s, const int
   if (rc == GCL_OK)
     for (int i = 0; i < nreq; ++i) results[i].latency_s += lag[i];
   return rc;
-}
+} GCL_CATCH_ALL
 
 }  // extern "C"

@@ -23,3 +23,40 @@ def test_library_exports_header(pkg):
     assert sorted(api.EXPORTS) == names
     assert lib.gcl_version() >= 100
     assert lib.gcl_status_string(-4).decode().startswith("bad input")
+
+
+def test_exceptions_stop_at_the_c_abi(tmp_path):
+    # the entry points are function-try-blocks over gcl::exception_status()
+    src = tmp_path / "guard.cpp"
+    src.write_text(r'''
+#include <cstdio>
+#include <new>
+#include <stdexcept>
+#include <vector>
+#include "gcl_guard.h"
+extern "C" int f_alloc(int k) try {
+  if (k == 0) throw std::bad_alloc();
+  if (k == 1) { std::vector<int> v; v.reserve(v.max_size() + 1ull); }
+  if (k == 2) throw std::runtime_error("x");
+  return GCL_OK;
+} GCL_CATCH_ALL
+int main() {
+  std::printf("%d %d %d %d\n", f_alloc(0), f_alloc(1), f_alloc(2), f_alloc(3));
+  return 0;
+}
+''')
+    exe = tmp_path / "guard"
+    import subprocess
+    cxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
+    subprocess.run([cxx, "-std=c++17", "-I", os.path.join(ROOT, "gpu-canonical-labeling_b200", "csrc"),
+                    "-o", str(exe), str(src)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()
+    assert out == ["-3", "-3", "-7", "0"]  # NOMEM, NOMEM, INTERNAL, OK
+
+
+def test_create_rejects_a_missing_device(pkg):
+    # device -1 never exists; without a GPU every device is missing
+    lib = pkg.api.load_library()
+    out = ctypes.c_void_p(1)
+    rc = lib.gcl_create(-1, ctypes.byref(out))
+    assert rc in (-1, -2) and not out.value
