@@ -366,15 +366,24 @@ void memo_put(gcl_server* S, const Graph& g, uint64_t key, const uint64_t* rows,
       S->memo.erase(it);
     }
   }
-  MemoEntry e;
-  e.in = g;
-  e.rows.assign(rows, rows + words);
-  e.label.assign(label, label + g.n);
-  e.cls = cls;
-  e.hash = hash;
-  S->memo.emplace(key, std::move(e));
-  S->memo_fifo.push_back(key);
-  S->memo_used += bytes;
+  try {
+    MemoEntry e;
+    e.in = g;
+    e.rows.assign(rows, rows + words);
+    e.label.assign(label, label + g.n);
+    e.cls = cls;
+    e.hash = hash;
+    auto ins = S->memo.emplace(key, std::move(e));
+    try {
+      S->memo_fifo.push_back(key);
+    } catch (...) {
+      S->memo.erase(ins.first);
+      throw;
+    }
+    S->memo_used += bytes;
+  } catch (...) {
+    // the memo is a cache: an entry that finds no host memory is not kept
+  }
 }
 
 bool memo_get(gcl_server* S, const Graph& g, uint64_t key, MemoEntry* out) {
