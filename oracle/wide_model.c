@@ -296,7 +296,7 @@ static int wm_start_item(wm_worker* w, wm_shared* G, uint32_t k, uint32_t v) {
 
 int gcl_wide_model(int n, const int32_t* rowptr, const int32_t* col, const int32_t* color,
                    int workers, unsigned seed, int cap, uint8_t* out_nxn, long* nodes_out,
-                   int* naut_out, long* events_out) {
+                   int* naut_out, long* events_out, uint32_t* auts_out) {
   if (n < 1 || workers < 1 || cap < 1) return -1;
   osearch S0;
   memset(&S0, 0, sizeof S0);
@@ -405,6 +405,7 @@ int gcl_wide_model(int n, const int32_t* rowptr, const int32_t* col, const int32
   if (nodes_out) *nodes_out = G.nodes;
   if (naut_out) *naut_out = G.naut;
   if (events_out) memcpy(events_out, G.events, sizeof G.events);
+  if (auts_out) memcpy(auts_out, G.auts, (size_t)G.naut * n * 4); /* cap x n entries */
   for (int i = 0; i < workers; ++i) {
     free(ws[i].pathcode);
     ws[i].S.auts = NULL; /* the shared store, freed below */

@@ -9,7 +9,10 @@ adopted best is pruned.  These tests run the same rules on the CPU under
 many interleavings of the workers and check that every schedule yields the
 sequential canonical matrix, and that the sequential result is the maximum
 over all leaves of the unpruned tree -- the property that makes the result
-independent of the order in which the leaves are met.
+independent of the order in which the leaves are met.  The automorphisms the
+model stores are also fed to the library's host Schreier-Sims: under every
+schedule they generate the whole automorphism group, which is what
+gcl_group_order relies on.
 """
 import os
 
@@ -97,3 +100,54 @@ def test_sequential_is_maximum_leaf(G, wm):
         assert np.array_equal(full, wm.canon(g)[0]), g.n
         checked += 1
     assert checked >= 8
+
+
+def _brute_order(g):
+    import itertools
+    n = g.n
+    e = {tuple(x) for x in g.edges().tolist()}
+    e |= {(b, a) for a, b in e}
+    col = g.color if g.color is not None else np.zeros(n, int)
+    return sum(1 for p in itertools.permutations(range(n))
+               if all(col[p[v]] == col[v] for v in range(n)) and all((p[a], p[b]) in e for a, b in e))
+
+
+def test_wide_model_automorphisms_generate_the_group(G, wm, pkg):
+    # gcl_group_order rests on this: the automorphisms a wide search stores
+    # generate Aut(G), whatever the schedule.  The model's store goes through
+    # the library's host Schreier-Sims (gcl_perm_group_order, no GPU needed).
+    import math
+    rng = np.random.default_rng(21)
+    cases = [(G.torus(k), 8 * k * k) for k in (5, 6, 7)]  # (C4 x C4 is Q4: 384)
+    cases += [(G.from_edges(n, [(i, (i + 1) % n) for i in range(n)]), 2 * n) for n in (5, 12)]
+    cases += [(G.from_edges(n, [(i, j) for i in range(n) for j in range(i + 1, n)]),
+               math.factorial(n)) for n in (4, 7)]
+    cases += [(G.from_edges(9, [(0, i) for i in range(1, 9)]), math.factorial(8))]
+    cube = [(a, a ^ (1 << b)) for a in range(16) for b in range(4) if a < a ^ (1 << b)]
+    cases += [(G.from_edges(16, cube), 384)]
+    c5 = G.from_edges(5, [(i, (i + 1) % 5) for i in range(5)])
+    cases += [(G.disjoint_union(c5, k), 10 ** k * math.factorial(k)) for k in (2, 3)]
+    for _ in range(25):
+        n = int(rng.integers(2, 8))
+        g = G.erdos_renyi(n, float(rng.uniform(0.15, 0.7)), rng)
+        if rng.random() < 0.4:
+            g = G.from_edges(n, g.edges(), rng.integers(0, 2, n))
+        cases.append((g, _brute_order(g)))
+    for i, (g, want) in enumerate(cases):
+        for workers, seed in ((1, 0), (3, i + 1), (8, 2 * i + 5)):
+            _, _, naut, _, store = wm.wide_model(g, workers, seed, cap=20000, auts=True)
+            assert naut < 20000
+            assert pkg.perm_group_order(store.astype(np.uint16)) == want, (i, g.n, workers)
+
+
+def test_wide_model_group_order_schedule_independent_on_cfi(G, wm, pkg):
+    rng = np.random.default_rng(77)
+    for i in range(8):
+        g = G.cfi_graph(int(rng.integers(3, 7)) * 2, rng, twist=bool(i % 2))
+        h = G.random_relabel(g, rng)
+        orders = set()
+        for x, workers, seed in ((g, 1, 0), (g, 4, 3 + i), (h, 7, 11 + i)):
+            _, _, naut, _, store = wm.wide_model(x, workers, seed, cap=20000, auts=True)
+            assert naut < 20000
+            orders.add(pkg.perm_group_order(store.astype(np.uint16)))
+        assert len(orders) == 1, (i, orders)
