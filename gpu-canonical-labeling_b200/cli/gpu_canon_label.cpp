@@ -20,6 +20,7 @@
 #include <utility>
 #include <vector>
 
+#include "../csrc/gcl_dimacs.h"
 #include "gcl.h"
 
 namespace {
@@ -29,57 +30,30 @@ struct Graph {
   std::vector<int32_t> rowptr, col, color;
 };
 
-// CSRGraph::fromDIMACS semantics (CSRGraph.cpp:40-119): 'c' and empty lines
-// skipped, 'p' sets the vertex count, 'n v c' sets a colour (1-based, vertex 0
-// and out-of-range ignored), 'e u v' is 1-based with self loops dropped and
-// both directions stored, rows sorted.  Duplicate edges (which the reference
-// keeps and then mis-refines) and out-of-range endpoints are rejected.
+// CSRGraph::fromDIMACS semantics (CSRGraph.cpp:40-119) through the reader
+// the file pipeline uses (csrc/gcl_dimacs.h).  Duplicate edges (which the
+// reference keeps and then mis-refines), out-of-range endpoints and more than
+// GCL_MAX_N vertices are rejected with a message.
 Graph read_dimacs(const std::string& path) {
-  std::ifstream in(path);
-  if (!in.is_open()) throw std::runtime_error("Failed to open DIMACS file: " + path);
-  unsigned n = 0;
-  std::vector<std::pair<unsigned, unsigned>> edges;
-  std::vector<std::pair<unsigned, int>> colors;
-  std::string line;
-  while (std::getline(in, line)) {
-    if (line.empty() || line[0] == 'c') continue;
-    std::istringstream iss(line);
-    char type = 0;
-    iss >> type;
-    if (type == 'p') {
-      std::string tmp;
-      unsigned m = 0;
-      iss >> tmp >> n >> m;
-    } else if (type == 'n') {
-      unsigned vid = 0;
-      int c = 0;
-      iss >> vid >> c;
-      if (vid == 0) continue;
-      colors.emplace_back(vid - 1, c);
-    } else if (type == 'e') {
-      unsigned u = 0, v = 0;
-      iss >> u >> v;
-      if (u == v) continue;
-      if (u == 0 || v == 0 || u > n || v > n)
-        throw std::runtime_error("edge endpoint out of range in " + path);
-      edges.emplace_back(u - 1, v - 1);
-      edges.emplace_back(v - 1, u - 1);
-    }
-  }
-  std::sort(edges.begin(), edges.end());
-  for (size_t i = 1; i < edges.size(); ++i)
-    if (edges[i] == edges[i - 1])
+  gcl::DimacsGraph d;
+  switch (gcl::read_dimacs_file(path.c_str(), GCL_MAX_N, &d)) {
+    case gcl::kDimacsOk:
+      break;
+    case gcl::kDimacsOpenFailed:
+      throw std::runtime_error("Failed to open DIMACS file: " + path);
+    case gcl::kDimacsBadEndpoint:
+      throw std::runtime_error("edge endpoint out of range in " + path);
+    case gcl::kDimacsDuplicateEdge:
       throw std::runtime_error("duplicate edge in " + path + " (parallel edges are not supported)");
+    default:
+      throw std::runtime_error("graph too large in " + path + " (more than " +
+                               std::to_string(GCL_MAX_N) + " vertices)");
+  }
   Graph g;
-  g.n = (int)n;
-  g.rowptr.assign(n + 1, 0);
-  g.col.resize(edges.size());
-  g.color.assign(n, 0);
-  for (auto& kv : colors)
-    if (kv.first < n) g.color[kv.first] = kv.second;
-  for (auto& e : edges) g.rowptr[e.first + 1]++;
-  for (unsigned i = 0; i < n; ++i) g.rowptr[i + 1] += g.rowptr[i];
-  for (size_t i = 0; i < edges.size(); ++i) g.col[i] = (int32_t)edges[i].second;
+  g.n = d.n;
+  g.rowptr = std::move(d.rowptr);
+  g.col = std::move(d.col);
+  g.color = std::move(d.color);
   return g;
 }
 

@@ -1,95 +1,38 @@
 // gcl_files.cu -- canonize DIMACS files with parsing overlapped with the GPU
 // (host code on top of the batched entry point).
 //
-// Files are taken in chunks.  Host threads parse chunk k (CSRGraph::fromDIMACS
-// semantics, CSRGraph.cpp:40-119) while the GPU canonizes chunk k-1; when
-// chunk k-1's copies back have landed its results go to the caller's
-// callback, in file order, on the calling thread, and chunk k is packed into
-// the pinned arena of its slot and launched.  Two slots alternate.
+// Files are taken in chunks.  Host threads parse chunk k (gcl_dimacs.h:
+// CSRGraph::fromDIMACS semantics, CSRGraph.cpp:40-119) while the GPU
+// canonizes chunk k-1; when chunk k-1's copies back have landed its results
+// go to the caller's callback, in file order, on the calling thread, and
+// chunk k is packed into the pinned arena of its slot and launched.  Two
+// slots alternate.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <atomic>
 #include <cstdint>
 #include <cstring>
-#include <fstream>
-#include <sstream>
-#include <string>
 #include <thread>
 #include <utility>
 #include <vector>
 
 #include "../../include/gcl.h"
+#include "gcl_dimacs.h"
 #include "gcl_guard.h"
 
 namespace {
 
-struct FGraph {
-  int32_t status = 0;  // 0 = parsed, else GCL_GRAPH_BAD_INPUT
-  int n = 0;
-  std::vector<int32_t> rowptr, col, color;
-  bool colored = false;
+struct FGraph : gcl::DimacsGraph {
+  int32_t status = 0;  // GCL_GRAPH_OK once parsed
 };
 
-// 'c' and empty lines skipped; 'p' sets n; 'n v c' sets the colour of vertex
-// v (1-based; 0 ignored); 'e u v' adds an undirected edge (1-based, self
-// loops dropped, both directions, rows sorted).  An unreadable file, an
-// endpoint out of range or a duplicate edge makes the graph bad input.
-FGraph parse_dimacs(const char* path) {
+// One file through the shared reader; any rejection is bad input, except a
+// vertex count above GCL_MAX_N, which is too large.
+FGraph parse_file(const char* path) {
   FGraph g;
-  std::ifstream in(path);
-  if (!in.is_open()) {
-    g.status = GCL_GRAPH_BAD_INPUT;
-    return g;
-  }
-  unsigned n = 0;
-  std::vector<std::pair<unsigned, unsigned>> edges;
-  std::vector<std::pair<unsigned, int>> colors;
-  std::string line;
-  bool bad = false;
-  while (std::getline(in, line)) {
-    if (line.empty() || line[0] == 'c') continue;
-    std::istringstream iss(line);
-    char type = 0;
-    iss >> type;
-    if (type == 'p') {
-      std::string tmp;
-      unsigned m = 0;
-      iss >> tmp >> n >> m;
-    } else if (type == 'n') {
-      unsigned vid = 0;
-      int c = 0;
-      iss >> vid >> c;
-      if (vid != 0) colors.emplace_back(vid - 1, c);
-    } else if (type == 'e') {
-      unsigned u = 0, v = 0;
-      iss >> u >> v;
-      if (u == v) continue;
-      if (u == 0 || v == 0 || u > n || v > n) {
-        bad = true;
-        break;
-      }
-      edges.emplace_back(u - 1, v - 1);
-      edges.emplace_back(v - 1, u - 1);
-    }
-  }
-  if (!bad && n > (unsigned)GCL_MAX_N) bad = true;
-  std::sort(edges.begin(), edges.end());
-  for (size_t i = 1; !bad && i < edges.size(); ++i) bad = edges[i] == edges[i - 1];
-  if (bad) {
-    g.status = GCL_GRAPH_BAD_INPUT;
-    return g;
-  }
-  g.n = (int)n;
-  g.rowptr.assign(n + 1, 0);
-  g.col.resize(edges.size());
-  g.color.assign(n, 0);
-  for (auto& kv : colors)
-    if (kv.first < n) g.color[kv.first] = kv.second;
-  g.colored = std::any_of(g.color.begin(), g.color.end(), [](int c) { return c != 0; });
-  for (auto& e : edges) g.rowptr[e.first + 1]++;
-  for (unsigned i = 0; i < n; ++i) g.rowptr[i + 1] += g.rowptr[i];
-  for (size_t i = 0; i < edges.size(); ++i) g.col[i] = (int32_t)edges[i].second;
+  const int rc = gcl::read_dimacs_file(path, GCL_MAX_N, &g);
+  if (rc != gcl::kDimacsOk) g.status = rc == gcl::kDimacsTooLarge ? GCL_GRAPH_TOO_LARGE : GCL_GRAPH_BAD_INPUT;
   return g;
 }
 
@@ -168,7 +111,7 @@ int parse_chunk(Slot& sl, const char* const* paths, int64_t first, int64_t cnt, 
   auto work = [&] {
     for (int64_t i = next++; i < cnt && !failed.load(); i = next++) {
       try {
-        sl.graphs[i] = parse_dimacs(paths[first + i]);
+        sl.graphs[i] = parse_file(paths[first + i]);
       } catch (...) {
         failed.store(true);
       }

@@ -193,7 +193,8 @@ int gcl_canon_batch_noalloc(void* stream, int count, const int64_t* d_voff,
  * GPU canonizes chunk k-1 through the batched path.  For every file, in
  * order and on the calling thread, cb receives its index, a GCL_GRAPH_*
  * status (an unreadable file, an endpoint out of range or a duplicate edge
- * is GCL_GRAPH_BAD_INPUT), n, the packed canonical rows (n * ceil(n/64)
+ * is GCL_GRAPH_BAD_INPUT, more than GCL_MAX_N vertices GCL_GRAPH_TOO_LARGE),
+ * n, the packed canonical rows (n * ceil(n/64)
  * words) and the labeling -- both NULL unless the status is GCL_GRAPH_OK,
  * valid only during the call -- and the statistics.  Returns GCL_OK once
  * every file has been delivered, else the first launch or copy error. */

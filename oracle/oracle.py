@@ -188,3 +188,29 @@ def exhaustive(g, max_leaves: int = 200000) -> Optional[np.ndarray]:
     if rc < 0:
         raise RuntimeError("exhaustive search failed")
     return None if rc else out
+
+
+def ref_read_dimacs(path: str, cap_n: int = 1 << 17, cap_m: int = 1 << 24):
+    """The reference's own CSRGraph::fromDIMACS on `path` (only for files on
+    which it is well defined): (n, rowptr, col, color), or None when the file
+    cannot be opened."""
+    lib = _load("reference")
+    if not hasattr(lib.gcl_ref_read_dimacs, "_typed"):
+        lib.gcl_ref_read_dimacs.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int64,
+                                            ctypes.POINTER(ctypes.c_int),
+                                            ctypes.POINTER(ctypes.c_int64), _P, _P, _P]
+        lib.gcl_ref_read_dimacs.restype = ctypes.c_int
+        lib.gcl_ref_read_dimacs._typed = True
+    n = ctypes.c_int(0)
+    m = ctypes.c_int64(0)
+    rp = np.zeros(cap_n + 1, np.int32)
+    cl = np.zeros(max(cap_m, 1), np.int32)
+    co = np.zeros(max(cap_n, 1), np.int32)
+    rc = lib.gcl_ref_read_dimacs(path.encode(), cap_n, cap_m, ctypes.byref(n), ctypes.byref(m),
+                                 _ptr(rp), _ptr(cl), _ptr(co))
+    if rc == 1:
+        return None
+    if rc != 0:
+        raise RuntimeError("reference reader: capacity too small")
+    k = n.value
+    return k, rp[:k + 1].copy(), cl[:m.value].copy(), co[:k].copy()

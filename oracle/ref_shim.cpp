@@ -17,6 +17,7 @@
 #include <cstdint>
 #include <cstring>
 #include <iostream>
+#include <stdexcept>
 #include <streambuf>
 #include <string>
 #include <vector>
@@ -116,6 +117,36 @@ int gcl_ref_canon_batch(int count, const int64_t* voff, const int64_t* eoff,
     if (rc) return rc;
   }
   return 0;
+}
+
+// The reference's own DIMACS reader, CSRGraph::fromDIMACS
+// (CSRGraph.cpp:40-119), for checking other readers.  Only files on which it
+// is well defined may be given: every edge endpoint within 1..n of the last
+// 'p' line before it, and every 'e' line with two numbers.  Returns 0 with n,
+// the CSR and the colours copied out; 1 when the file cannot be opened; 2
+// when n > cap_n or the entries > cap_m.
+int gcl_ref_read_dimacs(const char* path, int cap_n, int64_t cap_m, int* n_out,
+                        int64_t* m_out, int32_t* rowptr, int32_t* col, int32_t* color) {
+  CSRGraph g;
+  try {
+    g = CSRGraph::fromDIMACS(path);
+  } catch (const std::runtime_error&) {
+    return 1;
+  }
+  const unsigned n = g.vertexNum;
+  const int64_t m = n ? (int64_t)g.srcPtr[n] : 0;
+  int rc = 0;
+  if ((int64_t)n > cap_n || m > cap_m) {
+    rc = 2;
+  } else {
+    *n_out = (int)n;
+    *m_out = m;
+    for (unsigned i = 0; i <= n; ++i) rowptr[i] = n ? (int32_t)g.srcPtr[i] : 0;
+    for (int64_t e = 0; e < m; ++e) col[e] = (int32_t)g.dst[e];
+    for (unsigned i = 0; i < n; ++i) color[i] = g.color[i];
+  }
+  g.cleanup();
+  return rc;
 }
 
 }  // extern "C"
