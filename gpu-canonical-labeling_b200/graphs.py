@@ -84,29 +84,108 @@ def from_edges(n: int, edges: Iterable[Tuple[int, int]] | np.ndarray,
     return Graph(n, rowptr, col, c)
 
 
+_BLANK = " \t\r\v\f\n"
+_UINT_MAX = 2**32 - 1
+_INT_MAX = 2**31 - 1
+
+
+class _LineReader:
+    """Extractions from one line with the rules of std::istringstream >> x,
+    which CSRGraph::fromDIMACS applies to every line (CSRGraph.cpp:50-79):
+    blanks skipped; at the end of the line an extraction fails and leaves its
+    target alone; a number is an optional sign and decimal digits up to the
+    first non-digit, no digits store 0 and an overflow the type's limit; a
+    failed extraction stops the rest of the line."""
+
+    def __init__(self, line: str):
+        self.s, self.i, self.failed = line, 0, False
+
+    def _sentry(self) -> bool:
+        if self.failed:
+            return False
+        while self.i < len(self.s) and self.s[self.i] in _BLANK:
+            self.i += 1
+        if self.i == len(self.s):
+            self.failed = True
+            return False
+        return True
+
+    def char(self, default: str) -> str:
+        if not self._sentry():
+            return default
+        self.i += 1
+        return self.s[self.i - 1]
+
+    def word(self) -> None:
+        if self._sentry():
+            while self.i < len(self.s) and self.s[self.i] not in _BLANK:
+                self.i += 1
+
+    def _number(self):
+        neg = False
+        if self.s[self.i] in "+-":
+            neg = self.s[self.i] == "-"
+            self.i += 1
+        j = self.i
+        while self.i < len(self.s) and "0" <= self.s[self.i] <= "9":
+            self.i += 1
+        return neg, (int(self.s[j:self.i]) if self.i > j else None)
+
+    def uint(self, default: int) -> int:
+        if not self._sentry():
+            return default
+        neg, mag = self._number()
+        if mag is None or mag > _UINT_MAX:
+            self.failed = True
+            return 0 if mag is None else _UINT_MAX
+        return (-mag) % 2**32 if neg else mag
+
+    def int(self, default: int) -> int:
+        if not self._sentry():
+            return default
+        neg, mag = self._number()
+        if mag is None:
+            self.failed = True
+            return 0
+        v = -mag if neg else mag
+        if v > _INT_MAX or v < -_INT_MAX - 1:
+            self.failed = True
+            return _INT_MAX if v > 0 else -_INT_MAX - 1
+        return v
+
+
 def parse_dimacs(text: str) -> Graph:
-    """Parse DIMACS-like text with CSRGraph::fromDIMACS semantics."""
+    """Parse DIMACS text with CSRGraph::fromDIMACS semantics (CSRGraph.cpp:40-119):
+    'c' lines and empty lines skipped, the first non-blank character is the
+    line type, 'p <word> <n> <m>' sets n, 'n <v> <colour>' colours vertex v
+    (1-based, 0 or > n ignored), 'e <u> <v>' adds an edge (1-based, self loops
+    dropped), other types ignored.  Where the reference is undefined -- an
+    endpoint of 0 or above n, a repeated edge -- ValueError is raised, as the
+    C++ reader of the library (csrc/gcl_dimacs.h) rejects the file."""
     n = 0
     edges: List[Tuple[int, int]] = []
     colors: List[Tuple[int, int]] = []
-    for line in text.splitlines():
+    for line in text.split("\n"):
         if not line or line[0] == "c":
             continue
-        tok = line.split()
-        if not tok:
-            continue
-        t = tok[0][0]
+        r = _LineReader(line)
+        t = r.char("\0")
         if t == "p":
-            n = int(tok[2])
+            r.word()
+            n = r.uint(n)
+            r.uint(0)
         elif t == "n":
-            vid, col = int(tok[1]), int(tok[2])
-            if vid == 0:
-                continue
-            colors.append((vid - 1, col))
+            vid = r.uint(0)
+            col = r.int(0)
+            if vid != 0:
+                colors.append((vid - 1, col))
         elif t == "e":
-            u, v = int(tok[1]), int(tok[2])
+            u = r.uint(0)
+            v = r.uint(0)
             if u == v:
                 continue
+            if u == 0 or v == 0 or u > n or v > n:
+                raise ValueError("edge endpoint out of range")
             edges.append((u - 1, v - 1))
     color = np.zeros(n, dtype=np.int32)
     for v, c in colors:
@@ -116,7 +195,7 @@ def parse_dimacs(text: str) -> Graph:
 
 
 def read_dimacs(path: str) -> Graph:
-    with open(path, "r") as f:
+    with open(path, "r", newline="") as f:
         return parse_dimacs(f.read())
 
 

@@ -114,7 +114,7 @@ ODD_FILES = {
 
 @pytest.mark.skipif(not __import__("oracle").available("reference"),
                     reason="reference build (oracle/_ref) not present")
-def test_reader_matches_reference_on_odd_formatting(oracle_mod, dump, tmp_path):
+def test_reader_matches_reference_on_odd_formatting(G, oracle_mod, dump, tmp_path):
     paths = []
     for name, text in ODD_FILES.items():
         p = tmp_path / f"{name}.txt"
@@ -123,9 +123,12 @@ def test_reader_matches_reference_on_odd_formatting(oracle_mod, dump, tmp_path):
     for p, (rc, got) in zip(paths, dump(paths)):
         assert rc == 0, p.name
         _same_as_reference(oracle_mod, p, got)
+        h = G.read_dimacs(str(p))  # the Python reader follows the same rules
+        assert h.n == got[0] and np.array_equal(h.rowptr, got[1]), p.name
+        assert np.array_equal(h.col, got[2]) and np.array_equal(h.colors(), got[3]), p.name
 
 
-def test_reader_rejects_what_the_reference_leaves_undefined(dump, tmp_path):
+def test_reader_rejects_what_the_reference_leaves_undefined(G, dump, tmp_path):
     cases = {
         "duplicate": ("p edge 3 2\ne 1 2\ne 2 1\n", 3),
         "duplicate_same_way": ("p edge 3 2\ne 1 2\ne 1 2\n", 3),
@@ -146,6 +149,10 @@ def test_reader_rejects_what_the_reference_leaves_undefined(dump, tmp_path):
     want = [rc for _, rc in cases.values()] + [1]
     got = [rc for rc, _ in dump(paths)]
     assert got == want
+    for (text, rc) in cases.values():  # the Python reader raises where the C++ one rejects
+        if rc in (2, 3):
+            with pytest.raises(ValueError):
+                G.parse_dimacs(text)
 
 
 def test_reader_line_rules_where_the_reference_reads_uninitialised_values(dump, tmp_path):
