@@ -135,8 +135,8 @@ def _load_wide():
         raise FileNotFoundError(f"oracle library missing: {WIDE_SO} (run make -C oracle)")
     lib = ctypes.CDLL(WIDE_SO)
     lib.gcl_wide_model.argtypes = [ctypes.c_int, _P, _P, _P, ctypes.c_int, ctypes.c_uint,
-                                   ctypes.c_int, _P, ctypes.POINTER(ctypes.c_long),
-                                   ctypes.POINTER(ctypes.c_int), _P, _P]
+                                   ctypes.c_int, ctypes.c_int, _P, ctypes.POINTER(ctypes.c_long),
+                                   ctypes.POINTER(ctypes.c_int), _P, _P, _P]
     lib.gcl_wide_model.restype = ctypes.c_int
     lib.gcl_exhaustive_canon.argtypes = [ctypes.c_int, _P, _P, _P, ctypes.c_long, _P,
                                          ctypes.POINTER(ctypes.c_long)]
@@ -152,14 +152,18 @@ def _csr(g):
     return rp, (cl if cl.size else np.zeros(1, np.int32)), co
 
 
-def wide_model(g, workers: int, seed: int = 0, cap: int = 10000, auts: bool = False):
+def wide_model(g, workers: int, seed: int = 0, cap: int = 10000, auts: bool = False,
+               gate: bool = True, rounds: Optional[list] = None):
     """CPU model of the many-worker search (wide_model.c): `workers` simulated
     workers over the first path's sibling items, stepped round-robin (seed 0)
     or in a seeded random order.  Returns (canonical matrix, nodes, automorphisms
     stored, events) where events counts [leaves equivalent to a best found
     outside their item, nodes pruned as worse than the private best, leaves
     that beat the private best but not a newer shared one]; with auts=True a
-    fifth item, the stored automorphisms (naut x n, position -> image)."""
+    fifth item, the stored automorphisms (naut x n, position -> image).
+    gate: items start level by level as on the GPU; `rounds`, when a list,
+    receives the number of scheduling rounds (every worker steps once per
+    round), the first leaf's level D and the number of items."""
     lib = _load_wide()
     rp, cl, co = _csr(g)
     out = np.zeros((g.n, g.n), dtype=np.uint8)
@@ -167,10 +171,14 @@ def wide_model(g, workers: int, seed: int = 0, cap: int = 10000, auts: bool = Fa
     naut = ctypes.c_int(0)
     ev = np.zeros(3, dtype=np.int64)
     store = np.zeros((cap, max(g.n, 1)), dtype=np.uint32) if auts else None
-    rc = lib.gcl_wide_model(g.n, _ptr(rp), _ptr(cl), _ptr(co), workers, seed, cap, _ptr(out),
-                            ctypes.byref(nodes), ctypes.byref(naut), _ptr(ev), _ptr(store))
+    nr = (ctypes.c_long * 3)()
+    rc = lib.gcl_wide_model(g.n, _ptr(rp), _ptr(cl), _ptr(co), workers, seed, cap, int(gate),
+                            _ptr(out), ctypes.byref(nodes), ctypes.byref(naut), _ptr(ev),
+                            _ptr(store), nr)
     if rc != 0:
         raise RuntimeError(f"wide model failed rc={rc}")
+    if rounds is not None:
+        rounds.extend(int(x) for x in nr)
     if auts:
         return out, int(nodes.value), int(naut.value), ev, store[:naut.value, :g.n].copy()
     return out, int(nodes.value), int(naut.value), ev

@@ -16,6 +16,11 @@
  * tests/test_wide_model.py checks that every schedule gives the sequential
  * canonical matrix, and that the sequential result is the maximum over all
  * leaves (exhaustive search) -- the property the wide search rests on.
+ * With `gate` set, an item starts only once every item of the deeper levels
+ * is done, as the GPU's level gate orders them; `rounds` counts the
+ * scheduling rounds (every worker takes one step per round), the model's
+ * measure of the search's parallel time; rounds[1] and rounds[2] receive the
+ * first leaf's level D and the number of items.
  *
  * Built with the oracle (oracle/Makefile) into libgcl_wide_model.so; only
  * tests load it.
@@ -295,8 +300,9 @@ static int wm_start_item(wm_worker* w, wm_shared* G, uint32_t k, uint32_t v) {
 }
 
 int gcl_wide_model(int n, const int32_t* rowptr, const int32_t* col, const int32_t* color,
-                   int workers, unsigned seed, int cap, uint8_t* out_nxn, long* nodes_out,
-                   int* naut_out, long* events_out, uint32_t* auts_out) {
+                   int workers, unsigned seed, int cap, int gate, uint8_t* out_nxn,
+                   long* nodes_out, int* naut_out, long* events_out, uint32_t* auts_out,
+                   long* rounds_out) {
   if (n < 1 || workers < 1 || cap < 1) return -1;
   osearch S0;
   memset(&S0, 0, sizeof S0);
@@ -383,7 +389,14 @@ int gcl_wide_model(int n, const int32_t* rowptr, const int32_t* col, const int32
     ws[i].version = -1;
   }
   unsigned long long rs = 88172645463325252ull ^ (unsigned long long)seed;
-  for (int active = 1; active;) {
+  /* the level gate: an item starts once every item of the deeper levels is
+   * done (need[it] = items before the first one of its level) */
+  int* need = malloc(((size_t)G.nitems + 1) * sizeof(int));
+  for (int it = 0; it < G.nitems; ++it)
+    need[it] = it > 0 && G.item_k[it] == G.item_k[it - 1] ? need[it - 1] : it;
+  int done = 0;
+  long rounds = 0;
+  for (int active = 1; active; ++rounds) {
     for (int ii = 0; ii < workers; ++ii) {
       rs ^= rs << 13;
       rs ^= rs >> 7;
@@ -392,14 +405,24 @@ int gcl_wide_model(int n, const int32_t* rowptr, const int32_t* col, const int32
       wm_worker* w = &ws[i];
       if (w->busy) {
         wm_step(w, &G);
-        if (w->S.P.level <= w->item_k + 1) w->busy = 0;
-      } else if (G.next_item < G.nitems) {
+        if (w->S.P.level <= w->item_k + 1) {
+          w->busy = 0;
+          ++done;
+        }
+      } else if (G.next_item < G.nitems && (!gate || done >= need[G.next_item])) {
         int it = G.next_item++;
         if (wm_start_item(w, &G, G.item_k[it], G.item_v[it])) w->busy = w->S.P.level > w->item_k + 1;
+        if (!w->busy) ++done;
       }
     }
     active = G.next_item < G.nitems;
     for (int i = 0; i < workers; ++i) active |= ws[i].busy;
+  }
+  free(need);
+  if (rounds_out) {
+    rounds_out[0] = rounds;
+    rounds_out[1] = (long)G.D;
+    rounds_out[2] = G.nitems;
   }
   if (out_nxn) memcpy(out_nxn, G.g_hash, (size_t)n * n);
   if (nodes_out) *nodes_out = G.nodes;

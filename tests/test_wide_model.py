@@ -44,17 +44,21 @@ def _cases(G):
     return out
 
 
-def test_wide_model_matches_sequential(G, wm):
+@pytest.mark.parametrize("gate", [True, False])
+def test_wide_model_matches_sequential(G, wm, gate):
+    # with the level gate (the GPU's order) and without it: the rules alone
+    # carry the result
     for g in _cases(G):
         ref = wm.canon(g)[0]
         for workers in (1, 2, 3, 8):
             for seed in (0, 1, 2, 3):
-                mat, nodes, _, _ = wm.wide_model(g, workers, seed)
+                mat, nodes, _, _ = wm.wide_model(g, workers, seed, gate=gate)
                 assert np.array_equal(mat, ref), (g.n, workers, seed)
                 assert nodes >= 1
 
 
-def test_wide_model_cfi_exercises_changed_rules(G, wm):
+@pytest.mark.parametrize("gate", [True, False])
+def test_wide_model_cfi_exercises_changed_rules(G, wm, gate):
     # CFI graphs keep deep trees with many inequivalent leaves, so workers
     # meet bests found in other items, adopt newer bests and prune under them
     rng = np.random.default_rng(11)
@@ -64,10 +68,26 @@ def test_wide_model_cfi_exercises_changed_rules(G, wm):
         ref = wm.canon(g)[0]
         for workers in (2, 3, 5, 8):
             for seed in range(5):
-                mat, _, _, ev = wm.wide_model(g, workers, seed)
+                mat, _, _, ev = wm.wide_model(g, workers, seed, gate=gate)
                 assert np.array_equal(mat, ref), (i, g.n, workers, seed)
                 events += ev
     assert (events > 0).all(), events
+
+
+def test_wide_model_gate_serialises_trees(G, wm):
+    # On trees each level holds about one item, so the level gate runs the
+    # items one after another (rounds ~ nodes); without it the items run
+    # together and the rounds fall to about the first path's depth.
+    rng = np.random.default_rng(2)
+    g = G.from_edges(300, G.recursive_tree(300, rng))
+    ref = wm.canon(g)
+    r_gate, r_free = [], []
+    m1, nodes_gate, _, _ = wm.wide_model(g, 64, 0, gate=True, rounds=r_gate)
+    m2, nodes_free, _, _ = wm.wide_model(g, 64, 0, gate=False, rounds=r_free)
+    assert np.array_equal(m1, ref[0]) and np.array_equal(m2, ref[0])
+    depth = r_gate[1]
+    assert r_gate[0] > 0.5 * nodes_gate
+    assert r_free[0] <= depth + 2 and nodes_free <= 1.5 * ref[3]
 
 
 def test_wide_model_relabel_invariant(G, wm):
