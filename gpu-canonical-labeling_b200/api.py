@@ -48,6 +48,7 @@ GCL_OPT_WORKSPACE_BYTES = 2
 GCL_OPT_WIDE_MAX_WARPS = 3
 GCL_OPT_SMEM_STAGE = 4
 GCL_OPT_STREAM_PRIORITY = 5
+GCL_OPT_WIDE_GATE = 6
 GCL_MAX_N = 65536
 
 
@@ -175,6 +176,10 @@ class Context:
         (GCL_OPT_WIDE_MIN_N); GCL_MAX_N + 1 keeps the sequential traversal."""
         _check(self.lib.gcl_set_option(self.handle, GCL_OPT_WIDE_MIN_N, int(n)),
                "gcl_set_option")
+
+    def set_option(self, option: int, value: int):
+        """gcl_set_option: one of the GCL_OPT_* constants."""
+        _check(self.lib.gcl_set_option(self.handle, int(option), int(value)), "gcl_set_option")
 
     def close(self):
         if getattr(self, "handle", None):

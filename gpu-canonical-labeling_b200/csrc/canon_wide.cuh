@@ -117,6 +117,7 @@ struct WideArgs {
   SpLayout Lo;
   uint64_t slot_bytes;
   uint32_t pool;
+  uint32_t gate;  // 1: a level's items wait for the deeper levels (shared orbit cache)
   uint64_t smem_per_warp;
   uint64_t budget_ns;
   uint8_t* out_dense;    // n*n, or null
@@ -389,6 +390,33 @@ __device__ __noinline__ uint32_t wide_orbit_min(const WidePtrs& P, uint32_t v, u
   }
   r = __shfl_sync(GCL_FULL, r, 0);
   wide_unlock(&H->orb_lock);
+  return r;
+}
+
+// wide_orbit_min for items that do not wait for the deeper levels: items of
+// several levels run at once, so the warp unites in its own union-find
+// (W.dsu, free between items) instead of the shared one, and stops as soon
+// as v has a smaller root.
+__device__ __noinline__ uint32_t wide_orbit_min_own(const WidePtrs& P, uint32_t v, uint32_t k,
+                                                    uint32_t tf, uint32_t tl, uint32_t known,
+                                                    uint32_t stride, bool* ok) {
+  SpWarp& W = sp_w();
+  const uint32_t lane = lane_id();
+  const uint32_t n = W.n;
+  const uint32_t* mem = P.lelem + tf;
+  for (uint32_t i = lane; i < tl; i += 32) W.dsu[mem[i]] = mem[i];
+  __syncwarp();
+  uint32_t r = v;
+  for (uint32_t a = 0; a < known && r == v; ++a) {
+    if (__ldcg(P.fixlev + a) < k) continue;
+    if (!sp_dsu_apply<true>(P.auts + (uint64_t)a * stride, mem, tl, n)) {
+      *ok = false;
+      break;
+    }
+    uint32_t x = v;
+    if (lane == 0) x = sp_find(W.dsu, v, n);
+    r = __shfl_sync(GCL_FULL, x, 0);
+  }
   return r;
 }
 
@@ -677,7 +705,7 @@ __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
     const uint32_t k = D - 2 - lo;  // parent node level k+1, its target cell index k
     const uint32_t tf = P.tcfirst[k], tl = P.tclen[k];
     const uint32_t v = P.lelem[tf + 1 + (it - P.cum[lo])];
-    {
+    if (A.gate) {
       const int32_t gs = wide_gate(H, P.cum[lo], deadline);
       if (gs != kOk) {
         status = gs;
@@ -688,7 +716,8 @@ __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
     bool skip = false;
     if (known) {
       bool ok = true;
-      const uint32_t r = wide_orbit_min(P, v, lo, k, tf, tl, known, A.WL.stride, &ok);
+      const uint32_t r = A.gate ? wide_orbit_min(P, v, lo, k, tf, tl, known, A.WL.stride, &ok)
+                                : wide_orbit_min_own(P, v, k, tf, tl, known, A.WL.stride, &ok);
       if (!ok) {
         status = kTimeout;
         break;

@@ -233,6 +233,7 @@ struct gcl_context {
   uint64_t workspace_bytes = 0;  // per-pass workspace cap, 0 = GCL_WORKSPACE_GB
   int64_t wide_max_warps = 0;    // 0 = as many as fit
   bool smem_stage = true;        // sparse and wide kernels stage per-step arrays in shared memory
+  bool wide_gate = true;         // wide search: a level's items wait for the deeper levels
   // launch shape per size bucket (gcl_autotune / gcl_set_tuning): 0 / -1 = default
   int w64_per_sm = 0;            // resident blocks the warp kernel's occupancy allows
   int tune_w64_bps = 0;
@@ -552,6 +553,10 @@ int gcl_set_option(gcl_context* c, int option, int64_t value) {
       if (value != 0 && value != 1) return GCL_ERR_ARG;
       c->smem_stage = value != 0;
       return GCL_OK;
+    case GCL_OPT_WIDE_GATE:
+      if (value != 0 && value != 1) return GCL_ERR_ARG;
+      c->wide_gate = value != 0;
+      return GCL_OK;
     case GCL_OPT_STREAM_PRIORITY: {
       if (value != 0 && value != 1) return GCL_ERR_ARG;
       int lo = 0, hi = 0;
@@ -612,6 +617,7 @@ int gcl_canon_wide_device_async(gcl_context* c, const int32_t* d_rowptr, const i
   WA.Lo = Lo;
   WA.slot_bytes = Lo.bytes;
   WA.pool = kWidePool;
+  WA.gate = c->wide_gate ? 1u : 0u;
   WA.smem_per_warp = smw;
   WA.budget_ns = graph_budget_ns();
   WA.out_dense = d_out_dense;

@@ -90,12 +90,22 @@ void* gcl_stream(gcl_context* ctx);
  *   highest priority (the block scheduler then starts its blocks before those
  *   of lower-priority streams), 0 by one of the lowest.  Waits for the
  *   context's work first; the stream gcl_stream returned before is gone.
+ * GCL_OPT_WIDE_GATE: 1 (default) starts the wide search's items (the first
+ *   path's siblings) level by level, deepest first, each level once the
+ *   deeper ones are done, so their automorphisms prune it as in the
+ *   sequential order; 0 starts every item at once, each testing its vertex
+ *   against the automorphisms known at that moment.  Same canonical form
+ *   either way.  0 suits searches whose levels hold few items each (trees:
+ *   the gate runs their items one after another); it costs more nodes where
+ *   levels are wide, and an orbit test per item over the whole store.  Not
+ *   yet measured on a GPU.
  * Returns GCL_ERR_ARG for an unknown option or value. */
 #define GCL_OPT_WIDE_MIN_N 1
 #define GCL_OPT_WORKSPACE_BYTES 2
 #define GCL_OPT_WIDE_MAX_WARPS 3
 #define GCL_OPT_SMEM_STAGE 4
 #define GCL_OPT_STREAM_PRIORITY 5
+#define GCL_OPT_WIDE_GATE 6
 int gcl_set_option(gcl_context* ctx, int option, int64_t value);
 
 /* ---- one graph (drop-in for Nauty_Parallel, src/nauty_parallel.h:9-13) ---
