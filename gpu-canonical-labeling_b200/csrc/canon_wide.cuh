@@ -404,7 +404,7 @@ __device__ __noinline__ uint32_t wide_orbit_min_own(const WidePtrs& P, uint32_t 
   const uint32_t lane = lane_id();
   const uint32_t n = W.n;
   const uint32_t* mem = P.lelem + tf;
-  for (uint32_t i = lane; i < tl; i += 32) W.dsu[mem[i]] = mem[i];
+  for (uint32_t x = lane; x < n; x += 32) W.dsu[x] = x;
   __syncwarp();
   uint32_t r = v;
   for (uint32_t a = 0; a < known && r == v; ++a) {
