@@ -24,15 +24,29 @@ namespace {
 
 using Perm = std::vector<uint32_t>;
 
+// Coset representatives are kept as explicit permutations (u and u^-1, u16
+// images) while the chain holds at most this many entries (128 MiB); beyond
+// it a level falls back to walking its Schreier vector.
+constexpr uint64_t kTransversalEntries = 1ull << 26;
+
+struct Level {
+  uint32_t base = 0;
+  std::vector<int> S;              // strong generators fixing the base points before this one
+  std::vector<int32_t> sv;         // per point: generator that reached it, -1 base, -2 outside
+  std::vector<int32_t> slot;       // per point: its index in orbit, -1 outside
+  std::vector<uint32_t> orbit;     // the basic orbit in the order its points were reached
+  std::vector<uint32_t> applied;   // per orbit point: generators of S applied to it so far
+  std::vector<uint32_t> tested;    // per orbit point: generators whose Schreier generator sifted
+  std::vector<uint16_t> u, uinv;   // explicit representatives, orbit-major, n images each
+  bool explicit_u = false;
+};
+
 struct Chain {
   uint32_t n = 0;
-  std::vector<Perm> gens, inv;           // strong generators and their inverses
-  std::vector<uint32_t> base;
-  std::vector<std::vector<int>> S;       // S[i]: generators fixing base[0..i-1]
-  std::vector<std::vector<int32_t>> sv;  // Schreier vectors: generator reaching the point,
-                                         // -1 at the base point, -2 outside the orbit
-  std::vector<std::vector<uint32_t>> orbit;
-  uint64_t work = 0, work_cap = 0;       // multiplication budget (0 = none)
+  std::vector<Perm> gens, inv;  // strong generators and their inverses
+  std::vector<Level> lv;
+  uint64_t work = 0, work_cap = 0;  // multiplication budget (0 = none)
+  uint64_t entries = 0;             // explicit representative entries held
 
   bool is_id(const Perm& p) const {
     for (uint32_t x = 0; x < n; ++x)
@@ -48,113 +62,174 @@ struct Chain {
     return (int)gens.size() - 1;
   }
 
-  // orbit of base[i] under S[i], with its Schreier vector
-  void build_orbit(size_t i) {
-    std::vector<int32_t>& v = sv[i];
-    v.assign(n, -2);
-    std::vector<uint32_t>& o = orbit[i];
-    o.clear();
-    v[base[i]] = -1;
-    o.push_back(base[i]);
-    for (size_t k = 0; k < o.size(); ++k) {
-      const uint32_t x = o[k];
-      for (int g : S[i]) {
-        const uint32_t y = gens[g][x];
-        if (v[y] == -2) {
-          v[y] = g;
-          o.push_back(y);
-        }
-      }
-    }
-    work += (uint64_t)o.size() * S[i].size();
+  void drop_explicit(Level& L) {
+    entries -= L.u.size() + L.uinv.size();
+    std::vector<uint16_t>().swap(L.u);
+    std::vector<uint16_t>().swap(L.uinv);
+    L.explicit_u = false;
   }
 
-  // h <- u_x^{-1} h, where u_x maps base[i] to x (walks the Schreier vector)
-  void strip_rep(size_t i, uint32_t x, Perm& h) {
-    while (sv[i][x] >= 0) {
-      const Perm& gi = inv[sv[i][x]];
+  // y = g(x) joins the orbit; its representative is g u_x
+  void add_point(Level& L, size_t k, int g, uint32_t y) {
+    L.sv[y] = g;
+    L.slot[y] = (int32_t)L.orbit.size();
+    L.orbit.push_back(y);
+    L.applied.push_back(0);
+    L.tested.push_back(0);
+    if (!L.explicit_u) return;
+    if (entries + 2ull * n > kTransversalEntries) {
+      drop_explicit(L);
+      return;
+    }
+    const Perm& gp = gens[g];
+    const Perm& gi = inv[g];
+    const size_t base_off = k * n, off = L.u.size();
+    L.u.resize(off + n);
+    L.uinv.resize(off + n);
+    for (uint32_t z = 0; z < n; ++z) {
+      L.u[off + z] = (uint16_t)gp[L.u[base_off + z]];
+      L.uinv[off + z] = L.uinv[base_off + gi[z]];
+    }
+    entries += 2ull * n;
+    work += 2ull * n;
+  }
+
+  void new_level(uint32_t b) {
+    lv.emplace_back();
+    Level& L = lv.back();
+    L.base = b;
+    L.sv.assign(n, -2);
+    L.slot.assign(n, -1);
+    L.sv[b] = -1;
+    L.slot[b] = 0;
+    L.orbit.push_back(b);
+    L.applied.push_back(0);
+    L.tested.push_back(0);
+    if (entries + 2ull * n <= kTransversalEntries) {
+      L.explicit_u = true;
+      L.u.resize(n);
+      L.uinv.resize(n);
+      for (uint32_t z = 0; z < n; ++z) L.u[z] = L.uinv[z] = (uint16_t)z;
+      entries += 2ull * n;
+    }
+  }
+
+  // grow the basic orbit of level i under the generators added since the
+  // last call (the points already reached keep their representatives)
+  void extend(size_t i) {
+    Level& L = lv[i];
+    for (size_t k = 0; k < L.orbit.size(); ++k) {
+      const uint32_t x = L.orbit[k];
+      for (size_t gi = L.applied[k]; gi < L.S.size(); ++gi) {
+        const int g = L.S[gi];
+        const uint32_t y = gens[g][x];
+        if (L.sv[y] == -2) add_point(L, k, g, y);
+      }
+      work += L.S.size() - L.applied[k];
+      L.applied[k] = (uint32_t)L.S.size();
+    }
+  }
+
+  // h <- u_x^{-1} h, where u_x maps the level's base point to x
+  void strip(const Level& L, uint32_t x, Perm& h) {
+    if (L.explicit_u) {
+      const uint16_t* ui = L.uinv.data() + (size_t)L.slot[x] * n;
+      for (uint32_t p = 0; p < n; ++p) h[p] = ui[h[p]];
+      work += n;
+      return;
+    }
+    while (L.sv[x] >= 0) {
+      const Perm& gi = inv[L.sv[x]];
       for (uint32_t p = 0; p < n; ++p) h[p] = gi[h[p]];
       x = gi[x];
       work += n;
     }
   }
 
-  // sift h from level `from`; returns the level where it left the chain
-  // (base.size() if it passed every level) and leaves the residue in h
-  size_t sift(Perm& h, size_t from) {
-    for (size_t i = from; i < base.size(); ++i) {
-      const uint32_t x = h[base[i]];
-      if (sv[i][x] == -2) return i;
-      strip_rep(i, x, h);
+  // t <- u_p as a permutation
+  void rep(const Level& L, uint32_t p, Perm& t) {
+    if (L.explicit_u) {
+      const uint16_t* up = L.u.data() + (size_t)L.slot[p] * n;
+      for (uint32_t z = 0; z < n; ++z) t[z] = up[z];
+      work += n;
+      return;
     }
-    return base.size();
+    for (uint32_t z = 0; z < n; ++z) t[z] = z;
+    std::vector<int> path;
+    while (L.sv[p] >= 0) {
+      path.push_back(L.sv[p]);
+      p = inv[L.sv[p]][p];
+    }
+    for (size_t q = path.size(); q-- > 0;) {
+      const Perm& g = gens[path[q]];
+      for (uint32_t z = 0; z < n; ++z) t[z] = g[t[z]];
+      work += n;
+    }
   }
 
-  void new_level(uint32_t b) {
-    base.push_back(b);
-    S.emplace_back();
-    sv.emplace_back();
-    orbit.emplace_back();
+  // sift h from level `from`; returns the level where it left the chain
+  // (lv.size() if it passed every level) and leaves the residue in h
+  size_t sift(Perm& h, size_t from) {
+    for (size_t i = from; i < lv.size(); ++i) {
+      const uint32_t x = h[lv[i].base];
+      if (lv[i].sv[x] == -2) return i;
+      strip(lv[i], x, h);
+    }
+    return lv.size();
   }
 
   // a residue that left the chain at level j joins S[from..j] (it fixes the
-  // base points before j); a residue that passed every level moves a new
-  // base point
-  size_t insert(const Perm& h, size_t from, size_t j) {
-    if (j == base.size()) {
+  // base points before j); one that passed every level moves a new base point
+  void insert(const Perm& h, size_t from, size_t j) {
+    if (j == lv.size()) {
       uint32_t b = 0;
       while (b < n && h[b] == b) ++b;
       new_level(b);
     }
     const int id = add_gen(h);
-    for (size_t l = from; l <= j; ++l) S[l].push_back(id);
-    return j;
+    for (size_t l = from; l <= j; ++l) lv[l].S.push_back(id);
   }
 
-  // complete the chain: every Schreier generator of every level sifts to the
-  // identity (Schreier-Sims, deterministic form)
-  bool complete() {
-    if (base.empty()) return true;
-    size_t i = base.size() - 1;
-    for (size_t l = 0; l < base.size(); ++l) build_orbit(l);
+  // Deterministic Schreier-Sims from level i up to level 0: at every level
+  // each Schreier generator u_{s(p)}^-1 s u_p (p in the basic orbit, s in S)
+  // sifts through the deeper levels to the identity, else its residue
+  // becomes a strong generator and the deeper levels it joined are completed
+  // first.  Orbits only grow and keep their representatives, so each
+  // (point, generator) pair is tested once; pairs that are edges of the
+  // orbit's search tree give the identity and are skipped.
+  bool complete(size_t i) {
+    Perm t(n), h(n);
     while (true) {
-      bool changed = false;
-      build_orbit(i);
-      Perm h(n), t(n);
-      for (size_t k = 0; k < orbit[i].size() && !changed; ++k) {
-        const uint32_t p = orbit[i][k];
-        for (size_t si = 0; si < S[i].size() && !changed; ++si) {
-          const Perm& s = gens[S[i][si]];
-          // h = u_{s(p)}^{-1} s u_p
-          for (uint32_t x = 0; x < n; ++x) h[x] = x;
-          // u_p: base[i] -> p, built as a product along the Schreier vector
-          {
-            uint32_t y = p;
-            std::vector<int> path;
-            while (sv[i][y] >= 0) {
-              path.push_back(sv[i][y]);
-              y = inv[sv[i][y]][y];
-            }
-            for (size_t q = path.size(); q-- > 0;) {
-              const Perm& g = gens[path[q]];
-              for (uint32_t x = 0; x < n; ++x) h[x] = g[h[x]];
-              work += n;
-            }
-          }
-          for (uint32_t x = 0; x < n; ++x) t[x] = s[h[x]];
-          strip_rep(i, s[p], t);
+      extend(i);
+      size_t next = i;
+      bool inserted = false;
+      for (size_t k = 0; k < lv[i].orbit.size() && !inserted; ++k) {
+        const uint32_t p = lv[i].orbit[k];
+        for (size_t gi = lv[i].tested[k]; gi < lv[i].S.size(); ++gi) {
+          const int sid = lv[i].S[gi];
+          const Perm& s = gens[sid];
+          const uint32_t y = s[p];
+          lv[i].tested[k] = (uint32_t)gi + 1;
+          if (lv[i].sv[y] == sid) continue;  // a tree edge: u_y = s u_p
+          rep(lv[i], p, h);
+          for (uint32_t z = 0; z < n; ++z) t[z] = s[h[z]];
           work += n;
+          strip(lv[i], y, t);
           const size_t j = sift(t, i + 1);
-          if (j < base.size() || !is_id(t)) {
+          if (j < lv.size() || !is_id(t)) {
             insert(t, i + 1, j);
-            for (size_t l = i + 1; l < base.size(); ++l) build_orbit(l);
-            i = base.size() - 1;
-            changed = true;
+            next = j;
+            inserted = true;
+            break;
           }
           if (work_cap && work > work_cap) return false;
         }
       }
-      if (changed) continue;
+      if (work_cap && work > work_cap) return false;
+      if (inserted) {
+        i = next;
+        continue;
+      }
       if (i == 0) return true;
       --i;
     }
@@ -197,26 +272,22 @@ bool group_order(uint32_t n, const uint16_t* auts, uint64_t count, uint64_t stri
   for (uint64_t a = 0; a < count; ++a) {
     for (uint32_t x = 0; x < n; ++x) p[x] = auts[a * stride + x];
     if (C.is_id(p)) continue;
-    // skip generators the chain already contains
-    if (!C.base.empty()) {
-      Perm h = p;
-      const size_t j = C.sift(h, 0);
-      if (j == C.base.size() && C.is_id(h)) continue;
-      C.insert(h, 0, j);
-    } else {
-      C.insert(p, 0, 0);
-    }
-    if (!C.complete()) return false;
+    // a generator the chain already contains sifts to the identity
+    const size_t j = C.sift(p, 0);
+    if (j == C.lv.size() && C.is_id(p)) continue;
+    C.insert(p, 0, j);
+    if (!C.complete(j)) return false;
   }
   std::vector<uint64_t> f;
   double lg = 0;
-  for (size_t i = 0; i < C.base.size(); ++i) {
-    f.push_back(C.orbit[i].size());
-    lg += std::log10((double)C.orbit[i].size());
+  for (size_t i = 0; i < C.lv.size(); ++i) {
+    C.extend(i);
+    f.push_back(C.lv[i].orbit.size());
+    lg += std::log10((double)C.lv[i].orbit.size());
   }
   *log10_order = lg;
   *digits = big_product(f);
-  *base_len = C.base.size();
+  *base_len = C.lv.size();
   return true;
 }
 
