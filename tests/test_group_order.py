@@ -114,3 +114,32 @@ def test_group_order_brute_force_small(pkg, G):
         assert pkg.group_order(g, ctx=ctx) == _brute_aut(g)
     for g in G.small_batch(30, seed=5):  # trees: relabeling leaves the order alone
         assert pkg.group_order(g, ctx=ctx) == pkg.group_order(G.random_relabel(g, rng), ctx=ctx)
+
+
+def test_perm_group_order_large_orbits_and_many_generators(pkg):
+    # cases the completion must finish quickly: a vertex-transitive group of
+    # 4096 points (torus 64x64: translations, a rotation, a reflection) and
+    # 30 disjoint 5-cycles with their dihedral symmetries and the swaps of
+    # components as separate generators
+    import time
+    k = 64
+    n = k * k
+    idx = np.arange(n)
+    x, y = idx // k, idx % k
+    gens = [((x + 1) % k) * k + y, x * k + (y + 1) % k, y * k + (-x) % k, x * k + (-y) % k]
+    t = time.time()
+    assert pkg.perm_group_order(np.array(gens)) == 8 * n
+    gens = []
+    c = 30
+    for comp in range(c):
+        for g in ([1, 2, 3, 4, 0], [0, 4, 3, 2, 1]):
+            p = np.arange(5 * c)
+            p[5 * comp:5 * comp + 5] = 5 * comp + np.array(g)
+            gens.append(p)
+    for comp in range(c - 1):
+        p = np.arange(5 * c)
+        p[5 * comp:5 * comp + 5], p[5 * comp + 5:5 * comp + 10] = (np.arange(5 * comp + 5, 5 * comp + 10),
+                                                                    np.arange(5 * comp, 5 * comp + 5))
+        gens.append(p)
+    assert pkg.perm_group_order(np.array(gens)) == 10 ** c * math.factorial(c)
+    assert time.time() - t < 20
