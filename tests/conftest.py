@@ -21,6 +21,8 @@ os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200)")
+    config.addinivalue_line("markers", "gpu_staged: needs a B200; not yet run on one "
+                                       "(pytest -m gpu_staged)")
 
 
 @pytest.fixture(scope="session")

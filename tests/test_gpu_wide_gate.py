@@ -1,0 +1,62 @@
+"""The wide search with its level gate off (GCL_OPT_WIDE_GATE = 0) vs the
+oracle.
+
+Staged: marked gpu_staged, not gpu, until it has passed on a B200; run it
+with `pytest -m gpu_staged`.  Without the gate every first-path sibling
+starts at once and tests its vertex in its warp's own union-find; the CPU
+model of the search (tests/test_wide_model.py) shows the same canonical form
+under every schedule with or without the gate."""
+import time
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+pytestmark = [pytest.mark.gpu_staged,
+              pytest.mark.skipif(not torch.cuda.is_available(), reason="needs a CUDA GPU")]
+
+
+@pytest.fixture(scope="module")
+def free_ctx(pkg):
+    c = pkg.Context(0, wide_min_n=1)
+    c.set_option(pkg.api.GCL_OPT_WIDE_GATE, 0)
+    return c
+
+
+def test_gate_off_small_and_symmetric_vs_oracle(pkg, G, oracle_mod, free_ctx):
+    rng = np.random.default_rng(2024)
+    graphs = [G.torus(k) for k in (3, 4, 5, 6, 8, 10)]
+    graphs += [G.disjoint_union(G.random_regular(10, 3, rng), k) for k in (2, 3, 4)]
+    graphs += G.small_batch(120, seed=99)
+    graphs += [G.tree_plus_edges(int(rng.integers(10, 64)), rng) for _ in range(40)]
+    graphs += [G.cfi_graph(b, rng, twist=bool(b % 4)) for b in (4, 6, 8, 10, 12)]
+    for g in graphs:
+        mat = oracle_mod.canon(g)[0]
+        for _ in range(2):
+            assert np.array_equal(pkg.canon(g, ctx=free_ctx).matrix, mat)
+
+
+def test_gate_off_trees_vs_oracle_and_timing(pkg, G, oracle_mod, free_ctx):
+    rng = np.random.default_rng(7)
+    gated = pkg.Context(0, wide_min_n=1)
+    for n in (300, 1000, 2048):
+        g = G.from_edges(n, G.recursive_tree(n, rng))
+        mat = oracle_mod.canon(g)[0]
+        t = time.perf_counter()
+        a = pkg.canon(g, ctx=free_ctx).matrix
+        t_free = time.perf_counter() - t
+        t = time.perf_counter()
+        b = pkg.canon(g, ctx=gated).matrix
+        t_gate = time.perf_counter() - t
+        assert np.array_equal(a, mat) and np.array_equal(b, mat)
+        print(f"tree n={n}: gate off {t_free * 1e3:.1f} ms, gate on {t_gate * 1e3:.1f} ms")
+
+
+@pytest.mark.parametrize("max_aut", [1, 3])
+def test_gate_off_small_store(pkg, G, oracle_mod, free_ctx, max_aut):
+    rng = np.random.default_rng(5)
+    for g in (G.torus(8), G.disjoint_union(G.random_regular(10, 3, rng), 4),
+              G.tree_plus_edges(400, rng)):
+        mat = oracle_mod.canon(g, max_aut=max_aut)[0]
+        assert np.array_equal(pkg.canon(g, max_aut=max_aut, ctx=free_ctx).matrix, mat)
