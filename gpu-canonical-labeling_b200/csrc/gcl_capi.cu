@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstddef>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
@@ -87,6 +88,7 @@ constexpr uint64_t kWideStoreBytes = 1ull << 30;  // automorphism store of a wid
 constexpr uint64_t kWideStoreEntries = 1ull << 22;  // ... and at most this many entries
 constexpr uint32_t kWideFixCap = 4096;  // entries whose fix state a wide-search warp keeps
 constexpr uint64_t kGroupWorkCap = 40000000000ull;  // Schreier-Sims operations (~20 s)
+constexpr uint64_t kGroupWorkCapGeneral = 4000000000ull;  // before a graph's base is used
 
 // entries of a wide search's automorphism store: max_aut, within kWideStoreBytes
 static uint32_t wide_store_cap(uint32_t n, int max_aut) {
@@ -917,8 +919,27 @@ int gcl_group_order(gcl_context* c, const int32_t* rowptr, const int32_t* col,
   double lg = 0;
   std::string d;
   uint64_t base_len = 0;
-  if (!group_order(un, auts.data(), (uint64_t)st[0], WL.stride, kGroupWorkCap, &lg, &d, &base_len))
-    return GCL_ERR_TIMEOUT;
+  if (!group_order(un, auts.data(), (uint64_t)st[0], WL.stride, kGroupWorkCapGeneral, &lg, &d,
+                   &base_len)) {
+    // large orbits: the first path's individualized vertices are a base of
+    // Aut(G) (an automorphism fixing them fixes the first leaf's discrete
+    // partition), so Schreier generators sift on their base images alone
+    const uint8_t* sh = (const uint8_t*)c->wide_sh.p;
+    uint32_t D = 0;
+    GCL_TRY(cudaMemcpyAsync(&D, sh + WL.hdr + offsetof(WideHdr, D), sizeof(uint32_t),
+                            cudaMemcpyDeviceToHost, s));
+    GCL_TRY(cudaStreamSynchronize(s));
+    if (D < 1 || D > un) return GCL_ERR_INTERNAL;
+    std::vector<uint32_t> base(D);
+    if (D > 1)
+      GCL_TRY(cudaMemcpyAsync(base.data(), sh + WL.fseq, (size_t)(D - 1) * sizeof(uint32_t),
+                              cudaMemcpyDeviceToHost, s));
+    GCL_TRY(cudaStreamSynchronize(s));
+    const int rg = group_order_with_base(un, auts.data(), (uint64_t)st[0], WL.stride, base.data(),
+                                         D - 1, kGroupWorkCap, &lg, &d, &base_len);
+    if (rg == kOrderWorkCap) return GCL_ERR_TIMEOUT;
+    if (rg != kOrderOk) return GCL_ERR_INTERNAL;
+  }
   return put(d, lg, st[0]);
 } GCL_CATCH_ALL
 

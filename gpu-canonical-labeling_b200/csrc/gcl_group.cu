@@ -47,6 +47,12 @@ struct Chain {
   std::vector<Level> lv;
   uint64_t work = 0, work_cap = 0;  // multiplication budget (0 = none)
   uint64_t entries = 0;             // explicit representative entries held
+  // the levels' base points are a base of the group (only the identity fixes
+  // them all): Schreier generators are sifted on their base images alone
+  bool known_base = false;
+  bool not_a_base = false;  // an element other than the identity fixed every base point
+  std::vector<int> path;    // scratch: a representative's generator word
+  std::vector<uint32_t> bi; // scratch: base images
 
   bool is_id(const Perm& p) const {
     for (uint32_t x = 0; x < n; ++x)
@@ -167,6 +173,62 @@ struct Chain {
     }
   }
 
+  // the generators along the Schreier vector from x back to the base point
+  // (last applied first): u_x = path[0] path[1] ... path[k-1]
+  void word(const Level& L, uint32_t x) {
+    path.clear();
+    while (L.sv[x] >= 0) {
+      path.push_back(L.sv[x]);
+      x = inv[L.sv[x]][x];
+    }
+  }
+
+  // bi[m] <- u_p(bi[m]) for m in [lo, hi)
+  void apply_rep(const Level& L, uint32_t p, size_t lo, size_t hi) {
+    if (L.explicit_u) {
+      const uint16_t* up = L.u.data() + (size_t)L.slot[p] * n;
+      for (size_t m = lo; m < hi; ++m) bi[m] = up[bi[m]];
+      work += hi - lo;
+      return;
+    }
+    word(L, p);
+    for (size_t m = lo; m < hi; ++m) {
+      uint32_t z = bi[m];
+      for (size_t q = path.size(); q-- > 0;) z = gens[path[q]][z];
+      bi[m] = z;
+    }
+    work += (hi - lo) * path.size();
+  }
+
+  // bi[m] <- u_x^{-1}(bi[m]) for m in [lo, hi)
+  void apply_rep_inv(const Level& L, uint32_t x, size_t lo, size_t hi) {
+    if (L.explicit_u) {
+      const uint16_t* ui = L.uinv.data() + (size_t)L.slot[x] * n;
+      for (size_t m = lo; m < hi; ++m) bi[m] = ui[bi[m]];
+      work += hi - lo;
+      return;
+    }
+    word(L, x);
+    for (size_t m = lo; m < hi; ++m) {
+      uint32_t z = bi[m];
+      for (size_t q = 0; q < path.size(); ++q) z = inv[path[q]][z];
+      bi[m] = z;
+    }
+    work += (hi - lo) * path.size();
+  }
+
+  // sift the element whose base images are bi[from..] from level `from`;
+  // returns the level where it left the chain, lv.size() if it fixes every
+  // base point after the strips (with a known base: the identity)
+  size_t sift_images(size_t from) {
+    for (size_t i = from; i < lv.size(); ++i) {
+      const uint32_t x = bi[i];
+      if (lv[i].sv[x] == -2) return i;
+      apply_rep_inv(lv[i], x, i, lv.size());
+    }
+    return lv.size();
+  }
+
   // sift h from level `from`; returns the level where it left the chain
   // (lv.size() if it passed every level) and leaves the residue in h
   size_t sift(Perm& h, size_t from) {
@@ -211,11 +273,29 @@ struct Chain {
           const uint32_t y = s[p];
           lv[i].tested[k] = (uint32_t)gi + 1;
           if (lv[i].sv[y] == sid) continue;  // a tree edge: u_y = s u_p
+          if (known_base) {
+            // t = u_y^-1 s u_p fixes the base points up to i; its images of
+            // the deeper ones decide whether it is the identity
+            const size_t L = lv.size();
+            for (size_t m = i + 1; m < L; ++m) bi[m] = lv[m].base;
+            apply_rep(lv[i], p, i + 1, L);
+            for (size_t m = i + 1; m < L; ++m) bi[m] = s[bi[m]];
+            apply_rep_inv(lv[i], y, i + 1, L);
+            if (sift_images(i + 1) == L) {
+              if (work_cap && work > work_cap) return false;
+              continue;
+            }
+          }
           rep(lv[i], p, h);
           for (uint32_t z = 0; z < n; ++z) t[z] = s[h[z]];
           work += n;
           strip(lv[i], y, t);
           const size_t j = sift(t, i + 1);
+          if (known_base && j == lv.size()) {
+            // the base images said otherwise, or the points are no base
+            not_a_base = true;
+            return false;
+          }
           if (j < lv.size() || !is_id(t)) {
             insert(t, i + 1, j);
             next = j;
@@ -262,21 +342,23 @@ std::string big_product(const std::vector<uint64_t>& f) {
 
 }  // namespace
 
-bool group_order(uint32_t n, const uint16_t* auts, uint64_t count, uint64_t stride,
-                 uint64_t work_cap, double* log10_order, std::string* digits,
-                 uint64_t* base_len) {
-  Chain C;
-  C.n = n;
-  C.work_cap = work_cap;
+namespace {
+
+int run(Chain& C, const uint16_t* auts, uint64_t count, uint64_t stride, double* log10_order,
+        std::string* digits, uint64_t* base_len) {
+  const uint32_t n = C.n;
   Perm p(n);
   for (uint64_t a = 0; a < count; ++a) {
     for (uint32_t x = 0; x < n; ++x) p[x] = auts[a * stride + x];
     if (C.is_id(p)) continue;
     // a generator the chain already contains sifts to the identity
     const size_t j = C.sift(p, 0);
-    if (j == C.lv.size() && C.is_id(p)) continue;
+    if (j == C.lv.size()) {
+      if (C.is_id(p)) continue;
+      if (C.known_base) return kOrderNotABase;
+    }
     C.insert(p, 0, j);
-    if (!C.complete(j)) return false;
+    if (!C.complete(j)) return C.not_a_base ? kOrderNotABase : kOrderWorkCap;
   }
   std::vector<uint64_t> f;
   double lg = 0;
@@ -288,7 +370,35 @@ bool group_order(uint32_t n, const uint16_t* auts, uint64_t count, uint64_t stri
   *log10_order = lg;
   *digits = big_product(f);
   *base_len = C.lv.size();
-  return true;
+  return kOrderOk;
+}
+
+}  // namespace
+
+bool group_order(uint32_t n, const uint16_t* auts, uint64_t count, uint64_t stride,
+                 uint64_t work_cap, double* log10_order, std::string* digits,
+                 uint64_t* base_len) {
+  Chain C;
+  C.n = n;
+  C.work_cap = work_cap;
+  return run(C, auts, count, stride, log10_order, digits, base_len) == kOrderOk;
+}
+
+int group_order_with_base(uint32_t n, const uint16_t* auts, uint64_t count, uint64_t stride,
+                          const uint32_t* base, uint32_t nbase, uint64_t work_cap,
+                          double* log10_order, std::string* digits, uint64_t* base_len) {
+  Chain C;
+  C.n = n;
+  C.work_cap = work_cap;
+  C.known_base = true;
+  std::vector<char> seen(n, 0);
+  for (uint32_t m = 0; m < nbase; ++m) {
+    if (base[m] >= n || seen[base[m]]) return kOrderNotABase;
+    seen[base[m]] = 1;
+    C.new_level(base[m]);
+  }
+  C.bi.resize(nbase);
+  return run(C, auts, count, stride, log10_order, digits, base_len);
 }
 
 }  // namespace gcl

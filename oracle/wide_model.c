@@ -302,7 +302,7 @@ static int wm_start_item(wm_worker* w, wm_shared* G, uint32_t k, uint32_t v) {
 int gcl_wide_model(int n, const int32_t* rowptr, const int32_t* col, const int32_t* color,
                    int workers, unsigned seed, int cap, int gate, uint8_t* out_nxn,
                    long* nodes_out, int* naut_out, long* events_out, uint32_t* auts_out,
-                   long* rounds_out) {
+                   long* rounds_out, uint32_t* first_seq_out) {
   if (n < 1 || workers < 1 || cap < 1) return -1;
   osearch S0;
   memset(&S0, 0, sizeof S0);
@@ -419,6 +419,7 @@ int gcl_wide_model(int n, const int32_t* rowptr, const int32_t* col, const int32
     for (int i = 0; i < workers; ++i) active |= ws[i].busy;
   }
   free(need);
+  if (first_seq_out) memcpy(first_seq_out, G.first_seq, (size_t)G.first_seqlen * 4);
   if (rounds_out) {
     rounds_out[0] = rounds;
     rounds_out[1] = (long)G.D;

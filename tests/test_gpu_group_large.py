@@ -1,0 +1,25 @@
+"""Group order of graphs whose automorphism groups have large orbits, where
+the general Schreier-Sims completion exceeds its budget and gcl_group_order
+sifts on the first path's base images instead.
+
+Staged: marked gpu_staged, not gpu, until it has passed on a B200; run it
+with `pytest -m gpu_staged`.  The base-image completion itself is checked on
+the CPU (tests/test_group_base.py)."""
+import math
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+pytestmark = [pytest.mark.gpu_staged,
+              pytest.mark.skipif(not torch.cuda.is_available(), reason="needs a CUDA GPU")]
+
+
+def test_group_order_large_vertex_transitive(pkg, G):
+    ctx = pkg.Context(0)
+    assert pkg.group_order(G.torus(100), ctx=ctx) == 8 * 100 * 100
+    d = 12
+    cube = G.from_edges(1 << d, [(a, a ^ (1 << b)) for a in range(1 << d) for b in range(d)
+                                 if a < a ^ (1 << b)])
+    assert pkg.group_order(cube, ctx=ctx) == (1 << d) * math.factorial(d)
