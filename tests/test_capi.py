@@ -60,3 +60,33 @@ def test_create_rejects_a_missing_device(pkg):
     out = ctypes.c_void_p(1)
     rc = lib.gcl_create(-1, ctypes.byref(out))
     assert rc in (-1, -2) and not out.value
+
+
+def test_ctypes_structs_match_the_header(pkg, tmp_path):
+    # size and field offsets of every struct include/gcl.h passes by pointer,
+    # as the C compiler lays them out, against the Python binding's ctypes
+    api = pkg.api
+    structs = {"gcl_tuning": api.Tuning, "gcl_serve_config": api.ServeConfig,
+               "gcl_serve_result": api.ServeResult, "gcl_serve_stats": api.ServeStats}
+    lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "gcl.h"', "int main(void) {"]
+    for cname, py in structs.items():
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in py._fields_:
+            lines.append(f'  printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    import subprocess
+    cc = "/usr/bin/gcc" if os.path.exists("/usr/bin/gcc") else "gcc"
+    subprocess.run([cc, "-std=c11", "-I", os.path.join(ROOT, "include"), "-o", str(exe), str(src)],
+                   check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout
+    got = {}
+    for ln in out.splitlines():
+        s, f, v = ln.split()
+        got[(s, f)] = int(v)
+    for cname, py in structs.items():
+        assert got[(cname, "size")] == ctypes.sizeof(py), cname
+        for fname, _ in py._fields_:
+            assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)
