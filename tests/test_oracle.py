@@ -37,8 +37,10 @@ def test_port_matches_reference_fresh_seeds(G, oracle_mod):
         g = G.erdos_renyi(n, float(rng.uniform(0.02, 0.6)), rng)
         col = rng.integers(0, 3, n) if i % 2 else None
         graphs.append(G.from_edges(n, g.edges(), col))
-    # deep trees with many inequivalent leaves
+    # deep trees with many inequivalent leaves, and strongly regular / cube families
     graphs += [G.cfi_graph(b, rng, twist=bool(b % 4)) for b in (4, 6, 8, 10, 12)]
+    from test_gpu_hard_families import _families
+    graphs += _families(G)
     for g in graphs:
         a = oracle_mod.canon(g, kind="port")
         b = oracle_mod.canon(g, kind="reference")
