@@ -223,6 +223,7 @@ struct Chain {
   size_t sift_images(size_t from) {
     for (size_t i = from; i < lv.size(); ++i) {
       const uint32_t x = bi[i];
+      if (x == lv[i].base) continue;  // u of the base point is the identity
       if (lv[i].sv[x] == -2) return i;
       apply_rep_inv(lv[i], x, i, lv.size());
     }
@@ -234,6 +235,7 @@ struct Chain {
   size_t sift(Perm& h, size_t from) {
     for (size_t i = from; i < lv.size(); ++i) {
       const uint32_t x = h[lv[i].base];
+      if (x == lv[i].base) continue;  // u of the base point is the identity
       if (lv[i].sv[x] == -2) return i;
       strip(lv[i], x, h);
     }
