@@ -143,6 +143,7 @@ def test_wide_model_automorphisms_generate_the_group(G, wm, pkg):
     cases += [(G.from_edges(n, [(i, j) for i in range(n) for j in range(i + 1, n)]),
                math.factorial(n)) for n in (4, 7)]
     cases += [(G.from_edges(9, [(0, i) for i in range(1, 9)]), math.factorial(8))]
+    cases += [(G.from_edges(100, []), math.factorial(100))]  # S_100: a long base
     cube = [(a, a ^ (1 << b)) for a in range(16) for b in range(4) if a < a ^ (1 << b)]
     cases += [(G.from_edges(16, cube), 384)]
     c5 = G.from_edges(5, [(i, (i + 1) % 5) for i in range(5)])
