@@ -647,6 +647,9 @@ namespace {
 std::once_flag g_default_once;
 gcl_context* g_default = nullptr;
 int g_default_rc = GCL_OK;
+// calls through the process-wide context hold this lock: a context serves
+// one call at a time, and callers of the NULL context may be on any thread
+std::mutex g_default_mu;
 
 int default_context(gcl_context** out) {
   std::call_once(g_default_once, [] { g_default_rc = gcl_create(0, &g_default); });
@@ -803,9 +806,11 @@ int gcl_canon_batch(gcl_context* c, int count, const int64_t* voff, const int64_
 int gcl_canon_one(gcl_context* c, const int32_t* rowptr, const int32_t* col, const int32_t* color,
                   int n, int max_aut, uint8_t* out_nxn, int64_t* node_count, int64_t* num_aut) try {
   if (n < 0 || !rowptr || max_aut <= 0 || (n > 0 && !out_nxn)) return GCL_ERR_ARG;
+  std::unique_lock<std::mutex> shared_ctx;
   if (!c) {
     int rc = default_context(&c);
     if (rc != GCL_OK) return rc;
+    shared_ctx = std::unique_lock<std::mutex>(g_default_mu);
   }
   if (n == 0) {  // the reference's search visits the (discrete) root only
     if (node_count) *node_count = 1;
@@ -839,9 +844,11 @@ int gcl_iso(gcl_context* c, const int32_t* rp1, const int32_t* col1, const int32
             const int32_t* rp2, const int32_t* col2, const int32_t* color2, int n2, int max_aut,
             int* verdict) try {
   if (!verdict || n1 < 0 || n2 < 0 || !rp1 || !rp2 || max_aut <= 0) return GCL_ERR_ARG;
+  std::unique_lock<std::mutex> shared_ctx;
   if (!c) {
     int rc = default_context(&c);
     if (rc != GCL_OK) return rc;
+    shared_ctx = std::unique_lock<std::mutex>(g_default_mu);
   }
   std::vector<uint8_t> a((size_t)n1 * n1 + 1), b((size_t)n2 * n2 + 1);
   int rc = gcl_canon_one(c, rp1, col1, color1, n1, max_aut, a.data(), nullptr, nullptr);
@@ -863,9 +870,11 @@ int gcl_group_order(gcl_context* c, const int32_t* rowptr, const int32_t* col,
                     int digits_cap, int64_t* generators) try {
   if (n < 0 || !rowptr || !log10_order || (digits && digits_cap < 2)) return GCL_ERR_ARG;
   if (n > GCL_MAX_N) return GCL_ERR_TOO_LARGE;
+  std::unique_lock<std::mutex> shared_ctx;
   if (!c) {
     int rc = default_context(&c);
     if (rc != GCL_OK) return rc;
+    shared_ctx = std::unique_lock<std::mutex>(g_default_mu);
   }
   auto put = [&](const std::string& d, double lg, int64_t ng) {
     *log10_order = lg;

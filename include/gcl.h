@@ -113,7 +113,9 @@ int gcl_set_option(gcl_context* ctx, int option, int64_t value);
  * canonical vertex i = row i), the value Nauty_Parallel returns.  node_count
  * and num_aut (either may be NULL) receive the search statistics.  ctx may be
  * NULL: a process-wide context on device 0 is created on first use (the
- * reference hard-codes device 0, src/nauty_parallel.cu:642-643). */
+ * reference hard-codes device 0, src/nauty_parallel.cu:642-643); calls
+ * through it from several threads take turns.  gcl_iso and gcl_group_order
+ * take NULL the same way. */
 int gcl_canon_one(gcl_context* ctx, const int32_t* rowptr, const int32_t* col,
                   const int32_t* color, int n, int max_aut, uint8_t* out_nxn,
                   int64_t* node_count, int64_t* num_aut);
