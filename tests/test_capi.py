@@ -90,3 +90,22 @@ def test_ctypes_structs_match_the_header(pkg, tmp_path):
         assert got[(cname, "size")] == ctypes.sizeof(py), cname
         for fname, _ in py._fields_:
             assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)
+
+
+def test_no_cpu_fallback_without_a_gpu(pkg, G):
+    # the product path has no CPU fallback: without a device every call that
+    # canonizes raises instead of answering from the host
+    import torch
+    if torch.cuda.is_available():
+        import pytest
+        pytest.skip("a GPU is present")
+    g = G.torus(4)
+    for call in (lambda: pkg.canon(g), lambda: pkg.canon_batch([g, g]),
+                 lambda: pkg.is_isomorphic(g, g), lambda: pkg.group_order(g),
+                 lambda: pkg.Nauty_Parallel(g)):
+        try:
+            call()
+        except pkg.GclError as e:
+            assert e.rc in (-1, -2)
+        else:
+            raise AssertionError("a canonization ran without a GPU")
