@@ -117,7 +117,7 @@ struct WideArgs {
   SpLayout Lo;
   uint64_t slot_bytes;
   uint32_t pool;
-  uint32_t gate;  // 1: a level's items wait for the deeper levels (shared orbit cache)
+  uint32_t gate;  // 1: a level's items wait for the deeper levels (shared orbit cache); 0: not
   uint64_t smem_per_warp;
   uint64_t budget_ns;
   uint8_t* out_dense;    // n*n, or null

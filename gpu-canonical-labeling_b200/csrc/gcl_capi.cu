@@ -235,7 +235,7 @@ struct gcl_context {
   uint64_t workspace_bytes = 0;  // per-pass workspace cap, 0 = GCL_WORKSPACE_GB
   int64_t wide_max_warps = 0;    // 0 = as many as fit
   bool smem_stage = true;        // sparse and wide kernels stage per-step arrays in shared memory
-  bool wide_gate = true;         // wide search: a level's items wait for the deeper levels
+  int wide_gate = 1;             // wide search's level gate: 1 on, 0 off, 2 automatic
   // launch shape per size bucket (gcl_autotune / gcl_set_tuning): 0 / -1 = default
   int w64_per_sm = 0;            // resident blocks the warp kernel's occupancy allows
   int tune_w64_bps = 0;
@@ -556,8 +556,8 @@ int gcl_set_option(gcl_context* c, int option, int64_t value) {
       c->smem_stage = value != 0;
       return GCL_OK;
     case GCL_OPT_WIDE_GATE:
-      if (value != 0 && value != 1) return GCL_ERR_ARG;
-      c->wide_gate = value != 0;
+      if (value < 0 || value > 2) return GCL_ERR_ARG;
+      c->wide_gate = (int)value;
       return GCL_OK;
     case GCL_OPT_STREAM_PRIORITY: {
       if (value != 0 && value != 1) return GCL_ERR_ARG;
@@ -619,7 +619,7 @@ int gcl_canon_wide_device_async(gcl_context* c, const int32_t* d_rowptr, const i
   WA.Lo = Lo;
   WA.slot_bytes = Lo.bytes;
   WA.pool = kWidePool;
-  WA.gate = c->wide_gate ? 1u : 0u;
+  WA.gate = c->wide_gate == 0 ? 0u : 1u;
   WA.smem_per_warp = smw;
   WA.budget_ns = graph_budget_ns();
   WA.out_dense = d_out_dense;
@@ -630,6 +630,20 @@ int gcl_canon_wide_device_async(gcl_context* c, const int32_t* d_rowptr, const i
   cudaStream_t s = c->stream;
   wide_first_kernel<<<1, 32, 0, s>>>(WA);
   GCL_TRY(cudaGetLastError());
+  if (c->wide_gate == 2) {
+    // automatic level gate: off when the first path's levels hold fewer than
+    // 4 items each on average (trees), where it would run the items one
+    // after another.  Reads the first path's shape, so the call waits for
+    // the first kernel.
+    static_assert(offsetof(WideHdr, nitems) == offsetof(WideHdr, D) + sizeof(uint32_t),
+                  "D and nitems are read together");
+    uint32_t dn[2] = {0, 0};
+    GCL_TRY(cudaMemcpyAsync(dn, WA.sh + WL.hdr + offsetof(WideHdr, D), sizeof dn,
+                            cudaMemcpyDeviceToHost, s));
+    GCL_TRY(cudaStreamSynchronize(s));
+    const uint64_t levels = dn[0] > 1 ? dn[0] - 1u : 0u;
+    WA.gate = (uint64_t)dn[1] >= 4 * levels ? 1u : 0u;
+  }
   wide_items_kernel<<<(int)(warps / kSpWarps), kSpThreads, (size_t)(smw * kSpWarps), s>>>(WA);
   GCL_TRY(cudaGetLastError());
   wide_finish_kernel<<<1, 32, 0, s>>>(WA);

@@ -97,7 +97,10 @@ void* gcl_stream(gcl_context* ctx);
  *   against the automorphisms known at that moment.  Same canonical form
  *   either way.  0 suits searches whose levels hold few items each (trees:
  *   the gate runs their items one after another); it costs more nodes where
- *   levels are wide, and an orbit test per item over the whole store.  Not
+ *   levels are wide, and an orbit test per item over the whole store.  2
+ *   chooses per search: off when the first path's levels hold fewer than 4
+ *   items each on average, else on (gcl_canon_wide_device_async then waits
+ *   for its first kernel to read that shape).  Values other than 1 are not
  *   yet measured on a GPU.
  * Returns GCL_ERR_ARG for an unknown option or value. */
 #define GCL_OPT_WIDE_MIN_N 1

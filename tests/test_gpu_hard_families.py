@@ -54,7 +54,7 @@ def test_hard_families_batched_vs_oracle(pkg, G, oracle_mod):
         assert tuple(res.stats[k]) == (na, nodes), k
 
 
-@pytest.mark.parametrize("gate", [1, 0])
+@pytest.mark.parametrize("gate", [1, 0, 2])
 def test_hard_families_wide_vs_oracle(pkg, G, oracle_mod, gate):
     ctx = pkg.Context(0, wide_min_n=1)
     ctx.set_option(pkg.api.GCL_OPT_WIDE_GATE, gate)

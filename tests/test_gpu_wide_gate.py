@@ -60,3 +60,14 @@ def test_gate_off_small_store(pkg, G, oracle_mod, free_ctx, max_aut):
               G.tree_plus_edges(400, rng)):
         mat = oracle_mod.canon(g, max_aut=max_aut)[0]
         assert np.array_equal(pkg.canon(g, max_aut=max_aut, ctx=free_ctx).matrix, mat)
+
+
+def test_gate_auto_vs_oracle(pkg, G, oracle_mod):
+    # 2: off on trees (about one item per level), on for tori and regular graphs
+    ctx = pkg.Context(0, wide_min_n=1)
+    ctx.set_option(pkg.api.GCL_OPT_WIDE_GATE, 2)
+    rng = np.random.default_rng(12)
+    graphs = [G.from_edges(n, G.recursive_tree(n, rng)) for n in (100, 700)]
+    graphs += [G.torus(12), G.random_regular(300, 3, rng), G.cfi_graph(10, rng)]
+    for g in graphs:
+        assert np.array_equal(pkg.canon(g, ctx=ctx).matrix, oracle_mod.canon(g)[0])
