@@ -58,7 +58,7 @@ struct WideHdr {
   uint32_t orb_lock;   // guards the orbit cache
   int32_t orb_level;   // level index the orbit cache belongs to (-1 = none)
   uint32_t orb_known;  // store entries merged into the orbit cache
-  uint32_t pad;
+  uint32_t gate;       // the items kernel's level gate (1 on), set by the first kernel
   unsigned long long nodes;
   unsigned long long t0;  // start time (globaltimer ns)
 };
@@ -117,7 +117,7 @@ struct WideArgs {
   SpLayout Lo;
   uint64_t slot_bytes;
   uint32_t pool;
-  uint32_t gate;  // 1: a level's items wait for the deeper levels (shared orbit cache); 0: not
+  uint32_t gate;  // level gate: 1 on (a level's items wait for the deeper ones), 0 off, 2 auto
   uint64_t smem_per_warp;
   uint64_t budget_ns;
   uint8_t* out_dense;    // n*n, or null
@@ -275,6 +275,9 @@ __global__ void __launch_bounds__(32) wide_first_kernel(WideArgs A) {
     H->best_level = D;
     H->best_seqlen = seqlen;
     H->nodes = nodes;
+    // automatic gate: off when the levels hold fewer than 4 items each on
+    // average (trees), where it would run the items one after another
+    H->gate = A.gate == 2 ? (run >= 4u * (D - 1u) ? 1u : 0u) : (A.gate != 0 ? 1u : 0u);
     __threadfence();
     H->nitems = run;
   }
@@ -705,7 +708,7 @@ __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
     const uint32_t k = D - 2 - lo;  // parent node level k+1, its target cell index k
     const uint32_t tf = P.tcfirst[k], tl = P.tclen[k];
     const uint32_t v = P.lelem[tf + 1 + (it - P.cum[lo])];
-    if (A.gate) {
+    if (H->gate) {
       const int32_t gs = wide_gate(H, P.cum[lo], deadline);
       if (gs != kOk) {
         status = gs;
@@ -716,7 +719,7 @@ __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
     bool skip = false;
     if (known) {
       bool ok = true;
-      const uint32_t r = A.gate ? wide_orbit_min(P, v, lo, k, tf, tl, known, A.WL.stride, &ok)
+      const uint32_t r = H->gate ? wide_orbit_min(P, v, lo, k, tf, tl, known, A.WL.stride, &ok)
                                 : wide_orbit_min_own(P, v, k, tf, tl, known, A.WL.stride, &ok);
       if (!ok) {
         status = kTimeout;

@@ -619,7 +619,7 @@ int gcl_canon_wide_device_async(gcl_context* c, const int32_t* d_rowptr, const i
   WA.Lo = Lo;
   WA.slot_bytes = Lo.bytes;
   WA.pool = kWidePool;
-  WA.gate = c->wide_gate == 0 ? 0u : 1u;
+  WA.gate = (uint32_t)c->wide_gate;
   WA.smem_per_warp = smw;
   WA.budget_ns = graph_budget_ns();
   WA.out_dense = d_out_dense;
@@ -630,20 +630,6 @@ int gcl_canon_wide_device_async(gcl_context* c, const int32_t* d_rowptr, const i
   cudaStream_t s = c->stream;
   wide_first_kernel<<<1, 32, 0, s>>>(WA);
   GCL_TRY(cudaGetLastError());
-  if (c->wide_gate == 2) {
-    // automatic level gate: off when the first path's levels hold fewer than
-    // 4 items each on average (trees), where it would run the items one
-    // after another.  Reads the first path's shape, so the call waits for
-    // the first kernel.
-    static_assert(offsetof(WideHdr, nitems) == offsetof(WideHdr, D) + sizeof(uint32_t),
-                  "D and nitems are read together");
-    uint32_t dn[2] = {0, 0};
-    GCL_TRY(cudaMemcpyAsync(dn, WA.sh + WL.hdr + offsetof(WideHdr, D), sizeof dn,
-                            cudaMemcpyDeviceToHost, s));
-    GCL_TRY(cudaStreamSynchronize(s));
-    const uint64_t levels = dn[0] > 1 ? dn[0] - 1u : 0u;
-    WA.gate = (uint64_t)dn[1] >= 4 * levels ? 1u : 0u;
-  }
   wide_items_kernel<<<(int)(warps / kSpWarps), kSpThreads, (size_t)(smw * kSpWarps), s>>>(WA);
   GCL_TRY(cudaGetLastError());
   wide_finish_kernel<<<1, 32, 0, s>>>(WA);

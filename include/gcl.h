@@ -99,9 +99,8 @@ void* gcl_stream(gcl_context* ctx);
  *   the gate runs their items one after another); it costs more nodes where
  *   levels are wide, and an orbit test per item over the whole store.  2
  *   chooses per search: off when the first path's levels hold fewer than 4
- *   items each on average, else on (gcl_canon_wide_device_async then waits
- *   for its first kernel to read that shape).  Values other than 1 are not
- *   yet measured on a GPU.
+ *   items each on average, else on (decided on the device after the first
+ *   path).  Values other than 1 are not yet measured on a GPU.
  * Returns GCL_ERR_ARG for an unknown option or value. */
 #define GCL_OPT_WIDE_MIN_N 1
 #define GCL_OPT_WORKSPACE_BYTES 2
