@@ -393,7 +393,8 @@ class ServeConfig(ctypes.Structure):
                 ("mid_batch", ctypes.c_int), ("big_batch", ctypes.c_int), ("mid_n", ctypes.c_int),
                 ("big_n", ctypes.c_int), ("large_n", ctypes.c_int), ("max_aut", ctypes.c_int),
                 ("lane_bytes", ctypes.c_int64), ("table_slots", ctypes.c_int64),
-                ("store_bytes", ctypes.c_int64), ("memo_bytes", ctypes.c_int64)]
+                ("store_bytes", ctypes.c_int64), ("memo_bytes", ctypes.c_int64),
+                ("big_wide", ctypes.c_int)]
 
 
 class ServeResult(ctypes.Structure):

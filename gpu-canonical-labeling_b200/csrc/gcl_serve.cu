@@ -566,13 +566,14 @@ void complete(gcl_server* S, Lane* L) {
     const int g = L->first[k];
     if (L->large && L->err == GCL_OK) {
       // a wide search that ran out of per-warp orbit storage (or failed an
-      // internal check) has no result: the request goes to the big lanes,
-      // whose sequential search reruns with full storage
+      // internal check) has no result: the request goes to lanes of the
+      // batched sequential search (big, or mid when the big lanes are wide),
+      // which reruns it with full storage
       bool retry = false;
       for (int i = 0; i < r->ng; ++i) retry |= status[g + i] == 1 || status[g + i] == 4;
       if (retry) {
         std::lock_guard<std::mutex> lk(S->mu);
-        S->q[kBig].push_back(r);
+        S->q[S->cfg.big_wide ? kMid : kBig].push_back(r);
         continue;
       }
     }
@@ -792,7 +793,7 @@ int gcl_serve_create(int device, const gcl_serve_config* cfg, gcl_server** out) 
   S->cfg = c;
   S->max_batch[kSmall] = c.max_batch;
   S->max_batch[kMid] = c.mid_batch;
-  S->max_batch[kBig] = c.big_batch;
+  S->max_batch[kBig] = c.big_wide ? 1 : c.big_batch;
   S->max_batch[kLarge] = 1;
   int rc = GCL_OK;
   int dev_sms = 0;
@@ -811,7 +812,8 @@ int gcl_serve_create(int device, const gcl_serve_config* cfg, gcl_server** out) 
       break;
     }
     L->cls = i < nl[0] ? kSmall : i < nl[0] + nl[1] ? kMid : i < nl[0] + nl[1] + nl[2] ? kBig : kLarge;
-    L->large = L->cls == kLarge;
+    // lanes whose requests go through the wide search one at a time
+    L->large = L->cls == kLarge || (c.big_wide && L->cls == kBig);
     S->lanes.push_back(L);
     rc = gcl_create(device, &L->ctx);
     // short work first: small and mid lanes get high-priority streams
@@ -826,7 +828,13 @@ int gcl_serve_create(int device, const gcl_serve_config* cfg, gcl_server** out) 
       if (!L->large) rc = gcl_set_option(L->ctx, GCL_OPT_WORKSPACE_BYTES, c.lane_bytes);
       // a wide search takes one block per SM, leaving room on every SM for
       // the batches of the other lanes
-      else rc = gcl_set_option(L->ctx, GCL_OPT_WIDE_MAX_WARPS, (int64_t)std::max(dev_sms, 1) * 4);
+      else if (L->cls == kLarge)
+        rc = gcl_set_option(L->ctx, GCL_OPT_WIDE_MAX_WARPS, (int64_t)std::max(dev_sms, 1) * 4);
+      // a big graph's search has at most a few hundred items (trees: about
+      // one per first-path level), which 128 warps cover
+      else rc = gcl_set_option(L->ctx, GCL_OPT_WIDE_MAX_WARPS, 128);
+      if (rc == GCL_OK && L->large && c.big_wide)
+        rc = gcl_set_option(L->ctx, GCL_OPT_WIDE_GATE, 2);
       // searches of big and large graphs run for long: their blocks keep
       // their per-step arrays in device memory so that they never fill an
       // SM's shared memory and lock the small lanes' kernels out

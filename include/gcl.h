@@ -315,6 +315,13 @@ typedef struct {
   int64_t table_slots; /* canonical-hash table slots (power of two), 1 << 20  */
   int64_t store_bytes; /* device store of canonical forms, default 256 MiB    */
   int64_t memo_bytes;  /* host memo of exact repeats, default 64 MiB, < 0 = off */
+  int big_wide;        /* 1: the big lanes run each request through the wide
+                          search, one request at a time on up to 128 warps,
+                          and every wide search picks its level gate per graph
+                          (GCL_OPT_WIDE_GATE 2); a wide search that runs out
+                          of orbit storage is rerun on a mid lane.  Default 0:
+                          the batched sequential search.  Not yet measured on
+                          a GPU.                                               */
 } gcl_serve_config;
 
 #define GCL_REQ_CANON 0
