@@ -82,6 +82,8 @@ def parse():
                    help="largest request size (the 1%% tail is log-uniform on (2048, nmax])")
     p.add_argument("--serve-large-n", type=int, default=0,
                    help="server large_n (0 = the library default)")
+    p.add_argument("--serve-big-wide", action="store_true",
+                   help="server big_wide: big requests through the wide search")
     p.add_argument("--serve-plain", type=int, default=800,
                    help="requests replayed through the plain one-graph-per-launch form")
     p.add_argument("--no-single", action="store_true")
@@ -536,6 +538,8 @@ def serving_block(args, pkg, local):
                            n_max=args.serve_nmax)
     arena = G.pack(W.graphs)
     scfg = {"large_n": args.serve_large_n} if args.serve_large_n else {}
+    if args.serve_big_wide:
+        scfg["big_wide"] = 1
     srv = pkg.Server(local, **scfg)
     # warm-up on the same server (its lanes size their buffers): a short
     # replay of the first requests
