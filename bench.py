@@ -189,6 +189,9 @@ def reference_arm(args):
         per.append(t)
     pool.close()
     v = tot_g / tot_t
+    # one core: the same reference code in this process on the first 2,000 graphs
+    _cpu_init(kind, (arena.count, arena.voff, arena.eoff, arena.rowptr, arena.col, arena.color))
+    g1, t1 = _cpu_run((0, min(2000, arena.count)))
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_t / args.steps,
@@ -197,7 +200,9 @@ def reference_arm(args):
         "config": {"workload": WORKLOAD, "graphs_per_step": arena.count},
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": pool.cores, "kind": kind,
                          "sample": f"the full {arena.count}-graph batch per step, split over "
-                                   f"{pool.cores} processes"},
+                                   f"{pool.cores} processes",
+                         "value_1core": g1 / t1,
+                         "sample_1core": f"the first {g1} graphs in one process"},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "latency_ms": {"p50": float(np.percentile(per, 50)) * 1e3,
                        "p99": float(np.percentile(per, 99)) * 1e3},
