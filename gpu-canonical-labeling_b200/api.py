@@ -40,7 +40,7 @@ EXPORTS = [
     "gcl_canon_batch_noalloc", "gcl_set_option", "gcl_canon_wide_device_async",
     "gcl_serve_create", "gcl_serve_destroy", "gcl_serve_submit", "gcl_serve_poll",
     "gcl_serve_stats_get", "gcl_serve_replay", "gcl_group_order", "gcl_perm_group_order",
-    "gcl_autotune", "gcl_set_tuning", "gcl_canon_files",
+    "gcl_autotune", "gcl_set_tuning", "gcl_canon_files", "gcl_format_adjacency_device_async",
 ]
 
 GCL_OPT_WIDE_MIN_N = 1
@@ -118,11 +118,12 @@ def load_library(path: str = LIB_PATH):
                                          ctypes.c_int]
     lib.gcl_canon_wide_device_async.argtypes = [_P, _P, _P, _P, ctypes.c_int, ctypes.c_int64,
                                                 ctypes.c_int, _P, _P, _P, _P, _P]
+    lib.gcl_format_adjacency_device_async.argtypes = [_P, ctypes.c_int, _P, _P, _P, _P, _P]
     for name in ("gcl_create", "gcl_destroy", "gcl_sync", "gcl_canon_one", "gcl_canon_batch",
                  "gcl_canon_batch_device_async", "gcl_iso", "gcl_canon_batch_noalloc",
                  "gcl_set_option", "gcl_canon_wide_device_async", "gcl_group_order",
                  "gcl_perm_group_order", "gcl_autotune", "gcl_set_tuning",
-                 "gcl_canon_files"):
+                 "gcl_canon_files", "gcl_format_adjacency_device_async"):
         getattr(lib, name).restype = ctypes.c_int
     _lib = lib
     return lib

@@ -639,6 +639,10 @@ int gcl_canon_wide_device_async(gcl_context* c, const int32_t* d_rowptr, const i
 
 }  // extern "C"
 
+namespace gcl {
+int context_device(const gcl_context* c) { return c->device; }
+}  // namespace gcl
+
 // ---------------------------------------------------------------------------
 // Host-pointer entry points.
 // ---------------------------------------------------------------------------

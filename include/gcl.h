@@ -200,6 +200,19 @@ int gcl_canon_batch_noalloc(void* stream, int count, const int64_t* d_voff,
                             const int64_t* d_ooff, int32_t* d_out_label,
                             int64_t* d_out_stats, int32_t* d_out_status);
 
+/* ---- the reference's output text, written on the device -------------------
+ * print_canonical_adjacency_list (main.cpp:33-70) for every graph of a batch,
+ * from its bit-packed canonical rows (d_rows + d_roff[g]: n_g * ceil(n_g/64)
+ * words, the out_rows layout of gcl_canon_batch_device_async) -- the text of
+ * the reference's `output` file without an n x n byte matrix.  Two calls,
+ * asynchronous on gcl_stream(ctx): with d_text NULL it writes the byte
+ * offsets d_toff[count + 1] (d_toff[0] = 0); with d_text of d_toff[count]
+ * bytes (read them back first) it writes graph g's text at d_text +
+ * d_toff[g].  No reference counterpart as a call. */
+int gcl_format_adjacency_device_async(gcl_context* ctx, int count, const int64_t* d_voff,
+                                      const uint64_t* d_rows, const int64_t* d_roff,
+                                      int64_t* d_toff, char* d_text);
+
 /* ---- files: DIMACS parsing overlapped with the GPU -------------------------
  * Canonize `count` DIMACS files (the reference's graph.txt format,
  * CSRGraph::fromDIMACS, src/CSRGraph.cpp:40-119) in chunks of `chunk` files
