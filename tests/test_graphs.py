@@ -84,3 +84,34 @@ def test_serving_workload_mix(G):
     assert abs(len(W.kind) / W.arrival[-1] - 1000.0) < 100.0
     iso = np.nonzero(W.kind == 1)[0]
     assert all(W.graphs[W.g1[i]].n == W.graphs[W.g2[i]].n for i in iso)
+
+
+def test_cfi_graphs_cubic_and_twist_distinguished(G, oracle_mod):
+    # every vertex of a CFI graph over a cubic base has degree 3; the twisted
+    # and untwisted graphs over the same connected base are not isomorphic
+    # (colour refinement cannot tell them apart; the individualization search
+    # does), and a relabeling of either is
+    import numpy as np
+    for b in (4, 6, 8):
+        seed = 100 + b
+        g0 = G.cfi_graph(b, np.random.default_rng(seed), twist=False)
+        g1 = G.cfi_graph(b, np.random.default_rng(seed), twist=True)
+        assert g0.n == g1.n == 10 * b
+        assert set(np.diff(g0.rowptr).tolist()) == {3} == set(np.diff(g1.rowptr).tolist())
+        c0, c1 = oracle_mod.canon(g0)[0], oracle_mod.canon(g1)[0]
+        base = G.random_regular(b, 3, np.random.default_rng(seed))
+        if _connected(base):
+            assert not np.array_equal(c0, c1)
+        h = G.random_relabel(g1, np.random.default_rng(seed + 1))
+        assert np.array_equal(oracle_mod.canon(h)[0], c1)
+
+
+def _connected(g):
+    seen, stack = {0}, [0]
+    while stack:
+        u = stack.pop()
+        for v in g.col[g.rowptr[u]:g.rowptr[u + 1]]:
+            if int(v) not in seen:
+                seen.add(int(v))
+                stack.append(int(v))
+    return len(seen) == g.n
