@@ -60,3 +60,19 @@ def test_hard_families_wide_vs_oracle(pkg, G, oracle_mod, gate):
     ctx.set_option(pkg.api.GCL_OPT_WIDE_GATE, gate)
     for k, g in enumerate(_families(G)):
         assert np.array_equal(pkg.canon(g, ctx=ctx).matrix, oracle_mod.canon(g)[0]), k
+
+
+def test_cfi_pairs_iso_verdicts(pkg, G):
+    # twisted and untwisted CFI graphs over one connected cubic base: the
+    # classic pairs colour refinement cannot separate
+    ctx = pkg.Context(0)
+    for b in (6, 10, 16):
+        seed = 300 + b
+        g0 = G.cfi_graph(b, np.random.default_rng(seed), twist=False)
+        g1 = G.cfi_graph(b, np.random.default_rng(seed), twist=True)
+        h = G.random_relabel(g1, np.random.default_rng(seed + 1))
+        assert pkg.is_isomorphic(g1, h, ctx=ctx)
+        base = G.random_regular(b, 3, np.random.default_rng(seed))
+        from test_graphs import _connected
+        if _connected(base):
+            assert not pkg.is_isomorphic(g0, g1, ctx=ctx)
