@@ -135,7 +135,8 @@ def _load_wide():
         raise FileNotFoundError(f"oracle library missing: {WIDE_SO} (run make -C oracle)")
     lib = ctypes.CDLL(WIDE_SO)
     lib.gcl_wide_model.argtypes = [ctypes.c_int, _P, _P, _P, ctypes.c_int, ctypes.c_uint,
-                                   ctypes.c_int, ctypes.c_int, _P, ctypes.POINTER(ctypes.c_long),
+                                   ctypes.c_int, ctypes.c_int, ctypes.c_int, _P,
+                                   ctypes.POINTER(ctypes.c_long),
                                    ctypes.POINTER(ctypes.c_int), _P, _P, _P, _P]
     lib.gcl_wide_model.restype = ctypes.c_int
     lib.gcl_exhaustive_canon.argtypes = [ctypes.c_int, _P, _P, _P, ctypes.c_long, _P,
@@ -154,7 +155,7 @@ def _csr(g):
 
 def wide_model(g, workers: int, seed: int = 0, cap: int = 10000, auts: bool = False,
                gate: bool = True, rounds: Optional[list] = None,
-               first_seq: Optional[list] = None):
+               first_seq: Optional[list] = None, donate: bool = False):
     """CPU model of the many-worker search (wide_model.c): `workers` simulated
     workers over the first path's sibling items, stepped round-robin (seed 0)
     or in a seeded random order.  Returns (canonical matrix, nodes, automorphisms
@@ -165,7 +166,8 @@ def wide_model(g, workers: int, seed: int = 0, cap: int = 10000, auts: bool = Fa
     gate: items start level by level as on the GPU; `rounds`, when a list,
     receives the number of scheduling rounds (every worker steps once per
     round), the first leaf's level D and the number of items; `first_seq`,
-    when a list, the first path's individualized vertices."""
+    when a list, the first path's individualized vertices.  donate: busy
+    workers hand their shallowest untried child to idle ones."""
     lib = _load_wide()
     rp, cl, co = _csr(g)
     out = np.zeros((g.n, g.n), dtype=np.uint8)
@@ -176,7 +178,7 @@ def wide_model(g, workers: int, seed: int = 0, cap: int = 10000, auts: bool = Fa
     nr = (ctypes.c_long * 3)()
     fs = np.zeros(max(g.n, 1), dtype=np.uint32)
     rc = lib.gcl_wide_model(g.n, _ptr(rp), _ptr(cl), _ptr(co), workers, seed, cap, int(gate),
-                            _ptr(out), ctypes.byref(nodes), ctypes.byref(naut), _ptr(ev),
+                            int(donate), _ptr(out), ctypes.byref(nodes), ctypes.byref(naut), _ptr(ev),
                             _ptr(store), nr, _ptr(fs))
     if rc != 0:
         raise RuntimeError(f"wide model failed rc={rc}")

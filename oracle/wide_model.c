@@ -16,6 +16,8 @@
  * tests/test_wide_model.py checks that every schedule gives the sequential
  * canonical matrix, and that the sequential result is the maximum over all
  * leaves (exhaustive search) -- the property the wide search rests on.
+ * With `donate` set, a busy worker hands its shallowest untried child to an
+ * idle worker (work sharing below the first path's siblings).
  * With `gate` set, an item starts only once every item of the deeper levels
  * is done, as the GPU's level gate orders them; `rounds` counts the
  * scheduling rounds (every worker takes one step per round), the model's
@@ -63,7 +65,18 @@ typedef struct {
   uint32_t item_k;
   int best_local; /* the private best was found in this item (or is the first leaf) */
   int version;
+  int gift;       /* the current work is a donated subtree, not a first-path item */
 } wm_worker;
+
+/* A subtree handed over by a busy worker: the parent node (its partition at
+ * level L, its L-1 individualized vertices and L codes) and the child v. */
+typedef struct {
+  opart P;
+  uint32_t L;
+  uint32_t* seq;
+  int* pathcode;
+  uint32_t v;
+} wm_gift;
 
 static void wm_copy_part(opart* d, const opart* s, int n) {
   memcpy(d->elem, s->elem, (size_t)n * 4);
@@ -299,8 +312,85 @@ static int wm_start_item(wm_worker* w, wm_shared* G, uint32_t k, uint32_t v) {
   return 1;
 }
 
+/* The worker hands over its shallowest untried child: the next orbit
+ * representative of the target cell at the shallowest level of its item
+ * below the item's own node, which it then treats as tried.  Only at levels
+ * where a child's subtree is already finished (the path's child there is not
+ * the cell's least vertex, the one tried first), so that the automorphisms
+ * that subtree found prune the siblings before they are handed over. */
+static int wm_donate(wm_worker* w, wm_shared* G, wm_gift* g) {
+  osearch* S = &w->S;
+  opart* P = &S->P;
+  const int n = G->n;
+  for (uint32_t Lp = w->item_k + 2; Lp < P->level && (int)Lp <= S->tc_level_reached; ++Lp) {
+    otc* t = &S->tcs[Lp - 1];
+    if (t->counter >= (uint32_t)n) continue;
+    uint32_t least = (uint32_t)n;
+    for (uint32_t x = 0; x < (uint32_t)n && least == (uint32_t)n; ++x)
+      if (t->elems[x] >= 0) least = x;
+    if (P->seq[Lp - 1] == least) continue; /* the first child is still running */
+    if (S->num_aut > t->last_num_aut) {
+      wm_sync_auts(w, G);
+      /* orbits of the node at level Lp: automorphisms fixing its prefix */
+      uint32_t saved = P->seqlen;
+      P->seqlen = Lp - 1;
+      o_orbits(S, t);
+      P->seqlen = saved;
+      t->last_num_aut = S->num_aut;
+    }
+    if (!o_next_rep(S, t)) continue;
+    const uint32_t v = t->counter++;
+    uint32_t e1 = 0xffffffffu;
+    int e2 = 0x7fffffff, e3 = 0;
+    wm_copy_part(&g->P, P, n);
+    o_reconstruct(&g->P, Lp, &e1, &e2, &e3);
+    g->P.level = Lp;
+    g->L = Lp;
+    memcpy(g->seq, P->seq, (size_t)(Lp - 1) * 4);
+    memcpy(g->pathcode, w->pathcode, (size_t)Lp * sizeof(int));
+    g->v = v;
+    return 1;
+  }
+  return 0;
+}
+
+/* take a donated subtree: as an item whose parent is the gift's node */
+static int wm_start_gift(wm_worker* w, wm_shared* G, const wm_gift* gf) {
+  osearch* S = &w->S;
+  opart* P = &S->P;
+  const int n = G->n;
+  const uint32_t k = gf->L - 1;
+  wm_copy_part(P, &gf->P, n);
+  P->level = gf->L;
+  memcpy(P->seq, gf->seq, (size_t)k * 4);
+  P->seqlen = k;
+  S->tc_level_reached = (int)k;
+  o_select_tc(S);
+  otc* t = &S->tcs[k];
+  if (t->elems[gf->v] < 0) return 0;
+  wm_sync_auts(w, G);
+  t->last_num_aut = 0;
+  if (S->num_aut > 0) o_orbits(S, t);
+  t->last_num_aut = S->num_aut;
+  if (t->elems[gf->v] != (int32_t)gf->v) return 0;
+  t->counter = (uint32_t)n;
+  if (w->version != G->g_version) wm_adopt(w, G);
+  w->best_local = 0;
+  memcpy(w->pathcode, gf->pathcode, (size_t)gf->L * sizeof(int));
+  uint32_t e = 0;
+  while (e < gf->L && e < G->D && w->pathcode[e] == G->firstcode[e]) ++e;
+  S->eqlevfirst = e;
+  wm_recompare(w, gf->L);
+  w->item_k = k;
+  ++G->nodes;
+  P->seq[P->seqlen++] = gf->v;
+  o_individualize(P, gf->v, &S->code, t->first);
+  wm_classify(w, G);
+  return 1;
+}
+
 int gcl_wide_model(int n, const int32_t* rowptr, const int32_t* col, const int32_t* color,
-                   int workers, unsigned seed, int cap, int gate, uint8_t* out_nxn,
+                   int workers, unsigned seed, int cap, int gate, int donate, uint8_t* out_nxn,
                    long* nodes_out, int* naut_out, long* events_out, uint32_t* auts_out,
                    long* rounds_out, uint32_t* first_seq_out) {
   if (n < 1 || workers < 1 || cap < 1) return -1;
@@ -396,7 +486,19 @@ int gcl_wide_model(int n, const int32_t* rowptr, const int32_t* col, const int32
     need[it] = it > 0 && G.item_k[it] == G.item_k[it - 1] ? need[it - 1] : it;
   int done = 0;
   long rounds = 0;
+  /* donated subtrees waiting for a worker (at most one per idle worker) */
+  wm_gift* gifts = calloc((size_t)workers, sizeof(wm_gift));
+  for (int i = 0; i < workers; ++i) {
+    gifts[i].P.elem = malloc((size_t)n * 4);
+    gifts[i].P.lcs = malloc(((size_t)n + 1) * sizeof(ocell));
+    gifts[i].seq = malloc((size_t)n * 4 + 4);
+    gifts[i].pathcode = malloc(((size_t)n + 2) * sizeof(int));
+  }
+  int ngifts = 0;
   for (int active = 1; active; ++rounds) {
+    int idle = 0;
+    const int items_open = G.next_item < G.nitems && (!gate || done >= need[G.next_item]);
+    for (int i = 0; i < workers; ++i) idle += !ws[i].busy && !items_open;
     for (int ii = 0; ii < workers; ++ii) {
       rs ^= rs << 13;
       rs ^= rs >> 7;
@@ -407,17 +509,31 @@ int gcl_wide_model(int n, const int32_t* rowptr, const int32_t* col, const int32
         wm_step(w, &G);
         if (w->S.P.level <= w->item_k + 1) {
           w->busy = 0;
-          ++done;
+          if (!w->gift) ++done;
+        } else if (donate && ngifts < idle && wm_donate(w, &G, &gifts[ngifts])) {
+          ++ngifts;
         }
       } else if (G.next_item < G.nitems && (!gate || done >= need[G.next_item])) {
         int it = G.next_item++;
+        w->gift = 0;
         if (wm_start_item(w, &G, G.item_k[it], G.item_v[it])) w->busy = w->S.P.level > w->item_k + 1;
         if (!w->busy) ++done;
+      } else if (ngifts > 0) {
+        wm_gift* gf = &gifts[--ngifts];
+        w->gift = 1;
+        if (wm_start_gift(w, &G, gf)) w->busy = w->S.P.level > w->item_k + 1;
       }
     }
-    active = G.next_item < G.nitems;
+    active = G.next_item < G.nitems || ngifts > 0;
     for (int i = 0; i < workers; ++i) active |= ws[i].busy;
   }
+  for (int i = 0; i < workers; ++i) {
+    free(gifts[i].P.elem);
+    free(gifts[i].P.lcs);
+    free(gifts[i].seq);
+    free(gifts[i].pathcode);
+  }
+  free(gifts);
   free(need);
   if (first_seq_out) memcpy(first_seq_out, G.first_seq, (size_t)G.first_seqlen * 4);
   if (rounds_out) {

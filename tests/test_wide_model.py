@@ -172,3 +172,32 @@ def test_wide_model_group_order_schedule_independent_on_cfi(G, wm, pkg):
             assert naut < 20000
             orders.add(pkg.perm_group_order(store.astype(np.uint16)))
         assert len(orders) == 1, (i, orders)
+
+
+@pytest.mark.parametrize("gate", [True, False])
+def test_wide_model_donation_matches_sequential(G, wm, gate):
+    # busy workers hand untried children to idle ones (work sharing below the
+    # first path's siblings); every schedule still gives the sequential form
+    rng = np.random.default_rng(33)
+    graphs = [G.disjoint_union(G.random_regular(10, 3, rng), k) for k in (2, 3, 4)]
+    graphs += [G.cfi_graph(b, rng, twist=bool(b % 4)) for b in (6, 8, 12)]
+    graphs += [G.tree_plus_edges(n, rng) for n in (60, 150)] + [G.torus(6)]
+    for g in graphs:
+        ref = wm.canon(g)[0]
+        for workers in (2, 5, 16):
+            for seed in (0, 1, 2):
+                mat = wm.wide_model(g, workers, seed, gate=gate, donate=True)[0]
+                assert np.array_equal(mat, ref), (g.n, workers, seed)
+
+
+def test_wide_model_donation_splits_unions(G, wm):
+    # unions of identical components: a few items hold most of the tree;
+    # handing over children after a level's first child is done spreads them
+    rng = np.random.default_rng(3)
+    g = G.disjoint_union(G.random_regular(32, 3, rng), 5)
+    ref = wm.canon(g)[0]
+    r0, r1 = [], []
+    m0, nodes0, _, _ = wm.wide_model(g, 592, 0, cap=100000, gate=False, rounds=r0)
+    m1, nodes1, _, _ = wm.wide_model(g, 592, 0, cap=100000, gate=False, donate=True, rounds=r1)
+    assert np.array_equal(m0, ref) and np.array_equal(m1, ref)
+    assert r1[0] * 3 < r0[0] and nodes1 < nodes0
