@@ -49,6 +49,9 @@ extern "C" {
 #define GCL_GRAPH_OK 0
 #define GCL_GRAPH_BAD_INPUT 3
 #define GCL_GRAPH_TOO_LARGE 2
+#define GCL_GRAPH_INTERNAL 4  /* an internal consistency check failed: no result */
+#define GCL_GRAPH_TIMEOUT 5   /* the graph's time budget (GCL_GRAPH_BUDGET_S, default
+                                 600 s) ran out: no result                        */
 
 /* Largest vertex count the library canonizes. */
 #define GCL_MAX_N 65536
