@@ -628,6 +628,10 @@ int gcl_canon_wide_device_async(gcl_context* c, const int32_t* d_rowptr, const i
   WA.out_stats = d_out_stats;
   WA.out_status = d_out_status;
   cudaStream_t s = c->stream;
+  // the store's completion flags start clear: the buffer is reused across
+  // searches (and comes from the pool uninitialised), and a flag left set
+  // would let a reader take a slot that a writer has claimed but not filled
+  GCL_TRY(cudaMemsetAsync(WA.sh + WL.ready, 0, 4ull * cap, s));
   wide_first_kernel<<<1, 32, 0, s>>>(WA);
   GCL_TRY(cudaGetLastError());
   wide_items_kernel<<<(int)(warps / kSpWarps), kSpThreads, (size_t)(smw * kSpWarps), s>>>(WA);
