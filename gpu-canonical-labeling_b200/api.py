@@ -49,6 +49,7 @@ GCL_OPT_WIDE_MAX_WARPS = 3
 GCL_OPT_SMEM_STAGE = 4
 GCL_OPT_STREAM_PRIORITY = 5
 GCL_OPT_WIDE_GATE = 6
+GCL_OPT_WIDE_SHARE = 7
 GCL_MAX_N = 65536
 
 

@@ -59,6 +59,11 @@ struct WideHdr {
   int32_t orb_level;   // level index the orbit cache belongs to (-1 = none)
   uint32_t orb_known;  // store entries merged into the orbit cache
   uint32_t gate;       // the items kernel's level gate (1 on), set by the first kernel
+  // work sharing (the sharing items kernel only)
+  uint32_t busy;       // warps working on an item or a handed-over subtree
+  uint32_t hungry;     // warps waiting for a handed-over subtree
+  uint32_t qhead;      // handed-over subtrees taken
+  uint32_t qtail;      // handed-over subtrees published (slots claimed)
   unsigned long long nodes;
   unsigned long long t0;  // start time (globaltimer ns)
 };
@@ -66,11 +71,19 @@ struct WideHdr {
 // Byte layout of the device-wide region of one wide search.
 struct WideLayout {
   uint64_t hdr, fcode, fseq, flabel, fcert, lelem, linlev, lstb, tcfirst, tclen, cum;
-  uint64_t bcode, bseq, blabel, bcert, auts, ready, fixlev, orb, bytes;
+  uint64_t bcode, bseq, blabel, bcert, auts, ready, fixlev, orb, gq, gready, bytes;
   uint32_t cap, stride;
+  uint32_t qcap, gstride;  // handed-over subtrees: slots and words per slot (0 = none)
 };
 
-__host__ __device__ inline WideLayout wide_layout(uint32_t n, uint64_t m2, uint32_t cap) {
+// words of one handed-over subtree: its level L, the child v, the parent's
+// L-1 individualized vertices and its L codes (L <= n + 1)
+__host__ __device__ inline uint32_t wide_gift_words(uint32_t n) {
+  return ((2 * (n + 2) + 3) + 3) & ~3u;
+}
+
+__host__ __device__ inline WideLayout wide_layout(uint32_t n, uint64_t m2, uint32_t cap,
+                                                  uint32_t qcap = 0) {
   WideLayout L{};
   uint64_t o = 0;
   auto take = [&](uint64_t bytes) {
@@ -101,6 +114,10 @@ __host__ __device__ inline WideLayout wide_layout(uint32_t n, uint64_t m2, uint3
   L.ready = take(4ull * cap);
   L.fixlev = take(4ull * cap);
   L.orb = take(4 * N1);
+  L.qcap = qcap;
+  L.gstride = qcap ? wide_gift_words(n) : 0;
+  L.gq = take(4ull * qcap * L.gstride);
+  L.gready = take(4ull * qcap);
   L.bytes = o;
   return L;
 }
@@ -131,7 +148,7 @@ struct WidePtrs {
   WideHdr* H;
   int32_t *fcode, *bcode;
   uint32_t *fseq, *flabel, *fcert, *lelem, *linlev, *tcfirst, *tclen, *cum;
-  uint32_t *bseq, *blabel, *bcert, *ready, *fixlev, *orb;
+  uint32_t *bseq, *blabel, *bcert, *ready, *fixlev, *orb, *gq, *gready;
   uint64_t* lstb;
   uint16_t* auts;
 };
@@ -157,6 +174,8 @@ __device__ inline WidePtrs wide_ptrs(const WideArgs& A) {
   P.ready = (uint32_t*)(b + L.ready);
   P.fixlev = (uint32_t*)(b + L.fixlev);
   P.orb = (uint32_t*)(b + L.orb);
+  P.gq = (uint32_t*)(b + L.gq);
+  P.gready = (uint32_t*)(b + L.gready);
   P.lstb = (uint64_t*)(b + L.lstb);
   P.auts = (uint16_t*)(b + L.auts);
   return P;
@@ -189,6 +208,10 @@ __global__ void __launch_bounds__(32) wide_first_kernel(WideArgs A) {
     H->orb_lock = 0;
     H->orb_level = -1;
     H->orb_known = 0;
+    H->busy = 0;
+    H->hungry = 0;
+    H->qhead = 0;
+    H->qtail = 0;
     H->nodes = 1;
     H->t0 = global_ns();
   }
@@ -645,6 +668,251 @@ __device__ __noinline__ void wide_fix_init(uint32_t from, uint32_t to) {
   __syncwarp();
 }
 
+// ---------------------------------------------------------------------------
+// Work sharing inside items (the sharing items kernel).  A busy warp hands an
+// idle one the next untried child at the shallowest level of its item where
+// a child's subtree has already finished -- so the automorphisms that subtree
+// found prune the siblings before they leave -- and treats it as tried.  A
+// handed-over subtree is an entry of a device queue (its level L, the child,
+// the parent's vertices and codes); the receiver rebuilds the parent from the
+// first leaf and searches the child's subtree as it would an item's.  The
+// queue is never reused within a search (slots are taken in order and not
+// recycled), so a slot is written once and read once.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kGiftMaxWords = 1u << 26;  // 256 MiB of queue at most
+
+// Offer the next untried child of a level in [k+2, level) when warps are
+// waiting for work and the queue holds fewer entries than them.
+__device__ __noinline__ void wide_try_donate(const WidePtrs& P, const WideArgs& A, uint32_t k,
+                                             uint32_t level, int tcl) {
+  SpWarp& W = sp_w();
+  const uint32_t lane = lane_id();
+  WideHdr* H = P.H;
+  const uint32_t n = W.n;
+  uint32_t want = 0;
+  if (lane == 0) {
+    const uint32_t hungry = *(volatile uint32_t*)&H->hungry;
+    const uint32_t head = *(volatile uint32_t*)&H->qhead;
+    const uint32_t tail = *(volatile uint32_t*)&H->qtail;
+    want = hungry > tail - head && tail < A.WL.qcap;
+  }
+  if (!__shfl_sync(GCL_FULL, want, 0)) return;
+  for (uint32_t Lp = k + 2; Lp < level && (int)Lp <= tcl; ++Lp) {
+    const SpTc t = W.tc[Lp - 1];
+    if (t.counter >= n) continue;
+    // the child tried first is the cell's least vertex: while it is still the
+    // path's child at this level, its subtree has not finished
+    uint32_t least = kNone;
+    for (uint32_t q = lane; q < t.len; q += 32) least = min(least, W.elem[t.first + q]);
+    least = __reduce_min_sync(GCL_FULL, least);
+    if (W.seq[Lp - 1] == least) continue;
+    const uint32_t u = sp_next_rep(t);
+    if (u == kNone) continue;
+    uint32_t slot = kNone;
+    if (lane == 0) {
+      for (int tries = 0; tries < 64; ++tries) {
+        const uint32_t tl = *(volatile uint32_t*)&H->qtail;
+        if (tl >= A.WL.qcap) break;
+        if (atomicCAS(&H->qtail, tl, tl + 1) == tl) {
+          slot = tl;
+          break;
+        }
+      }
+    }
+    slot = __shfl_sync(GCL_FULL, slot, 0);
+    if (slot == kNone) return;
+    uint32_t* e = P.gq + (uint64_t)slot * A.WL.gstride;
+    const uint32_t np = A.n + 2;
+    if (lane == 0) {
+      e[0] = Lp;
+      e[1] = u;
+    }
+    for (uint32_t i = lane; i + 1 < Lp; i += 32) e[2 + i] = W.seq[i];
+    for (uint32_t i = lane; i < Lp; i += 32) e[2 + np + i] = (uint32_t)W.pathcode[i];
+    __threadfence();
+    __syncwarp();
+    if (lane == 0) {
+      W.tc[Lp - 1].counter = u + 1;  // tried: the receiver searches it
+      *(volatile uint32_t*)&P.gready[slot] = 1u;
+    }
+    __syncwarp();
+    return;
+  }
+}
+
+// Wait for a handed-over subtree.  1: its slot in *slot (the warp now counts
+// as busy); 0: the search is over (no warp busy and the queue empty); else a
+// status.  The busy count is read before the queue, so a subtree published by
+// a warp that then finished is seen.
+__device__ __noinline__ int32_t wide_take_gift(const WidePtrs& P, uint64_t deadline,
+                                               uint32_t* slot) {
+  WideHdr* H = P.H;
+  int32_t st = 0;
+  uint32_t got = kNone;
+  if (lane_id() == 0) {
+    atomicAdd(&H->hungry, 1u);
+    uint32_t sleep_ns = 512;
+    for (uint32_t i = 0;; ++i) {
+      const int32_t hs = *(volatile int32_t*)&H->status;
+      if (hs != kOk) {
+        st = hs;
+        break;
+      }
+      const uint32_t busy = *(volatile uint32_t*)&H->busy;
+      __threadfence();
+      const uint32_t head = *(volatile uint32_t*)&H->qhead;
+      const uint32_t tail = *(volatile uint32_t*)&H->qtail;
+      if (head < tail) {
+        if (atomicCAS(&H->qhead, head, head + 1) == head) {
+          got = head;
+          break;
+        }
+        continue;
+      }
+      if (busy == 0) break;  // st = 0: nothing left anywhere
+      if (i >= kWideGateSpinLimit || (deadline && (i & 15u) == 0 && global_ns() > deadline)) {
+        st = kTimeout;
+        break;
+      }
+      __nanosleep(sleep_ns);
+      if (sleep_ns < 32768) sleep_ns <<= 1;
+    }
+    if (got != kNone) {
+      atomicAdd(&H->busy, 1u);
+      // the publisher fills the slot after claiming it
+      uint32_t j = 0;
+      while (!*(volatile uint32_t*)&P.gready[got] && j < kWideSpinLimit) {
+        __nanosleep(64);
+        ++j;
+      }
+      if (j >= kWideSpinLimit) st = kTimeout;
+      else st = 1;
+      __threadfence();
+    }
+    atomicSub(&H->hungry, 1u);
+  }
+  st = __shfl_sync(GCL_FULL, st, 0);
+  *slot = __shfl_sync(GCL_FULL, got, 0);
+  return st;
+}
+
+// Rebuild the parent node of a handed-over subtree: the first leaf taken back
+// to the level its sequence shares with the first path, the rest of its
+// vertices individualized and refined (each code checked against the one the
+// giver saw).  Leaves W at the parent (level L = *k + 1) with W.seq, W.pathcode
+// and the target-cell headers of the replayed levels; *tf, *tl: the parent's
+// target cell; *v: the child; *eqlev: leading codes equal to the first path's.
+__device__ __noinline__ int32_t wide_gift_node(const WidePtrs& P, const WideArgs& A, uint32_t slot,
+                                               uint32_t D, uint32_t* k, uint32_t* tf,
+                                               uint32_t* tl, uint32_t* v, uint32_t* eqlev) {
+  SpWarp& W = sp_w();
+  const uint32_t lane = lane_id();
+  const uint32_t n = W.n, np = n + 2;
+  const uint32_t* e = P.gq + (uint64_t)slot * A.WL.gstride;
+  const uint32_t L = __ldcg(e), vv = __ldcg(e + 1);
+  if (L < 2 || L > n || vv >= n) return kInternal;
+  // levels shared with the first path: its first c vertices
+  const uint32_t lim = min(L - 1, D - 1);
+  uint32_t c = lim;
+  for (uint32_t j0 = 0; j0 < lim; j0 += 32) {
+    const uint32_t j = j0 + lane;
+    const uint32_t b = __ballot_sync(GCL_FULL, j < lim && __ldcg(e + 2 + j) != P.fseq[j]);
+    if (b) {
+      c = j0 + (uint32_t)(__ffs(b) - 1);
+      break;
+    }
+  }
+  for (uint32_t i = lane; i < n; i += 32) {
+    const uint32_t x = P.lelem[i];
+    W.elem[i] = x;
+    W.pos[x] = i;
+    W.inlev[i] = P.linlev[i];
+  }
+  for (uint32_t w = lane; w < W.nw; w += 32) W.stb[w] = P.lstb[w];
+  __syncwarp();
+  bm_resummarize(W.stb, W.sts, W.nw, W.nsw);
+  if (lane == 0) W.ncells = n;
+  __syncwarp();
+  if (!sp_backtrack(c + 1)) return kInternal;
+  for (uint32_t i = lane; i < c; i += 32) W.seq[i] = P.fseq[i];
+  for (uint32_t i = lane; i <= c; i += 32) W.pathcode[i] = P.fcode[i];
+  __syncwarp();
+  for (uint32_t lvl = c + 1; lvl < L; ++lvl) {
+    const uint32_t t = sp_first_nonsingleton();
+    if (t == kNone) return kInternal;
+    const uint32_t len = sp_cell_end(W, t) - t;
+    const uint32_t u = __ldcg(e + 2 + (lvl - 1));
+    if (u >= n || W.pos[u] < t || W.pos[u] >= t + len) return kInternal;
+    __syncwarp();
+    if (lane == 0) {
+      SpTc h;
+      h.first = t;
+      h.len = len;
+      h.counter = n;
+      h.last = 0;
+      h.rslot = -1;
+      h.pad = 0;
+      W.tc[lvl - 1] = h;
+      W.seq[lvl - 1] = u;
+    }
+    __syncwarp();
+    if (!sp_individualize(lvl, u, t)) return kInternal;
+    const int code = sp_refine(lvl);
+    if (code < 0 || (uint32_t)code != __ldcg(e + 2 + np + lvl)) return kInternal;
+    __syncwarp();
+    if (lane == 0) W.pathcode[lvl] = code;
+    __syncwarp();
+  }
+  const uint32_t t = sp_first_nonsingleton();
+  if (t == kNone) return kInternal;
+  const uint32_t len = sp_cell_end(W, t) - t;
+  if (W.pos[vv] < t || W.pos[vv] >= t + len) return kInternal;
+  uint32_t q = min(L, D);
+  for (uint32_t j0 = 0; j0 < min(L, D); j0 += 32) {
+    const uint32_t j = j0 + lane;
+    const uint32_t b = __ballot_sync(GCL_FULL, j < min(L, D) && W.pathcode[j] != W.fcode[j]);
+    if (b) {
+      q = j0 + (uint32_t)(__ffs(b) - 1);
+      break;
+    }
+  }
+  *k = L - 1;
+  *tf = t;
+  *tl = len;
+  *v = vv;
+  *eqlev = q;
+  return kOk;
+}
+
+// Least vertex of v's orbit in the parent's target cell [tf, tf+tl) under the
+// known automorphisms that fix the parent's k vertices W.seq[0..k), in the
+// warp's own union-find; stops at the first smaller root.
+__device__ __noinline__ uint32_t wide_gift_orbit_min(const WidePtrs& P, uint32_t v, uint32_t k,
+                                                     uint32_t tf, uint32_t tl, uint32_t known,
+                                                     uint32_t stride, bool* ok) {
+  SpWarp& W = sp_w();
+  const uint32_t lane = lane_id();
+  const uint32_t n = W.n;
+  for (uint32_t x = lane; x < n; x += 32) W.dsu[x] = x;
+  __syncwarp();
+  uint32_t r = v;
+  for (uint32_t a = 0; a < known && r == v; ++a) {
+    const uint16_t* pm = P.auts + (uint64_t)a * stride;
+    bool moves = false;
+    for (uint32_t i = lane; i < k; i += 32) moves |= __ldcg(pm + W.seq[i]) != W.seq[i];
+    if (__any_sync(GCL_FULL, moves)) continue;
+    if (!sp_dsu_apply<true>(pm, W.elem + tf, tl, n)) {
+      *ok = false;
+      break;
+    }
+    uint32_t x = v;
+    if (lane == 0) x = sp_find(W.dsu, v, n);
+    r = __shfl_sync(GCL_FULL, x, 0);
+  }
+  return r;
+}
+
+template <bool kShare>
 __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
   extern __shared__ __align__(16) uint8_t sp_dyn[];
   const int warp = (int)(threadIdx.x >> 5);
@@ -694,8 +962,44 @@ __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
     uint32_t it = 0;
     if (lane == 0) it = atomicAdd(&H->next_item, 1u);
     it = __shfl_sync(GCL_FULL, it, 0);
-    if (it >= nitems) break;
+    bool gift = false;
+    uint32_t k = 0, tf = 0, tl = 0, v = 0, gift_eq = 0;
+    bool skip = false;
+    if (it >= nitems) {
+      if constexpr (!kShare) {
+        break;
+      } else {
+        // no item left: wait for a subtree another warp hands over
+        uint32_t slot = 0;
+        const int32_t gs = wide_take_gift(P, deadline, &slot);
+        if (gs == 0) break;
+        if (gs != 1) {
+          status = gs;
+          break;
+        }
+        gift = true;
+        const int32_t ns = wide_gift_node(P, A, slot, D, &k, &tf, &tl, &v, &gift_eq);
+        if (ns != kOk) {
+          status = ns;
+          break;
+        }
+        known = wide_ready_prefix(P, known, cap);
+        if (known) {
+          bool ok = true;
+          const uint32_t r = wide_gift_orbit_min(P, v, k, tf, tl, known, A.WL.stride, &ok);
+          if (!ok) {
+            status = kTimeout;
+            break;
+          }
+          skip = r != v;
+        }
+      }
+    }
     if (*(volatile int32_t*)&H->status != kOk) break;
+    if (!gift) {
+      if constexpr (kShare) {
+        if (lane == 0) atomicAdd(&H->busy, 1u);
+      }
     // item -> level (cum is ascending over levels taken deepest first)
     uint32_t lo = 0, hi = D - 1;  // cum[lo] <= it < cum[hi]
     while (hi - lo > 1) {
@@ -705,9 +1009,10 @@ __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
       else
         hi = mid;
     }
-    const uint32_t k = D - 2 - lo;  // parent node level k+1, its target cell index k
-    const uint32_t tf = P.tcfirst[k], tl = P.tclen[k];
-    const uint32_t v = P.lelem[tf + 1 + (it - P.cum[lo])];
+    k = D - 2 - lo;  // parent node level k+1, its target cell index k
+    tf = P.tcfirst[k];
+    tl = P.tclen[k];
+    v = P.lelem[tf + 1 + (it - P.cum[lo])];
     if (H->gate) {
       const int32_t gs = wide_gate(H, P.cum[lo], deadline);
       if (gs != kOk) {
@@ -716,7 +1021,6 @@ __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
       }
     }
     known = wide_ready_prefix(P, known, cap);
-    bool skip = false;
     if (known) {
       bool ok = true;
       const uint32_t r = H->gate ? wide_orbit_min(P, v, lo, k, tf, tl, known, A.WL.stride, &ok)
@@ -727,8 +1031,10 @@ __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
       }
       skip = r != v;  // an equivalent sibling is covered by its orbit's least vertex
     }
+    }
     do {
     if (skip) break;
+    if (!gift) {
     // the parent node: the first leaf backtracked to level k+1
     for (uint32_t i = lane; i < n; i += 32) {
       const uint32_t e = P.lelem[i];
@@ -754,10 +1060,18 @@ __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
     for (uint32_t i = lane; i < k; i += 32) W.seq[i] = P.fseq[i];
     for (uint32_t i = lane; i <= k; i += 32) W.pathcode[i] = P.fcode[i];
     __syncwarp();
+    } else {
+      if (lane == 0) {  // the subtree's DFS logs its changes from here
+        W.utop = 0;
+        W.ulog_bad = 0;
+      }
+      __syncwarp();
+    }
     // the previous item's sequence shares the first path's first
-    // min(k, prev_k) vertices with this one
-    sp_fix_clamp(min(k, prev_k), fix_init);
-    prev_k = k;
+    // min(k, prev_k) vertices with this one (a handed-over subtree's
+    // sequence may share none)
+    sp_fix_clamp(gift ? 0u : min(k, prev_k), fix_init);
+    prev_k = gift ? 0u : k;
     if (lane == 0) {
       SpTc h;
       h.first = tf;
@@ -775,8 +1089,9 @@ __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
       status = kTimeout;
       break;
     }
-    bool best_local = best.version == 0;  // the first leaf anchors gca jumps
-    uint32_t eqlevfirst = k + 1, seqlen = k, level = k + 1;
+    // the first leaf anchors gca jumps (not for a handed-over subtree)
+    bool best_local = !gift && best.version == 0;
+    uint32_t eqlevfirst = gift ? gift_eq : k + 1, seqlen = k, level = k + 1;
     int eqlevcanon = 0, comp_canon = 0, tcl = (int)k + 1;
     wide_recompare(k + 1, best.canon_level, &eqlevcanon, &comp_canon);
     // the item's node
@@ -802,6 +1117,9 @@ __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
           __shfl_sync(GCL_FULL, lane == 0 ? global_ns() : 0ull, 0) > deadline) {
         status = kTimeout;
         break;
+      }
+      if constexpr (kShare) {
+        if (!have_node && (iter & 7) == 0) wide_try_donate(P, A, k, level, tcl);
       }
       int bt = -1;
       bool recompare = false;
@@ -991,7 +1309,13 @@ __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
     } while (0);
     if (status != kOk) break;
     __syncwarp();
-    if (lane == 0) atomicAdd(&H->done, 1u);  // opens the next level's gate when it is the last
+    if (lane == 0) {
+      if (!gift) atomicAdd(&H->done, 1u);  // opens the next level's gate when it is the last
+      if constexpr (kShare) {
+        __threadfence();  // what this warp handed over is published before it stops counting
+        atomicSub(&H->busy, 1u);
+      }
+    }
     __syncwarp();
   }
   if (status != kOk) wide_fail(H, status);

@@ -236,6 +236,7 @@ struct gcl_context {
   int64_t wide_max_warps = 0;    // 0 = as many as fit
   bool smem_stage = true;        // sparse and wide kernels stage per-step arrays in shared memory
   int wide_gate = 1;             // wide search's level gate: 1 on, 0 off, 2 automatic
+  bool wide_share = false;       // wide search: busy warps hand subtrees to idle ones
   // launch shape per size bucket (gcl_autotune / gcl_set_tuning): 0 / -1 = default
   int w64_per_sm = 0;            // resident blocks the warp kernel's occupancy allows
   int tune_w64_bps = 0;
@@ -340,7 +341,10 @@ int gcl_create(int device, gcl_context** out) try {
     e = cudaFuncSetAttribute(sp_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              kSpSmemPerBlock);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(wide_items_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(wide_items_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             kSpSmemPerBlock);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(wide_items_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              kSpSmemPerBlock);
   if (e != cudaSuccess) {
     c->deferred.release();
@@ -559,6 +563,10 @@ int gcl_set_option(gcl_context* c, int option, int64_t value) {
       if (value < 0 || value > 2) return GCL_ERR_ARG;
       c->wide_gate = (int)value;
       return GCL_OK;
+    case GCL_OPT_WIDE_SHARE:
+      if (value != 0 && value != 1) return GCL_ERR_ARG;
+      c->wide_share = value != 0;
+      return GCL_OK;
     case GCL_OPT_STREAM_PRIORITY: {
       if (value != 0 && value != 1) return GCL_ERR_ARG;
       int lo = 0, hi = 0;
@@ -590,13 +598,19 @@ int gcl_canon_wide_device_async(gcl_context* c, const int32_t* d_rowptr, const i
   const uint32_t un = (uint32_t)n;
   const uint64_t m2 = (uint64_t)std::max<int64_t>(m, 1);
   const uint32_t cap = wide_store_cap(un, max_aut);
-  const WideLayout WL = wide_layout(un, m2, cap);
+  // work sharing: a queue of handed-over subtrees, never recycled within a
+  // search, of at most 65,536 entries and 256 MiB
+  const uint32_t qcap = c->wide_share
+                            ? (uint32_t)std::min<uint64_t>(65536, kGiftMaxWords / wide_gift_words(un))
+                            : 0u;
+  const WideLayout WL = wide_layout(un, m2, cap, qcap);
   const SpLayout Lo = sp_layout(un, m2, kWidePool, 0, std::min<uint32_t>(cap, kWideFixCap));
   uint64_t smw = c->smem_stage ? sp_smem_bytes(un) : 0;
   if (smw * kSpWarps > (uint64_t)kSpSmemPerBlock) smw = 0;
   int per_sm = 0;
-  GCL_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, wide_items_kernel, kSpThreads,
-                                                        (size_t)(smw * kSpWarps)));
+  GCL_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &per_sm, c->wide_share ? wide_items_kernel<true> : wide_items_kernel<false>, kSpThreads,
+      (size_t)(smw * kSpWarps)));
   const uint64_t budget = ctx_workspace(c);
   int64_t warps = std::min<int64_t>((int64_t)c->sms * std::max(per_sm, 1) * kSpWarps,
                                     std::max<int64_t>(kSpWarps, (int64_t)(budget / Lo.bytes)));
@@ -632,9 +646,13 @@ int gcl_canon_wide_device_async(gcl_context* c, const int32_t* d_rowptr, const i
   // searches (and comes from the pool uninitialised), and a flag left set
   // would let a reader take a slot that a writer has claimed but not filled
   GCL_TRY(cudaMemsetAsync(WA.sh + WL.ready, 0, 4ull * cap, s));
+  if (qcap) GCL_TRY(cudaMemsetAsync(WA.sh + WL.gready, 0, 4ull * qcap, s));
   wide_first_kernel<<<1, 32, 0, s>>>(WA);
   GCL_TRY(cudaGetLastError());
-  wide_items_kernel<<<(int)(warps / kSpWarps), kSpThreads, (size_t)(smw * kSpWarps), s>>>(WA);
+  if (c->wide_share)
+    wide_items_kernel<true><<<(int)(warps / kSpWarps), kSpThreads, (size_t)(smw * kSpWarps), s>>>(WA);
+  else
+    wide_items_kernel<false><<<(int)(warps / kSpWarps), kSpThreads, (size_t)(smw * kSpWarps), s>>>(WA);
   GCL_TRY(cudaGetLastError());
   wide_finish_kernel<<<1, 32, 0, s>>>(WA);
   GCL_TRY(cudaGetLastError());

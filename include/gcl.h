@@ -104,6 +104,14 @@ void* gcl_stream(gcl_context* ctx);
  *   chooses per search: off when the first path's levels hold fewer than 4
  *   items each on average, else on (decided on the device after the first
  *   path).  Values other than 1 are not yet measured on a GPU.
+ * GCL_OPT_WIDE_SHARE: 1 lets a busy warp of the wide search hand an idle
+ *   one an untried child below its first-path sibling -- at the shallowest
+ *   level where a child's subtree has already finished, so that the
+ *   automorphisms found there prune the siblings first -- through a device
+ *   queue (up to 65,536 entries, 256 MiB); the receiver rebuilds the parent
+ *   from the first leaf.  Same canonical form.  For trees whose work sits in
+ *   a few siblings (unions of identical components).  Default 0.  Not yet
+ *   measured on a GPU.
  * Returns GCL_ERR_ARG for an unknown option or value. */
 #define GCL_OPT_WIDE_MIN_N 1
 #define GCL_OPT_WORKSPACE_BYTES 2
@@ -111,6 +119,7 @@ void* gcl_stream(gcl_context* ctx);
 #define GCL_OPT_SMEM_STAGE 4
 #define GCL_OPT_STREAM_PRIORITY 5
 #define GCL_OPT_WIDE_GATE 6
+#define GCL_OPT_WIDE_SHARE 7
 int gcl_set_option(gcl_context* ctx, int option, int64_t value);
 
 /* ---- one graph (drop-in for Nauty_Parallel, src/nauty_parallel.h:9-13) ---

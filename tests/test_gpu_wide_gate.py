@@ -71,3 +71,31 @@ def test_gate_auto_vs_oracle(pkg, G, oracle_mod):
     graphs += [G.torus(12), G.random_regular(300, 3, rng), G.cfi_graph(10, rng)]
     for g in graphs:
         assert np.array_equal(pkg.canon(g, ctx=ctx).matrix, oracle_mod.canon(g)[0])
+
+
+@pytest.mark.parametrize("gate", [1, 0])
+def test_work_sharing_vs_oracle(pkg, G, oracle_mod, gate):
+    # GCL_OPT_WIDE_SHARE: busy warps hand subtrees to idle ones; unions of
+    # identical components keep most of their tree in a few siblings
+    import time
+    rng = np.random.default_rng(44)
+    ctx = pkg.Context(0, wide_min_n=1)
+    ctx.set_option(pkg.api.GCL_OPT_WIDE_GATE, gate)
+    ctx.set_option(pkg.api.GCL_OPT_WIDE_SHARE, 1)
+    plain = pkg.Context(0, wide_min_n=1)
+    plain.set_option(pkg.api.GCL_OPT_WIDE_GATE, gate)
+    comp = G.random_regular(32, 3, rng)
+    graphs = [G.disjoint_union(comp, k) for k in (2, 3, 4, 5)]
+    graphs += [G.cfi_graph(b, rng) for b in (8, 16)] + [G.torus(10), G.tree_plus_edges(400, rng)]
+    graphs += G.small_batch(40, seed=44)
+    for g in graphs:
+        want = oracle_mod.canon(g)[0]
+        t = time.perf_counter()
+        a = pkg.canon(g, ctx=ctx).matrix
+        t_share = time.perf_counter() - t
+        t = time.perf_counter()
+        b = pkg.canon(g, ctx=plain).matrix
+        t_plain = time.perf_counter() - t
+        assert np.array_equal(a, want) and np.array_equal(b, want), g.n
+        if g.n >= 96:
+            print(f"n={g.n}: sharing {t_share * 1e3:.1f} ms, without {t_plain * 1e3:.1f} ms")
