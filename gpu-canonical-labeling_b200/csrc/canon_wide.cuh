@@ -1000,66 +1000,66 @@ __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
       if constexpr (kShare) {
         if (lane == 0) atomicAdd(&H->busy, 1u);
       }
-    // item -> level (cum is ascending over levels taken deepest first)
-    uint32_t lo = 0, hi = D - 1;  // cum[lo] <= it < cum[hi]
-    while (hi - lo > 1) {
-      const uint32_t mid = (lo + hi) >> 1;
-      if (P.cum[mid] <= it)
-        lo = mid;
-      else
-        hi = mid;
-    }
-    k = D - 2 - lo;  // parent node level k+1, its target cell index k
-    tf = P.tcfirst[k];
-    tl = P.tclen[k];
-    v = P.lelem[tf + 1 + (it - P.cum[lo])];
-    if (H->gate) {
-      const int32_t gs = wide_gate(H, P.cum[lo], deadline);
-      if (gs != kOk) {
-        status = gs;
-        break;
+      // item -> level (cum is ascending over levels taken deepest first)
+      uint32_t lo = 0, hi = D - 1;  // cum[lo] <= it < cum[hi]
+      while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (P.cum[mid] <= it)
+          lo = mid;
+        else
+          hi = mid;
       }
-    }
-    known = wide_ready_prefix(P, known, cap);
-    if (known) {
-      bool ok = true;
-      const uint32_t r = H->gate ? wide_orbit_min(P, v, lo, k, tf, tl, known, A.WL.stride, &ok)
-                                : wide_orbit_min_own(P, v, k, tf, tl, known, A.WL.stride, &ok);
-      if (!ok) {
-        status = kTimeout;
-        break;
+      k = D - 2 - lo;  // parent node level k+1, its target cell index k
+      tf = P.tcfirst[k];
+      tl = P.tclen[k];
+      v = P.lelem[tf + 1 + (it - P.cum[lo])];
+      if (H->gate) {
+        const int32_t gs = wide_gate(H, P.cum[lo], deadline);
+        if (gs != kOk) {
+          status = gs;
+          break;
+        }
       }
-      skip = r != v;  // an equivalent sibling is covered by its orbit's least vertex
-    }
+      known = wide_ready_prefix(P, known, cap);
+      if (known) {
+        bool ok = true;
+        const uint32_t r = H->gate ? wide_orbit_min(P, v, lo, k, tf, tl, known, A.WL.stride, &ok)
+                                  : wide_orbit_min_own(P, v, k, tf, tl, known, A.WL.stride, &ok);
+        if (!ok) {
+          status = kTimeout;
+          break;
+        }
+        skip = r != v;  // an equivalent sibling is covered by its orbit's least vertex
+      }
     }
     do {
     if (skip) break;
     if (!gift) {
-    // the parent node: the first leaf backtracked to level k+1
-    for (uint32_t i = lane; i < n; i += 32) {
-      const uint32_t e = P.lelem[i];
-      W.elem[i] = e;
-      W.pos[e] = i;
-      W.inlev[i] = P.linlev[i];
-    }
-    for (uint32_t w = lane; w < W.nw; w += 32) W.stb[w] = P.lstb[w];
-    __syncwarp();
-    bm_resummarize(W.stb, W.sts, W.nw, W.nsw);
-    if (lane == 0) W.ncells = n;
-    __syncwarp();
-    if (!sp_backtrack(k + 1) || sp_cell_end(W, tf) - tf != tl) {
-      status = kInternal;
-      break;
-    }
-    __syncwarp();
-    if (lane == 0) {  // the item's DFS logs its changes from here
-      W.utop = 0;
-      W.ulog_bad = 0;
-    }
-    __syncwarp();
-    for (uint32_t i = lane; i < k; i += 32) W.seq[i] = P.fseq[i];
-    for (uint32_t i = lane; i <= k; i += 32) W.pathcode[i] = P.fcode[i];
-    __syncwarp();
+      // the parent node: the first leaf backtracked to level k+1
+      for (uint32_t i = lane; i < n; i += 32) {
+        const uint32_t e = P.lelem[i];
+        W.elem[i] = e;
+        W.pos[e] = i;
+        W.inlev[i] = P.linlev[i];
+      }
+      for (uint32_t w = lane; w < W.nw; w += 32) W.stb[w] = P.lstb[w];
+      __syncwarp();
+      bm_resummarize(W.stb, W.sts, W.nw, W.nsw);
+      if (lane == 0) W.ncells = n;
+      __syncwarp();
+      if (!sp_backtrack(k + 1) || sp_cell_end(W, tf) - tf != tl) {
+        status = kInternal;
+        break;
+      }
+      __syncwarp();
+      if (lane == 0) {  // the item's DFS logs its changes from here
+        W.utop = 0;
+        W.ulog_bad = 0;
+      }
+      __syncwarp();
+      for (uint32_t i = lane; i < k; i += 32) W.seq[i] = P.fseq[i];
+      for (uint32_t i = lane; i <= k; i += 32) W.pathcode[i] = P.fcode[i];
+      __syncwarp();
     } else {
       if (lane == 0) {  // the subtree's DFS logs its changes from here
         W.utop = 0;
