@@ -73,6 +73,44 @@ def test_gate_auto_vs_oracle(pkg, G, oracle_mod):
         assert np.array_equal(pkg.canon(g, ctx=ctx).matrix, oracle_mod.canon(g)[0])
 
 
+def _wide_direct(pkg, ctx, g):
+    """The wide search through the device entry point, which has no
+    fallback: (status, n x n matrix)."""
+    import ctypes
+    dev = torch.device("cuda", 0)
+    P = ctypes.c_void_p
+    lib = pkg.api.load_library()
+    n = g.n
+    rp = torch.from_numpy(np.ascontiguousarray(g.rowptr, np.int32)).to(dev)
+    cl = torch.from_numpy(np.ascontiguousarray(g.col if g.col.size else np.zeros(1), np.int32)).to(dev)
+    co = None if g.color is None else torch.from_numpy(np.ascontiguousarray(g.color, np.int32)).to(dev)
+    dense = torch.zeros(max(n * n, 1), dtype=torch.uint8, device=dev)
+    status = torch.full((1,), -1, dtype=torch.int32, device=dev)
+    rc = lib.gcl_canon_wide_device_async(ctx.handle, P(rp.data_ptr()), P(cl.data_ptr()),
+                                         None if co is None else P(co.data_ptr()), n,
+                                         int(g.col.size), 10000, P(dense.data_ptr()), None, None,
+                                         None, P(status.data_ptr()))
+    assert rc == 0
+    ctx.sync()
+    return int(status.item()), dense[:n * n].cpu().numpy().reshape(n, n)
+
+
+@pytest.mark.parametrize("gate", [1, 0, 2])
+def test_work_sharing_no_fallback(pkg, G, oracle_mod, gate):
+    # through the device entry point: a hand-over that failed would show as a
+    # status here instead of being covered by the host's sequential fallback
+    rng = np.random.default_rng(45)
+    ctx = pkg.Context(0, wide_min_n=1)
+    ctx.set_option(pkg.api.GCL_OPT_WIDE_GATE, gate)
+    ctx.set_option(pkg.api.GCL_OPT_WIDE_SHARE, 1)
+    comp = G.random_regular(24, 3, rng)
+    for g in [G.disjoint_union(comp, k) for k in (2, 3, 4, 5)] + [G.cfi_graph(10, rng),
+                                                                   G.tree_plus_edges(300, rng)]:
+        st, mat = _wide_direct(pkg, ctx, g)
+        assert st == 0, (g.n, st)
+        assert np.array_equal(mat, oracle_mod.canon(g)[0]), g.n
+
+
 @pytest.mark.parametrize("gate", [1, 0])
 def test_work_sharing_vs_oracle(pkg, G, oracle_mod, gate):
     # GCL_OPT_WIDE_SHARE: busy warps hand subtrees to idle ones; unions of
