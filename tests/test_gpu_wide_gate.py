@@ -95,14 +95,16 @@ def _wide_direct(pkg, ctx, g):
     return int(status.item()), dense[:n * n].cpu().numpy().reshape(n, n)
 
 
+@pytest.mark.parametrize("share", [0, 1])
 @pytest.mark.parametrize("gate", [1, 0, 2])
-def test_work_sharing_no_fallback(pkg, G, oracle_mod, gate):
-    # through the device entry point: a hand-over that failed would show as a
-    # status here instead of being covered by the host's sequential fallback
+def test_gate_and_sharing_no_fallback(pkg, G, oracle_mod, gate, share):
+    # through the device entry point: a search that failed (a hand-over, the
+    # own-union-find orbit test) would show as a status here instead of being
+    # covered by the host's sequential fallback
     rng = np.random.default_rng(45)
     ctx = pkg.Context(0, wide_min_n=1)
     ctx.set_option(pkg.api.GCL_OPT_WIDE_GATE, gate)
-    ctx.set_option(pkg.api.GCL_OPT_WIDE_SHARE, 1)
+    ctx.set_option(pkg.api.GCL_OPT_WIDE_SHARE, share)
     comp = G.random_regular(24, 3, rng)
     for g in [G.disjoint_union(comp, k) for k in (2, 3, 4, 5)] + [G.cfi_graph(10, rng),
                                                                    G.tree_plus_edges(300, rng)]:
