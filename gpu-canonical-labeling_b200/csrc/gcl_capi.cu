@@ -972,8 +972,13 @@ int gcl_group_order(gcl_context* c, const int32_t* rowptr, const int32_t* col,
     GCL_TRY(cudaStreamSynchronize(s));
     const int rg = group_order_with_base(un, auts.data(), (uint64_t)st[0], WL.stride, base.data(),
                                          D - 1, kGroupWorkCap, &lg, &d, &base_len);
-    if (rg == kOrderWorkCap) return GCL_ERR_TIMEOUT;
-    if (rg != kOrderOk) return GCL_ERR_INTERNAL;
+    if (rg == kOrderNotABase) return GCL_ERR_INTERNAL;
+    // long bases with large orbits (S_n-like): the stored automorphisms are a
+    // strong generating set for the first path, whose basic orbits give the order
+    if (rg == kOrderWorkCap &&
+        !group_order_base_orbits(un, auts.data(), (uint64_t)st[0], WL.stride, base.data(), D - 1,
+                                 &lg, &d))
+      return GCL_ERR_TIMEOUT;
   }
   return put(d, lg, st[0]);
 } GCL_CATCH_ALL

@@ -386,6 +386,50 @@ bool group_order(uint32_t n, const uint16_t* auts, uint64_t count, uint64_t stri
   return run(C, auts, count, stride, log10_order, digits, base_len) == kOrderOk;
 }
 
+bool group_order_base_orbits(uint32_t n, const uint16_t* auts, uint64_t count, uint64_t stride,
+                             const uint32_t* base, uint32_t nbase, double* log10_order,
+                             std::string* digits) {
+  // level of each automorphism: the first base point it moves (nbase: none)
+  std::vector<uint32_t> lev(count);
+  std::vector<std::vector<uint64_t>> at(nbase);
+  for (uint64_t a = 0; a < count; ++a) {
+    const uint16_t* pm = auts + a * stride;
+    uint32_t j = 0;
+    while (j < nbase && pm[base[j]] == base[j]) ++j;
+    if (j < nbase) at[j].push_back(a);
+  }
+  // deepest level first: the generators fixing b_0..b_{i-1} are those of
+  // levels >= i, so each level adds its own to one running union-find
+  std::vector<uint32_t> par(n), size(n, 1);
+  for (uint32_t x = 0; x < n; ++x) par[x] = x;
+  auto find = [&](uint32_t x) {
+    while (par[x] != x) {
+      par[x] = par[par[x]];
+      x = par[x];
+    }
+    return x;
+  };
+  std::vector<uint64_t> f(nbase, 1);
+  for (uint32_t i = nbase; i-- > 0;) {
+    for (uint64_t a : at[i]) {
+      const uint16_t* pm = auts + a * stride;
+      for (uint32_t x = 0; x < n; ++x) {
+        uint32_t rx = find(x), ry = find(pm[x]);
+        if (rx == ry) continue;
+        if (size[rx] < size[ry]) std::swap(rx, ry);
+        par[ry] = rx;
+        size[rx] += size[ry];
+      }
+    }
+    f[i] = size[find(base[i])];
+  }
+  double lg = 0;
+  for (uint64_t x : f) lg += std::log10((double)x);
+  *log10_order = lg;
+  *digits = big_product(f);
+  return true;
+}
+
 int group_order_with_base(uint32_t n, const uint16_t* auts, uint64_t count, uint64_t stride,
                           const uint32_t* base, uint32_t nbase, uint64_t work_cap,
                           double* log10_order, std::string* digits, uint64_t* base_len) {

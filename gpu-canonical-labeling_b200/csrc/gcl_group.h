@@ -28,4 +28,16 @@ int group_order_with_base(uint32_t n, const uint16_t* auts, uint64_t count, uint
                           const uint32_t* base, uint32_t nbase, uint64_t work_cap,
                           double* log10_order, std::string* digits, uint64_t* base_len);
 
+// The order as the product over the first path's levels of the orbit of its
+// vertex b_i under the stored automorphisms that fix b_0..b_{i-1} -- the
+// search's group order (nauty's grpsize).  Valid for automorphisms a complete
+// search stored, all of them: every first-path sibling in the orbit of b_i is
+// either searched, and a leaf equivalent to the first leaf under it gives an
+// automorphism fixing b_0..b_{i-1} that moves b_i there, or skipped as
+// equivalent to one that is; so these automorphisms form a strong generating
+// set for that base.  O(stored x n).
+bool group_order_base_orbits(uint32_t n, const uint16_t* auts, uint64_t count, uint64_t stride,
+                             const uint32_t* base, uint32_t nbase, double* log10_order,
+                             std::string* digits);
+
 }  // namespace gcl

@@ -27,6 +27,14 @@ extern "C" int order_generic(unsigned n, const unsigned short* a, unsigned long 
   std::memcpy(out, d.c_str(), d.size() + 1);
   return 0;
 }
+extern "C" int order_orbits(unsigned n, const unsigned short* a, unsigned long long count,
+                            const unsigned* base, unsigned nbase, char* out, int out_cap) {
+  double lg; std::string d;
+  if (!gcl::group_order_base_orbits(n, a, count, n, base, nbase, &lg, &d)) return 1;
+  if ((int)d.size() + 1 > out_cap) return 3;
+  std::memcpy(out, d.c_str(), d.size() + 1);
+  return 0;
+}
 extern "C" int order_base(unsigned n, const unsigned short* a, unsigned long long count,
                           const unsigned* base, unsigned nbase, unsigned long long cap,
                           char* out, int out_cap) {
@@ -56,6 +64,8 @@ def grp(tmp_path_factory):
                                   ctypes.c_char_p, ctypes.c_int]
     lib.order_base.argtypes = [ctypes.c_uint, P, ctypes.c_ulonglong, P, ctypes.c_uint,
                                ctypes.c_ulonglong, ctypes.c_char_p, ctypes.c_int]
+    lib.order_orbits.argtypes = [ctypes.c_uint, P, ctypes.c_ulonglong, P, ctypes.c_uint,
+                                 ctypes.c_char_p, ctypes.c_int]
 
     def generic(perms, cap=0):
         p = np.ascontiguousarray(perms, dtype=np.uint16)
@@ -71,6 +81,14 @@ def grp(tmp_path_factory):
         rc = lib.order_base(p.shape[1], p.ctypes.data if p.size else None, p.shape[0],
                             b.ctypes.data if b.size else None, b.size, cap, buf, len(buf))
         return rc, (int(buf.value.decode()) if rc == 0 else None)
+    def orbits(perms, base):
+        p = np.ascontiguousarray(perms, dtype=np.uint16)
+        b = np.ascontiguousarray(base, dtype=np.uint32)
+        buf = ctypes.create_string_buffer(1 << 16)
+        rc = lib.order_orbits(p.shape[1], p.ctypes.data if p.size else None, p.shape[0],
+                              b.ctypes.data if b.size else None, b.size, buf, len(buf))
+        return rc, (int(buf.value.decode()) if rc == 0 else None)
+    based.orbits = orbits
     return generic, based
 
 
@@ -105,8 +123,37 @@ def test_known_base_matches_general_completion(G, wm, grp):
         store, fs = _model(wm, g, seed=i)
         rc1, a = generic(store)
         rc2, b = based(store, fs)
-        assert rc1 == 0 and rc2 == 0, (i, rc1, rc2)
-        assert a == b, (i, g.n, a, b)
+        rc3, c = based.orbits(store, fs)
+        assert rc1 == 0 and rc2 == 0 and rc3 == 0, (i, rc1, rc2, rc3)
+        assert a == b == c, (i, g.n, a, b, c)
+
+
+def test_base_orbit_product_on_every_schedule(G, wm, grp):
+    # the stored automorphisms of any schedule (gate on or off, work handed
+    # over or not) are a strong generating set for the first path: the product
+    # of its basic orbits equals the Schreier-Sims order
+    generic, based = grp
+    rng = np.random.default_rng(19)
+    graphs = [G.torus(4, 6), G.cfi_graph(6, rng), G.disjoint_union(G.random_regular(8, 3, rng), 3)]
+    graphs += [G.from_edges(10, [])] + list(G.small_batch(20, seed=19))
+    for i, g in enumerate(graphs):
+        for workers, seed, gate, donate in ((1, 0, True, False), (5, 3, False, False),
+                                            (9, 7, True, True), (4, 2, False, True)):
+            fs = []
+            _, _, naut, _, store = wm.wide_model(g, workers, seed, cap=100000, auts=True,
+                                                 first_seq=fs, gate=gate, donate=donate)
+            rc, a = generic(store)
+            rc2, c = based.orbits(store, fs)
+            assert rc == 0 and rc2 == 0 and a == c, (i, workers, seed, gate, donate, a, c)
+
+
+def test_base_orbit_product_for_a_large_symmetric_group(G, wm, grp):
+    # S_120 (the empty graph): instant from the basic orbits
+    import math
+    _, based = grp
+    store, fs = _model(wm, G.from_edges(120, []))
+    rc, c = based.orbits(store, fs)
+    assert rc == 0 and c == math.factorial(120)
 
 
 def test_known_base_finishes_where_representatives_do_not_fit(grp):
