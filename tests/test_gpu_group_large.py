@@ -23,3 +23,10 @@ def test_group_order_large_vertex_transitive(pkg, G):
     cube = G.from_edges(1 << d, [(a, a ^ (1 << b)) for a in range(1 << d) for b in range(d)
                                  if a < a ^ (1 << b)])
     assert pkg.group_order(cube, ctx=ctx) == (1 << d) * math.factorial(d)
+
+
+def test_group_order_long_base(pkg, G):
+    # S_600: both Schreier-Sims budgets run out; the first path's basic
+    # orbits give the order
+    ctx = pkg.Context(0)
+    assert pkg.group_order(G.from_edges(600, []), ctx=ctx) == math.factorial(600)
