@@ -87,6 +87,13 @@ def parse():
                    help="server large_n (0 = the library default)")
     p.add_argument("--serve-big-wide", action="store_true",
                    help="server big_wide: big requests through the wide search")
+    p.add_argument("--single-gate", type=int, default=1, choices=(0, 1, 2),
+                   help="level gate of the single-graph block's wide searches")
+    p.add_argument("--single-share", action="store_true",
+                   help="work sharing in the single-graph block's wide searches")
+    p.add_argument("--single-extra", action="store_true",
+                   help="add a tree of 2,048 vertices and a union of five cubic graphs "
+                        "to the single-graph block")
     p.add_argument("--serve-plain", type=int, default=800,
                    help="requests replayed through the plain one-graph-per-launch form")
     p.add_argument("--no-single", action="store_true")
@@ -683,7 +690,14 @@ def single_graph_block(args, pkg, local, with_cpu):
     cases = [("reg3_n1024", G.random_regular(1024, 3, rng), True),
              ("reg3_n4096", G.random_regular(4096, 3, rng), False),
              ("torus_32x32", G.torus(32), True), ("torus_64x64", G.torus(64), True)]
+    if args.single_extra:
+        cases += [("tree_n2048", G.from_edges(2048, G.recursive_tree(2048, rng)), True),
+                  ("union_5x_reg3_32", G.disjoint_union(G.random_regular(32, 3, rng), 5), True)]
     ctx = pkg.Context(local)
+    if args.single_gate != 1:
+        ctx.set_option(pkg.api.GCL_OPT_WIDE_GATE, args.single_gate)
+    if args.single_share:
+        ctx.set_option(pkg.api.GCL_OPT_WIDE_SHARE, 1)
     pkg.canon(G.from_edges(3, [(0, 1)]), ctx=ctx)
     out = {}
     O = None
