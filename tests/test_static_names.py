@@ -12,6 +12,10 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 FILES = ["bench.py", "__graft_entry__.py", "gpu-canonical-labeling_b200/api.py",
          "gpu-canonical-labeling_b200/graphs.py", "gpu-canonical-labeling_b200/build.py",
          "gpu-canonical-labeling_b200/__init__.py", "oracle/oracle.py"]
+# the tests too: those marked gpu or gpu_staged run only on a GPU
+FILES += sorted(os.path.join("tests", f) for f in os.listdir(os.path.join(ROOT, "tests"))
+                if f.startswith("test_") and f.endswith(".py"))
+FILES += ["tests/conftest.py", "tests/golden/make_golden.py"]
 
 
 def _module_names(top):
