@@ -155,7 +155,7 @@ def _csr(g):
 
 def wide_model(g, workers: int, seed: int = 0, cap: int = 10000, auts: bool = False,
                gate: bool = True, rounds: Optional[list] = None,
-               first_seq: Optional[list] = None, donate: bool = False):
+               first_seq: Optional[list] = None, donate: int = 0):
     """CPU model of the many-worker search (wide_model.c): `workers` simulated
     workers over the first path's sibling items, stepped round-robin (seed 0)
     or in a seeded random order.  Returns (canonical matrix, nodes, automorphisms
@@ -167,13 +167,15 @@ def wide_model(g, workers: int, seed: int = 0, cap: int = 10000, auts: bool = Fa
     receives the number of scheduling rounds (every worker steps once per
     round), the first leaf's level D and the number of items; `first_seq`,
     when a list, the first path's individualized vertices.  donate: busy
-    workers hand their shallowest untried child to idle ones."""
+    workers hand their shallowest untried child to idle ones (1: with the
+    parent's partition; 2: the receiver rebuilds it from the first leaf, as
+    the GPU does, and events[3] counts replayed codes that differed)."""
     lib = _load_wide()
     rp, cl, co = _csr(g)
     out = np.zeros((g.n, g.n), dtype=np.uint8)
     nodes = ctypes.c_long(0)
     naut = ctypes.c_int(0)
-    ev = np.zeros(3, dtype=np.int64)
+    ev = np.zeros(4, dtype=np.int64)
     store = np.zeros((cap, max(g.n, 1)), dtype=np.uint32) if auts else None
     nr = (ctypes.c_long * 3)()
     fs = np.zeros(max(g.n, 1), dtype=np.uint32)
@@ -187,8 +189,8 @@ def wide_model(g, workers: int, seed: int = 0, cap: int = 10000, auts: bool = Fa
     if first_seq is not None:
         first_seq.extend(int(x) for x in fs[:max(int(nr[1]) - 1, 0)])
     if auts:
-        return out, int(nodes.value), int(naut.value), ev, store[:naut.value, :g.n].copy()
-    return out, int(nodes.value), int(naut.value), ev
+        return out, int(nodes.value), int(naut.value), ev[:3] if donate != 2 else ev, store[:naut.value, :g.n].copy()
+    return out, int(nodes.value), int(naut.value), ev[:3] if donate != 2 else ev
 
 
 def exhaustive(g, max_leaves: int = 200000) -> Optional[np.ndarray]:

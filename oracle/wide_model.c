@@ -55,7 +55,8 @@ typedef struct {
   /* how often the changed rules fired: [0] a leaf equivalent to a best found
    * outside the item, [1] a node pruned as worse than the private best,
    * [2] a leaf that beat the private best but not a newer shared one */
-  long events[3];
+  long events[4]; /* [3]: handed-over subtrees whose replayed codes differed */
+  int replay;     /* receivers rebuild a handed-over parent from the first leaf */
 } wm_shared;
 
 typedef struct {
@@ -360,10 +361,44 @@ static int wm_start_gift(wm_worker* w, wm_shared* G, const wm_gift* gf) {
   opart* P = &S->P;
   const int n = G->n;
   const uint32_t k = gf->L - 1;
-  wm_copy_part(P, &gf->P, n);
-  P->level = gf->L;
-  memcpy(P->seq, gf->seq, (size_t)k * 4);
-  P->seqlen = k;
+  if (G->replay) {
+    /* as the GPU does: the first leaf back to the level the gift's sequence
+     * shares with the first path, then its remaining vertices individualized
+     * and refined, each code checked against the giver's */
+    uint32_t c = 0;
+    const uint32_t lim = k < G->D - 1 ? k : G->D - 1;
+    while (c < lim && gf->seq[c] == G->first_seq[c]) ++c;
+    wm_copy_part(P, &G->leafP, n);
+    P->level = G->D;
+    uint32_t e1 = 0xffffffffu;
+    int e2 = 0x7fffffff, e3 = 0;
+    o_reconstruct(P, c + 1, &e1, &e2, &e3);
+    P->level = c + 1;
+    memcpy(P->seq, G->first_seq, (size_t)c * 4);
+    P->seqlen = c;
+    for (uint32_t lvl = c + 1; lvl < gf->L; ++lvl) {
+      int tc = -1;
+      for (uint32_t i = 0; i < P->ncells; ++i)
+        if (P->lcs[i].length > 1) {
+          tc = (int)i;
+          break;
+        }
+      if (tc < 0) {
+        G->events[3]++;
+        return 0;
+      }
+      const uint32_t u = gf->seq[lvl - 1];
+      int code = 0;
+      P->seq[P->seqlen++] = u;
+      o_individualize(P, u, &code, P->lcs[tc].first);
+      if (code != gf->pathcode[lvl]) G->events[3]++;
+    }
+  } else {
+    wm_copy_part(P, &gf->P, n);
+    P->level = gf->L;
+    memcpy(P->seq, gf->seq, (size_t)k * 4);
+    P->seqlen = k;
+  }
   S->tc_level_reached = (int)k;
   o_select_tc(S);
   otc* t = &S->tcs[k];
@@ -410,6 +445,7 @@ int gcl_wide_model(int n, const int32_t* rowptr, const int32_t* col, const int32
   memset(&G, 0, sizeof G);
   G.n = n;
   G.cap = cap;
+  G.replay = donate == 2;
   G.auts = malloc((size_t)cap * n * 4 + 4);
   G.nodes = 1;
   /* the first path, recording each level's target cell (sorted members) */

@@ -201,3 +201,27 @@ def test_wide_model_donation_splits_unions(G, wm):
     m1, nodes1, _, _ = wm.wide_model(g, 592, 0, cap=100000, gate=False, donate=True, rounds=r1)
     assert np.array_equal(m0, ref) and np.array_equal(m1, ref)
     assert r1[0] * 3 < r0[0] and nodes1 < nodes0
+
+
+def test_wide_model_replayed_parents_match(G, wm):
+    # the GPU's receiver rebuilds a handed-over parent from the first leaf:
+    # back to the level shared with the first path, then the remaining
+    # vertices individualized -- the codes must be the giver's, and the
+    # canonical form the sequential one
+    rng = np.random.default_rng(34)
+    graphs = [G.disjoint_union(G.random_regular(10, 3, rng), k) for k in (2, 3, 4)]
+    graphs += [G.disjoint_union(G.random_regular(32, 3, rng), 5)]
+    graphs += [G.cfi_graph(b, rng) for b in (6, 10)] + [G.tree_plus_edges(150, rng)]
+    for g in graphs:
+        ref = wm.canon(g)[0]
+        for workers, seed, gate in ((3, 1, True), (16, 2, False), (64, 0, False)):
+            r = []
+            mat, _, _, ev = wm.wide_model(g, workers, seed, gate=gate, donate=2, rounds=r)
+            assert np.array_equal(mat, ref), (g.n, workers, seed, gate)
+            assert ev[3] == 0, (g.n, workers, seed)
+    # the unions hand work over, so parents are rebuilt
+    r0, r1 = [], []
+    g = graphs[3]
+    wm.wide_model(g, 64, 0, gate=False, rounds=r0)
+    wm.wide_model(g, 64, 0, gate=False, donate=2, rounds=r1)
+    assert r1[0] < r0[0]
