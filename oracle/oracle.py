@@ -6,7 +6,12 @@ Two checkers live here:
                    reference's sequential labeler (canon_oracle.c).
 * ``reference`` -- ``_ref/libgcl_ref.so``: the reference's own sequential
                    sources (src/sequential.cpp et al.) compiled unchanged by
-                   ``make -C oracle ref``, behind ref_shim.cpp.
+                   ``make -C oracle ref``, behind ref_shim.cpp; also its
+                   DIMACS reader (``ref_read_dimacs``).
+
+and a model: ``libgcl_wide_model.so`` (wide_model.c), the many-worker search's
+rules on the CPU (``wide_model``) and an unpruned maximum-leaf search
+(``exhaustive``).
 
 Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg use
 this module, and only as the checker / the timed CPU baseline.
