@@ -159,7 +159,7 @@ def _csr(g):
 
 
 def wide_model(g, workers: int, seed: int = 0, cap: int = 10000, auts: bool = False,
-               gate: bool = True, rounds: Optional[list] = None,
+               gate: int = 1, rounds: Optional[list] = None,
                first_seq: Optional[list] = None, donate: int = 0):
     """CPU model of the many-worker search (wide_model.c): `workers` simulated
     workers over the first path's sibling items, stepped round-robin (seed 0)
@@ -168,7 +168,8 @@ def wide_model(g, workers: int, seed: int = 0, cap: int = 10000, auts: bool = Fa
     outside their item, nodes pruned as worse than the private best, leaves
     that beat the private best but not a newer shared one]; with auts=True a
     fifth item, the stored automorphisms (naut x n, position -> image).
-    gate: items start level by level as on the GPU; `rounds`, when a list,
+    gate: items start level by level as on the GPU (0 off, 2 the GPU's
+    automatic choice); `rounds`, when a list,
     receives the number of scheduling rounds (every worker steps once per
     round), the first leaf's level D and the number of items; `first_seq`,
     when a list, the first path's individualized vertices.  donate: busy

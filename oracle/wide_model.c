@@ -517,6 +517,9 @@ int gcl_wide_model(int n, const int32_t* rowptr, const int32_t* col, const int32
   unsigned long long rs = 88172645463325252ull ^ (unsigned long long)seed;
   /* the level gate: an item starts once every item of the deeper levels is
    * done (need[it] = items before the first one of its level) */
+  /* gate 2: on unless the levels hold fewer than 4 items each on average,
+   * the GPU's automatic choice */
+  if (gate == 2) gate = G.nitems >= 4 * (int)(G.D > 1 ? G.D - 1 : 0);
   int* need = malloc(((size_t)G.nitems + 1) * sizeof(int));
   for (int it = 0; it < G.nitems; ++it)
     need[it] = it > 0 && G.item_k[it] == G.item_k[it - 1] ? need[it - 1] : it;

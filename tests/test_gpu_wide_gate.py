@@ -139,3 +139,15 @@ def test_work_sharing_vs_oracle(pkg, G, oracle_mod, gate):
         assert np.array_equal(a, want) and np.array_equal(b, want), g.n
         if g.n >= 96:
             print(f"n={g.n}: sharing {t_share * 1e3:.1f} ms, without {t_plain * 1e3:.1f} ms")
+
+
+def test_option_values_checked(pkg):
+    ctx = pkg.Context(0)
+    for opt, bad in ((pkg.api.GCL_OPT_WIDE_GATE, 3), (pkg.api.GCL_OPT_WIDE_GATE, -1),
+                     (pkg.api.GCL_OPT_WIDE_SHARE, 2)):
+        with pytest.raises(pkg.GclError) as e:
+            ctx.set_option(opt, bad)
+        assert e.value.rc == -1
+    for opt, good in ((pkg.api.GCL_OPT_WIDE_GATE, 0), (pkg.api.GCL_OPT_WIDE_GATE, 2),
+                      (pkg.api.GCL_OPT_WIDE_SHARE, 1), (pkg.api.GCL_OPT_WIDE_SHARE, 0)):
+        ctx.set_option(opt, good)

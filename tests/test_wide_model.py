@@ -225,3 +225,17 @@ def test_wide_model_replayed_parents_match(G, wm):
     wm.wide_model(g, 64, 0, gate=False, rounds=r0)
     wm.wide_model(g, 64, 0, gate=False, donate=2, rounds=r1)
     assert r1[0] < r0[0]
+
+
+def test_wide_model_automatic_gate(G, wm):
+    # gate 2 (the GPU's automatic rule): off for a tree (about one item per
+    # level), on for a torus (many items per level) -- same rounds as the
+    # explicit settings it picks
+    rng = np.random.default_rng(2)
+    tree = G.from_edges(300, G.recursive_tree(300, rng))
+    torus = G.torus(10)
+    for g, picks in ((tree, 0), (torus, 1)):
+        r_auto, r_pick = [], []
+        m1 = wm.wide_model(g, 64, 0, gate=2, rounds=r_auto)[0]
+        m2 = wm.wide_model(g, 64, 0, gate=picks, rounds=r_pick)[0]
+        assert np.array_equal(m1, m2) and r_auto[0] == r_pick[0], (g.n, picks)
