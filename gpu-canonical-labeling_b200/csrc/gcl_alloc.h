@@ -1,0 +1,67 @@
+// gcl_alloc.h -- every device and pinned host allocation of the library.
+//
+// A failed allocation is returned to the caller and leaves nothing behind:
+// the runtime also records the failure as the thread's last error, which a
+// later launch check (cudaGetLastError) would report against a kernel that
+// ran fine -- after a wide search that found no workspace falls back to the
+// sequential search, for one.  So the record is cleared here.
+//
+// GCL_FAULT_ALLOC_AT=k in the environment (k >= 1) makes the k-th allocation
+// of the process (device and pinned host counted together) fail as out of
+// memory, once, without calling the allocator.  It is a test hook for the
+// callers' error paths: the call that needed the memory returns
+// GCL_ERR_NOMEM (or falls back, where it has a fallback) and the context
+// stays usable.  Unset, or not a positive integer: no effect.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <cstdlib>
+
+namespace gcl {
+
+inline int64_t alloc_fault_target() {
+  static const int64_t k = [] {
+    const char* s = std::getenv("GCL_FAULT_ALLOC_AT");
+    if (!s || !*s) return (int64_t)0;
+    char* end = nullptr;
+    const long long v = std::strtoll(s, &end, 10);
+    return (*end == '\0' && v > 0) ? (int64_t)v : (int64_t)0;
+  }();
+  return k;
+}
+
+// true for the one allocation that is to fail
+inline bool alloc_fault_hit() {
+  const int64_t k = alloc_fault_target();
+  if (k == 0) return false;
+  static std::atomic<int64_t> seen{0};
+  return seen.fetch_add(1, std::memory_order_relaxed) + 1 == k;
+}
+
+// stream-ordered device allocation (cudaMallocAsync); *p is null on failure
+inline cudaError_t device_alloc(void** p, size_t bytes, cudaStream_t s) {
+  *p = nullptr;
+  if (alloc_fault_hit()) return cudaErrorMemoryAllocation;
+  const cudaError_t e = cudaMallocAsync(p, bytes, s);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    (void)cudaGetLastError();
+  }
+  return e;
+}
+
+// pinned host allocation (cudaHostAlloc); *p is null on failure
+inline cudaError_t pinned_alloc(void** p, size_t bytes) {
+  *p = nullptr;
+  if (alloc_fault_hit()) return cudaErrorMemoryAllocation;
+  const cudaError_t e = cudaHostAlloc(p, bytes, cudaHostAllocDefault);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    (void)cudaGetLastError();
+  }
+  return e;
+}
+
+}  // namespace gcl

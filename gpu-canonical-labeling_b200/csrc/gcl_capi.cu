@@ -24,6 +24,7 @@
 #include "canon_sparse.cuh"
 #include "canon_warp64.cuh"
 #include "canon_wide.cuh"
+#include "gcl_alloc.h"
 #include "gcl_group.h"
 #include "gcl_guard.h"
 
@@ -193,7 +194,7 @@ struct DevBuf {
     if (p) cudaFreeAsync(p, stream);
     p = nullptr;
     cap = 0;
-    cudaError_t e = cudaMallocAsync(&p, want, stream);
+    cudaError_t e = device_alloc(&p, want, stream);
     if (e == cudaSuccess) cap = want;
     return e;
   }
@@ -201,6 +202,20 @@ struct DevBuf {
     if (p) cudaFreeAsync(p, stream);
     p = nullptr;
     cap = 0;
+  }
+};
+
+// A host-pointer entry point that returns early (an error, or an exception)
+// may leave copies from or to the caller's buffers queued on its stream, and
+// the caller may reuse or free those buffers once the call has returned: the
+// stream is drained first.  A call that completed has synchronized already
+// and sets `done`.
+struct DrainOnExit {
+  cudaStream_t s;
+  bool done = false;
+  explicit DrainOnExit(cudaStream_t st) : s(st) {}
+  ~DrainOnExit() {
+    if (!done) cudaStreamSynchronize(s);
   }
 };
 
@@ -703,6 +718,7 @@ int canon_wide_host(gcl_context* c, const int32_t* rowptr, const int32_t* col,
   if (m > 0 && !col) return GCL_ERR_ARG;
   GCL_TRY(cudaSetDevice(c->device));
   cudaStream_t s = c->stream;
+  DrainOnExit drain(s);
   GCL_TRY(c->rowptr.ensure(((size_t)n + 1) * sizeof(int32_t)));
   GCL_TRY(c->col.ensure(std::max<size_t>((size_t)m, 1) * sizeof(int32_t)));
   GCL_TRY(c->dense.ensure(std::max<size_t>((size_t)n * n, 1)));
@@ -729,6 +745,7 @@ int canon_wide_host(gcl_context* c, const int32_t* rowptr, const int32_t* col,
   if (status != kOk) return graph_status_to_rc(status);
   GCL_TRY(cudaMemcpyAsync(out_nxn, c->dense.p, (size_t)n * n, cudaMemcpyDeviceToHost, s));
   GCL_TRY(cudaStreamSynchronize(s));
+  drain.done = true;
   return GCL_OK;
 }
 
@@ -767,6 +784,7 @@ int gcl_canon_batch(gcl_context* c, int count, const int64_t* voff, const int64_
   GCL_TRY(c->col.ensure(std::max<size_t>(ne, 1) * sizeof(int32_t)));
   GCL_TRY(c->status.ensure(count * sizeof(int32_t)));
   cudaStream_t s = c->stream;
+  DrainOnExit drain(s);
   GCL_TRY(cudaMemcpyAsync(c->voff.p, voff, (count + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s));
   GCL_TRY(cudaMemcpyAsync(c->eoff.p, eoff, (count + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s));
   GCL_TRY(cudaMemcpyAsync(c->rowptr.p, rowptr, nrp * sizeof(int32_t), cudaMemcpyHostToDevice, s));
@@ -824,6 +842,7 @@ int gcl_canon_batch(gcl_context* c, int count, const int64_t* voff, const int64_
     GCL_TRY(cudaMemcpyAsync(out_stats, d_stats, 2 * count * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
   GCL_TRY(cudaMemcpyAsync(out_status, c->status.p, count * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
   GCL_TRY(cudaStreamSynchronize(s));
+  drain.done = true;
   for (int g = 0; g < count; ++g)
     if (out_status[g] != kOk) return graph_status_to_rc(out_status[g]);
   return GCL_OK;
@@ -917,6 +936,7 @@ int gcl_group_order(gcl_context* c, const int32_t* rowptr, const int32_t* col,
   if (m > 0 && !col) return GCL_ERR_ARG;
   GCL_TRY(cudaSetDevice(c->device));
   cudaStream_t s = c->stream;
+  DrainOnExit drain(s);
   GCL_TRY(c->rowptr.ensure(((size_t)n + 1) * sizeof(int32_t)));
   GCL_TRY(c->col.ensure(std::max<size_t>((size_t)m, 1) * sizeof(int32_t)));
   GCL_TRY(c->stats.ensure(2 * sizeof(int64_t)));
@@ -980,6 +1000,7 @@ int gcl_group_order(gcl_context* c, const int32_t* rowptr, const int32_t* col,
                                  &lg, &d))
       return GCL_ERR_TIMEOUT;
   }
+  drain.done = true;
   return put(d, lg, st[0]);
 } GCL_CATCH_ALL
 

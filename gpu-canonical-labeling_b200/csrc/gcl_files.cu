@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "../../include/gcl.h"
+#include "gcl_alloc.h"
 #include "gcl_dimacs.h"
 #include "gcl_guard.h"
 
@@ -45,7 +46,7 @@ struct Pinned {
     p = nullptr;
     cap = 0;
     const size_t want = std::max<size_t>(b + b / 2, 4096);
-    cudaError_t e = cudaHostAlloc(&p, want, cudaHostAllocDefault);
+    cudaError_t e = gcl::pinned_alloc(&p, want);
     if (e == cudaSuccess) cap = want;
     return e;
   }
@@ -64,7 +65,7 @@ struct Dev {
     p = nullptr;
     cap = 0;
     const size_t want = std::max<size_t>(b + b / 2, 4096);
-    cudaError_t e = cudaMallocAsync(&p, want, s);
+    cudaError_t e = gcl::device_alloc(&p, want, s);
     if (e == cudaSuccess) cap = want;
     return e;
   }

@@ -27,6 +27,7 @@
 #include <vector>
 
 #include "../../include/gcl.h"
+#include "gcl_alloc.h"
 #include "gcl_device.cuh"
 #include "gcl_guard.h"
 
@@ -159,7 +160,7 @@ struct HostBuf {
     if (bytes <= cap && p) return cudaSuccess;
     const size_t want = std::max<size_t>(std::max<size_t>(bytes, 4096), 2 * cap);
     void* q = nullptr;
-    cudaError_t e = cudaHostAlloc(&q, want, cudaHostAllocDefault);
+    cudaError_t e = pinned_alloc(&q, want);
     if (e != cudaSuccess) return e;
     if (p) retired.push_back(p);
     p = q;
@@ -191,7 +192,7 @@ struct DevMem {
     if (p) cudaFreeAsync(p, stream);
     p = nullptr;
     cap = 0;
-    cudaError_t e = cudaMallocAsync(&p, want, stream);
+    cudaError_t e = device_alloc(&p, want, stream);
     if (e == cudaSuccess) cap = want;
     return e;
   }

@@ -24,7 +24,11 @@
  * GCL_OPT_WIDE_MIN_N).
  *
  * Errors are returned as negative status codes; nothing calls exit().  All
- * calls are synchronous unless named *_async.
+ * calls are synchronous unless named *_async; a synchronous call that fails
+ * has no copy from or to the caller's buffers left in flight when it returns.
+ * After GCL_ERR_NOMEM the context stays usable.  For tests of those paths,
+ * GCL_FAULT_ALLOC_AT=k in the environment (k >= 1) makes the k-th device or
+ * pinned host allocation of the process fail as out of memory, once.
  */
 #ifndef GCL_H
 #define GCL_H
