@@ -339,6 +339,9 @@ int gcl_create(int device, gcl_context** out) try {
       uint64_t keep = ~0ull;
       cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
     }
+    // an optional setting: a failure above must not surface in a later
+    // launch check as the thread's last error
+    (void)cudaGetLastError();
   }
   int per_sm = 0;
   if (e == cudaSuccess)
