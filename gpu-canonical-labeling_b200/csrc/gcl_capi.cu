@@ -88,8 +88,10 @@ constexpr uint32_t kWidePool = 64;  // per-level orbit arrays of a wide-search w
 constexpr uint64_t kWideStoreBytes = 1ull << 30;  // automorphism store of a wide search
 constexpr uint64_t kWideStoreEntries = 1ull << 22;  // ... and at most this many entries
 constexpr uint32_t kWideFixCap = 4096;  // entries whose fix state a wide-search warp keeps
-constexpr uint64_t kGroupWorkCap = 40000000000ull;  // Schreier-Sims operations (~20 s)
-constexpr uint64_t kGroupWorkCapGeneral = 4000000000ull;  // before a graph's base is used
+constexpr uint64_t kGroupWorkCap = 40000000000ull;  // Schreier-Sims operations (~25 s)
+// the check of a search's group order: Schreier-Sims operations for each of
+// the general and the known-base completion (~0.3 s and ~0.6 s)
+constexpr uint64_t kGroupCheckCap = 400000000ull;
 
 // entries of a wide search's automorphism store: max_aut, within kWideStoreBytes
 static uint32_t wide_store_cap(uint32_t n, int max_aut) {
@@ -974,35 +976,27 @@ int gcl_group_order(gcl_context* c, const int32_t* rowptr, const int32_t* col,
                             (size_t)st[0] * WL.stride * sizeof(uint16_t),
                             cudaMemcpyDeviceToHost, s));
   GCL_TRY(cudaStreamSynchronize(s));
+  // the first path's individualized vertices are a base of Aut(G): an
+  // automorphism fixing them fixes the first leaf's discrete partition
+  const uint8_t* sh = (const uint8_t*)c->wide_sh.p;
+  uint32_t D = 0;
+  GCL_TRY(cudaMemcpyAsync(&D, sh + WL.hdr + offsetof(WideHdr, D), sizeof(uint32_t),
+                          cudaMemcpyDeviceToHost, s));
+  GCL_TRY(cudaStreamSynchronize(s));
+  if (D < 1 || D > un) return GCL_ERR_INTERNAL;
+  std::vector<uint32_t> base(D);
+  if (D > 1)
+    GCL_TRY(cudaMemcpyAsync(base.data(), sh + WL.fseq, (size_t)(D - 1) * sizeof(uint32_t),
+                            cudaMemcpyDeviceToHost, s));
+  GCL_TRY(cudaStreamSynchronize(s));
+  // the product of the basic orbits, checked by Schreier-Sims where that
+  // finishes within its work budget
   double lg = 0;
   std::string d;
-  uint64_t base_len = 0;
-  if (!group_order(un, auts.data(), (uint64_t)st[0], WL.stride, kGroupWorkCapGeneral, &lg, &d,
-                   &base_len)) {
-    // large orbits: the first path's individualized vertices are a base of
-    // Aut(G) (an automorphism fixing them fixes the first leaf's discrete
-    // partition), so Schreier generators sift on their base images alone
-    const uint8_t* sh = (const uint8_t*)c->wide_sh.p;
-    uint32_t D = 0;
-    GCL_TRY(cudaMemcpyAsync(&D, sh + WL.hdr + offsetof(WideHdr, D), sizeof(uint32_t),
-                            cudaMemcpyDeviceToHost, s));
-    GCL_TRY(cudaStreamSynchronize(s));
-    if (D < 1 || D > un) return GCL_ERR_INTERNAL;
-    std::vector<uint32_t> base(D);
-    if (D > 1)
-      GCL_TRY(cudaMemcpyAsync(base.data(), sh + WL.fseq, (size_t)(D - 1) * sizeof(uint32_t),
-                              cudaMemcpyDeviceToHost, s));
-    GCL_TRY(cudaStreamSynchronize(s));
-    const int rg = group_order_with_base(un, auts.data(), (uint64_t)st[0], WL.stride, base.data(),
-                                         D - 1, kGroupWorkCap, &lg, &d, &base_len);
-    if (rg == kOrderNotABase) return GCL_ERR_INTERNAL;
-    // long bases with large orbits (S_n-like): the stored automorphisms are a
-    // strong generating set for the first path, whose basic orbits give the order
-    if (rg == kOrderWorkCap &&
-        !group_order_base_orbits(un, auts.data(), (uint64_t)st[0], WL.stride, base.data(), D - 1,
-                                 &lg, &d))
-      return GCL_ERR_TIMEOUT;
-  }
+  int checked = 0;
+  const int rg = group_order_of_search(un, auts.data(), (uint64_t)st[0], WL.stride, base.data(),
+                                       D - 1, kGroupCheckCap, &lg, &d, &checked);
+  if (rg != kOrderOk) return GCL_ERR_INTERNAL;
   drain.done = true;
   return put(d, lg, st[0]);
 } GCL_CATCH_ALL

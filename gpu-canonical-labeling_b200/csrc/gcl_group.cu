@@ -389,8 +389,9 @@ bool group_order(uint32_t n, const uint16_t* auts, uint64_t count, uint64_t stri
 bool group_order_base_orbits(uint32_t n, const uint16_t* auts, uint64_t count, uint64_t stride,
                              const uint32_t* base, uint32_t nbase, double* log10_order,
                              std::string* digits) {
-  // level of each automorphism: the first base point it moves (nbase: none)
-  std::vector<uint32_t> lev(count);
+  for (uint32_t m = 0; m < nbase; ++m)
+    if (base[m] >= n) return false;
+  // automorphisms by level: the first base point each moves (none: dropped)
   std::vector<std::vector<uint64_t>> at(nbase);
   for (uint64_t a = 0; a < count; ++a) {
     const uint16_t* pm = auts + a * stride;
@@ -445,6 +446,28 @@ int group_order_with_base(uint32_t n, const uint16_t* auts, uint64_t count, uint
   }
   C.bi.resize(nbase);
   return run(C, auts, count, stride, log10_order, digits, base_len);
+}
+
+int group_order_of_search(uint32_t n, const uint16_t* auts, uint64_t count, uint64_t stride,
+                          const uint32_t* base, uint32_t nbase, uint64_t check_cap,
+                          double* log10_order, std::string* digits, int* checked) {
+  *checked = 0;
+  if (!group_order_base_orbits(n, auts, count, stride, base, nbase, log10_order, digits))
+    return kOrderNotABase;
+  if (check_cap == 0) return kOrderOk;
+  double lg = 0;
+  std::string d;
+  uint64_t bl = 0;
+  // the general completion first (cheapest where the orbits are short),
+  // then the completion on the search's base (long orbits)
+  int rc = group_order(n, auts, count, stride, check_cap, &lg, &d, &bl) ? kOrderOk : kOrderWorkCap;
+  if (rc == kOrderWorkCap)
+    rc = group_order_with_base(n, auts, count, stride, base, nbase, check_cap, &lg, &d, &bl);
+  if (rc == kOrderNotABase) return kOrderNotABase;
+  if (rc == kOrderWorkCap) return kOrderOk;  // unchecked: the orbit product stands
+  if (d != *digits) return kOrderMismatch;
+  *checked = 1;
+  return kOrderOk;
 }
 
 }  // namespace gcl

@@ -13,7 +13,7 @@ bool group_order(uint32_t n, const uint16_t* auts, uint64_t count, uint64_t stri
                  uint64_t work_cap, double* log10_order, std::string* digits,
                  uint64_t* base_len);
 
-enum { kOrderOk = 0, kOrderWorkCap = 1, kOrderNotABase = 2 };
+enum { kOrderOk = 0, kOrderWorkCap = 1, kOrderNotABase = 2, kOrderMismatch = 3 };
 
 // Same, given a base: nbase distinct points that only the identity fixes all
 // of (for a graph, the individualized vertices of the search's first path:
@@ -35,9 +35,21 @@ int group_order_with_base(uint32_t n, const uint16_t* auts, uint64_t count, uint
 // either searched, and a leaf equivalent to the first leaf under it gives an
 // automorphism fixing b_0..b_{i-1} that moves b_i there, or skipped as
 // equivalent to one that is; so these automorphisms form a strong generating
-// set for that base.  O(stored x n).
+// set for that base.  O(stored x n).  false: a base point is not below n.
 bool group_order_base_orbits(uint32_t n, const uint16_t* auts, uint64_t count, uint64_t stride,
                              const uint32_t* base, uint32_t nbase, double* log10_order,
                              std::string* digits);
+
+// The order of Aut(G) from a complete search: the `count` automorphisms it
+// stored (every one it found) and its first path's nbase individualized
+// vertices.  The order is the product of the basic orbits
+// (group_order_base_orbits); the Schreier-Sims completion checks it, general
+// and then on the known base, within check_cap operations each (0: no
+// check).  kOrderOk, with *checked = 1 when a completion finished and agreed
+// and 0 when both ran out of work; kOrderMismatch when a completion gave
+// another order; kOrderNotABase for a base that is none.
+int group_order_of_search(uint32_t n, const uint16_t* auts, uint64_t count, uint64_t stride,
+                          const uint32_t* base, uint32_t nbase, uint64_t check_cap,
+                          double* log10_order, std::string* digits, int* checked);
 
 }  // namespace gcl

@@ -273,16 +273,18 @@ int gcl_set_tuning(gcl_context* ctx, const gcl_tuning* tuning);
  * The reference never computes |Aut(G)|; it prints how many automorphisms it
  * stored (sequential.cpp:83), which depends on the traversal and max_aut.
  * gcl_group_order runs the wide search with a store that keeps every
- * automorphism found (they generate the group) and builds a base and strong
- * generating set (Schreier-Sims) on the host: *log10_order = log10 |Aut|,
+ * automorphism found.  The first path's individualized vertices are a base
+ * of Aut(G) and those automorphisms a strong generating set for it, so the
+ * order is the product over the first path of each vertex's orbit under the
+ * stored automorphisms that fix the vertices before it (nauty's grpsize).
+ * The host checks it with the Schreier-Sims completion (general, then on that
+ * base) where one finishes within its work budget (about a second) and
+ * returns GCL_ERR_INTERNAL if one disagrees.  *log10_order = log10 |Aut|,
  * digits (if not NULL) the order in decimal, *generators the automorphisms
- * the search stored.  When Schreier-Sims exceeds its work cap, with and
- * then without the first path as a known base, the order is the product of
- * the first path's basic orbits under the stored automorphisms (they are a
- * strong generating set for that base; nauty's grpsize).  GCL_ERR_TOO_LARGE
- * if the search found more automorphisms than its 1 GiB store holds,
- * GCL_ERR_ARG if digits_cap is too small.  gcl_perm_group_order returns
- * GCL_ERR_TIMEOUT when its Schreier-Sims exceeds the work cap.
+ * the search stored.  GCL_ERR_TOO_LARGE if the search found more
+ * automorphisms than its 1 GiB store holds, GCL_ERR_ARG if digits_cap is too
+ * small.  gcl_perm_group_order returns GCL_ERR_TIMEOUT when its
+ * Schreier-Sims exceeds the work cap.
  * gcl_perm_group_order is the host part alone: the order of the group
  * generated by `count` permutations of {0..n-1} (row a at perms + a*n). */
 int gcl_group_order(gcl_context* ctx, const int32_t* rowptr, const int32_t* col,

@@ -1,10 +1,11 @@
 """Group order of graphs whose automorphism groups have large orbits, where
-the general Schreier-Sims completion exceeds its budget and gcl_group_order
-sifts on the first path's base images instead.
+the Schreier-Sims check of gcl_group_order (general, then on the first
+path's base images) may exceed its budget and the first path's basic orbits
+give the order unchecked.
 
 Staged: marked gpu_staged, not gpu, until it has passed on a B200; run it
-with `pytest -m gpu_staged`.  The base-image completion itself is checked on
-the CPU (tests/test_group_base.py)."""
+with `pytest -m gpu_staged`.  The host part is checked on the CPU
+(tests/test_group_base.py)."""
 import math
 
 import numpy as np
@@ -26,7 +27,7 @@ def test_group_order_large_vertex_transitive(pkg, G):
 
 
 def test_group_order_long_base(pkg, G):
-    # S_600: both Schreier-Sims budgets run out; the first path's basic
-    # orbits give the order
+    # S_600: both Schreier-Sims checks run out of budget; the first path's
+    # basic orbits give the order
     ctx = pkg.Context(0)
     assert pkg.group_order(G.from_edges(600, []), ctx=ctx) == math.factorial(600)

@@ -35,6 +35,16 @@ extern "C" int order_orbits(unsigned n, const unsigned short* a, unsigned long l
   std::memcpy(out, d.c_str(), d.size() + 1);
   return 0;
 }
+extern "C" int order_search(unsigned n, const unsigned short* a, unsigned long long count,
+                            const unsigned* base, unsigned nbase, unsigned long long cap,
+                            int* checked, char* out, int out_cap) {
+  double lg; std::string d;
+  const int rc = gcl::group_order_of_search(n, a, count, n, base, nbase, cap, &lg, &d, checked);
+  if (rc) return rc;
+  if ((int)d.size() + 1 > out_cap) return 3;
+  std::memcpy(out, d.c_str(), d.size() + 1);
+  return 0;
+}
 extern "C" int order_base(unsigned n, const unsigned short* a, unsigned long long count,
                           const unsigned* base, unsigned nbase, unsigned long long cap,
                           char* out, int out_cap) {
@@ -64,6 +74,8 @@ def grp(tmp_path_factory):
                                   ctypes.c_char_p, ctypes.c_int]
     lib.order_base.argtypes = [ctypes.c_uint, P, ctypes.c_ulonglong, P, ctypes.c_uint,
                                ctypes.c_ulonglong, ctypes.c_char_p, ctypes.c_int]
+    lib.order_search.argtypes = [ctypes.c_uint, P, ctypes.c_ulonglong, P, ctypes.c_uint,
+                                 ctypes.c_ulonglong, P, ctypes.c_char_p, ctypes.c_int]
     lib.order_orbits.argtypes = [ctypes.c_uint, P, ctypes.c_ulonglong, P, ctypes.c_uint,
                                  ctypes.c_char_p, ctypes.c_int]
 
@@ -88,7 +100,17 @@ def grp(tmp_path_factory):
         rc = lib.order_orbits(p.shape[1], p.ctypes.data if p.size else None, p.shape[0],
                               b.ctypes.data if b.size else None, b.size, buf, len(buf))
         return rc, (int(buf.value.decode()) if rc == 0 else None)
+    def search(perms, base, cap):
+        p = np.ascontiguousarray(perms, dtype=np.uint16)
+        b = np.ascontiguousarray(base, dtype=np.uint32)
+        buf = ctypes.create_string_buffer(1 << 16)
+        checked = ctypes.c_int(-1)
+        rc = lib.order_search(p.shape[1], p.ctypes.data if p.size else None, p.shape[0],
+                              b.ctypes.data if b.size else None, b.size, cap,
+                              ctypes.byref(checked), buf, len(buf))
+        return rc, (int(buf.value.decode()) if rc == 0 else None), checked.value
     based.orbits = orbits
+    based.search = search
     return generic, based
 
 
@@ -186,3 +208,48 @@ def test_points_that_are_no_base_are_reported_when_met(grp):
     assert rc == 2
     rc, order = based(np.array([cyc, swap, fix01]), list(range(6)))
     assert rc == 0 and order == math.factorial(7)
+
+
+CHECK_CAP = 400_000_000  # the library's check budget (kGroupCheckCap in csrc/gcl_capi.cu)
+
+
+def test_search_order_is_checked_where_schreier_sims_finishes(G, wm, grp):
+    # gcl::group_order_of_search: the basic-orbit product, with the
+    # Schreier-Sims completion agreeing wherever it finishes in its budget
+    generic, based = grp
+    rng = np.random.default_rng(31)
+    graphs = [G.torus(k) for k in (4, 7, 12)] + [G.cfi_graph(8, rng), G.from_edges(9, [])]
+    graphs += [G.disjoint_union(G.random_regular(10, 3, rng), 4), G.tree_plus_edges(80, rng)]
+    graphs += list(G.small_batch(30, seed=31))
+    for i, g in enumerate(graphs):
+        store, fs = _model(wm, g, seed=i)
+        rc, order, checked = based.search(store, fs, CHECK_CAP)
+        rc1, want = generic(store)
+        assert rc == 0 and rc1 == 0 and order == want and checked == 1, (i, g.n, order, want)
+        # no check asked for: the same order, unchecked
+        assert based.search(store, fs, 0) == (0, want, 0)
+
+
+def test_search_order_of_a_large_symmetric_group_is_immediate(G, wm, grp):
+    # S_300 (the empty graph): both completions run out of their check budget
+    # (about a second) and the basic-orbit product stands; before, the general
+    # and the known-base completion ran for tens of seconds first
+    import time
+    _, based = grp
+    store, fs = _model(wm, G.from_edges(300, []))
+    t = time.time()
+    rc, order, checked = based.search(store, fs, CHECK_CAP)
+    assert rc == 0 and order == math.factorial(300) and checked == 0
+    assert time.time() - t < 10
+
+
+def test_search_order_mismatch_is_reported(grp):
+    # a planted mistake: generators of S_4 that are no strong generating set
+    # for the base (0, 1, 2) -- the basic-orbit product gives 4, Schreier-Sims 24
+    _, based = grp
+    cyc = [1, 2, 3, 0]
+    swap = [1, 0, 2, 3]
+    rc, _, _ = based.search(np.array([cyc, swap]), [0, 1, 2], CHECK_CAP)
+    assert rc == 3  # kOrderMismatch
+    rc, order, checked = based.search(np.array([cyc, swap]), [0, 1, 2], 0)
+    assert (rc, order, checked) == (0, 4, 0)  # unchecked, the product alone is wrong here
