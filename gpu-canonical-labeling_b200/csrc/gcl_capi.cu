@@ -990,7 +990,7 @@ int gcl_group_order(gcl_context* c, const int32_t* rowptr, const int32_t* col,
                             cudaMemcpyDeviceToHost, s));
   GCL_TRY(cudaStreamSynchronize(s));
   // the product of the basic orbits, checked by Schreier-Sims where that
-  // finishes within its work budget
+  // finishes within its work budget (its order wins a disagreement)
   double lg = 0;
   std::string d;
   int checked = 0;

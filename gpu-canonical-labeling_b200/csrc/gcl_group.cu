@@ -465,7 +465,14 @@ int group_order_of_search(uint32_t n, const uint16_t* auts, uint64_t count, uint
     rc = group_order_with_base(n, auts, count, stride, base, nbase, check_cap, &lg, &d, &bl);
   if (rc == kOrderNotABase) return kOrderNotABase;
   if (rc == kOrderWorkCap) return kOrderOk;  // unchecked: the orbit product stands
-  if (d != *digits) return kOrderMismatch;
+  if (d != *digits) {
+    // the stored automorphisms are no strong generating set for the base:
+    // the completion's order (of the group they generate) is the one to trust
+    *log10_order = lg;
+    *digits = d;
+    *checked = -1;
+    return kOrderOk;
+  }
   *checked = 1;
   return kOrderOk;
 }

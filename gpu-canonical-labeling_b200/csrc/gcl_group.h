@@ -13,7 +13,7 @@ bool group_order(uint32_t n, const uint16_t* auts, uint64_t count, uint64_t stri
                  uint64_t work_cap, double* log10_order, std::string* digits,
                  uint64_t* base_len);
 
-enum { kOrderOk = 0, kOrderWorkCap = 1, kOrderNotABase = 2, kOrderMismatch = 3 };
+enum { kOrderOk = 0, kOrderWorkCap = 1, kOrderNotABase = 2 };
 
 // Same, given a base: nbase distinct points that only the identity fixes all
 // of (for a graph, the individualized vertices of the search's first path:
@@ -45,9 +45,11 @@ bool group_order_base_orbits(uint32_t n, const uint16_t* auts, uint64_t count, u
 // vertices.  The order is the product of the basic orbits
 // (group_order_base_orbits); the Schreier-Sims completion checks it, general
 // and then on the known base, within check_cap operations each (0: no
-// check).  kOrderOk, with *checked = 1 when a completion finished and agreed
-// and 0 when both ran out of work; kOrderMismatch when a completion gave
-// another order; kOrderNotABase for a base that is none.
+// check).  kOrderOk with *checked = 1 when a completion finished and agreed,
+// 0 when both ran out of work, and -1 when a completion finished with
+// another order, which is then the one returned (the order of the group the
+// automorphisms generate, which needs less of them than the product does);
+// kOrderNotABase for a base that is none.
 int group_order_of_search(uint32_t n, const uint16_t* auts, uint64_t count, uint64_t stride,
                           const uint32_t* base, uint32_t nbase, uint64_t check_cap,
                           double* log10_order, std::string* digits, int* checked);

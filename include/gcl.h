@@ -278,8 +278,8 @@ int gcl_set_tuning(gcl_context* ctx, const gcl_tuning* tuning);
  * order is the product over the first path of each vertex's orbit under the
  * stored automorphisms that fix the vertices before it (nauty's grpsize).
  * The host checks it with the Schreier-Sims completion (general, then on that
- * base) where one finishes within its work budget (about a second) and
- * returns GCL_ERR_INTERNAL if one disagrees.  *log10_order = log10 |Aut|,
+ * base), whose order is returned when one finishes within its work budget
+ * (about a second).  *log10_order = log10 |Aut|,
  * digits (if not NULL) the order in decimal, *generators the automorphisms
  * the search stored.  GCL_ERR_TOO_LARGE if the search found more
  * automorphisms than its 1 GiB store holds, GCL_ERR_ARG if digits_cap is too

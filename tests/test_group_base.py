@@ -243,13 +243,13 @@ def test_search_order_of_a_large_symmetric_group_is_immediate(G, wm, grp):
     assert time.time() - t < 10
 
 
-def test_search_order_mismatch_is_reported(grp):
+def test_search_order_disagreement_returns_the_completion(grp):
     # a planted mistake: generators of S_4 that are no strong generating set
-    # for the base (0, 1, 2) -- the basic-orbit product gives 4, Schreier-Sims 24
+    # for the base (0, 1, 2) -- the basic-orbit product gives 4, Schreier-Sims
+    # 24, and the completion's order is returned, flagged
     _, based = grp
     cyc = [1, 2, 3, 0]
     swap = [1, 0, 2, 3]
-    rc, _, _ = based.search(np.array([cyc, swap]), [0, 1, 2], CHECK_CAP)
-    assert rc == 3  # kOrderMismatch
-    rc, order, checked = based.search(np.array([cyc, swap]), [0, 1, 2], 0)
-    assert (rc, order, checked) == (0, 4, 0)  # unchecked, the product alone is wrong here
+    assert based.search(np.array([cyc, swap]), [0, 1, 2], CHECK_CAP) == (0, 24, -1)
+    # unchecked, the product alone is wrong here
+    assert based.search(np.array([cyc, swap]), [0, 1, 2], 0) == (0, 4, 0)
