@@ -996,7 +996,14 @@ int gcl_group_order(gcl_context* c, const int32_t* rowptr, const int32_t* col,
   int checked = 0;
   const int rg = group_order_of_search(un, auts.data(), (uint64_t)st[0], WL.stride, base.data(),
                                        D - 1, kGroupCheckCap, &lg, &d, &checked);
-  if (rg != kOrderOk) return GCL_ERR_INTERNAL;
+  if (rg != kOrderOk) {
+    // the first path is no base (an internal inconsistency): the general
+    // completion alone, with the full budget
+    uint64_t base_len = 0;
+    if (!group_order(un, auts.data(), (uint64_t)st[0], WL.stride, kGroupWorkCap, &lg, &d,
+                     &base_len))
+      return GCL_ERR_INTERNAL;
+  }
   drain.done = true;
   return put(d, lg, st[0]);
 } GCL_CATCH_ALL
