@@ -41,6 +41,7 @@ EXPORTS = [
     "gcl_serve_create", "gcl_serve_destroy", "gcl_serve_submit", "gcl_serve_poll",
     "gcl_serve_stats_get", "gcl_serve_replay", "gcl_group_order", "gcl_perm_group_order",
     "gcl_autotune", "gcl_set_tuning", "gcl_canon_files", "gcl_format_adjacency_device_async",
+    "gcl_wide_counters",
 ]
 
 GCL_OPT_WIDE_MIN_N = 1
@@ -50,6 +51,13 @@ GCL_OPT_SMEM_STAGE = 4
 GCL_OPT_STREAM_PRIORITY = 5
 GCL_OPT_WIDE_GATE = 6
 GCL_OPT_WIDE_SHARE = 7
+GCL_OPT_COUNTERS = 8
+
+# gcl_wide_counters, in index order (include/gcl.h)
+WIDE_COUNTERS = ("items", "items_pruned", "gifts_taken", "gifts_given", "nodes", "leaves",
+                 "auts_first", "auts_best", "best_published", "publish_retries",
+                 "refine_cycles", "orbit_cycles", "gate_cycles", "gift_wait_cycles",
+                 "leaf_cycles", "warp_cycles")
 GCL_MAX_N = 65536
 
 
@@ -120,11 +128,12 @@ def load_library(path: str = LIB_PATH):
     lib.gcl_canon_wide_device_async.argtypes = [_P, _P, _P, _P, ctypes.c_int, ctypes.c_int64,
                                                 ctypes.c_int, _P, _P, _P, _P, _P]
     lib.gcl_format_adjacency_device_async.argtypes = [_P, ctypes.c_int, _P, _P, _P, _P, _P]
+    lib.gcl_wide_counters.argtypes = [_P, _P, ctypes.c_int]
     for name in ("gcl_create", "gcl_destroy", "gcl_sync", "gcl_canon_one", "gcl_canon_batch",
                  "gcl_canon_batch_device_async", "gcl_iso", "gcl_canon_batch_noalloc",
                  "gcl_set_option", "gcl_canon_wide_device_async", "gcl_group_order",
                  "gcl_perm_group_order", "gcl_autotune", "gcl_set_tuning",
-                 "gcl_canon_files", "gcl_format_adjacency_device_async"):
+                 "gcl_canon_files", "gcl_format_adjacency_device_async", "gcl_wide_counters"):
         getattr(lib, name).restype = ctypes.c_int
     _lib = lib
     return lib
@@ -200,6 +209,15 @@ class Context:
 
     def sync(self):
         _check(self.lib.gcl_sync(self.handle), "gcl_sync")
+
+    def wide_counters(self) -> dict:
+        """Counters of the last wide search on this context, by name
+        (gcl_wide_counters; needs GCL_OPT_COUNTERS set before that search)."""
+        out = np.zeros(len(WIDE_COUNTERS), dtype=np.int64)
+        k = self.lib.gcl_wide_counters(self.handle, _ptr(out), len(out))
+        if k < 0:
+            _check(k, "gcl_wide_counters")
+        return {name: int(out[i]) for i, name in enumerate(WIDE_COUNTERS[:k])}
 
 
 _default: Optional[Context] = None

@@ -66,6 +66,51 @@ struct WideHdr {
   uint32_t qtail;      // handed-over subtrees published (slots claimed)
   unsigned long long nodes;
   unsigned long long t0;  // start time (globaltimer ns)
+  // opt-in counters of the items kernel (GCL_OPT_COUNTERS; zeroed by the
+  // host before a counted search, untouched otherwise)
+  unsigned long long cnt[16];
+};
+// the header's region is 256 bytes: the counters move no other region
+static_assert(sizeof(WideHdr) <= 256, "WideHdr outgrew its 256-byte region");
+
+// Counters of the items kernel, summed over its warps (gcl_wide_counters):
+// events, and clock64 cycles spent in each part of the work.
+enum WideCounter : uint32_t {
+  kCntItems,           // items searched (not pruned by an orbit)
+  kCntItemsPruned,     // items skipped as equivalent to a smaller sibling
+  kCntGiftsTaken,      // handed-over subtrees searched or pruned
+  kCntGiftsGiven,      // subtrees handed over
+  kCntNodes,           // search-tree nodes
+  kCntLeaves,          // leaves reached (discrete partitions)
+  kCntAutsFirst,       // automorphisms from a leaf equal to the first leaf
+  kCntAutsBest,        // automorphisms from a leaf equal to the best leaf
+  kCntBestPublished,   // leaves that became the shared best
+  kCntPublishRetries,  // publish attempts that met a moved shared best
+  kCntRefineCycles,    // individualize + refine
+  kCntOrbitCycles,     // orbit tests of items and of target cells
+  kCntGateCycles,      // waiting at the level gate
+  kCntGiftWaitCycles,  // waiting for a handed-over subtree
+  kCntLeafCycles,      // leaf certificates and their comparisons
+  kCntWarpCycles,      // the warps' whole time in the kernel
+  kWideCounters
+};
+
+template <bool kOn>
+struct WideCnt {  // counting off: every call compiles to nothing
+  __device__ __forceinline__ void add(uint32_t, unsigned long long) {}
+  __device__ __forceinline__ unsigned long long now() const { return 0; }
+  __device__ __forceinline__ void flush(WideHdr*) {}
+};
+template <>
+struct WideCnt<true> {
+  unsigned long long v[kWideCounters] = {};
+  __device__ __forceinline__ void add(uint32_t i, unsigned long long x) { v[i] += x; }
+  __device__ __forceinline__ unsigned long long now() const { return (unsigned long long)clock64(); }
+  __device__ __forceinline__ void flush(WideHdr* H) {
+    if (lane_id() == 0)
+      for (uint32_t i = 0; i < kWideCounters; ++i)
+        if (v[i]) atomicAdd(&H->cnt[i], v[i]);
+  }
 };
 
 // Byte layout of the device-wide region of one wide search.
@@ -682,8 +727,9 @@ __device__ __noinline__ void wide_fix_init(uint32_t from, uint32_t to) {
 constexpr uint32_t kGiftMaxWords = 1u << 26;  // 256 MiB of queue at most
 
 // Offer the next untried child of a level in [k+2, level) when warps are
-// waiting for work and the queue holds fewer entries than them.
-__device__ __noinline__ void wide_try_donate(const WidePtrs& P, const WideArgs& A, uint32_t k,
+// waiting for work and the queue holds fewer entries than them; true when
+// a subtree was handed over.
+__device__ __noinline__ bool wide_try_donate(const WidePtrs& P, const WideArgs& A, uint32_t k,
                                              uint32_t level, int tcl) {
   SpWarp& W = sp_w();
   const uint32_t lane = lane_id();
@@ -696,7 +742,7 @@ __device__ __noinline__ void wide_try_donate(const WidePtrs& P, const WideArgs& 
     const uint32_t tail = *(volatile uint32_t*)&H->qtail;
     want = hungry > tail - head && tail < A.WL.qcap;
   }
-  if (!__shfl_sync(GCL_FULL, want, 0)) return;
+  if (!__shfl_sync(GCL_FULL, want, 0)) return false;
   for (uint32_t Lp = k + 2; Lp < level && (int)Lp <= tcl; ++Lp) {
     const SpTc t = W.tc[Lp - 1];
     if (t.counter >= n) continue;
@@ -720,7 +766,7 @@ __device__ __noinline__ void wide_try_donate(const WidePtrs& P, const WideArgs& 
       }
     }
     slot = __shfl_sync(GCL_FULL, slot, 0);
-    if (slot == kNone) return;
+    if (slot == kNone) return false;
     uint32_t* e = P.gq + (uint64_t)slot * A.WL.gstride;
     const uint32_t np = A.n + 2;
     if (lane == 0) {
@@ -736,8 +782,9 @@ __device__ __noinline__ void wide_try_donate(const WidePtrs& P, const WideArgs& 
       *(volatile uint32_t*)&P.gready[slot] = 1u;
     }
     __syncwarp();
-    return;
+    return true;
   }
+  return false;
 }
 
 // Wait for a handed-over subtree.  1: its slot in *slot (the warp now counts
@@ -912,7 +959,7 @@ __device__ __noinline__ uint32_t wide_gift_orbit_min(const WidePtrs& P, uint32_t
   return r;
 }
 
-template <bool kShare>
+template <bool kShare, bool kCount>
 __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
   extern __shared__ __align__(16) uint8_t sp_dyn[];
   const int warp = (int)(threadIdx.x >> 5);
@@ -920,6 +967,8 @@ __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
   const WidePtrs P = wide_ptrs(A);
   WideHdr* H = P.H;
   if (H->status != kOk || H->nitems == 0) return;
+  WideCnt<kCount> cnt;
+  const unsigned long long t_start = cnt.now();
   SpWarp& W = sp_w();
   const uint32_t n = A.n, D = H->D, nitems = H->nitems, cap = A.WL.cap;
   uint8_t* slot = A.slots + ((uint64_t)blockIdx.x * kSpWarps + (uint64_t)warp) * A.slot_bytes;
@@ -971,14 +1020,19 @@ __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
       } else {
         // no item left: wait for a subtree another warp hands over
         uint32_t slot = 0;
+        unsigned long long tc = cnt.now();
         const int32_t gs = wide_take_gift(P, deadline, &slot);
+        cnt.add(kCntGiftWaitCycles, cnt.now() - tc);
         if (gs == 0) break;
         if (gs != 1) {
           status = gs;
           break;
         }
         gift = true;
+        cnt.add(kCntGiftsTaken, 1);
+        tc = cnt.now();
         const int32_t ns = wide_gift_node(P, A, slot, D, &k, &tf, &tl, &v, &gift_eq);
+        cnt.add(kCntRefineCycles, cnt.now() - tc);
         if (ns != kOk) {
           status = ns;
           break;
@@ -986,7 +1040,9 @@ __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
         known = wide_ready_prefix(P, known, cap);
         if (known) {
           bool ok = true;
+          tc = cnt.now();
           const uint32_t r = wide_gift_orbit_min(P, v, k, tf, tl, known, A.WL.stride, &ok);
+          cnt.add(kCntOrbitCycles, cnt.now() - tc);
           if (!ok) {
             status = kTimeout;
             break;
@@ -1014,7 +1070,9 @@ __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
       tl = P.tclen[k];
       v = P.lelem[tf + 1 + (it - P.cum[lo])];
       if (H->gate) {
+        const unsigned long long tc = cnt.now();
         const int32_t gs = wide_gate(H, P.cum[lo], deadline);
+        cnt.add(kCntGateCycles, cnt.now() - tc);
         if (gs != kOk) {
           status = gs;
           break;
@@ -1023,14 +1081,17 @@ __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
       known = wide_ready_prefix(P, known, cap);
       if (known) {
         bool ok = true;
+        const unsigned long long tc = cnt.now();
         const uint32_t r = H->gate ? wide_orbit_min(P, v, lo, k, tf, tl, known, A.WL.stride, &ok)
                                   : wide_orbit_min_own(P, v, k, tf, tl, known, A.WL.stride, &ok);
+        cnt.add(kCntOrbitCycles, cnt.now() - tc);
         if (!ok) {
           status = kTimeout;
           break;
         }
         skip = r != v;  // an equivalent sibling is covered by its orbit's least vertex
       }
+      cnt.add(skip ? kCntItemsPruned : kCntItems, 1);
     }
     do {
     if (skip) break;
@@ -1100,11 +1161,13 @@ __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
     __syncwarp();
     ++seqlen;
     ++my_nodes;
+    unsigned long long tr = cnt.now();
     if (!sp_individualize(level, v, tf)) {
       status = kInternal;
       break;
     }
     int code = sp_refine(level);
+    cnt.add(kCntRefineCycles, cnt.now() - tr);
     if (code < 0) {
       status = kInternal;
       break;
@@ -1119,7 +1182,8 @@ __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
         break;
       }
       if constexpr (kShare) {
-        if (!have_node && (iter & 7) == 0) wide_try_donate(P, A, k, level, tcl);
+        if (!have_node && (iter & 7) == 0 && wide_try_donate(P, A, k, level, tcl))
+          cnt.add(kCntGiftsGiven, 1);
       }
       int bt = -1;
       bool recompare = false;
@@ -1150,6 +1214,8 @@ __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
         if (eqlevfirst != Lv && comp_canon < 0) {
           dec = 4;
         } else if (W.ncells == n) {
+          cnt.add(kCntLeaves, 1);
+          const unsigned long long tc = cnt.now();
           sp_leaf_cert(W.ccert);
           if (eqlevfirst == Lv && sp_cmp_leaf(W.ccert, W.flabel, W.fcert, false) == 0) dec = 1;
           if (dec == 0) {
@@ -1161,12 +1227,15 @@ __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
             }
             dec = comp_canon == 0 ? 2 : (comp_canon > 0 ? 3 : 4);
           }
+          cnt.add(kCntLeafCycles, cnt.now() - tc);
         }
         if (dec == 1) {
+          cnt.add(kCntAutsFirst, 1);
           wide_store_aut<false>(P, W.flabel, cap, A.WL.stride, D);
           const int gg = sp_gca(W.fseq, D - 1, seqlen);
           bt = gg >= 0 ? gg : (int)Lv - 1;
         } else if (dec == 2) {
+          cnt.add(kCntAutsBest, 1);
           wide_store_aut<false>(P, W.blabel, cap, A.WL.stride, D);
           const int gg = best_local ? sp_gca(W.bseq, best.best_seqlen, seqlen) : -1;
           bt = gg >= 0 ? gg : (int)Lv - 1;
@@ -1176,6 +1245,7 @@ __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
           // adopted and the leaf compared again
           int res = 0;
           for (int tries = 0; tries < 64 && res == 0; ++tries) {
+            if (tries) cnt.add(kCntPublishRetries, 1);
             const int r = wide_try_publish(P, A, Lv, seqlen, &best);
             if (r != 0) {
               res = r;
@@ -1186,6 +1256,7 @@ __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
             if (c == 0) res = 2;
           }
           if (res == 1) {
+            cnt.add(kCntBestPublished, 1);
             // the leaf is the new shared best and the private one
             sp_copy_u32(W.bcert, W.ccert, (uint32_t)A.m);
             sp_copy_u32(W.blabel, W.elem, n);
@@ -1198,7 +1269,10 @@ __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
             comp_canon = 0;
           } else if (res == 2 || res == 4) {
             // equivalent to, or worse than, the adopted best
-            if (res == 2) wide_store_aut<false>(P, W.blabel, cap, A.WL.stride, D);
+            if (res == 2) {
+              cnt.add(kCntAutsBest, 1);
+              wide_store_aut<false>(P, W.blabel, cap, A.WL.stride, D);
+            }
             best_local = false;
             recompare = true;
           } else {
@@ -1241,7 +1315,10 @@ __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
               fix_init = known;
             }
             if (known > (uint32_t)W.tc[idx].last) {
-              if (!sp_orbits<true>(idx, (int)known, seqlen)) {
+              const unsigned long long tc = cnt.now();
+              const bool orb_ok = sp_orbits<true>(idx, (int)known, seqlen);
+              cnt.add(kCntOrbitCycles, cnt.now() - tc);
+              if (!orb_ok) {
                 status = W.pool_top >= W.pool_cap ? kAutOverflow : kInternal;
                 break;
               }
@@ -1264,11 +1341,13 @@ __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
               __syncwarp();
               ++seqlen;
               ++my_nodes;
+              tr = cnt.now();
               if (!sp_individualize(level, u, t.first)) {
                 status = kInternal;
                 break;
               }
               code = sp_refine(level);
+              cnt.add(kCntRefineCycles, cnt.now() - tr);
               if (code < 0) {
                 status = kInternal;
                 break;
@@ -1320,6 +1399,9 @@ __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
   }
   if (status != kOk) wide_fail(H, status);
   if (lane == 0) atomicAdd(&H->nodes, my_nodes);
+  cnt.add(kCntNodes, my_nodes);
+  cnt.add(kCntWarpCycles, cnt.now() - t_start);
+  cnt.flush(H);
 }
 
 // ---------------------------------------------------------------------------

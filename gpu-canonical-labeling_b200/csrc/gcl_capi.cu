@@ -254,6 +254,8 @@ struct gcl_context {
   bool smem_stage = true;        // sparse and wide kernels stage per-step arrays in shared memory
   int wide_gate = 1;             // wide search's level gate: 1 on, 0 off, 2 automatic
   bool wide_share = false;       // wide search: busy warps hand subtrees to idle ones
+  bool wide_count = false;       // wide search: the items kernel's counters (GCL_OPT_COUNTERS)
+  bool counted = false;          // the last wide search was counted
   // launch shape per size bucket (gcl_autotune / gcl_set_tuning): 0 / -1 = default
   int w64_per_sm = 0;            // resident blocks the warp kernel's occupancy allows
   int tune_w64_bps = 0;
@@ -289,6 +291,13 @@ static uint64_t workspace_budget() {
 
 static uint64_t ctx_workspace(const gcl_context* c) {
   return c->workspace_bytes ? c->workspace_bytes : workspace_budget();
+}
+
+// the items kernel of the wide search: with or without work sharing, with
+// or without its counters
+static void (*wide_items_fn(bool share, bool count))(WideArgs) {
+  if (share) return count ? wide_items_kernel<true, true> : wide_items_kernel<true, false>;
+  return count ? wide_items_kernel<false, true> : wide_items_kernel<false, false>;
 }
 
 static int cuda_status(cudaError_t e) {
@@ -360,12 +369,10 @@ int gcl_create(int device, gcl_context** out) try {
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(sp_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              kSpSmemPerBlock);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(wide_items_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             kSpSmemPerBlock);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(wide_items_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             kSpSmemPerBlock);
+  for (int share = 0; share < 2 && e == cudaSuccess; ++share)
+    for (int count = 0; count < 2 && e == cudaSuccess; ++count)
+      e = cudaFuncSetAttribute(wide_items_fn(share != 0, count != 0),
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, kSpSmemPerBlock);
   if (e != cudaSuccess) {
     c->deferred.release();
     if (c->stream) {
@@ -401,6 +408,20 @@ int gcl_sync(gcl_context* c) {
   if (!c) return GCL_ERR_ARG;
   GCL_TRY(cudaStreamSynchronize(c->stream));
   return GCL_OK;
+}
+
+int gcl_wide_counters(gcl_context* c, int64_t* out, int cap) {
+  if (!c || !out || cap < 0) return GCL_ERR_ARG;
+  if (!c->counted || !c->wide_sh.p) return GCL_ERR_ARG;  // no counted search yet
+  // the header is the first region of the search's device block (offset 0)
+  GCL_TRY(cudaSetDevice(c->device));
+  unsigned long long v[kWideCounters];
+  GCL_TRY(cudaMemcpyAsync(v, (const uint8_t*)c->wide_sh.p + offsetof(WideHdr, cnt), sizeof v,
+                          cudaMemcpyDeviceToHost, c->stream));
+  GCL_TRY(cudaStreamSynchronize(c->stream));
+  const int k = cap < (int)kWideCounters ? cap : (int)kWideCounters;
+  for (int i = 0; i < k; ++i) out[i] = (int64_t)v[i];
+  return k;
 }
 
 int gcl_canon_batch_device_async(gcl_context* c, int count, const int64_t* d_voff,
@@ -587,6 +608,10 @@ int gcl_set_option(gcl_context* c, int option, int64_t value) {
       if (value != 0 && value != 1) return GCL_ERR_ARG;
       c->wide_share = value != 0;
       return GCL_OK;
+    case GCL_OPT_COUNTERS:
+      if (value != 0 && value != 1) return GCL_ERR_ARG;
+      c->wide_count = value != 0;
+      return GCL_OK;
     case GCL_OPT_STREAM_PRIORITY: {
       if (value != 0 && value != 1) return GCL_ERR_ARG;
       int lo = 0, hi = 0;
@@ -628,9 +653,9 @@ int gcl_canon_wide_device_async(gcl_context* c, const int32_t* d_rowptr, const i
   uint64_t smw = c->smem_stage ? sp_smem_bytes(un) : 0;
   if (smw * kSpWarps > (uint64_t)kSpSmemPerBlock) smw = 0;
   int per_sm = 0;
-  GCL_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-      &per_sm, c->wide_share ? wide_items_kernel<true> : wide_items_kernel<false>, kSpThreads,
-      (size_t)(smw * kSpWarps)));
+  void (*const items)(WideArgs) = wide_items_fn(c->wide_share, c->wide_count);
+  GCL_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, items, kSpThreads,
+                                                        (size_t)(smw * kSpWarps)));
   const uint64_t budget = ctx_workspace(c);
   int64_t warps = std::min<int64_t>((int64_t)c->sms * std::max(per_sm, 1) * kSpWarps,
                                     std::max<int64_t>(kSpWarps, (int64_t)(budget / Lo.bytes)));
@@ -667,13 +692,15 @@ int gcl_canon_wide_device_async(gcl_context* c, const int32_t* d_rowptr, const i
   // would let a reader take a slot that a writer has claimed but not filled
   GCL_TRY(cudaMemsetAsync(WA.sh + WL.ready, 0, 4ull * cap, s));
   if (qcap) GCL_TRY(cudaMemsetAsync(WA.sh + WL.gready, 0, 4ull * qcap, s));
+  c->counted = false;
+  if (c->wide_count)
+    GCL_TRY(cudaMemsetAsync(WA.sh + WL.hdr + offsetof(WideHdr, cnt), 0,
+                            sizeof(((WideHdr*)nullptr)->cnt), s));
   wide_first_kernel<<<1, 32, 0, s>>>(WA);
   GCL_TRY(cudaGetLastError());
-  if (c->wide_share)
-    wide_items_kernel<true><<<(int)(warps / kSpWarps), kSpThreads, (size_t)(smw * kSpWarps), s>>>(WA);
-  else
-    wide_items_kernel<false><<<(int)(warps / kSpWarps), kSpThreads, (size_t)(smw * kSpWarps), s>>>(WA);
+  items<<<(int)(warps / kSpWarps), kSpThreads, (size_t)(smw * kSpWarps), s>>>(WA);
   GCL_TRY(cudaGetLastError());
+  c->counted = c->wide_count;
   wide_finish_kernel<<<1, 32, 0, s>>>(WA);
   GCL_TRY(cudaGetLastError());
   return GCL_OK;

@@ -116,6 +116,11 @@ void* gcl_stream(gcl_context* ctx);
  *   from the first leaf.  Same canonical form.  For trees whose work sits in
  *   a few siblings (unions of identical components).  Default 0.  Not yet
  *   measured on a GPU.
+ * GCL_OPT_COUNTERS: 1 makes the wide searches of the context count events
+ *   and clock cycles per part of the work (gcl_wide_counters), in a
+ *   separately compiled items kernel; 0 (default) runs the kernel without
+ *   them.  The counterpart of the reference's per-block section counters
+ *   (src/structs.cuh:25-77), opt-in and without files.
  * Returns GCL_ERR_ARG for an unknown option or value. */
 #define GCL_OPT_WIDE_MIN_N 1
 #define GCL_OPT_WORKSPACE_BYTES 2
@@ -124,7 +129,24 @@ void* gcl_stream(gcl_context* ctx);
 #define GCL_OPT_STREAM_PRIORITY 5
 #define GCL_OPT_WIDE_GATE 6
 #define GCL_OPT_WIDE_SHARE 7
+#define GCL_OPT_COUNTERS 8
 int gcl_set_option(gcl_context* ctx, int option, int64_t value);
+
+/* Counters of the context's last wide search (gcl_canon_one on a graph of
+ * at least GCL_OPT_WIDE_MIN_N vertices, gcl_canon_wide_device_async,
+ * gcl_group_order), summed over the warps of its items kernel, when
+ * GCL_OPT_COUNTERS was 1 for it.  Waits for the context's stream, writes up
+ * to cap values to out and returns how many (16 in this version), or
+ * GCL_ERR_ARG when that search was not counted.  In index order:
+ *   0 items searched, 1 items pruned by an orbit, 2 handed-over subtrees
+ *   taken, 3 subtrees handed over, 4 search-tree nodes, 5 leaves, 6
+ *   automorphisms from the first leaf, 7 automorphisms from the best leaf, 8
+ *   leaves that became the shared best, 9 publish retries after the shared
+ *   best moved; clock cycles (clock64, summed over warps) 10 individualize +
+ *   refine, 11 orbit tests, 12 waiting at the level gate, 13 waiting for a
+ *   handed-over subtree, 14 leaf certificates and comparisons, 15 the warps'
+ *   whole time in the kernel. */
+int gcl_wide_counters(gcl_context* ctx, int64_t* out, int cap);
 
 /* ---- one graph (drop-in for Nauty_Parallel, src/nauty_parallel.h:9-13) ---
  * out_nxn receives the n*n canonical adjacency matrix (row-major, 0/1 bytes,
