@@ -809,16 +809,17 @@ int gcl_canon_batch(gcl_context* c, int count, const int64_t* voff, const int64_
   if (eoff[count] > 0 && !col) return GCL_ERR_ARG;
   GCL_TRY(cudaSetDevice(c->device));
   const size_t nv = (size_t)voff[count], ne = (size_t)eoff[count];
-  const size_t nrp = nv + (size_t)count;
-  GCL_TRY(c->voff.ensure((count + 1) * sizeof(int64_t)));
-  GCL_TRY(c->eoff.ensure((count + 1) * sizeof(int64_t)));
+  const size_t cnt = (size_t)count;  // byte counts in size_t, not int
+  const size_t nrp = nv + cnt;
+  GCL_TRY(c->voff.ensure((cnt + 1) * sizeof(int64_t)));
+  GCL_TRY(c->eoff.ensure((cnt + 1) * sizeof(int64_t)));
   GCL_TRY(c->rowptr.ensure(nrp * sizeof(int32_t)));
   GCL_TRY(c->col.ensure(std::max<size_t>(ne, 1) * sizeof(int32_t)));
-  GCL_TRY(c->status.ensure(count * sizeof(int32_t)));
+  GCL_TRY(c->status.ensure(cnt * sizeof(int32_t)));
   cudaStream_t s = c->stream;
   DrainOnExit drain(s);
-  GCL_TRY(cudaMemcpyAsync(c->voff.p, voff, (count + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s));
-  GCL_TRY(cudaMemcpyAsync(c->eoff.p, eoff, (count + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+  GCL_TRY(cudaMemcpyAsync(c->voff.p, voff, (cnt + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+  GCL_TRY(cudaMemcpyAsync(c->eoff.p, eoff, (cnt + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s));
   GCL_TRY(cudaMemcpyAsync(c->rowptr.p, rowptr, nrp * sizeof(int32_t), cudaMemcpyHostToDevice, s));
   if (ne) GCL_TRY(cudaMemcpyAsync(c->col.p, col, ne * sizeof(int32_t), cudaMemcpyHostToDevice, s));
   int32_t* d_color = nullptr;
@@ -832,9 +833,9 @@ int gcl_canon_batch(gcl_context* c, int count, const int64_t* voff, const int64_
   size_t dense_bytes = 0;
   if (out_dense) {
     dense_bytes = (size_t)ooff[count];
-    GCL_TRY(c->ooff.ensure((count + 1) * sizeof(int64_t)));
+    GCL_TRY(c->ooff.ensure((cnt + 1) * sizeof(int64_t)));
     GCL_TRY(c->dense.ensure(std::max<size_t>(dense_bytes, 1)));
-    GCL_TRY(cudaMemcpyAsync(c->ooff.p, ooff, (count + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+    GCL_TRY(cudaMemcpyAsync(c->ooff.p, ooff, (cnt + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s));
     d_dense = (uint8_t*)c->dense.p;
     d_ooff = (int64_t*)c->ooff.p;
   }
@@ -843,9 +844,9 @@ int gcl_canon_batch(gcl_context* c, int count, const int64_t* voff, const int64_
   size_t rows_words = 0;
   if (out_rows) {
     rows_words = (size_t)roff[count];
-    GCL_TRY(c->roff.ensure((count + 1) * sizeof(int64_t)));
+    GCL_TRY(c->roff.ensure((cnt + 1) * sizeof(int64_t)));
     GCL_TRY(c->rows.ensure(std::max<size_t>(rows_words, 1) * sizeof(uint64_t)));
-    GCL_TRY(cudaMemcpyAsync(c->roff.p, roff, (count + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+    GCL_TRY(cudaMemcpyAsync(c->roff.p, roff, (cnt + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s));
     d_rows = (uint64_t*)c->rows.p;
     d_roff = (int64_t*)c->roff.p;
   }
@@ -856,7 +857,7 @@ int gcl_canon_batch(gcl_context* c, int count, const int64_t* voff, const int64_
   }
   int64_t* d_stats = nullptr;
   if (out_stats) {
-    GCL_TRY(c->stats.ensure(2 * count * sizeof(int64_t)));
+    GCL_TRY(c->stats.ensure(2 * cnt * sizeof(int64_t)));
     d_stats = (int64_t*)c->stats.p;
   }
   int rc = gcl_canon_batch_device_async(c, count, (int64_t*)c->voff.p, (int64_t*)c->eoff.p,
@@ -871,8 +872,8 @@ int gcl_canon_batch(gcl_context* c, int count, const int64_t* voff, const int64_
     GCL_TRY(cudaMemcpyAsync(out_rows, d_rows, rows_words * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
   if (d_label) GCL_TRY(cudaMemcpyAsync(out_label, d_label, nv * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
   if (d_stats)
-    GCL_TRY(cudaMemcpyAsync(out_stats, d_stats, 2 * count * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-  GCL_TRY(cudaMemcpyAsync(out_status, c->status.p, count * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    GCL_TRY(cudaMemcpyAsync(out_stats, d_stats, 2 * cnt * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+  GCL_TRY(cudaMemcpyAsync(out_status, c->status.p, cnt * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
   GCL_TRY(cudaStreamSynchronize(s));
   drain.done = true;
   for (int g = 0; g < count; ++g)
