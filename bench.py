@@ -77,6 +77,9 @@ def parse():
     p.add_argument("--e2e-contexts", type=int, default=1,
                    help="also time e2e with this many contexts on host threads, so one "
                         "step's copies run under another's kernels (1 = off)")
+    p.add_argument("--e2e-mapped", action="store_true",
+                   help="also time e2e through gcl_canon_batch_mapped (arena and results in "
+                        "mapped host memory, no staging copies; key e2e_mapped)")
     p.add_argument("--no-serving", action="store_true")
     p.add_argument("--serve-requests", type=int, default=4000)
     p.add_argument("--serve-rate", type=float, default=350.0,
@@ -480,6 +483,49 @@ def gpu_arm(args):
         return max_over_ranks(wall, world, dev)
 
     e2e_ov_s = e2e_overlap(args.e2e_contexts) if args.e2e_contexts > 1 and not args.no_e2e else None
+
+    def e2e_mapped():
+        # the arena and the outputs in mapped host memory of the context: the
+        # warp kernel reads the graphs and writes the rows over the bus, with
+        # no staging copies (set up once, outside the timed steps)
+        held = []
+
+        def mapped(a, dtype=None):
+            m = ctx.host_array(a.shape, dtype or a.dtype)
+            m[...] = a
+            held.append(m)
+            return m
+        m_voff, m_eoff, m_rp, m_col, m_roff = (mapped(a) for a in (
+            arena.voff, arena.eoff, arena.rowptr, arena.col, roff))
+        m_rows = mapped(np.zeros(h_rows.shape, np.uint64))
+        m_stats = mapped(np.zeros((count, 2), np.int64))
+        m_status = mapped(np.zeros(count, np.int32))
+
+        def call():
+            rc = lib.gcl_canon_batch_mapped(ctx.handle, count, pp(m_voff), pp(m_eoff), pp(m_rp),
+                                            pp(m_col), None, args.max_aut, None, None,
+                                            pp(m_rows), pp(m_roff), None, pp(m_stats),
+                                            pp(m_status))
+            if rc != 0:
+                raise RuntimeError(f"gcl_canon_batch_mapped failed: {rc}")
+        for _ in range(max(2, args.warmup // 2)):
+            call()
+        barrier()
+        ts = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            call()
+            ts.append(time.perf_counter() - t0)
+        barrier()
+        # the same canonical forms as the staged-copy path (h_rows: its last step)
+        same = bool(np.array_equal(m_rows.view(np.int64), h_rows))
+        for m in held:
+            ctx.host_free(m)
+        if not same:
+            raise RuntimeError("gcl_canon_batch_mapped: rows differ from gcl_canon_batch")
+        return max_over_ranks(float(np.sum(ts)), world, dev)
+
+    e2e_map_s = e2e_mapped() if args.e2e_mapped and not args.no_e2e else None
     h2d = sum(a.nbytes for a in (h_voff, h_eoff, h_rp, h_col, h_roff))
     d2h = h_rows.nbytes + h_stats.nbytes + h_status.nbytes
     h2d_dense = sum(a.nbytes for a in (h_voff, h_eoff, h_rp, h_col, h_ooff))
@@ -516,6 +562,13 @@ def gpu_arm(args):
                                 "output": "bit-packed canonical rows; steps split over "
                                           "contexts on host threads, wall clock"}}
                if e2e_ov_s is not None else {}),
+            **({"e2e_mapped": {"value": job_rate(count, world, args.steps, e2e_map_s),
+                               "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                               "d2h_bytes_per_step": int(d2h),
+                               "output": "bit-packed canonical rows; arena and results in "
+                                         "mapped host memory, read and written by the "
+                                         "kernels over the bus"}}
+               if e2e_map_s is not None else {}),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_kind": peak_kind,

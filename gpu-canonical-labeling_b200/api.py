@@ -41,7 +41,7 @@ EXPORTS = [
     "gcl_serve_create", "gcl_serve_destroy", "gcl_serve_submit", "gcl_serve_poll",
     "gcl_serve_stats_get", "gcl_serve_replay", "gcl_group_order", "gcl_perm_group_order",
     "gcl_autotune", "gcl_set_tuning", "gcl_canon_files", "gcl_format_adjacency_device_async",
-    "gcl_wide_counters",
+    "gcl_wide_counters", "gcl_host_alloc", "gcl_host_free", "gcl_canon_batch_mapped",
 ]
 
 GCL_OPT_WIDE_MIN_N = 1
@@ -129,11 +129,16 @@ def load_library(path: str = LIB_PATH):
                                                 ctypes.c_int, _P, _P, _P, _P, _P]
     lib.gcl_format_adjacency_device_async.argtypes = [_P, ctypes.c_int, _P, _P, _P, _P, _P]
     lib.gcl_wide_counters.argtypes = [_P, _P, ctypes.c_int]
+    lib.gcl_host_alloc.argtypes = [_P, ctypes.c_size_t, ctypes.POINTER(_P)]
+    lib.gcl_host_free.argtypes = [_P, _P]
+    lib.gcl_canon_batch_mapped.argtypes = [_P, ctypes.c_int, _P, _P, _P, _P, _P, ctypes.c_int,
+                                           _P, _P, _P, _P, _P, _P, _P]
     for name in ("gcl_create", "gcl_destroy", "gcl_sync", "gcl_canon_one", "gcl_canon_batch",
                  "gcl_canon_batch_device_async", "gcl_iso", "gcl_canon_batch_noalloc",
                  "gcl_set_option", "gcl_canon_wide_device_async", "gcl_group_order",
                  "gcl_perm_group_order", "gcl_autotune", "gcl_set_tuning",
-                 "gcl_canon_files", "gcl_format_adjacency_device_async", "gcl_wide_counters"):
+                 "gcl_canon_files", "gcl_format_adjacency_device_async", "gcl_wide_counters",
+                 "gcl_host_alloc", "gcl_host_free", "gcl_canon_batch_mapped"):
         getattr(lib, name).restype = ctypes.c_int
     _lib = lib
     return lib
@@ -209,6 +214,21 @@ class Context:
 
     def sync(self):
         _check(self.lib.gcl_sync(self.handle), "gcl_sync")
+
+    def host_array(self, shape, dtype) -> np.ndarray:
+        """A numpy array in mapped host memory of this context (gcl_host_alloc),
+        for gcl_canon_batch_mapped; freed with the context."""
+        dt = np.dtype(dtype)
+        count = int(np.prod(shape))
+        p = _P()
+        _check(self.lib.gcl_host_alloc(self.handle, max(count * dt.itemsize, 1), ctypes.byref(p)),
+               "gcl_host_alloc")
+        buf = (ctypes.c_uint8 * max(count * dt.itemsize, 1)).from_address(p.value)
+        return np.frombuffer(buf, dtype=dt, count=count).reshape(shape)
+
+    def host_free(self, a: np.ndarray):
+        """Frees an array from host_array (gcl_host_free); it must not be used after."""
+        _check(self.lib.gcl_host_free(self.handle, ctypes.c_void_p(a.ctypes.data)), "gcl_host_free")
 
     def wide_counters(self) -> dict:
         """Counters of the last wide search on this context, by name
@@ -385,6 +405,49 @@ def canon_batch(graphs: Union[Arena, Sequence[Graph]], max_aut: int = 10000,
     _check(rc, "gcl_canon_batch")
     return BatchResult(out, ooff, lab, stats[:arena.count], status[:arena.count], arena,
                        prow, roff)
+
+
+def canon_batch_mapped(graphs: Union[Arena, Sequence[Graph]], max_aut: int = 10000,
+                       ctx: Optional[Context] = None, dense: bool = True, label: bool = True,
+                       rows: bool = False) -> BatchResult:
+    """canon_batch through gcl_canon_batch_mapped: the arena is copied into
+    mapped host memory of the context and the results come back there (no
+    staging copies for graphs up to 64 vertices)."""
+    ctx = ctx or default_context()
+    arena = graphs if isinstance(graphs, Arena) else pack(graphs)
+    held = []
+
+    def alloc(shape, dtype):
+        held.append(ctx.host_array(shape, dtype))
+        return held[-1]
+
+    def mapped(a):
+        m = alloc(a.shape, a.dtype)
+        m[...] = a
+        return m
+    ooff = arena.out_offsets()
+    roff = rows_offsets(arena)
+    voff, eoff, rp = mapped(arena.voff), mapped(arena.eoff), mapped(arena.rowptr)
+    col = mapped(arena.col) if arena.col.size else None
+    color = mapped(arena.color) if arena.color.any() else None
+    m_ooff, m_roff = mapped(ooff), mapped(roff)
+    out = alloc((max(int(ooff[-1]), 1),), np.uint8) if dense else None
+    prow = alloc((max(int(roff[-1]), 1),), np.uint64) if rows else None
+    lab = alloc((max(int(arena.voff[-1]), 1),), np.int32) if label else None
+    stats = alloc((max(arena.count, 1), 2), np.int64)
+    status = alloc((max(arena.count, 1),), np.int32)
+    try:
+        rc = ctx.lib.gcl_canon_batch_mapped(ctx.handle, arena.count, _ptr(voff), _ptr(eoff),
+                                            _ptr(rp), _ptr(col), _ptr(color), max_aut, _ptr(out),
+                                            _ptr(m_ooff), _ptr(prow), _ptr(m_roff), _ptr(lab),
+                                            _ptr(stats), _ptr(status))
+        _check(rc, "gcl_canon_batch_mapped")
+        cp = lambda a: None if a is None else np.array(a)  # noqa: E731  (off the mapped buffers)
+        return BatchResult(cp(out), ooff, cp(lab), cp(stats[:arena.count]),
+                           cp(status[:arena.count]), arena, cp(prow), roff)
+    finally:
+        for a in held:
+            ctx.host_free(a)
 
 
 def is_isomorphic(g1: Graph, g2: Graph, max_aut: int = 10000,

@@ -64,4 +64,26 @@ inline cudaError_t pinned_alloc(void** p, size_t bytes) {
   return e;
 }
 
+// pinned host allocation mapped into the device's address space
+// (gcl_host_alloc): kernels read and write it in place over the bus; *p and
+// *dev are null on failure
+inline cudaError_t mapped_alloc(void** p, void** dev, size_t bytes) {
+  *p = nullptr;
+  *dev = nullptr;
+  if (alloc_fault_hit()) return cudaErrorMemoryAllocation;
+  cudaError_t e = cudaHostAlloc(p, bytes, cudaHostAllocMapped | cudaHostAllocPortable);
+  if (e == cudaSuccess) {
+    e = cudaHostGetDevicePointer(dev, *p, 0);
+    if (e != cudaSuccess) {
+      cudaFreeHost(*p);
+      *dev = nullptr;
+    }
+  }
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    (void)cudaGetLastError();
+  }
+  return e;
+}
+
 }  // namespace gcl

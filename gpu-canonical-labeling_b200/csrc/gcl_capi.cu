@@ -25,6 +25,7 @@
 #include "canon_warp64.cuh"
 #include "canon_wide.cuh"
 #include "gcl_alloc.h"
+#include "gcl_batch_check.h"
 #include "gcl_group.h"
 #include "gcl_guard.h"
 
@@ -255,6 +256,13 @@ struct gcl_context {
   int wide_gate = 1;             // wide search's level gate: 1 on, 0 off, 2 automatic
   bool wide_share = false;       // wide search: busy warps hand subtrees to idle ones
   bool wide_count = false;       // wide search: the items kernel's counters (GCL_OPT_COUNTERS)
+  // mapped host buffers (gcl_host_alloc): host address, size, device address
+  struct Mapped {
+    uint8_t* p;
+    size_t bytes;
+    uint8_t* dev;
+  };
+  std::vector<Mapped> mapped;
   bool counted = false;          // the last wide search was counted
   // launch shape per size bucket (gcl_autotune / gcl_set_tuning): 0 / -1 = default
   int w64_per_sm = 0;            // resident blocks the warp kernel's occupancy allows
@@ -292,6 +300,8 @@ static uint64_t workspace_budget() {
 static uint64_t ctx_workspace(const gcl_context* c) {
   return c->workspace_bytes ? c->workspace_bytes : workspace_budget();
 }
+
+static_assert(kBatchSmallN == kW64MaxN, "the host checks and the warp kernel agree on small n");
 
 // the items kernel of the wide search: with or without work sharing, with
 // or without its counters
@@ -398,6 +408,7 @@ int gcl_destroy(gcl_context* c) {
     cudaStreamSynchronize(c->stream);
     cudaStreamDestroy(c->stream);
   }
+  for (const auto& h : c->mapped) cudaFreeHost(h.p);
   delete c;
   return GCL_OK;
 }
@@ -740,6 +751,20 @@ int graph_status_to_rc(int32_t s) {
   }
 }
 
+// The device address of [p, p + count) when that range lies whole in one of
+// the context's mapped host buffers (gcl_host_alloc); null otherwise.
+template <typename T>
+T* mapped_alias(const gcl_context* c, const T* p, size_t count) {
+  if (!p) return nullptr;
+  const uintptr_t b = (uintptr_t)p;
+  const size_t bytes = count * sizeof(T);
+  for (const auto& h : c->mapped) {
+    const uintptr_t lo = (uintptr_t)h.p, hi = lo + h.bytes;
+    if (b >= lo && b <= hi && bytes <= hi - b) return (T*)(h.dev + (b - lo));
+  }
+  return nullptr;
+}
+
 // Wide search of one graph given in host memory; the dense matrix and the
 // statistics come back to the host.  GCL_ERR_INTERNAL: no result (workspace
 // outgrown or an internal check), the caller falls back.
@@ -794,23 +819,16 @@ int gcl_canon_batch(gcl_context* c, int count, const int64_t* voff, const int64_
       (out_dense && !ooff) || (out_rows && !roff))
     return GCL_ERR_ARG;
   if (count == 0) return GCL_OK;
-  if (voff[0] != 0 || eoff[0] != 0) return GCL_ERR_ARG;
-  int max_n = 0;
-  int64_t max_m2 = 0;
-  for (int g = 0; g < count; ++g) {
-    const int64_t n = voff[g + 1] - voff[g], m = eoff[g + 1] - eoff[g];
-    if (n > kW64MaxN) max_m2 = std::max(max_m2, m);
-    if (n < 0 || m < 0 || n > GCL_MAX_N) return n > GCL_MAX_N ? GCL_ERR_TOO_LARGE : GCL_ERR_ARG;
-    if (rowptr[voff[g] + g] != 0 || rowptr[voff[g + 1] + g] != m) return GCL_ERR_BAD_INPUT;
-    if (out_dense && ooff[g + 1] - ooff[g] != n * n) return GCL_ERR_ARG;
-    if (out_rows && roff[g + 1] - roff[g] != n * ((n + 63) / 64)) return GCL_ERR_ARG;
-    max_n = std::max<int>(max_n, (int)n);
-  }
-  if (eoff[count] > 0 && !col) return GCL_ERR_ARG;
+  BatchShape B;
+  const int rcb = check_batch(count, voff, eoff, rowptr, col, out_dense ? ooff : nullptr,
+                              out_rows ? roff : nullptr, &B);
+  if (rcb != GCL_OK) return rcb;
+  const int max_n = B.max_n;
+  const int64_t max_m2 = B.max_m2;
   GCL_TRY(cudaSetDevice(c->device));
-  const size_t nv = (size_t)voff[count], ne = (size_t)eoff[count];
+  const size_t nv = B.nv, ne = B.ne;
   const size_t cnt = (size_t)count;  // byte counts in size_t, not int
-  const size_t nrp = nv + cnt;
+  const size_t nrp = B.nrp;
   GCL_TRY(c->voff.ensure((cnt + 1) * sizeof(int64_t)));
   GCL_TRY(c->eoff.ensure((cnt + 1) * sizeof(int64_t)));
   GCL_TRY(c->rowptr.ensure(nrp * sizeof(int32_t)));
@@ -915,6 +933,99 @@ int gcl_canon_one(gcl_context* c, const int32_t* rowptr, const int32_t* col, con
   if (rc != GCL_OK) return rc;
   if (num_aut) *num_aut = st[0];
   if (node_count) *node_count = st[1];
+  return GCL_OK;
+} GCL_CATCH_ALL
+
+int gcl_host_alloc(gcl_context* c, size_t bytes, void** out) try {
+  if (!c || !out || bytes == 0) return GCL_ERR_ARG;
+  *out = nullptr;
+  GCL_TRY(cudaSetDevice(c->device));
+  void *p = nullptr, *dev = nullptr;
+  GCL_TRY(mapped_alloc(&p, &dev, bytes));
+  try {
+    c->mapped.push_back({(uint8_t*)p, bytes, (uint8_t*)dev});
+  } catch (...) {
+    cudaFreeHost(p);
+    throw;
+  }
+  *out = p;
+  return GCL_OK;
+} GCL_CATCH_ALL
+
+int gcl_host_free(gcl_context* c, void* p) try {
+  if (!c || !p) return GCL_ERR_ARG;
+  for (size_t i = 0; i < c->mapped.size(); ++i) {
+    if (c->mapped[i].p != (uint8_t*)p) continue;
+    cudaStreamSynchronize(c->stream);  // no kernel of the context still uses it
+    cudaFreeHost(p);
+    c->mapped.erase(c->mapped.begin() + (std::ptrdiff_t)i);
+    return GCL_OK;
+  }
+  return GCL_ERR_ARG;
+} GCL_CATCH_ALL
+
+int gcl_canon_batch_mapped(gcl_context* c, int count, const int64_t* voff, const int64_t* eoff,
+                           const int32_t* rowptr, const int32_t* col, const int32_t* color,
+                           int max_aut, uint8_t* out_dense, const int64_t* ooff,
+                           uint64_t* out_rows, const int64_t* roff, int32_t* out_label,
+                           int64_t* out_stats, int32_t* out_status) try {
+  if (!c || count < 0 || max_aut <= 0 || !voff || !eoff || !rowptr || !out_status ||
+      (out_dense && !ooff) || (out_rows && !roff))
+    return GCL_ERR_ARG;
+  if (count == 0) return GCL_OK;
+  const size_t cnt = (size_t)count;
+  // the offsets first: the host checks below read the arrays they delimit
+  if (!mapped_alias(c, voff, cnt + 1) || !mapped_alias(c, eoff, cnt + 1) ||
+      (out_dense && !mapped_alias(c, ooff, cnt + 1)) ||
+      (out_rows && !mapped_alias(c, roff, cnt + 1)))
+    return GCL_ERR_ARG;
+  // ascending vertex offsets keep every rowptr index the checks read below
+  // voff[count] + count, the extent checked here
+  for (int g = 0; g < count; ++g)
+    if (voff[g + 1] < voff[g]) return GCL_ERR_ARG;
+  if (voff[0] != 0 || !mapped_alias(c, rowptr, (size_t)voff[count] + cnt)) return GCL_ERR_ARG;
+  BatchShape B;
+  const int rcb = check_batch(count, voff, eoff, rowptr, col, out_dense ? ooff : nullptr,
+                              out_rows ? roff : nullptr, &B);
+  if (rcb != GCL_OK) return rcb;
+  // every array whole in the context's mapped buffers: the kernels read and
+  // write them in place
+  const int64_t* d_voff = mapped_alias(c, voff, cnt + 1);
+  const int64_t* d_eoff = mapped_alias(c, eoff, cnt + 1);
+  const int32_t* d_rowptr = mapped_alias(c, rowptr, B.nrp);
+  const int32_t* d_col = B.ne ? mapped_alias(c, col, B.ne) : nullptr;
+  const int32_t* d_color = color && B.nv ? mapped_alias(c, color, B.nv) : nullptr;
+  uint8_t* d_dense = out_dense ? mapped_alias(c, out_dense, B.dense_bytes) : nullptr;
+  const int64_t* d_ooff = out_dense ? mapped_alias(c, ooff, cnt + 1) : nullptr;
+  uint64_t* d_rows = out_rows ? mapped_alias(c, out_rows, B.rows_words) : nullptr;
+  const int64_t* d_roff = out_rows ? mapped_alias(c, roff, cnt + 1) : nullptr;
+  int32_t* d_label = out_label && B.nv ? mapped_alias(c, out_label, B.nv) : nullptr;
+  int64_t* d_stats = out_stats ? mapped_alias(c, out_stats, 2 * cnt) : nullptr;
+  int32_t* d_status = mapped_alias(c, out_status, cnt);
+  if (!d_rowptr || (B.ne && !d_col) || (color && B.nv && !d_color) || (out_dense && !d_dense) ||
+      (out_rows && !d_rows) || (out_label && B.nv && !d_label) || (out_stats && !d_stats) ||
+      !d_status)
+    return GCL_ERR_ARG;
+  // the kernels for larger graphs read the CSR again at every refinement
+  // step: those batches go through device copies (DMA from the same buffers)
+  if (B.max_n > kW64MaxN)
+    return gcl_canon_batch(c, count, voff, eoff, rowptr, col, color, max_aut, out_dense, ooff,
+                           out_rows, roff, out_label, out_stats, out_status);
+  GCL_TRY(cudaSetDevice(c->device));
+  cudaStream_t s = c->stream;
+  DrainOnExit drain(s);
+  if (!d_col) {  // no edges: a valid address all the same
+    GCL_TRY(c->col.ensure(sizeof(int32_t)));
+    d_col = (const int32_t*)c->col.p;
+  }
+  const int rc = gcl_canon_batch_device_async(c, count, d_voff, d_eoff, d_rowptr, d_col, d_color,
+                                              max_aut, B.max_n, B.max_m2, d_dense, d_ooff,
+                                              d_rows, d_roff, d_label, d_stats, d_status);
+  if (rc != GCL_OK) return rc;
+  GCL_TRY(cudaStreamSynchronize(s));
+  drain.done = true;
+  for (int g = 0; g < count; ++g)
+    if (out_status[g] != kOk) return graph_status_to_rc(out_status[g]);
   return GCL_OK;
 } GCL_CATCH_ALL
 

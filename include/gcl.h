@@ -198,6 +198,24 @@ int gcl_canon_batch_device_async(gcl_context* ctx, int count,
                                  int32_t* d_out_status);
 int gcl_sync(gcl_context* ctx);
 
+/* Batches whose arrays live in mapped host memory: gcl_host_alloc returns
+ * pinned host memory of the context that its kernels can address (freed by
+ * gcl_host_free or with the context).  gcl_canon_batch_mapped takes the
+ * arguments of gcl_canon_batch, every array (inputs and outputs, whole)
+ * inside such buffers, else GCL_ERR_ARG before any device work; for a batch
+ * of graphs up to 64 vertices the kernels read the arena and write the
+ * results in place over the bus, with no staging copies, so the transfers
+ * overlap the search.  Batches with larger graphs (whose kernels read the CSR
+ * again at every step) are copied as gcl_canon_batch does.  Synchronous.
+ * Not yet measured on a GPU. */
+int gcl_host_alloc(gcl_context* ctx, size_t bytes, void** out);
+int gcl_host_free(gcl_context* ctx, void* ptr);
+int gcl_canon_batch_mapped(gcl_context* ctx, int count, const int64_t* voff,
+                           const int64_t* eoff, const int32_t* rowptr, const int32_t* col,
+                           const int32_t* color, int max_aut, uint8_t* out_dense,
+                           const int64_t* ooff, uint64_t* out_rows, const int64_t* roff,
+                           int32_t* out_label, int64_t* out_stats, int32_t* out_status);
+
 /* ---- one graph, wide search, device pointers --------------------------------
  * The wide search (see GCL_OPT_WIDE_MIN_N) of one graph already on the
  * device: rowptr[n+1], col[m], color[n] or NULL.  Outputs as in the batched
