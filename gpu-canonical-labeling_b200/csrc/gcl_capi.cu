@@ -664,9 +664,8 @@ int gcl_canon_wide_device_async(gcl_context* c, const int32_t* d_rowptr, const i
   uint64_t smw = c->smem_stage ? sp_smem_bytes(un) : 0;
   if (smw * kSpWarps > (uint64_t)kSpSmemPerBlock) smw = 0;
   int per_sm = 0;
-  void (*const items)(WideArgs) = wide_items_fn(c->wide_share, c->wide_count);
-  GCL_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, items, kSpThreads,
-                                                        (size_t)(smw * kSpWarps)));
+  GCL_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &per_sm, wide_items_fn(c->wide_share, c->wide_count), kSpThreads, (size_t)(smw * kSpWarps)));
   const uint64_t budget = ctx_workspace(c);
   int64_t warps = std::min<int64_t>((int64_t)c->sms * std::max(per_sm, 1) * kSpWarps,
                                     std::max<int64_t>(kSpWarps, (int64_t)(budget / Lo.bytes)));
@@ -709,7 +708,19 @@ int gcl_canon_wide_device_async(gcl_context* c, const int32_t* d_rowptr, const i
                             sizeof(((WideHdr*)nullptr)->cnt), s));
   wide_first_kernel<<<1, 32, 0, s>>>(WA);
   GCL_TRY(cudaGetLastError());
-  items<<<(int)(warps / kSpWarps), kSpThreads, (size_t)(smw * kSpWarps), s>>>(WA);
+  const int grid = (int)(warps / kSpWarps);
+  const size_t smem = (size_t)(smw * kSpWarps);
+  if (c->wide_share) {
+    if (c->wide_count)
+      wide_items_kernel<true, true><<<grid, kSpThreads, smem, s>>>(WA);
+    else
+      wide_items_kernel<true, false><<<grid, kSpThreads, smem, s>>>(WA);
+  } else {
+    if (c->wide_count)
+      wide_items_kernel<false, true><<<grid, kSpThreads, smem, s>>>(WA);
+    else
+      wide_items_kernel<false, false><<<grid, kSpThreads, smem, s>>>(WA);
+  }
   GCL_TRY(cudaGetLastError());
   c->counted = c->wide_count;
   wide_finish_kernel<<<1, 32, 0, s>>>(WA);
