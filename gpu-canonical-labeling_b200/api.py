@@ -42,6 +42,7 @@ EXPORTS = [
     "gcl_serve_stats_get", "gcl_serve_replay", "gcl_group_order", "gcl_perm_group_order",
     "gcl_autotune", "gcl_set_tuning", "gcl_canon_files", "gcl_format_adjacency_device_async",
     "gcl_wide_counters", "gcl_host_alloc", "gcl_host_free", "gcl_canon_batch_mapped",
+    "gcl_canon_one_rows",
 ]
 
 GCL_OPT_WIDE_MIN_N = 1
@@ -129,6 +130,7 @@ def load_library(path: str = LIB_PATH):
                                                 ctypes.c_int, _P, _P, _P, _P, _P]
     lib.gcl_format_adjacency_device_async.argtypes = [_P, ctypes.c_int, _P, _P, _P, _P, _P]
     lib.gcl_wide_counters.argtypes = [_P, _P, ctypes.c_int]
+    lib.gcl_canon_one_rows.argtypes = [_P, _P, _P, _P, ctypes.c_int, ctypes.c_int, _P, _P, _P]
     lib.gcl_host_alloc.argtypes = [_P, ctypes.c_size_t, ctypes.POINTER(_P)]
     lib.gcl_host_free.argtypes = [_P, _P]
     lib.gcl_canon_batch_mapped.argtypes = [_P, ctypes.c_int, _P, _P, _P, _P, _P, ctypes.c_int,
@@ -138,7 +140,8 @@ def load_library(path: str = LIB_PATH):
                  "gcl_set_option", "gcl_canon_wide_device_async", "gcl_group_order",
                  "gcl_perm_group_order", "gcl_autotune", "gcl_set_tuning",
                  "gcl_canon_files", "gcl_format_adjacency_device_async", "gcl_wide_counters",
-                 "gcl_host_alloc", "gcl_host_free", "gcl_canon_batch_mapped"):
+                 "gcl_host_alloc", "gcl_host_free", "gcl_canon_batch_mapped",
+                 "gcl_canon_one_rows"):
         getattr(lib, name).restype = ctypes.c_int
     _lib = lib
     return lib
@@ -278,6 +281,20 @@ def canon(g: Graph, max_aut: int = 10000, ctx: Optional[Context] = None) -> Cano
                                ctypes.byref(nodes), ctypes.byref(naut))
     _check(rc, "gcl_canon_one")
     return CanonResult(out, int(nodes.value), int(naut.value))
+
+
+def canon_rows(g: Graph, max_aut: int = 10000, ctx: Optional[Context] = None):
+    """(packed rows, nodes, num_aut) of one graph (gcl_canon_one_rows): the
+    canonical matrix as n rows of ceil(n/64) words (unpack_rows gives it)."""
+    ctx = ctx or default_context()
+    rp, cl, co = _csr(g)
+    rows = np.zeros(max(g.n * ((g.n + 63) // 64), 1), dtype=np.uint64)
+    nodes = ctypes.c_int64()
+    naut = ctypes.c_int64()
+    rc = ctx.lib.gcl_canon_one_rows(ctx.handle, _ptr(rp), _ptr(cl), _ptr(co), g.n, max_aut,
+                                    _ptr(rows), ctypes.byref(nodes), ctypes.byref(naut))
+    _check(rc, "gcl_canon_one_rows")
+    return rows[: g.n * ((g.n + 63) // 64)], int(nodes.value), int(naut.value)
 
 
 @dataclass

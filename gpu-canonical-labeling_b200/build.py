@@ -53,7 +53,8 @@ def build_lib(force: bool = False, verbose: bool = False) -> str:
 def build_cli(force: bool = False) -> str:
     if not os.path.exists(CLI_SRC):
         return ""
-    deps = [CLI_SRC, LIB, os.path.join(ROOT, "include", "gcl.h"), os.path.join(CSRC, "gcl_dimacs.h")]
+    deps = [CLI_SRC, LIB, os.path.join(ROOT, "include", "gcl.h"), os.path.join(CSRC, "gcl_dimacs.h"),
+            os.path.join(CSRC, "gcl_format.h")]
     if force or _stale(CLI_BIN, deps):
         os.makedirs(os.path.dirname(CLI_BIN), exist_ok=True)
         cmd = [HOST_CXX, "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"), CLI_SRC,

@@ -12,15 +12,14 @@
 #include <algorithm>
 #include <cstdint>
 #include <fstream>
-#include <iomanip>
 #include <iostream>
-#include <sstream>
 #include <stdexcept>
 #include <string>
 #include <utility>
 #include <vector>
 
 #include "../csrc/gcl_dimacs.h"
+#include "../csrc/gcl_format.h"
 #include "gcl.h"
 
 namespace {
@@ -77,29 +76,23 @@ void print_help(const char* prog) {
 }
 
 // The reference's adjacency-list format (main.cpp:33-70): "%3u : " prefix,
-// " j" tokens, lines wrapped before column 80, ";" terminator.
-void print_adjacency_list(const std::vector<unsigned char>& A, int n, std::ostream& out) {
-  const int max_width = 80;
+// " j" tokens, lines wrapped before column 80, ";" terminator -- written row
+// by row from the packed canonical rows (gcl::format_row).
+void print_adjacency_list(const std::vector<uint64_t>& rows, int n, std::ostream& out) {
+  const size_t words = ((size_t)n + 63) / 64;
+  std::string text;
   for (int i = 0; i < n; ++i) {
-    std::ostringstream ps;
-    ps << std::setw(3) << i << " : ";
-    const std::string prefix = ps.str();
-    out << prefix;
-    int width = (int)prefix.size();
-    bool first = true;
-    for (int j = 0; j < n; ++j) {
-      if (!A[(size_t)i * n + j]) continue;
-      const std::string tok = " " + std::to_string(j);
-      if (!first && width + (int)tok.size() + 1 > max_width) {
-        out << "\n    ";
-        width = 4;
-      }
-      out << tok;
-      width += (int)tok.size();
-      first = false;
+    const uint64_t* row = rows.data() + (size_t)i * words;
+    const uint64_t len = gcl::format_row(row, (uint32_t)n, (uint32_t)i, nullptr);
+    const size_t at = text.size();
+    text.resize(at + len);
+    gcl::format_row(row, (uint32_t)n, (uint32_t)i, &text[at]);
+    if (text.size() >= (1u << 20)) {
+      out.write(text.data(), (std::streamsize)text.size());
+      text.clear();
     }
-    out << ";\n";
   }
+  out.write(text.data(), (std::streamsize)text.size());
 }
 
 struct Options {
@@ -122,18 +115,21 @@ gcl_context* context(bool sequential) {
   return c;
 }
 
-std::vector<unsigned char> canonicalize(const Graph& g, const Options& o) {
-  std::vector<unsigned char> out((size_t)g.n * g.n);
+// The canonical form as packed rows (n rows of ceil(n/64) words); false when
+// the library reports an error.
+bool canonicalize(const Graph& g, const Options& o, std::vector<uint64_t>* rows) {
+  std::vector<uint64_t>& out = *rows;
+  out.assign((size_t)g.n * (((size_t)g.n + 63) / 64), 0);
   bool colored = std::any_of(g.color.begin(), g.color.end(), [](int c) { return c != 0; });
   int64_t nodes = 0, num_aut = 0;
   gcl_context* c = context(o.sequential);
-  int rc = c ? gcl_canon_one(c, g.rowptr.data(), g.col.empty() ? nullptr : g.col.data(),
-                             colored ? g.color.data() : nullptr, g.n, (int)o.max_aut,
-                             out.empty() ? nullptr : out.data(), &nodes, &num_aut)
+  int rc = c ? gcl_canon_one_rows(c, g.rowptr.data(), g.col.empty() ? nullptr : g.col.data(),
+                                  colored ? g.color.data() : nullptr, g.n, (int)o.max_aut,
+                                  out.empty() ? nullptr : out.data(), &nodes, &num_aut)
              : GCL_ERR_CUDA;
   if (rc != GCL_OK) {
     std::cerr << "[ERROR] " << gcl_status_string(rc) << "\n";
-    return {};
+    return false;
   }
   if (o.sequential) {
     std::cout << "Total automorphisms discovered (sequential): " << num_aut << std::endl;
@@ -150,7 +146,7 @@ std::vector<unsigned char> canonicalize(const Graph& g, const Options& o) {
     else
       std::cout << "Automorphism group order: " << digits.data() << std::endl;
   }
-  return out;
+  return true;
 }
 
 }  // namespace
@@ -196,8 +192,8 @@ int main(int argc, char* argv[]) {
   try {
     if (files.size() == 1) {
       const Graph g = read_dimacs(files[0]);
-      const std::vector<unsigned char> canon = canonicalize(g, opt);
-      if (canon.empty() && g.n > 0) {
+      std::vector<uint64_t> canon;
+      if (!canonicalize(g, opt, &canon)) {
         std::cerr << "[ERROR] Canonical labeling failed.\n";
         return 1;
       }
@@ -213,21 +209,18 @@ int main(int argc, char* argv[]) {
     const Graph g2 = read_dimacs(files[1]);
     std::cout << "\nGraph 1: " << files[0] << "\n";
     std::cout << "Computing canonical form...\n";
-    const std::vector<unsigned char> c1 = canonicalize(g1, opt);
+    std::vector<uint64_t> c1, c2;
+    const bool ok1 = canonicalize(g1, opt, &c1);
     std::cout << "\nGraph 2: " << files[1] << "\n";
     std::cout << "Computing canonical form...\n";
-    const std::vector<unsigned char> c2 = canonicalize(g2, opt);
-    if ((c1.empty() && g1.n > 0) || (c2.empty() && g2.n > 0)) {
+    const bool ok2 = canonicalize(g2, opt, &c2);
+    if (!ok1 || !ok2) {
       std::cerr << "[ERROR] Canonical labeling failed.\n";
       return 1;
     }
-    bool same = g1.n == g2.n;
-    for (int i = 0; same && i < g1.n; ++i)
-      for (int j = i + 1; j < g1.n; ++j)
-        if ((c1[(size_t)i * g1.n + j] != 0) != (c2[(size_t)i * g1.n + j] != 0)) {
-          same = false;
-          break;
-        }
+    // equal upper triangles (main.cpp:73-90) of symmetric matrices with a
+    // zero diagonal: equal rows; unequal sizes are not isomorphic
+    const bool same = g1.n == g2.n && c1 == c2;
     std::cout << "\nResult: " << (same ? "ISOMORPHIC" : "NOT ISOMORPHIC") << "\n";
     return 0;
   } catch (const std::exception& e) {

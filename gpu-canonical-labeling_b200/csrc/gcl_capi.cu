@@ -776,11 +776,13 @@ T* mapped_alias(const gcl_context* c, const T* p, size_t count) {
   return nullptr;
 }
 
-// Wide search of one graph given in host memory; the dense matrix and the
-// statistics come back to the host.  GCL_ERR_INTERNAL: no result (workspace
-// outgrown or an internal check), the caller falls back.
+// Wide search of one graph given in host memory; the dense matrix (out_nxn)
+// or the packed rows (out_rows) and the statistics come back to the host.
+// GCL_ERR_INTERNAL: no result (workspace outgrown or an internal check), the
+// caller falls back.
 int canon_wide_host(gcl_context* c, const int32_t* rowptr, const int32_t* col,
-                    const int32_t* color, int n, int max_aut, uint8_t* out_nxn, int64_t* st) {
+                    const int32_t* color, int n, int max_aut, uint8_t* out_nxn,
+                    uint64_t* out_rows, int64_t* st) {
   const int64_t m = rowptr[n];
   if (rowptr[0] != 0 || m < 0) return GCL_ERR_BAD_INPUT;
   if (m > 0 && !col) return GCL_ERR_ARG;
@@ -789,7 +791,9 @@ int canon_wide_host(gcl_context* c, const int32_t* rowptr, const int32_t* col,
   DrainOnExit drain(s);
   GCL_TRY(c->rowptr.ensure(((size_t)n + 1) * sizeof(int32_t)));
   GCL_TRY(c->col.ensure(std::max<size_t>((size_t)m, 1) * sizeof(int32_t)));
-  GCL_TRY(c->dense.ensure(std::max<size_t>((size_t)n * n, 1)));
+  const size_t row_words = (size_t)n * (((size_t)n + 63) / 64);
+  if (out_nxn) GCL_TRY(c->dense.ensure(std::max<size_t>((size_t)n * n, 1)));
+  if (out_rows) GCL_TRY(c->rows.ensure(std::max<size_t>(row_words, 1) * sizeof(uint64_t)));
   GCL_TRY(c->stats.ensure(2 * sizeof(int64_t)));
   GCL_TRY(c->status.ensure(sizeof(int32_t)));
   GCL_TRY(cudaMemcpyAsync(c->rowptr.p, rowptr, ((size_t)n + 1) * sizeof(int32_t),
@@ -801,9 +805,10 @@ int canon_wide_host(gcl_context* c, const int32_t* rowptr, const int32_t* col,
     GCL_TRY(cudaMemcpyAsync(c->color.p, color, (size_t)n * sizeof(int32_t), cudaMemcpyHostToDevice, s));
     d_color = (int32_t*)c->color.p;
   }
-  int rc = gcl_canon_wide_device_async(c, (int32_t*)c->rowptr.p, (int32_t*)c->col.p, d_color, n,
-                                       m, max_aut, (uint8_t*)c->dense.p, nullptr, nullptr,
-                                       (int64_t*)c->stats.p, (int32_t*)c->status.p);
+  int rc = gcl_canon_wide_device_async(
+      c, (int32_t*)c->rowptr.p, (int32_t*)c->col.p, d_color, n, m, max_aut,
+      out_nxn ? (uint8_t*)c->dense.p : nullptr, out_rows ? (uint64_t*)c->rows.p : nullptr,
+      nullptr, (int64_t*)c->stats.p, (int32_t*)c->status.p);
   if (rc != GCL_OK) return rc == GCL_ERR_NOMEM ? GCL_ERR_INTERNAL : rc;
   int32_t status = 0;
   GCL_TRY(cudaMemcpyAsync(&status, c->status.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
@@ -811,9 +816,53 @@ int canon_wide_host(gcl_context* c, const int32_t* rowptr, const int32_t* col,
   GCL_TRY(cudaStreamSynchronize(s));
   if (status == kAutOverflow) return GCL_ERR_INTERNAL;
   if (status != kOk) return graph_status_to_rc(status);
-  GCL_TRY(cudaMemcpyAsync(out_nxn, c->dense.p, (size_t)n * n, cudaMemcpyDeviceToHost, s));
+  if (out_nxn)
+    GCL_TRY(cudaMemcpyAsync(out_nxn, c->dense.p, (size_t)n * n, cudaMemcpyDeviceToHost, s));
+  if (out_rows)
+    GCL_TRY(cudaMemcpyAsync(out_rows, c->rows.p, row_words * sizeof(uint64_t),
+                            cudaMemcpyDeviceToHost, s));
   GCL_TRY(cudaStreamSynchronize(s));
   drain.done = true;
+  return GCL_OK;
+}
+
+// gcl_canon_one with the dense matrix (out_nxn) or the packed rows (out_rows)
+int canon_one(gcl_context* c, const int32_t* rowptr, const int32_t* col, const int32_t* color,
+              int n, int max_aut, uint8_t* out_nxn, uint64_t* out_rows, int64_t* node_count,
+              int64_t* num_aut) {
+  std::unique_lock<std::mutex> shared_ctx;
+  if (!c) {
+    int rc = default_context(&c);
+    if (rc != GCL_OK) return rc;
+    shared_ctx = std::unique_lock<std::mutex>(g_default_mu);
+  }
+  if (n == 0) {  // the reference's search visits the (discrete) root only
+    if (node_count) *node_count = 1;
+    if (num_aut) *num_aut = 0;
+    return GCL_OK;
+  }
+  int64_t st[2] = {0, 0};
+  if ((int64_t)n >= c->wide_min_n && n <= GCL_MAX_N) {
+    const int rcw = canon_wide_host(c, rowptr, col, color, n, max_aut, out_nxn, out_rows, st);
+    if (rcw != GCL_ERR_INTERNAL) {  // no result for want of workspace: sequential search
+      if (rcw == GCL_OK) {
+        if (num_aut) *num_aut = st[0];
+        if (node_count) *node_count = st[1];
+      }
+      return rcw;
+    }
+  }
+  const int64_t voff[2] = {0, n};
+  const int64_t eoff[2] = {0, rowptr[n]};
+  const int64_t ooff[2] = {0, (int64_t)n * n};
+  const int64_t roff[2] = {0, (int64_t)n * (((int64_t)n + 63) / 64)};
+  int32_t status = 0;
+  int rc = gcl_canon_batch(c, 1, voff, eoff, rowptr, col, color, max_aut, out_nxn,
+                           out_nxn ? ooff : nullptr, out_rows, out_rows ? roff : nullptr, nullptr,
+                           st, &status);
+  if (rc != GCL_OK) return rc;
+  if (num_aut) *num_aut = st[0];
+  if (node_count) *node_count = st[1];
   return GCL_OK;
 }
 
@@ -913,38 +962,14 @@ int gcl_canon_batch(gcl_context* c, int count, const int64_t* voff, const int64_
 int gcl_canon_one(gcl_context* c, const int32_t* rowptr, const int32_t* col, const int32_t* color,
                   int n, int max_aut, uint8_t* out_nxn, int64_t* node_count, int64_t* num_aut) try {
   if (n < 0 || !rowptr || max_aut <= 0 || (n > 0 && !out_nxn)) return GCL_ERR_ARG;
-  std::unique_lock<std::mutex> shared_ctx;
-  if (!c) {
-    int rc = default_context(&c);
-    if (rc != GCL_OK) return rc;
-    shared_ctx = std::unique_lock<std::mutex>(g_default_mu);
-  }
-  if (n == 0) {  // the reference's search visits the (discrete) root only
-    if (node_count) *node_count = 1;
-    if (num_aut) *num_aut = 0;
-    return GCL_OK;
-  }
-  int64_t st[2] = {0, 0};
-  if ((int64_t)n >= c->wide_min_n && n <= GCL_MAX_N) {
-    const int rcw = canon_wide_host(c, rowptr, col, color, n, max_aut, out_nxn, st);
-    if (rcw != GCL_ERR_INTERNAL) {  // no result for want of workspace: sequential search
-      if (rcw == GCL_OK) {
-        if (num_aut) *num_aut = st[0];
-        if (node_count) *node_count = st[1];
-      }
-      return rcw;
-    }
-  }
-  const int64_t voff[2] = {0, n};
-  const int64_t eoff[2] = {0, rowptr[n]};
-  const int64_t ooff[2] = {0, (int64_t)n * n};
-  int32_t status = 0;
-  int rc = gcl_canon_batch(c, 1, voff, eoff, rowptr, col, color, max_aut, out_nxn, ooff, nullptr,
-                           nullptr, nullptr, st, &status);
-  if (rc != GCL_OK) return rc;
-  if (num_aut) *num_aut = st[0];
-  if (node_count) *node_count = st[1];
-  return GCL_OK;
+  return canon_one(c, rowptr, col, color, n, max_aut, out_nxn, nullptr, node_count, num_aut);
+} GCL_CATCH_ALL
+
+int gcl_canon_one_rows(gcl_context* c, const int32_t* rowptr, const int32_t* col,
+                       const int32_t* color, int n, int max_aut, uint64_t* out_rows,
+                       int64_t* node_count, int64_t* num_aut) try {
+  if (n < 0 || !rowptr || max_aut <= 0 || (n > 0 && !out_rows)) return GCL_ERR_ARG;
+  return canon_one(c, rowptr, col, color, n, max_aut, nullptr, out_rows, node_count, num_aut);
 } GCL_CATCH_ALL
 
 int gcl_host_alloc(gcl_context* c, size_t bytes, void** out) try {

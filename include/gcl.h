@@ -159,6 +159,13 @@ int gcl_wide_counters(gcl_context* ctx, int64_t* out, int cap);
 int gcl_canon_one(gcl_context* ctx, const int32_t* rowptr, const int32_t* col,
                   const int32_t* color, int n, int max_aut, uint8_t* out_nxn,
                   int64_t* node_count, int64_t* num_aut);
+/* The same with the canonical matrix bit-packed: out_rows receives n rows of
+ * ceil(n/64) words, bit j of row i (word j/64, bit j%64) set iff canonical
+ * vertices i and j are adjacent (gcl_canon_batch's out_rows), so a large
+ * graph's result is n*n/8 bytes to copy and to read, not n*n. */
+int gcl_canon_one_rows(gcl_context* ctx, const int32_t* rowptr, const int32_t* col,
+                       const int32_t* color, int n, int max_aut, uint64_t* out_rows,
+                       int64_t* node_count, int64_t* num_aut);
 
 /* ---- batched: many graphs in one ragged CSR arena ----------------------
  * Graph g has n_g = voff[g+1]-voff[g] vertices; its local rowptr (n_g + 1
