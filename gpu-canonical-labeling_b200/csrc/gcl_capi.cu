@@ -1075,18 +1075,15 @@ int gcl_iso(gcl_context* c, const int32_t* rp1, const int32_t* col1, const int32
     if (rc != GCL_OK) return rc;
     shared_ctx = std::unique_lock<std::mutex>(g_default_mu);
   }
-  std::vector<uint8_t> a((size_t)n1 * n1 + 1), b((size_t)n2 * n2 + 1);
-  int rc = gcl_canon_one(c, rp1, col1, color1, n1, max_aut, a.data(), nullptr, nullptr);
-  if (rc == GCL_OK) rc = gcl_canon_one(c, rp2, col2, color2, n2, max_aut, b.data(), nullptr, nullptr);
+  // packed canonical rows: equal upper triangles (main.cpp:73-90) of
+  // symmetric matrices with a zero diagonal are equal rows
+  std::vector<uint64_t> a((size_t)n1 * (((size_t)n1 + 63) / 64) + 1);
+  std::vector<uint64_t> b((size_t)n2 * (((size_t)n2 + 63) / 64) + 1);
+  int rc = canon_one(c, rp1, col1, color1, n1, max_aut, nullptr, a.data(), nullptr, nullptr);
+  if (rc == GCL_OK)
+    rc = canon_one(c, rp2, col2, color2, n2, max_aut, nullptr, b.data(), nullptr, nullptr);
   if (rc != GCL_OK) return rc;
-  int same = n1 == n2;
-  for (int i = 0; same && i < n1; ++i)
-    for (int j = i + 1; j < n1; ++j)
-      if ((a[(size_t)i * n1 + j] != 0) != (b[(size_t)i * n1 + j] != 0)) {
-        same = 0;
-        break;
-      }
-  *verdict = same;
+  *verdict = n1 == n2 && a == b;
   return GCL_OK;
 } GCL_CATCH_ALL
 
