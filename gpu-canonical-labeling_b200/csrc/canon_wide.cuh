@@ -1407,13 +1407,20 @@ __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
 // ---------------------------------------------------------------------------
 // 3. Outputs from the shared best leaf (one warp).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(32) wide_finish_kernel(WideArgs A) {
+constexpr int kWideFinishThreads = 128;
+
+// A warp per canonical row (grid-stride): the row's packed words, each lane
+// building whole words from the row's certificate entries, and its dense
+// bytes, zeroed and then set -- no two lanes write the same byte or word.
+__global__ void __launch_bounds__(kWideFinishThreads) wide_finish_kernel(WideArgs A) {
   const uint32_t lane = lane_id();
+  const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   const WidePtrs P = wide_ptrs(A);
   const WideHdr* H = P.H;
   const uint32_t n = A.n;
   const int32_t status = H->status;
-  if (lane == 0) {
+  if (warp == 0 && lane == 0) {
     A.out_status[0] = status;
     if (A.out_stats) {
       A.out_stats[0] = (int64_t)H->naut;
@@ -1422,27 +1429,32 @@ __global__ void __launch_bounds__(32) wide_finish_kernel(WideArgs A) {
   }
   if (status != kOk) return;
   if (A.out_label)
-    for (uint32_t j = lane; j < n; j += 32) A.out_label[j] = (int32_t)P.blabel[j];
+    for (uint64_t j = warp * 32 + lane; j < n; j += warps * 32)
+      A.out_label[j] = (int32_t)P.blabel[j];
   if (A.out_rows) {
     const uint32_t words = (n + 63) / 64;
-    for (uint32_t i = lane; i < n; i += 32) {
-      uint64_t* row = A.out_rows + (uint64_t)i * words;
-      for (uint32_t w = 0; w < words; ++w) row[w] = 0;
+    for (uint64_t i = warp; i < n; i += warps) {
+      uint64_t* row = A.out_rows + i * words;
       const uint32_t v = P.blabel[i];
-      for (int32_t j = A.rp[v]; j < A.rp[v + 1]; ++j) {
-        const uint32_t c = P.bcert[j];
-        row[c >> 6] |= bit64(c & 63);
+      const int32_t b = A.rp[v], e = A.rp[v + 1];
+      for (uint32_t w = lane; w < words; w += 32) {
+        uint64_t x = 0;
+        for (int32_t j = b; j < e; ++j) {
+          const uint32_t c = P.bcert[j];
+          if ((c >> 6) == w) x |= bit64(c & 63);
+        }
+        row[w] = x;
       }
     }
   }
   if (A.out_dense) {
-    const uint64_t nn = (uint64_t)n * n;
-    for (uint64_t i = lane; i < nn; i += 32) A.out_dense[i] = 0;
-    __syncwarp();
-    for (uint32_t i = 0; i < n; ++i) {
+    for (uint64_t i = warp; i < n; i += warps) {
+      uint8_t* row = A.out_dense + i * n;
+      for (uint32_t j = lane; j < n; j += 32) row[j] = 0;
+      __syncwarp();
       const uint32_t v = P.blabel[i];
-      for (int32_t j = A.rp[v] + (int32_t)lane; j < A.rp[v + 1]; j += 32)
-        A.out_dense[(uint64_t)i * n + P.bcert[j]] = 1;
+      for (int32_t j = A.rp[v] + (int32_t)lane; j < A.rp[v + 1]; j += 32) row[P.bcert[j]] = 1;
+      __syncwarp();
     }
   }
 }

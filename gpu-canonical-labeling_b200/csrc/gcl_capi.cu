@@ -723,7 +723,12 @@ int gcl_canon_wide_device_async(gcl_context* c, const int32_t* d_rowptr, const i
   }
   GCL_TRY(cudaGetLastError());
   c->counted = c->wide_count;
-  wide_finish_kernel<<<1, 32, 0, s>>>(WA);
+  // a warp per canonical row, up to 8 blocks of 4 warps per SM
+  const int64_t finish_warps_per_block = kWideFinishThreads / 32;
+  const int finish_blocks = (int)std::max<int64_t>(
+      1, std::min<int64_t>(((int64_t)n + finish_warps_per_block - 1) / finish_warps_per_block,
+                           (int64_t)std::max(c->sms, 1) * 8));
+  wide_finish_kernel<<<finish_blocks, kWideFinishThreads, 0, s>>>(WA);
   GCL_TRY(cudaGetLastError());
   return GCL_OK;
 } GCL_CATCH_ALL
