@@ -1409,6 +1409,20 @@ __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
 // ---------------------------------------------------------------------------
 constexpr int kWideFinishThreads = 128;
 
+// Word w of canonical row i of the best leaf's packed matrix: bit c % 64 for
+// every certificate entry c (a neighbour's canonical position) of the row's
+// vertex with c / 64 == w.
+__host__ __device__ inline uint64_t wide_row_word(const int32_t* rp, const uint32_t* label,
+                                                  const uint32_t* cert, uint32_t i, uint32_t w) {
+  const uint32_t v = label[i];
+  uint64_t x = 0;
+  for (int32_t j = rp[v]; j < rp[v + 1]; ++j) {
+    const uint32_t c = cert[j];
+    if ((c >> 6) == w) x |= 1ull << (c & 63);
+  }
+  return x;
+}
+
 // A warp per canonical row (grid-stride): the row's packed words, each lane
 // building whole words from the row's certificate entries, and its dense
 // bytes, zeroed and then set -- no two lanes write the same byte or word.
@@ -1435,16 +1449,8 @@ __global__ void __launch_bounds__(kWideFinishThreads) wide_finish_kernel(WideArg
     const uint32_t words = (n + 63) / 64;
     for (uint64_t i = warp; i < n; i += warps) {
       uint64_t* row = A.out_rows + i * words;
-      const uint32_t v = P.blabel[i];
-      const int32_t b = A.rp[v], e = A.rp[v + 1];
-      for (uint32_t w = lane; w < words; w += 32) {
-        uint64_t x = 0;
-        for (int32_t j = b; j < e; ++j) {
-          const uint32_t c = P.bcert[j];
-          if ((c >> 6) == w) x |= bit64(c & 63);
-        }
-        row[w] = x;
-      }
+      for (uint32_t w = lane; w < words; w += 32)
+        row[w] = wide_row_word(A.rp, P.blabel, P.bcert, (uint32_t)i, w);
     }
   }
   if (A.out_dense) {
