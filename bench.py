@@ -128,7 +128,7 @@ _W = {}
 
 def _cpu_init(kind, arrays):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle  # the checker / CPU baseline (test infrastructure)
+    import oracle  # the oracle: the timed CPU baseline (test infrastructure)
     G = importlib.import_module(PKG + ".graphs")
     _W["oracle"] = oracle
     _W["kind"] = kind
@@ -756,7 +756,7 @@ def single_graph_block(args, pkg, local, with_cpu):
     O = None
     if with_cpu:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
-        import oracle as O  # the reference's CPU path (checker / baseline)
+        import oracle as O  # the reference's CPU path (the oracle / baseline)
     for name, g, cpu in cases:
         rel = G.random_relabel(g, rng)
         pkg.canon(g, ctx=ctx)  # warm-up (workspace)

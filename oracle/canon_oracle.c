@@ -1,4 +1,4 @@
-/* canon_oracle.c -- TEST INFRASTRUCTURE ONLY (the parity checker).
+/* canon_oracle.c -- TEST INFRASTRUCTURE ONLY (the parity oracle).
  *
  * A plain-C restatement of the reference's sequential canonical labeler.
  * Every function names the reference file:line range whose behaviour it

@@ -2,7 +2,7 @@
  *
  * CPU restatement of the reference's sequential individualization-refinement
  * canonical labeler (src/sequential.cpp, src/partition_refinement.cpp,
- * src/perm_group.cpp).  Used by tests/ as the parity checker, by
+ * src/perm_group.cpp).  Used by tests/ as the parity oracle, by
  * __graft_entry__.smoke() and by bench.py's cpu_baseline leg.  The product
  * library never links or calls it.
  *

@@ -1,6 +1,6 @@
-"""ctypes front-end for the CPU checkers -- TEST INFRASTRUCTURE ONLY.
+"""ctypes front-end for the CPU oracles -- TEST INFRASTRUCTURE ONLY.
 
-Two checkers live here:
+Two oracles live here:
 
 * ``port``      -- ``libgcl_oracle.so``: the plain-C restatement of the
                    reference's sequential labeler (canon_oracle.c).
@@ -14,7 +14,7 @@ rules on the CPU (``wide_model``) and an unpruned maximum-leaf search
 (``exhaustive``).
 
 Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg use
-this module, and only as the checker / the timed CPU baseline.
+this module, and only as the oracle / the timed CPU baseline.
 """
 from __future__ import annotations
 
@@ -95,7 +95,7 @@ def canon(g, max_aut: int = 10000, kind: str = "port") -> Tuple[np.ndarray, np.n
 
 def canon_batch(arena, max_aut: int = 10000, kind: str = "port",
                 want_matrix: bool = True):
-    """Run the checker over an Arena.  Returns (out_arena or None, ooff,
+    """Run the oracle over an Arena.  Returns (out_arena or None, ooff,
     num_aut[count], nodes[count])."""
     lib = _load(kind)
     ooff = arena.out_offsets()

@@ -22,7 +22,7 @@ torch = pytest.importorskip("torch")
 def dropin(oracle_mod):
     if not os.path.exists(BIN):
         if not oracle_mod.available("reference"):
-            pytest.skip("the reference's sources were not available to build the checkers")
+            pytest.skip("the reference's sources were not available to build the oracles")
         subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "dropin"], check=True)
     return BIN
 

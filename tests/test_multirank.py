@@ -2,7 +2,7 @@
 
 Graphs are independent, so a batch shards by graph with no collective on the
 data path: each rank canonizes its own size-balanced range (here with the CPU
-checker standing in for its GPU) and the results are gathered at the end; the
+oracle standing in for its GPU) and the results are gathered at the end; the
 job's time is the slowest rank's (bench.py's max_over_ranks / job_rate)."""
 import os
 import socket

@@ -1,4 +1,4 @@
-"""The CPU checker (oracle/canon_oracle.c) against the reference's golden
+"""The CPU oracle (oracle/canon_oracle.c) against the reference's golden
 vectors, and against the reference itself where it was compiled here."""
 import hashlib
 
