@@ -72,20 +72,30 @@ constexpr int kMaxDevices = 64;
 std::mutex g_noalloc_mu;
 NoAllocDevice g_noalloc_dev[kMaxDevices];
 
+// A failed runtime call of the set-up: its error is returned as a status and
+// not left behind as the thread's last error, where a later launch check of
+// the caller's own work would find it.
+int noalloc_fail() {
+  (void)cudaGetLastError();
+  return GCL_ERR_CUDA;
+}
+
 // Once per device, with that device current: resolve the scratch's device
-// address and the launch shape.
+// address and the launch shape.  The result is kept for the life of the
+// process; a cudaDeviceReset of the device discards the module that holds the
+// array, so the entry point must not be called on a device after a reset.
 int noalloc_setup(int dev, NoAllocDevice** out) {
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
   NoAllocDevice& d = g_noalloc_dev[dev];
   if (!d.ready) {
     void* p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return GCL_ERR_CUDA;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return noalloc_fail();
     int sms = 0, per_sm = 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
-      return GCL_ERR_CUDA;
+      return noalloc_fail();
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, w64_noalloc_kernel, kW64Threads,
                                                       0) != cudaSuccess)
-      return GCL_ERR_CUDA;
+      return noalloc_fail();
     d.scratch = static_cast<uint8_t*>(p);
     d.grid = std::min(kNoAllocSlots / kW64Warps, std::max(1, sms * std::max(per_sm, 1)));
     d.ready = true;
@@ -108,16 +118,19 @@ extern "C" int gcl_canon_batch_noalloc(void* stream, int count, const int64_t* d
   if (max_n > kW64MaxN) return GCL_ERR_TOO_LARGE;  // this entry point: n <= 64 only
   if (count == 0) return GCL_OK;
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return GCL_ERR_CUDA;
+  if (cudaGetDevice(&dev) != cudaSuccess) return noalloc_fail();
   if (dev < 0 || dev >= kMaxDevices) return GCL_ERR_ARG;
   NoAllocDevice* d = nullptr;
   const int rc = noalloc_setup(dev, &d);
   if (rc != GCL_OK) return rc;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // A non-sticky error left by the caller's earlier work would otherwise be
+  // reported by the launch check below as this call's failure.
+  (void)cudaGetLastError();
   // The scratch keeps the previous call's contents; only the work counter
   // must start at zero (representatives and ring entries are written before
   // they are read within each graph's search).
-  if (cudaMemsetAsync(d->scratch, 0, kNoAllocHeader, s) != cudaSuccess) return GCL_ERR_CUDA;
+  if (cudaMemsetAsync(d->scratch, 0, kNoAllocHeader, s) != cudaSuccess) return noalloc_fail();
 
   BatchArgs A;
   A.count = count;
@@ -143,5 +156,5 @@ extern "C" int gcl_canon_batch_noalloc(void* stream, int count, const int64_t* d
   A.budget_ns = budget_s > 0 ? (uint64_t)(budget_s * 1e9) : 0;
   const int grid = (int)std::min<int64_t>(d->grid, ((int64_t)count + kW64Warps - 1) / kW64Warps);
   w64_noalloc_kernel<<<grid, kW64Threads, 0, s>>>(A, d->scratch);
-  return cudaGetLastError() == cudaSuccess ? GCL_OK : GCL_ERR_CUDA;
+  return cudaGetLastError() == cudaSuccess ? GCL_OK : noalloc_fail();
 }
