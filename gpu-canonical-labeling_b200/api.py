@@ -122,7 +122,8 @@ def load_library(path: str = LIB_PATH):
                                  ctypes.POINTER(Tuning)]
     lib.gcl_set_tuning.argtypes = [_P, ctypes.POINTER(Tuning)]
     lib.gcl_group_order.argtypes = [_P, _P, _P, _P, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
-                                    ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int64)]
+                                    ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int64),
+                                    ctypes.POINTER(ctypes.c_int)]
     lib.gcl_perm_group_order.argtypes = [ctypes.c_int, _P, ctypes.c_int64,
                                          ctypes.POINTER(ctypes.c_double), ctypes.c_char_p,
                                          ctypes.c_int]
@@ -329,18 +330,23 @@ def canon_files(paths: Sequence[str], max_aut: int = 10000, ctx: Optional[Contex
     return out
 
 
-def group_order(g: Graph, ctx: Optional[Context] = None) -> int:
+def group_order(g: Graph, ctx: Optional[Context] = None, return_checked: bool = False):
     """|Aut(g)| (colour-preserving), exact, from the automorphisms the wide
-    search finds (gcl_group_order)."""
+    search finds (gcl_group_order).  With return_checked, (order, checked):
+    checked is 1 when a Schreier-Sims completion confirmed the order, -1 when
+    the completion's differing order was returned, 0 when no completion
+    finished within its budget (the first path's orbit product, unchecked)."""
     ctx = ctx or default_context()
     rp, cl, co = _csr(g)
     lg = ctypes.c_double()
     ngen = ctypes.c_int64()
+    chk = ctypes.c_int()
     buf = ctypes.create_string_buffer(1 << 20)
     rc = ctx.lib.gcl_group_order(ctx.handle, _ptr(rp), _ptr(cl), _ptr(co), g.n, ctypes.byref(lg),
-                                 buf, len(buf), ctypes.byref(ngen))
+                                 buf, len(buf), ctypes.byref(ngen), ctypes.byref(chk))
     _check(rc, "gcl_group_order")
-    return int(buf.value.decode())
+    order = int(buf.value.decode())
+    return (order, chk.value) if return_checked else order
 
 
 def perm_group_order(perms) -> int:
@@ -501,7 +507,8 @@ class ServeResult(ctypes.Structure):
     _fields_ = [("id", ctypes.c_int64), ("status", ctypes.c_int32), ("verdict", ctypes.c_int32),
                 ("repeat", ctypes.c_int32), ("batch", ctypes.c_int32),
                 ("class_id", ctypes.c_int64), ("canon_hash", ctypes.c_uint64),
-                ("latency_s", ctypes.c_double)]
+                ("latency_s", ctypes.c_double), ("admit_s", ctypes.c_double),
+                ("launch_s", ctypes.c_double), ("gpu_done_s", ctypes.c_double)]
 
 
 class ServeStats(ctypes.Structure):
@@ -509,7 +516,8 @@ class ServeStats(ctypes.Structure):
                                               "memo_hits", "class_repeats", "classes",
                                               "large_graphs")] + [
         ("class_batches", ctypes.c_int64 * 4), ("class_batch_ns", ctypes.c_int64 * 4),
-        ("class_queue_ns", ctypes.c_int64 * 4)]
+        ("class_queue_ns", ctypes.c_int64 * 4), ("class_max_launch_ns", ctypes.c_int64 * 4),
+        ("class_max_complete_ns", ctypes.c_int64 * 4)]
 
 
 def _serve_sigs(lib):

@@ -138,13 +138,16 @@ bool canonicalize(const Graph& g, const Options& o, std::vector<uint64_t>* rows)
   if (o.group_order) {
     double lg = 0;
     std::vector<char> digits(1 << 20);
+    int checked = 0;
     int rg = gcl_group_order(c, g.rowptr.data(), g.col.empty() ? nullptr : g.col.data(),
                              colored ? g.color.data() : nullptr, g.n, &lg, digits.data(),
-                             (int)digits.size(), nullptr);
+                             (int)digits.size(), nullptr, &checked);
     if (rg != GCL_OK)
       std::cerr << "[ERROR] group order: " << gcl_status_string(rg) << "\n";
     else
-      std::cout << "Automorphism group order: " << digits.data() << std::endl;
+      std::cout << "Automorphism group order: " << digits.data()
+                << (checked == 0 ? " (unchecked: Schreier-Sims budget exceeded)" : "")
+                << std::endl;
   }
   return true;
 }

@@ -1094,7 +1094,7 @@ int gcl_iso(gcl_context* c, const int32_t* rp1, const int32_t* col1, const int32
 
 int gcl_group_order(gcl_context* c, const int32_t* rowptr, const int32_t* col,
                     const int32_t* color, int n, double* log10_order, char* digits,
-                    int digits_cap, int64_t* generators) try {
+                    int digits_cap, int64_t* generators, int* checked) try {
   if (n < 0 || !rowptr || !log10_order || (digits && digits_cap < 2)) return GCL_ERR_ARG;
   if (n > GCL_MAX_N) return GCL_ERR_TOO_LARGE;
   std::unique_lock<std::mutex> shared_ctx;
@@ -1103,15 +1103,17 @@ int gcl_group_order(gcl_context* c, const int32_t* rowptr, const int32_t* col,
     if (rc != GCL_OK) return rc;
     shared_ctx = std::unique_lock<std::mutex>(g_default_mu);
   }
-  auto put = [&](const std::string& d, double lg, int64_t ng) {
+  if (checked) *checked = 0;
+  auto put = [&](const std::string& d, double lg, int64_t ng, int chk) {
     *log10_order = lg;
     if (generators) *generators = ng;
+    if (checked) *checked = chk;
     if (!digits) return GCL_OK;
     if ((int)d.size() + 1 > digits_cap) return GCL_ERR_ARG;
     std::memcpy(digits, d.c_str(), d.size() + 1);
     return GCL_OK;
   };
-  if (n <= 1) return put("1", 0.0, 0);
+  if (n <= 1) return put("1", 0.0, 0, 1);
   // a wide search whose store takes every automorphism it finds
   const int64_t m = rowptr[n];
   if (rowptr[0] != 0 || m < 0) return GCL_ERR_BAD_INPUT;
@@ -1170,9 +1172,9 @@ int gcl_group_order(gcl_context* c, const int32_t* rowptr, const int32_t* col,
   // finishes within its work budget (its order wins a disagreement)
   double lg = 0;
   std::string d;
-  int checked = 0;
+  int chk = 0;
   const int rg = group_order_of_search(un, auts.data(), (uint64_t)st[0], WL.stride, base.data(),
-                                       D - 1, kGroupCheckCap, &lg, &d, &checked);
+                                       D - 1, kGroupCheckCap, &lg, &d, &chk);
   if (rg != kOrderOk) {
     // the first path is no base (an internal inconsistency): the general
     // completion alone, with the full budget
@@ -1180,9 +1182,10 @@ int gcl_group_order(gcl_context* c, const int32_t* rowptr, const int32_t* col,
     if (!group_order(un, auts.data(), (uint64_t)st[0], WL.stride, kGroupWorkCap, &lg, &d,
                      &base_len))
       return GCL_ERR_INTERNAL;
+    chk = 1;
   }
   drain.done = true;
-  return put(d, lg, st[0]);
+  return put(d, lg, st[0], chk);
 } GCL_CATCH_ALL
 
 int gcl_perm_group_order(int n, const uint16_t* perms, int64_t count, double* log10_order,

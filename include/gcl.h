@@ -251,7 +251,9 @@ int gcl_canon_wide_device_async(gcl_context* ctx, const int32_t* d_rowptr,
  *   no result.
  *   The first call on a device resolves the scratch's device address and the
  *   launch shape for that device; make that first call before any stream
- *   capture on the device.
+ *   capture on the device.  That set-up is kept for the life of the process:
+ *   after a cudaDeviceReset of a device, do not call this entry point on it
+ *   again (the reset discards the array the kept address points into).
  *   All calls share the one scratch array, which keeps the last call's
  *   contents: calls that overlap on the GPU (other streams, other threads)
  *   race and corrupt each other; serialize them. */
@@ -328,7 +330,12 @@ int gcl_set_tuning(gcl_context* ctx, const gcl_tuning* tuning);
  * base), whose order is returned when one finishes within its work budget
  * (about a second).  *log10_order = log10 |Aut|,
  * digits (if not NULL) the order in decimal, *generators the automorphisms
- * the search stored.  GCL_ERR_TOO_LARGE if the search found more
+ * the search stored, *checked (if not NULL) how the order was confirmed:
+ * 1 a finished Schreier-Sims completion gave the same order; -1 it gave a
+ * different one, which is returned (the stored automorphisms generate the
+ * group but are no strong generating set for the first path); 0 neither
+ * completion finished within its budget and the orbit product is returned
+ * unchecked.  GCL_ERR_TOO_LARGE if the search found more
  * automorphisms than its 1 GiB store holds, GCL_ERR_ARG if digits_cap is too
  * small.  gcl_perm_group_order returns GCL_ERR_TIMEOUT when its
  * Schreier-Sims exceeds the work cap.
@@ -336,7 +343,7 @@ int gcl_set_tuning(gcl_context* ctx, const gcl_tuning* tuning);
  * generated by `count` permutations of {0..n-1} (row a at perms + a*n). */
 int gcl_group_order(gcl_context* ctx, const int32_t* rowptr, const int32_t* col,
                     const int32_t* color, int n, double* log10_order, char* digits,
-                    int digits_cap, int64_t* generators);
+                    int digits_cap, int64_t* generators, int* checked);
 int gcl_perm_group_order(int n, const uint16_t* perms, int64_t count, double* log10_order,
                          char* digits, int digits_cap);
 
@@ -420,6 +427,11 @@ typedef struct {
   int64_t class_id;    /* isomorphism class of (the first) graph, -1 unknown   */
   uint64_t canon_hash; /* 64-bit hash of the canonical form                    */
   double latency_s;    /* submit -> result ready (host steady clock)           */
+  /* the request's timeline, seconds after submit like latency_s (0 for a
+     memo answer): taken into a batch, the batch's work enqueued on its lane
+     (copies, kernels), and the lane's stream reached the batch's end on the
+     GPU (its completion callback ran) */
+  double admit_s, launch_s, gpu_done_s;
 } gcl_serve_result;
 
 typedef struct {
@@ -428,6 +440,11 @@ typedef struct {
   /* per request class (small, mid, big, large): batches launched, their
      summed launch-to-result time and summed time queued before launch (ns) */
   int64_t class_batches[4], class_batch_ns[4], class_queue_ns[4];
+  /* per request class: the longest host time the dispatcher spent enqueuing
+     one batch (packing, copies and launches issued) and finishing one
+     (results handed out), ns -- the dispatcher serves every lane, so this is
+     time no other lane could be launched or finished */
+  int64_t class_max_launch_ns[4], class_max_complete_ns[4];
 } gcl_serve_stats;
 
 /* cfg may be NULL (all defaults); zero fields take their default. */

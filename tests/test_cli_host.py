@@ -26,9 +26,9 @@ int gcl_create(int device, gcl_context** out) { (void)device; *out = (gcl_contex
 int gcl_set_option(gcl_context* c, int o, int64_t v) { (void)c; (void)o; (void)v; return 0; }
 const char* gcl_status_string(int s) { (void)s; return "stand-in error"; }
 int gcl_group_order(gcl_context* c, const int32_t* rp, const int32_t* col, const int32_t* color,
-                    int n, double* lg, char* digits, int cap, int64_t* gens) {
+                    int n, double* lg, char* digits, int cap, int64_t* gens, int* checked) {
   (void)c; (void)rp; (void)col; (void)color; (void)n; (void)lg; (void)digits; (void)cap;
-  (void)gens;
+  (void)gens; (void)checked;
   return -7;
 }
 int gcl_canon_one_rows(gcl_context* c, const int32_t* rp, const int32_t* col,

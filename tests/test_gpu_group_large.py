@@ -19,15 +19,20 @@ pytestmark = [pytest.mark.gpu_staged,
 
 def test_group_order_large_vertex_transitive(pkg, G):
     ctx = pkg.Context(0)
-    assert pkg.group_order(G.torus(100), ctx=ctx) == 8 * 100 * 100
+    # checked: 1 confirmed by a completion, 0 unchecked within the budget;
+    # never -1 (a completion that disagrees with the orbit product)
+    order, checked = pkg.group_order(G.torus(100), ctx=ctx, return_checked=True)
+    assert order == 8 * 100 * 100 and checked in (0, 1)
     d = 12
     cube = G.from_edges(1 << d, [(a, a ^ (1 << b)) for a in range(1 << d) for b in range(d)
                                  if a < a ^ (1 << b)])
-    assert pkg.group_order(cube, ctx=ctx) == (1 << d) * math.factorial(d)
+    order, checked = pkg.group_order(cube, ctx=ctx, return_checked=True)
+    assert order == (1 << d) * math.factorial(d) and checked in (0, 1)
 
 
 def test_group_order_long_base(pkg, G):
     # S_600: both Schreier-Sims checks run out of budget; the first path's
     # basic orbits give the order
     ctx = pkg.Context(0)
-    assert pkg.group_order(G.from_edges(600, []), ctx=ctx) == math.factorial(600)
+    order, checked = pkg.group_order(G.from_edges(600, []), ctx=ctx, return_checked=True)
+    assert order == math.factorial(600) and checked in (0, 1)
