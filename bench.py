@@ -74,6 +74,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-sustained", action="store_true",
+                   help="skip the one-second repeat of the step that samples clocks")
     p.add_argument("--e2e-contexts", type=int, default=1,
                    help="also time e2e with this many contexts on host threads, so one "
                         "step's copies run under another's kernels (1 = off)")
@@ -112,12 +114,25 @@ def workload(args):
     return G.pack(G.small_batch(args.graphs, seed=args.seed))
 
 
-def algorithmic_bytes(arena, nodes: np.ndarray) -> int:
-    """B(g) = (4(n+1) + 8m) + n^2 + nodes(g) * (4(n+1) + 8m + 32n), summed."""
+def bench_config(args, count: int, world: int) -> dict:
+    """The workload both arms run (the GPU arm and --impl reference print the
+    same dict)."""
+    return {"workload": WORKLOAD, "graphs_per_step_per_gpu": count, "max_aut": args.max_aut,
+            "seed": args.seed, "parallelism": f"graph-sharded x{world} (no collective)",
+            "l2": "GPU arm: flushed between steps (256 MiB write outside the timed events)",
+            "output": "canonical forms (bit-packed rows on the GPU arm), stats and status "
+                      "per graph"}
+
+
+def algorithmic_bytes(arena, nodes: np.ndarray, packed: bool = False) -> int:
+    """B(g) = (4(n+1) + 8m) + n^2 + nodes(g) * (4(n+1) + 8m + 32n), summed.
+    With packed, the n^2 byte matrix is charged as the bit-packed rows the
+    timed call writes instead: n * ceil(n/64) 8-byte words."""
     n = arena.sizes().astype(np.int64)
     m = (np.diff(arena.eoff) // 2).astype(np.int64)
     csr = 4 * (n + 1) + 8 * m
-    return int((csr + n * n + nodes.astype(np.int64) * (csr + 32 * n)).sum())
+    out = n * ((n + 63) // 64) * 8 if packed else n * n
+    return int((csr + out + nodes.astype(np.int64) * (csr + 32 * n)).sum())
 
 
 # --------------------------------------------------------------------------
@@ -207,7 +222,7 @@ def reference_arm(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_t / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
         "data": "synthetic (seeded generator, same graphs as the GPU arm)",
-        "config": {"workload": WORKLOAD, "graphs_per_step": arena.count},
+        "config": bench_config(args, arena.count, int(os.environ.get("WORLD_SIZE", "1"))),
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": pool.cores, "kind": kind,
                          "sample": f"the full {arena.count}-graph batch per step, split over "
                                    f"{pool.cores} processes",
@@ -246,7 +261,7 @@ def job_rate(graphs_per_rank: int, world: int, steps: int, seconds: float) -> fl
 # GPU side
 # --------------------------------------------------------------------------
 class Clocks:
-    """SM clock and throttle reasons sampled through NVML every ~2 ms on a
+    """SM clock and throttle reasons sampled through NVML every ~0.2 ms on a
     background thread (read-only queries; no setting is changed)."""
 
     REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
@@ -270,7 +285,7 @@ class Clocks:
                 self.samples.append((time.perf_counter(), sm, rs))
             except Exception:
                 pass
-            time.sleep(0.002)
+            time.sleep(0.0002)
 
     def start(self):
         import threading
@@ -301,7 +316,7 @@ class Clocks:
             return None
         reasons = sorted({k for _, _, rs in rows for k, bit in self.REASONS.items() if rs & bit})
         return {"sm_mhz": float(np.median([r[1] for r in rows])), "sm_max_mhz": self.max_mhz,
-                "reasons": reasons, "samples": len(rows), "source": "nvml, 2 ms period"}
+                "reasons": reasons, "samples": len(rows), "source": "nvml, 0.2 ms period"}
 
 
 def read_traffic():
@@ -404,6 +419,38 @@ def gpu_arm(args):
     per = np.array([a.elapsed_time(b) for a, b in evs])  # ms
     dev_ms = max_over_ranks(float(per.sum()), world, dev)
     value = job_rate(count, world, args.steps, dev_ms / 1e3)
+
+    # The same steps repeated for about a second after the timed region, so
+    # the clocks are sampled over a window long enough to mean something
+    # (K steps of this batch last only milliseconds).  Reported beside the
+    # headline, not in it.
+    sus_steps = 0 if args.no_sustained else int(
+        min(20000, max(args.steps, np.ceil(1.0 / max(float(per.mean()) / 1e3, 1e-6)))))
+    sustained = None
+    if sus_steps:
+        sclocks = Clocks(local)
+        sclocks.start()
+        sev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(sus_steps)]
+        barrier()
+        ts0 = time.perf_counter()
+        for i in range(sus_steps):
+            flush.zero_()
+            stream.wait_stream(torch.cuda.current_stream())
+            sev[i][0].record(stream)
+            launch()
+            sev[i][1].record(stream)
+            torch.cuda.current_stream().wait_stream(stream)
+        barrier()
+        sclocks.mark(ts0, time.perf_counter())
+        sclk = sclocks.stop()
+        sper = np.array([a.elapsed_time(b) for a, b in sev])
+        sus_ms = max_over_ranks(float(sper.sum()), world, dev)
+        sustained = {"value": job_rate(count, world, sus_steps, sus_ms / 1e3), "unit": UNIT,
+                     "steps": sus_steps, "device_seconds": sus_ms / 1e3,
+                     "wall_seconds": time.perf_counter() - ts0, "clocks": sclk,
+                     "note": "the timed step repeated after the timed region (L2 flushed "
+                             "between steps) to sample clocks over about a second"}
 
     # end to end through the C ABI: pinned host buffers, copies inside
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
@@ -535,19 +582,17 @@ def gpu_arm(args):
     if rank == 0:
         peak, peak_kind = measured_peak()
         alg = algorithmic_bytes(arena, nodes)
+        alg_packed = algorithmic_bytes(arena, nodes, packed=True)
         kern_ms = float(per.mean())
         achieved = alg / (kern_ms / 1e3) / 1e9
+        achieved_packed = alg_packed / (kern_ms / 1e3) / 1e9
         traffic = read_traffic()
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
             "data": "synthetic (seeded generator)",
-            "config": {"workload": WORKLOAD, "graphs_per_step_per_gpu": count,
-                       "max_aut": args.max_aut, "seed": args.seed,
-                       "parallelism": f"graph-sharded x{world} (no collective)",
-                       "l2": "flushed between steps (256 MiB write outside the timed events)",
-                       "output": "bit-packed canonical rows, stats and status per graph"},
+            "config": bench_config(args, count, world),
             "e2e": {"value": job_rate(count, world, args.steps, e2e_s), "unit": UNIT,
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                     "output": "bit-packed canonical rows (n x ceil(n/64) words per graph)"},
@@ -572,10 +617,14 @@ def gpu_arm(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_kind": peak_kind,
-                         "algorithmic_bytes_per_launch": alg},
+                         "algorithmic_bytes_per_launch": alg,
+                         "algorithmic_bytes_packed_output": alg_packed,
+                         "achieved_packed_output": achieved_packed,
+                         "frac_packed_output": achieved_packed / peak},
             "latency_ms": {"p50": float(np.percentile(per, 50)),
                            "p99": float(np.percentile(per, 99))},
             "clocks": clk,
+            **({"sustained": sustained} if sustained else {}),
         }
 
     # the plain form: one graph per launch (device-resident, same kernels)
@@ -648,6 +697,30 @@ def gpu_arm(args):
 # --------------------------------------------------------------------------
 # Secondary workloads, reported beside the headline
 # --------------------------------------------------------------------------
+def _tail_timeline(res, lat, ns):
+    """Where the slowest 1% of each size class spent its time: medians over
+    those requests of the time queued (arrival -> taken into a batch), the
+    host's enqueueing, the batch on the GPU and the hand-out after it."""
+    out = {}
+    adm = np.array([r.admit_s for r in res]) * 1e3
+    lau = np.array([r.launch_s for r in res]) * 1e3
+    gpu = np.array([r.gpu_done_s for r in res]) * 1e3
+    launched = np.array([r.batch > 0 for r in res])
+    for name, m in (("n<=64", ns <= 64), ("65-256", (ns > 64) & (ns <= 256)),
+                    ("257-2048", (ns > 256) & (ns <= 2048)), (">2048", ns > 2048)):
+        m = m & launched
+        if not m.any():
+            continue
+        cut = np.percentile(lat[m], 99)
+        t = m & (lat >= cut)
+        out[name] = {"requests": int(t.sum()), "latency": float(np.median(lat[t])),
+                     "queued": float(np.median(adm[t])),
+                     "enqueue": float(np.median(lau[t] - adm[t])),
+                     "gpu": float(np.median(gpu[t] - lau[t])),
+                     "hand_out": float(np.median(lat[t] - gpu[t]))}
+    return out
+
+
 def serving_block(args, pkg, local):
     """Open-loop Poisson stream through the serving loop (gcl_serve_replay),
     then the plain form: the same requests one at a time, one launch each."""
@@ -700,6 +773,10 @@ def serving_block(args, pkg, local):
                              "mean_queue_ms": st["class_queue_ns"][c] / 1e6 / max(st["class_batches"][c], 1)}
                       for c, name in enumerate(("small", "mid", "big", "large"))},
         "class_repeats": st["class_repeats"],
+        "dispatcher_max_ms": {name: {"launch": st["class_max_launch_ns"][c] / 1e6,
+                                     "complete": st["class_max_complete_ns"][c] / 1e6}
+                              for c, name in enumerate(("small", "mid", "big", "large"))},
+        "tail_timeline_ms": _tail_timeline(res, lat, ns),
     }
     # the plain form under the same arrivals: the first requests served one
     # at a time in arrival order, each graph through its own gcl_canon_one

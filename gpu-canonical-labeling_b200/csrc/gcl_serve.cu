@@ -238,7 +238,7 @@ struct Req {
   uint64_t key[2] = {0, 0};
   uint64_t* out_rows = nullptr;
   int32_t* out_label = nullptr;
-  Clock::time_point t0;
+  Clock::time_point t0, t_admit, t_launch;
 };
 
 struct MemoEntry {
@@ -258,6 +258,7 @@ enum { kSmall = 0, kMid = 1, kBig = 2, kLarge = 3, kClasses = 4 };
 
 struct Lane {
   Clock::time_point t_launch;
+  std::atomic<int64_t> t_gpu_done{0};  // steady-clock ns when the stream reached the batch's end
   gcl_context* ctx = nullptr;
   cudaStream_t s = nullptr;
   int cls = kSmall;
@@ -333,6 +334,8 @@ namespace {
 
 void CUDART_CB lane_done_cb(void* arg) {
   auto* pr = (std::pair<gcl_server*, Lane*>*)arg;
+  pr->second->t_gpu_done.store(
+      std::chrono::duration_cast<std::chrono::nanoseconds>(Clock::now().time_since_epoch()).count());
   {
     std::lock_guard<std::mutex> lk(pr->first->mu);
     pr->second->ready.store(true);
@@ -561,6 +564,8 @@ void complete(gcl_server* S, Lane* L) {
   const uint64_t* rows = L->h_rows.as<uint64_t>();
   const int32_t* label = L->h_label.as<int32_t>();
   const Clock::time_point now = Clock::now();
+  const Clock::time_point t_gpu{std::chrono::duration_cast<Clock::duration>(
+      std::chrono::nanoseconds(L->t_gpu_done.load()))};
   int64_t repeats = 0, classes = 0;
   for (size_t k = 0; k < L->reqs.size(); ++k) {
     Req* r = L->reqs[k];
@@ -610,6 +615,9 @@ void complete(gcl_server* S, Lane* L) {
       }
     }
     res.latency_s = std::chrono::duration<double>(now - r->t0).count();
+    res.admit_s = std::chrono::duration<double>(r->t_admit - r->t0).count();
+    res.launch_s = std::chrono::duration<double>(r->t_launch - r->t0).count();
+    res.gpu_done_s = std::chrono::duration<double>(t_gpu - r->t0).count();
     push_done(S, res);
     delete r;
   }
@@ -658,6 +666,8 @@ void dispatcher(gcl_server* S) {
     for (size_t i = 0; i < S->lanes.size(); ++i) {
       Lane* L = S->lanes[i];
       if (L->busy && L->ready.load()) {
+        const Clock::time_point tc = Clock::now();
+        const int cls = L->cls;
         if (cudaStreamQuery(L->s) == cudaSuccess) {
           complete(S, L);
         } else {
@@ -666,6 +676,12 @@ void dispatcher(gcl_server* S) {
             complete(S, L);
           else
             fail_batch(S, L, rc_of(e));
+        }
+        const int64_t dt =
+            std::chrono::duration_cast<std::chrono::nanoseconds>(Clock::now() - tc).count();
+        {
+          std::lock_guard<std::mutex> lk(S->mu);
+          S->st.class_max_complete_ns[cls] = std::max(S->st.class_max_complete_ns[cls], dt);
         }
         progress = true;
       }
@@ -682,16 +698,27 @@ void dispatcher(gcl_server* S) {
       L->t_launch = Clock::now();
       {
         int64_t q = 0;
-        for (Req* r : L->reqs)
+        for (Req* r : L->reqs) {
+          r->t_admit = L->t_launch;
           q += std::chrono::duration_cast<std::chrono::nanoseconds>(L->t_launch - r->t0).count();
+        }
         std::lock_guard<std::mutex> lk(S->mu);
         S->st.class_queue_ns[L->cls] += q / (int64_t)L->reqs.size();
       }
       L->ready.store(false);
+      L->t_gpu_done.store(0);
       int rc = launch(S, L);
       if (rc == GCL_OK) {
         cudaError_t e = cudaLaunchHostFunc(L->s, lane_done_cb, &cb[i]);
         if (e != cudaSuccess) rc = rc_of(e);
+      }
+      {
+        const Clock::time_point tl = Clock::now();
+        for (Req* r : L->reqs) r->t_launch = tl;
+        const int64_t dt =
+            std::chrono::duration_cast<std::chrono::nanoseconds>(tl - L->t_launch).count();
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->st.class_max_launch_ns[L->cls] = std::max(S->st.class_max_launch_ns[L->cls], dt);
       }
       if (rc != GCL_OK) {
         cudaStreamSynchronize(L->s);
@@ -1029,7 +1056,14 @@ int gcl_serve_replay(gcl_server* S, int nreq, const double* arrival_s, const int
   }
   gen.join();
   if (rc == GCL_OK)
-    for (int i = 0; i < nreq; ++i) results[i].latency_s += lag[i];
+    for (int i = 0; i < nreq; ++i) {
+      results[i].latency_s += lag[i];
+      if (results[i].batch) {
+        results[i].admit_s += lag[i];
+        results[i].launch_s += lag[i];
+        results[i].gpu_done_s += lag[i];
+      }
+    }
   return rc;
 } GCL_CATCH_ALL
 

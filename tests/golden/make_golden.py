@@ -1,6 +1,7 @@
 """Generate tests/golden/golden.json by running the reference's own sequential
 canonical labeler (src/sequential.cpp et al., compiled unchanged from the
-reference sources by ``make -C oracle ref`` into oracle/_ref/libgcl_ref.so).
+reference sources by ``make -C oracle ref REF_SRC=<reference>/src`` into
+oracle/_ref/libgcl_ref.so).
 
 Each record holds a seeded input graph and the reference's outputs for it:
 the best leaf's vertex order (``label``, position -> vertex), the SHA-256 of
@@ -90,7 +91,8 @@ def cases():
 
 def main():
     if not O.available("reference"):
-        raise SystemExit("oracle/_ref/libgcl_ref.so missing: run make -C oracle ref")
+        raise SystemExit("oracle/_ref/libgcl_ref.so missing: run make -C oracle ref "
+                         "REF_SRC=<reference>/src")
     recs = []
     for name, g, max_aut in cases():
         mat, lab, na, nodes = O.canon(g, max_aut=max_aut, kind="reference")
