@@ -8,7 +8,8 @@
 //
 // GCL_FAULT_ALLOC_AT=k in the environment (k >= 1) makes the k-th allocation
 // of the process (device and pinned host counted together) fail as out of
-// memory, once, without calling the allocator.  It is a test hook for the
+// memory, once, without calling the allocator, and says so on stderr
+// ("gcl: injected allocation failure k").  It is a test hook for the
 // callers' error paths: the call that needed the memory returns
 // GCL_ERR_NOMEM (or falls back, where it has a fallback) and the context
 // stays usable.  Unset, or not a positive integer: no effect.
@@ -17,6 +18,7 @@
 
 #include <atomic>
 #include <cstdint>
+#include <cstdio>
 #include <cstdlib>
 
 namespace gcl {
@@ -37,7 +39,9 @@ inline bool alloc_fault_hit() {
   const int64_t k = alloc_fault_target();
   if (k == 0) return false;
   static std::atomic<int64_t> seen{0};
-  return seen.fetch_add(1, std::memory_order_relaxed) + 1 == k;
+  if (seen.fetch_add(1, std::memory_order_relaxed) + 1 != k) return false;
+  std::fprintf(stderr, "gcl: injected allocation failure %lld\n", (long long)k);
+  return true;
 }
 
 // stream-ordered device allocation (cudaMallocAsync); *p is null on failure

@@ -256,6 +256,7 @@ struct gcl_context {
   int wide_gate = 1;             // wide search's level gate: 1 on, 0 off, 2 automatic
   bool wide_share = false;       // wide search: busy warps hand subtrees to idle ones
   bool wide_count = false;       // wide search: the items kernel's counters (GCL_OPT_COUNTERS)
+  uint32_t wide_pool = kWidePool;  // wide search: per-level orbit arrays of a warp
   // mapped host buffers (gcl_host_alloc): host address, size, device address
   struct Mapped {
     uint8_t* p;
@@ -660,7 +661,8 @@ int gcl_canon_wide_device_async(gcl_context* c, const int32_t* d_rowptr, const i
                             ? (uint32_t)std::min<uint64_t>(65536, kGiftMaxWords / wide_gift_words(un))
                             : 0u;
   const WideLayout WL = wide_layout(un, m2, cap, qcap);
-  const SpLayout Lo = sp_layout(un, m2, kWidePool, 0, std::min<uint32_t>(cap, kWideFixCap));
+  const uint32_t pool = std::min<uint32_t>(c->wide_pool, un + 2);
+  const SpLayout Lo = sp_layout(un, m2, pool, 0, std::min<uint32_t>(cap, kWideFixCap));
   uint64_t smw = c->smem_stage ? sp_smem_bytes(un) : 0;
   if (smw * kSpWarps > (uint64_t)kSpSmemPerBlock) smw = 0;
   int per_sm = 0;
@@ -687,7 +689,7 @@ int gcl_canon_wide_device_async(gcl_context* c, const int32_t* d_rowptr, const i
   WA.slots = (uint8_t*)c->wide_slots.p;
   WA.Lo = Lo;
   WA.slot_bytes = Lo.bytes;
-  WA.pool = kWidePool;
+  WA.pool = pool;
   WA.gate = (uint32_t)c->wide_gate;
   WA.smem_per_warp = smw;
   WA.budget_ns = graph_budget_ns();
@@ -1135,15 +1137,25 @@ int gcl_group_order(gcl_context* c, const int32_t* rowptr, const int32_t* col,
     d_color = (int32_t*)c->color.p;
   }
   const int max_aut = 0x7fffffff;
-  int rc = gcl_canon_wide_device_async(c, (int32_t*)c->rowptr.p, (int32_t*)c->col.p, d_color, n,
-                                       m, max_aut, nullptr, nullptr, nullptr,
-                                       (int64_t*)c->stats.p, (int32_t*)c->status.p);
-  if (rc != GCL_OK) return rc;
   int32_t status = 0;
   int64_t st[2] = {0, 0};
-  GCL_TRY(cudaMemcpyAsync(&status, c->status.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-  GCL_TRY(cudaMemcpyAsync(st, c->stats.p, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-  GCL_TRY(cudaStreamSynchronize(s));
+  // A warp whose item goes deeper than its per-level orbit arrays reach
+  // ends the search with kAutOverflow (the canonizing calls then rerun the
+  // graph sequentially); the group order needs this search's automorphisms,
+  // so it reruns the wide search with an orbit array for every level.
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    const uint32_t saved_pool = c->wide_pool;
+    if (attempt) c->wide_pool = (uint32_t)n + 2;
+    const int rc = gcl_canon_wide_device_async(c, (int32_t*)c->rowptr.p, (int32_t*)c->col.p,
+                                               d_color, n, m, max_aut, nullptr, nullptr, nullptr,
+                                               (int64_t*)c->stats.p, (int32_t*)c->status.p);
+    c->wide_pool = saved_pool;
+    if (rc != GCL_OK) return rc;
+    GCL_TRY(cudaMemcpyAsync(&status, c->status.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    GCL_TRY(cudaMemcpyAsync(st, c->stats.p, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    GCL_TRY(cudaStreamSynchronize(s));
+    if (status != kAutOverflow) break;
+  }
   if (status != kOk) return graph_status_to_rc(status);
   const uint32_t un = (uint32_t)n;
   const uint32_t cap = wide_store_cap(un, max_aut);

@@ -118,18 +118,22 @@ def _run_child(spec_path, k, mode_timeout=120):
     assert p.returncode == 0, (k, p.stdout[-2000:], p.stderr[-2000:])
     line = [ln for ln in p.stdout.splitlines() if ln.startswith("LOG ")]
     assert line, (k, p.stdout[-2000:], p.stderr[-2000:])
-    return json.loads(line[-1][4:])
+    fired = f"gcl: injected allocation failure {k}" in p.stderr
+    return json.loads(line[-1][4:]), fired
 
 
 def _sweep(spec_path):
-    """Runs sessions with k = 1, 2, ... until one meets no injected fault;
-    returns the names of the calls that met one and that first k."""
+    """Runs sessions with k = 1, 2, ... until the k-th allocation is never
+    reached (the library reports on stderr when it fails one); returns the
+    names of the calls that met an injected failure and that first k.  A
+    failure a call recovers from (the wide search falls back to the
+    sequential one) counts as reached but is met by no call."""
     faulted = set()
     # every k up to 40, then every 4th: a session's k-th allocation is the
-    # same with or without the fault until it happens, so the sessions that
-    # meet a fault are exactly k <= its number of allocations
+    # same with or without the fault until it happens, so the sessions whose
+    # fault fires are exactly k <= its number of allocations
     for k in list(range(1, 41)) + list(range(44, MAX_K + 1, 4)):
-        log = _run_child(spec_path, k)
+        log, fired = _run_child(spec_path, k)
         hit = False
         for name, attempt, rc in log:
             assert rc != "mismatch", (k, name, attempt)
@@ -141,7 +145,8 @@ def _sweep(spec_path):
                     faulted.add(name)
             else:
                 assert rc == 0, (k, name, rc)  # the repeated call succeeds
-        if not hit:
+        assert fired or not hit, k  # a NOMEM comes only from the injected failure
+        if not fired:
             return faulted, k
     raise AssertionError(f"still faulting at k = {MAX_K}")
 
