@@ -66,6 +66,9 @@ struct WideHdr {
   uint32_t qtail;      // handed-over subtrees published (slots claimed)
   unsigned long long nodes;
   unsigned long long t0;  // start time (globaltimer ns)
+  // how long a level's other items wait for its first item (the probe)
+  // before they start anyway: twice the first path's duration
+  unsigned long long probe_ns;
   // opt-in counters of the items kernel (GCL_OPT_COUNTERS; zeroed by the
   // host before a counted search, untouched otherwise)
   unsigned long long cnt[16];
@@ -180,6 +183,7 @@ struct WideArgs {
   uint64_t slot_bytes;
   uint32_t pool;
   uint32_t gate;  // level gate: 1 on (a level's items wait for the deeper ones), 0 off, 2 auto
+  uint32_t probe;  // under the gate: a level's first item runs before the rest of the level
   uint64_t smem_per_warp;
   uint64_t budget_ns;
   uint8_t* out_dense;    // n*n, or null
@@ -346,6 +350,7 @@ __global__ void __launch_bounds__(32) wide_first_kernel(WideArgs A) {
     // automatic gate: off when the levels hold fewer than 4 items each on
     // average (trees), where it would run the items one after another
     H->gate = A.gate == 2 ? (run >= 4u * (D - 1u) ? 1u : 0u) : (A.gate != 0 ? 1u : 0u);
+    H->probe_ns = max(2ull * (global_ns() - H->t0), 20000ull);
     __threadfence();
     H->nitems = run;
   }
@@ -698,6 +703,35 @@ __device__ __noinline__ int32_t wide_gate(WideHdr* H, uint32_t need, uint64_t de
       }
       __nanosleep(sleep_ns);
       if (sleep_ns < 32768) sleep_ns <<= 1;
+    }
+    __threadfence();
+  }
+  return __shfl_sync(GCL_FULL, st, 0);
+}
+
+// The probe's wait: like wide_gate, but past `soft` (globaltimer ns) the
+// warp stops waiting and starts its item anyway (kOk): a first item whose
+// subtree is large would otherwise hold its whole level back.
+__device__ __noinline__ int32_t wide_gate_soft(WideHdr* H, uint32_t need, uint64_t soft,
+                                               uint64_t deadline) {
+  int32_t st = kOk;
+  if (lane_id() == 0) {
+    uint32_t sleep_ns = 256;
+    for (uint32_t i = 0; i < kWideGateSpinLimit; ++i) {
+      if (*(volatile uint32_t*)&H->done >= need) break;
+      const int32_t hs = *(volatile int32_t*)&H->status;
+      if (hs != kOk) {
+        st = hs;
+        break;
+      }
+      const uint64_t now = global_ns();
+      if (now > soft) break;
+      if (deadline && now > deadline) {
+        st = kTimeout;
+        break;
+      }
+      __nanosleep(sleep_ns);
+      if (sleep_ns < 8192) sleep_ns <<= 1;
     }
     __threadfence();
   }
@@ -1071,7 +1105,17 @@ __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
       v = P.lelem[tf + 1 + (it - P.cum[lo])];
       if (H->gate) {
         const unsigned long long tc = cnt.now();
-        const int32_t gs = wide_gate(H, P.cum[lo], deadline);
+        int32_t gs = wide_gate(H, P.cum[lo], deadline);
+        // with the probe, the level's other items also wait for its first
+        // item, up to twice the first path's duration: the automorphisms
+        // that one finds prune them (it is done when `done` passes the
+        // deeper levels' items, since no other item of the level can finish
+        // before it)
+        if (gs == kOk && A.probe && it != P.cum[lo])
+          gs = wide_gate_soft(H, P.cum[lo] + 1u,
+                              __shfl_sync(GCL_FULL, lane == 0 ? global_ns() : 0ull, 0) +
+                                  *(volatile unsigned long long*)&H->probe_ns,
+                              deadline);
         cnt.add(kCntGateCycles, cnt.now() - tc);
         if (gs != kOk) {
           status = gs;

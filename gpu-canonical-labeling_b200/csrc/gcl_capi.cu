@@ -257,6 +257,7 @@ struct gcl_context {
   bool wide_share = false;       // wide search: busy warps hand subtrees to idle ones
   bool wide_count = false;       // wide search: the items kernel's counters (GCL_OPT_COUNTERS)
   uint32_t wide_pool = kWidePool;  // wide search: per-level orbit arrays of a warp
+  bool wide_probe = true;          // wide search: a level's first item runs before the rest
   // mapped host buffers (gcl_host_alloc): host address, size, device address
   struct Mapped {
     uint8_t* p;
@@ -624,6 +625,10 @@ int gcl_set_option(gcl_context* c, int option, int64_t value) {
       if (value != 0 && value != 1) return GCL_ERR_ARG;
       c->wide_count = value != 0;
       return GCL_OK;
+    case GCL_OPT_WIDE_PROBE:
+      if (value != 0 && value != 1) return GCL_ERR_ARG;
+      c->wide_probe = value != 0;
+      return GCL_OK;
     case GCL_OPT_STREAM_PRIORITY: {
       if (value != 0 && value != 1) return GCL_ERR_ARG;
       int lo = 0, hi = 0;
@@ -691,6 +696,7 @@ int gcl_canon_wide_device_async(gcl_context* c, const int32_t* d_rowptr, const i
   WA.slot_bytes = Lo.bytes;
   WA.pool = pool;
   WA.gate = (uint32_t)c->wide_gate;
+  WA.probe = c->wide_probe ? 1u : 0u;
   WA.smem_per_warp = smw;
   WA.budget_ns = graph_budget_ns();
   WA.out_dense = d_out_dense;

@@ -116,6 +116,12 @@ void* gcl_stream(gcl_context* ctx);
  *   from the first leaf.  Same canonical form.  For trees whose work sits in
  *   a few siblings (unions of identical components).  Default 0.  Not yet
  *   measured on a GPU.
+ * GCL_OPT_WIDE_PROBE: 1 (default) makes, under the level gate, the first
+ *   item of each level run alone before the rest of that level starts, so
+ *   the automorphisms it finds prune its siblings as they would in the
+ *   sequential order (on vertex-transitive graphs such as tori one sibling
+ *   per level covers the whole cell); 0 starts a level's items together.
+ *   Same canonical form either way.
  * GCL_OPT_COUNTERS: 1 makes the wide searches of the context count events
  *   and clock cycles per part of the work (gcl_wide_counters), in a
  *   separately compiled items kernel; 0 (default) runs the kernel without
@@ -130,6 +136,7 @@ void* gcl_stream(gcl_context* ctx);
 #define GCL_OPT_WIDE_GATE 6
 #define GCL_OPT_WIDE_SHARE 7
 #define GCL_OPT_COUNTERS 8
+#define GCL_OPT_WIDE_PROBE 9
 int gcl_set_option(gcl_context* ctx, int option, int64_t value);
 
 /* Counters of the context's last wide search (gcl_canon_one on a graph of

@@ -160,7 +160,7 @@ def _csr(g):
 
 def wide_model(g, workers: int, seed: int = 0, cap: int = 10000, auts: bool = False,
                gate: int = 1, rounds: Optional[list] = None,
-               first_seq: Optional[list] = None, donate: int = 0):
+               first_seq: Optional[list] = None, donate: int = 0, probe: bool = False):
     """CPU model of the many-worker search (wide_model.c): `workers` simulated
     workers over the first path's sibling items, stepped round-robin (seed 0)
     or in a seeded random order.  Returns (canonical matrix, nodes, automorphisms
@@ -169,7 +169,8 @@ def wide_model(g, workers: int, seed: int = 0, cap: int = 10000, auts: bool = Fa
     that beat the private best but not a newer shared one]; with auts=True a
     fifth item, the stored automorphisms (naut x n, position -> image).
     gate: items start level by level as on the GPU (0 off, 2 the GPU's
-    automatic choice); `rounds`, when a list,
+    automatic choice; with probe, each level's first item runs before the
+    rest of the level, GCL_OPT_WIDE_PROBE); `rounds`, when a list,
     receives the number of scheduling rounds (every worker steps once per
     round), the first leaf's level D and the number of items; `first_seq`,
     when a list, the first path's individualized vertices.  donate: busy
@@ -185,7 +186,8 @@ def wide_model(g, workers: int, seed: int = 0, cap: int = 10000, auts: bool = Fa
     store = np.zeros((cap, max(g.n, 1)), dtype=np.uint32) if auts else None
     nr = (ctypes.c_long * 3)()
     fs = np.zeros(max(g.n, 1), dtype=np.uint32)
-    rc = lib.gcl_wide_model(g.n, _ptr(rp), _ptr(cl), _ptr(co), workers, seed, cap, int(gate),
+    rc = lib.gcl_wide_model(g.n, _ptr(rp), _ptr(cl), _ptr(co), workers, seed, cap,
+                            int(gate) | (8 if probe else 0),
                             int(donate), _ptr(out), ctypes.byref(nodes), ctypes.byref(naut), _ptr(ev),
                             _ptr(store), nr, _ptr(fs))
     if rc != 0:

@@ -19,7 +19,10 @@
  * With `donate` set, a busy worker hands its shallowest untried child to an
  * idle worker (work sharing below the first path's siblings).
  * With `gate` set, an item starts only once every item of the deeper levels
- * is done, as the GPU's level gate orders them; `rounds` counts the
+ * is done, as the GPU's level gate orders them; gate | 8 adds the probe:
+ * the first item of each level runs alone, the rest of the level once it is
+ * done or 2D rounds after it started, whichever comes first (the GPU waits
+ * twice the first path's duration; GCL_OPT_WIDE_PROBE); `rounds` counts the
  * scheduling rounds (every worker takes one step per round), the model's
  * measure of the search's parallel time; rounds[1] and rounds[2] receive the
  * first leaf's level D and the number of items.
@@ -519,10 +522,18 @@ int gcl_wide_model(int n, const int32_t* rowptr, const int32_t* col, const int32
    * done (need[it] = items before the first one of its level) */
   /* gate 2: on unless the levels hold fewer than 4 items each on average,
    * the GPU's automatic choice */
+  const int probe = (gate & 8) != 0;
+  gate &= 7;
   if (gate == 2) gate = G.nitems >= 4 * (int)(G.D > 1 ? G.D - 1 : 0);
   int* need = malloc(((size_t)G.nitems + 1) * sizeof(int));
-  for (int it = 0; it < G.nitems; ++it)
-    need[it] = it > 0 && G.item_k[it] == G.item_k[it - 1] ? need[it - 1] : it;
+  int* lfirst = malloc(((size_t)G.nitems + 1) * sizeof(int));
+  int first = 0; /* the first item of the current level */
+  for (int it = 0; it < G.nitems; ++it) {
+    if (it == 0 || G.item_k[it] != G.item_k[it - 1]) first = it;
+    need[it] = first;
+    lfirst[it] = first;
+  }
+  long probe_start = -1; /* round the current level's probe started */
   int done = 0;
   long rounds = 0;
   /* donated subtrees waiting for a worker (at most one per idle worker) */
@@ -534,9 +545,13 @@ int gcl_wide_model(int n, const int32_t* rowptr, const int32_t* col, const int32
     gifts[i].pathcode = malloc(((size_t)n + 2) * sizeof(int));
   }
   int ngifts = 0;
+#define WM_OPEN(it)                                                                         \
+  (!gate || (done >= need[it] &&                                                            \
+             (!probe || (it) == lfirst[it] || done > lfirst[it] ||                          \
+              (probe_start >= 0 && rounds >= probe_start + 2 * (long)G.D))))
   for (int active = 1; active; ++rounds) {
     int idle = 0;
-    const int items_open = G.next_item < G.nitems && (!gate || done >= need[G.next_item]);
+    const int items_open = G.next_item < G.nitems && WM_OPEN(G.next_item);
     for (int i = 0; i < workers; ++i) idle += !ws[i].busy && !items_open;
     for (int ii = 0; ii < workers; ++ii) {
       rs ^= rs << 13;
@@ -552,8 +567,9 @@ int gcl_wide_model(int n, const int32_t* rowptr, const int32_t* col, const int32
         } else if (donate && ngifts < idle && wm_donate(w, &G, &gifts[ngifts])) {
           ++ngifts;
         }
-      } else if (G.next_item < G.nitems && (!gate || done >= need[G.next_item])) {
+      } else if (G.next_item < G.nitems && WM_OPEN(G.next_item)) {
         int it = G.next_item++;
+        if (it == lfirst[it]) probe_start = rounds;
         w->gift = 0;
         if (wm_start_item(w, &G, G.item_k[it], G.item_v[it])) w->busy = w->S.P.level > w->item_k + 1;
         if (!w->busy) ++done;
@@ -574,6 +590,7 @@ int gcl_wide_model(int n, const int32_t* rowptr, const int32_t* col, const int32
   }
   free(gifts);
   free(need);
+  free(lfirst);
   if (first_seq_out) memcpy(first_seq_out, G.first_seq, (size_t)G.first_seqlen * 4);
   if (rounds_out) {
     rounds_out[0] = rounds;

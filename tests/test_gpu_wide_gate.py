@@ -141,10 +141,35 @@ def test_work_sharing_vs_oracle(pkg, G, oracle_mod, gate):
             print(f"n={g.n}: sharing {t_share * 1e3:.1f} ms, without {t_plain * 1e3:.1f} ms")
 
 
+@pytest.mark.parametrize("probe", [0, 1])
+def test_probe_vs_oracle(pkg, G, oracle_mod, probe):
+    # GCL_OPT_WIDE_PROBE: under the gate a level's first item runs before the
+    # rest of the level; same canonical form either way, and on tori the
+    # probe's automorphisms prune the other siblings (far fewer nodes)
+    ctx = pkg.Context(0, wide_min_n=1)
+    ctx.set_option(pkg.api.GCL_OPT_WIDE_PROBE, probe)
+    rng = np.random.default_rng(3131)
+    graphs = [G.torus(k) for k in (4, 6, 8, 12, 16)]
+    graphs += [G.disjoint_union(G.random_regular(10, 3, rng), k) for k in (2, 3, 4)]
+    graphs += [G.cfi_graph(b, rng, twist=bool(b % 4)) for b in (6, 10, 14)]
+    graphs += [G.random_regular(200, 3, rng), G.tree_plus_edges(300, rng)]
+    graphs += G.small_batch(60, seed=3131)
+    for g in graphs:
+        mat = oracle_mod.canon(g)[0]
+        for _ in range(2):
+            assert np.array_equal(pkg.canon(g, ctx=ctx).matrix, mat), g.n
+    nodes = pkg.canon(G.torus(16), ctx=ctx).nodes
+    seq_nodes = oracle_mod.canon(G.torus(16))[3]
+    if probe:
+        assert nodes <= 3 * seq_nodes, (nodes, seq_nodes)
+    ctx.close()
+
+
 def test_option_values_checked(pkg):
     ctx = pkg.Context(0)
     for opt, bad in ((pkg.api.GCL_OPT_WIDE_GATE, 3), (pkg.api.GCL_OPT_WIDE_GATE, -1),
-                     (pkg.api.GCL_OPT_WIDE_SHARE, 2)):
+                     (pkg.api.GCL_OPT_WIDE_SHARE, 2), (pkg.api.GCL_OPT_WIDE_PROBE, 2),
+                     (pkg.api.GCL_OPT_WIDE_PROBE, -1)):
         with pytest.raises(pkg.GclError) as e:
             ctx.set_option(opt, bad)
         assert e.value.rc == -1

@@ -239,3 +239,24 @@ def test_wide_model_automatic_gate(G, wm):
         m1 = wm.wide_model(g, 64, 0, gate=2, rounds=r_auto)[0]
         m2 = wm.wide_model(g, 64, 0, gate=picks, rounds=r_pick)[0]
         assert np.array_equal(m1, m2) and r_auto[0] == r_pick[0], (g.n, picks)
+
+
+def test_wide_model_probe_matches_sequential_and_prunes_tori(G, wm):
+    # The probe (GCL_OPT_WIDE_PROBE): under the gate each level's first item
+    # runs alone before the rest of the level (at most 2D rounds), so the
+    # automorphisms it finds prune its siblings.  Every schedule still gives
+    # the sequential form; on tori one sibling per level covers the whole
+    # cell, and the nodes fall to the sequential count.
+    rng = np.random.default_rng(77)
+    cases = _cases(G) + [G.cfi_graph(12, rng), G.disjoint_union(G.random_regular(16, 3, rng), 4)]
+    for g in cases:
+        ref = wm.canon(g)[0]
+        for workers, seed in ((1, 0), (3, 1), (8, 2), (64, 0), (64, 3)):
+            mat = wm.wide_model(g, workers, seed, gate=True, probe=True)[0]
+            assert np.array_equal(mat, ref), (g.n, workers, seed)
+    for k in (16, 32):
+        g = G.torus(k)
+        seq_nodes = wm.canon(g)[3]
+        _, nodes_plain, _, _ = wm.wide_model(g, 592, 0, gate=True)
+        _, nodes_probe, _, _ = wm.wide_model(g, 592, 0, gate=True, probe=True)
+        assert nodes_probe == seq_nodes < nodes_plain, (k, nodes_probe, seq_nodes, nodes_plain)
