@@ -52,7 +52,7 @@ def test_dropin_parallel_path_reaches_the_library(G, dropin, tmp_path):
     assert r.returncode == 1 and "Canonical labeling failed" in r.stderr
 
 
-@pytest.mark.gpu_staged
+@pytest.mark.gpu
 @pytest.mark.skipif(not torch.cuda.is_available(), reason="needs a CUDA GPU")
 def test_dropin_parallel_equals_sequential_on_gpu(G, dropin, tmp_path):
     rng = np.random.default_rng(4)

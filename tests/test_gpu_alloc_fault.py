@@ -8,10 +8,7 @@ query and the file pipeline (or, in the second test, a server).  Each call
 either gives the oracle's result or fails with GCL_ERR_NOMEM -- the wide
 search may instead fall back to the sequential one -- and the same call
 repeated on the same context (server) then gives the oracle's result.  No
-device fault is involved.
-
-Staged: marked gpu_staged, not gpu, until it has passed on a B200; run it
-with `pytest -m gpu_staged`."""
+device fault is involved."""
 import json
 import os
 import pickle
@@ -23,7 +20,7 @@ import pytest
 
 torch = pytest.importorskip("torch")
 
-pytestmark = [pytest.mark.gpu_staged,
+pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not torch.cuda.is_available(), reason="needs a CUDA GPU")]
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))

@@ -2,10 +2,7 @@
 (GCL_GRAPH_BUDGET_S, read at each call) ends with GCL_ERR_TIMEOUT (its
 status GCL_GRAPH_TIMEOUT), no result, and the context stays usable -- the same graph
 with a normal budget then gives the oracle's form.  No fault is involved:
-the search loop reads the global timer and returns.
-
-Staged: marked gpu_staged, not gpu, until it has passed on a B200; run it
-with `pytest -m gpu_staged`."""
+the search loop reads the global timer and returns."""
 import os
 
 import numpy as np
@@ -13,7 +10,7 @@ import pytest
 
 torch = pytest.importorskip("torch")
 
-pytestmark = [pytest.mark.gpu_staged,
+pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not torch.cuda.is_available(), reason="needs a CUDA GPU")]
 
 

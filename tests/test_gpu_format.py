@@ -1,10 +1,7 @@
 """gcl_format_adjacency_device_async: the reference's `output` text written
 on the device from packed canonical rows, for a whole batch, against a
 restatement of print_canonical_adjacency_list over the oracle's matrices.
-
-Staged: marked gpu_staged, not gpu, until it has passed on a B200; run it
-with `pytest -m gpu_staged`.  The row format itself is checked on the CPU
-(tests/test_format.py)."""
+The row format itself is checked on the CPU (tests/test_format.py)."""
 import ctypes
 
 import numpy as np
@@ -14,7 +11,7 @@ from test_cli import reference_listing
 
 torch = pytest.importorskip("torch")
 
-pytestmark = [pytest.mark.gpu_staged,
+pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not torch.cuda.is_available(), reason="needs a CUDA GPU")]
 
 

@@ -1,10 +1,7 @@
 """Group order of graphs whose automorphism groups have large orbits, where
 the Schreier-Sims check of gcl_group_order (general, then on the first
 path's base images) may exceed its budget and the first path's basic orbits
-give the order unchecked.
-
-Staged: marked gpu_staged, not gpu, until it has passed on a B200; run it
-with `pytest -m gpu_staged`.  The host part is checked on the CPU
+give the order unchecked.  The host part is checked on the CPU
 (tests/test_group_base.py)."""
 import math
 
@@ -13,10 +10,10 @@ import pytest
 
 torch = pytest.importorskip("torch")
 
-pytestmark = [pytest.mark.gpu_staged,
-              pytest.mark.skipif(not torch.cuda.is_available(), reason="needs a CUDA GPU")]
+pytestmark = [pytest.mark.skipif(not torch.cuda.is_available(), reason="needs a CUDA GPU")]
 
 
+@pytest.mark.gpu
 def test_group_order_large_vertex_transitive(pkg, G):
     ctx = pkg.Context(0)
     # checked: 1 confirmed by a completion, 0 unchecked within the budget;
@@ -30,6 +27,7 @@ def test_group_order_large_vertex_transitive(pkg, G):
     assert order == (1 << d) * math.factorial(d) and checked in (0, 1)
 
 
+@pytest.mark.gpu_staged
 def test_group_order_long_base(pkg, G):
     # S_600: both Schreier-Sims checks run out of budget; the first path's
     # basic orbits give the order

@@ -1,17 +1,14 @@
 """Graph families with deep, wide search trees through every GPU path, bit
 for bit against the oracle: Cai-Fuerer-Immerman graphs (refinement leaves
 them almost undivided), Paley graphs, rook's graphs, hypercubes and
-strongly symmetric unions.
-
-Staged: marked gpu_staged, not gpu, until it has passed on a B200; run it
-with `pytest -m gpu_staged`.  The oracle itself is checked on the CFI graphs
+strongly symmetric unions.  The oracle itself is checked on the CFI graphs
 against the reference's own sequential code (tests/test_oracle.py)."""
 import numpy as np
 import pytest
 
 torch = pytest.importorskip("torch")
 
-pytestmark = [pytest.mark.gpu_staged,
+pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not torch.cuda.is_available(), reason="needs a CUDA GPU")]
 
 

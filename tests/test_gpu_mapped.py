@@ -2,10 +2,7 @@
 the same results as gcl_canon_batch, the warp kernel reading the arena and
 writing the results in place over the bus; batches with larger graphs go
 through device copies; arrays outside the context's mapped buffers, whole,
-are refused before any device work.
-
-Staged: marked gpu_staged, not gpu, until it has passed on a B200; run it
-with `pytest -m gpu_staged`."""
+are refused before any device work."""
 import ctypes
 
 import numpy as np
@@ -13,7 +10,7 @@ import pytest
 
 torch = pytest.importorskip("torch")
 
-pytestmark = [pytest.mark.gpu_staged,
+pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not torch.cuda.is_available(), reason="needs a CUDA GPU")]
 
 

@@ -1,15 +1,12 @@
 """gcl_canon_one_rows (the CLI's path): the packed form of gcl_canon_one's
 matrix, through the wide search (n >= 65 by default) and the sequential
-path, with the sequential path's statistics unchanged.
-
-Staged: marked gpu_staged, not gpu, until it has passed on a B200; run it
-with `pytest -m gpu_staged`."""
+path, with the sequential path's statistics unchanged."""
 import numpy as np
 import pytest
 
 torch = pytest.importorskip("torch")
 
-pytestmark = [pytest.mark.gpu_staged,
+pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not torch.cuda.is_available(), reason="needs a CUDA GPU")]
 
 

@@ -3,10 +3,7 @@ through the wide search with the automatic level gate instead of the batched
 sequential search.  Canonical forms must equal those of each graph canonized
 alone (the wide search's labeling is one of the equivalent best leaves, so
 the labelings are checked by applying them); the timing of a burst of trees
-is printed beside the default configuration's.
-
-Staged: marked gpu_staged, not gpu, until it has passed on a B200; run it
-with `pytest -m gpu_staged -s`."""
+is printed beside the default configuration's."""
 import time
 
 import numpy as np
@@ -14,7 +11,7 @@ import pytest
 
 torch = pytest.importorskip("torch")
 
-pytestmark = [pytest.mark.gpu_staged,
+pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not torch.cuda.is_available(), reason="needs a CUDA GPU")]
 
 

@@ -3,16 +3,13 @@ the counted items kernel gives the same canonical form as the plain one,
 and its counters agree with the search's own statistics -- every stored
 automorphism came from a leaf equal to the first or the best leaf, the
 nodes are the search's minus the first path's, every handed-over subtree
-was taken.
-
-Staged: marked gpu_staged, not gpu, until it has passed on a B200; run it
-with `pytest -m gpu_staged`."""
+was taken."""
 import numpy as np
 import pytest
 
 torch = pytest.importorskip("torch")
 
-pytestmark = [pytest.mark.gpu_staged,
+pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not torch.cuda.is_available(), reason="needs a CUDA GPU")]
 
 

@@ -1,11 +1,9 @@
-"""The wide search with its level gate off (GCL_OPT_WIDE_GATE = 0) vs the
-oracle.
-
-Staged: marked gpu_staged, not gpu, until it has passed on a B200; run it
-with `pytest -m gpu_staged`.  Without the gate every first-path sibling
-starts at once and tests its vertex in its warp's own union-find; the CPU
-model of the search (tests/test_wide_model.py) shows the same canonical form
-under every schedule with or without the gate."""
+"""The wide search with its level gate off (GCL_OPT_WIDE_GATE = 0), the
+automatic gate, work sharing and the level probe, vs the oracle.  Without
+the gate every first-path sibling starts at once and tests its vertex in its
+warp's own union-find; the CPU model of the search (tests/test_wide_model.py)
+shows the same canonical form under every schedule with or without the
+gate."""
 import time
 
 import numpy as np
@@ -13,7 +11,7 @@ import pytest
 
 torch = pytest.importorskip("torch")
 
-pytestmark = [pytest.mark.gpu_staged,
+pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not torch.cuda.is_available(), reason="needs a CUDA GPU")]
 
 
