@@ -20,6 +20,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
+#include <mutex>
 
 namespace gcl {
 
@@ -44,11 +45,52 @@ inline bool alloc_fault_hit() {
   return true;
 }
 
-// stream-ordered device allocation (cudaMallocAsync); *p is null on failure
+// The library's own stream-ordered memory pool on the current device,
+// created on first use, or null (then the device's default pool serves).
+// It keeps up to kPoolKeepBytes of freed memory mapped instead of returning
+// it to the driver at every synchronization (the default pool's release
+// threshold is 0): workspaces that are freed and grown again, as the serving
+// lanes' are when a larger graph arrives, then reuse memory instead of
+// mapping new memory while other streams are busy.
+constexpr uint64_t kPoolKeepBytes = 16ull << 30;
+inline cudaMemPool_t library_pool() {
+  constexpr int kMaxDev = 64;
+  static std::mutex mu;
+  static cudaMemPool_t pools[kMaxDev] = {};
+  static bool tried[kMaxDev] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDev) {
+    (void)cudaGetLastError();
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lk(mu);
+  if (!tried[dev]) {
+    tried[dev] = true;
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    if (cudaMemPoolCreate(&pool, &props) == cudaSuccess) {
+      uint64_t keep = kPoolKeepBytes;
+      if (cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess)
+        (void)cudaGetLastError();
+      pools[dev] = pool;
+    } else {
+      (void)cudaGetLastError();
+    }
+  }
+  return pools[dev];
+}
+
+// stream-ordered device allocation (cudaMallocAsync, from the library's
+// pool); *p is null on failure
 inline cudaError_t device_alloc(void** p, size_t bytes, cudaStream_t s) {
   *p = nullptr;
   if (alloc_fault_hit()) return cudaErrorMemoryAllocation;
-  const cudaError_t e = cudaMallocAsync(p, bytes, s);
+  cudaMemPool_t pool = library_pool();
+  const cudaError_t e = pool ? cudaMallocFromPoolAsync(p, bytes, pool, s)
+                             : cudaMallocAsync(p, bytes, s);
   if (e != cudaSuccess) {
     *p = nullptr;
     (void)cudaGetLastError();

@@ -503,7 +503,10 @@ int gcl_canon_batch_device_async(gcl_context* c, int count, const int64_t* d_vof
   if (cap < maut) {
     // graphs whose ring outgrew `cap`: rerun with the full ring
     if (c->work_big_aut < maut || !c->work_big.p) {
-      c->big_slots = std::max(c->sms, 1);
+      // few graphs outgrow the first ring (at most n - 1 = 63 automorphisms
+      // were stored on every graph of up to 64 vertices tried), so a few
+      // blocks take them: the full-size ring costs about 0.7 MB per warp
+      c->big_slots = std::min(std::max(c->sms, 1), 16);
       GCL_TRY(c->work_big.ensure((uint64_t)c->big_slots * kW64Warps * w64_slot_bytes(maut)));
       c->work_big_aut = maut;
     }

@@ -2,14 +2,17 @@
 // over several device contexts, a device canonical-hash table and a host
 // memo of exact repeats.
 //
-// One dispatcher thread owns every launch.  Each lane is a gcl_context (its
-// own stream and workspace).  When a lane is free the dispatcher takes the
-// queued requests that fit the lane (graph count, device-memory footprint),
-// packs them into the lane's pinned arena, and enqueues copy-in, the
-// batched search, the table kernel and copy-out on the lane's stream; a host
-// callback at the end of the stream wakes the dispatcher, which hands the
-// results to pollers.  Lanes run concurrently, so batches formed while
-// others are on the GPU overlap with them.
+// One dispatcher thread forms the batches and hands out the results; each
+// lane is a gcl_context (its own stream and workspace) with its own launch
+// thread.  When a lane is free the dispatcher takes the queued requests that
+// fit the lane (graph count, device-memory footprint) and passes them to the
+// lane's thread, which packs them into the lane's pinned arena and enqueues
+// copy-in, the batched search, the table kernel and copy-out on the lane's
+// stream; a host callback at the end of the stream wakes the dispatcher,
+// which hands the results to pollers.  Lanes run concurrently, so batches
+// formed while others are on the GPU overlap with them, and a lane whose
+// enqueueing is slow (a workspace that grows for a larger graph) holds up
+// no other lane.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -258,6 +261,14 @@ enum { kSmall = 0, kMid = 1, kBig = 2, kLarge = 3, kClasses = 4 };
 
 struct Lane {
   Clock::time_point t_launch;
+  // the lane's launch thread: the dispatcher sets `go` (under the server's
+  // lock) once the batch is in `reqs`; a failed enqueue leaves its status in
+  // launch_rc and marks the lane ready
+  std::thread worker;
+  std::condition_variable cv_go;
+  bool go = false, quit = false;
+  int launch_rc = GCL_OK;
+  std::pair<gcl_server*, Lane*> cbarg{nullptr, nullptr};
   std::atomic<int64_t> t_gpu_done{0};  // steady-clock ns when the stream reached the batch's end
   gcl_context* ctx = nullptr;
   cudaStream_t s = nullptr;
@@ -657,10 +668,45 @@ void fail_batch(gcl_server* S, Lane* L, int rc) {
   L->err = GCL_OK;
 }
 
+// A lane's launch thread: packs and enqueues each batch the dispatcher hands
+// it.  The requests' enqueue time is stamped before the completion callback
+// is enqueued, since the dispatcher may finish (and free) them as soon as
+// the callback has run.
+void lane_worker(gcl_server* S, Lane* L) {
+  cudaSetDevice(S->device);
+  while (true) {
+    {
+      std::unique_lock<std::mutex> lk(S->mu);
+      L->cv_go.wait(lk, [&] { return L->go || L->quit; });
+      if (!L->go) break;
+      L->go = false;
+    }
+    int rc = launch(S, L);
+    const Clock::time_point tl = Clock::now();
+    for (Req* r : L->reqs) r->t_launch = tl;
+    const int64_t dt =
+        std::chrono::duration_cast<std::chrono::nanoseconds>(tl - L->t_launch).count();
+    {
+      std::lock_guard<std::mutex> lk(S->mu);
+      S->st.class_max_launch_ns[L->cls] = std::max(S->st.class_max_launch_ns[L->cls], dt);
+    }
+    if (rc == GCL_OK) {
+      const cudaError_t e = cudaLaunchHostFunc(L->s, lane_done_cb, &L->cbarg);
+      if (e != cudaSuccess) rc = rc_of(e);
+    }
+    if (rc != GCL_OK) {
+      {
+        std::lock_guard<std::mutex> lk(S->mu);
+        L->launch_rc = rc;
+        L->ready.store(true);
+      }
+      S->cv_work.notify_one();
+    }
+  }
+}
+
 void dispatcher(gcl_server* S) {
   cudaSetDevice(S->device);
-  std::vector<std::pair<gcl_server*, Lane*>> cb(S->lanes.size());
-  for (size_t i = 0; i < S->lanes.size(); ++i) cb[i] = {S, S->lanes[i]};
   while (true) {
     bool progress = false;
     for (size_t i = 0; i < S->lanes.size(); ++i) {
@@ -668,7 +714,13 @@ void dispatcher(gcl_server* S) {
       if (L->busy && L->ready.load()) {
         const Clock::time_point tc = Clock::now();
         const int cls = L->cls;
-        if (cudaStreamQuery(L->s) == cudaSuccess) {
+        if (L->launch_rc != GCL_OK) {
+          // the enqueue failed: drain what was queued, report the error
+          cudaStreamSynchronize(L->s);
+          const int rc = L->launch_rc;
+          L->launch_rc = GCL_OK;
+          fail_batch(S, L, rc);
+        } else if (cudaStreamQuery(L->s) == cudaSuccess) {
           complete(S, L);
         } else {
           cudaError_t e = cudaStreamSynchronize(L->s);
@@ -707,23 +759,12 @@ void dispatcher(gcl_server* S) {
       }
       L->ready.store(false);
       L->t_gpu_done.store(0);
-      int rc = launch(S, L);
-      if (rc == GCL_OK) {
-        cudaError_t e = cudaLaunchHostFunc(L->s, lane_done_cb, &cb[i]);
-        if (e != cudaSuccess) rc = rc_of(e);
-      }
       {
-        const Clock::time_point tl = Clock::now();
-        for (Req* r : L->reqs) r->t_launch = tl;
-        const int64_t dt =
-            std::chrono::duration_cast<std::chrono::nanoseconds>(tl - L->t_launch).count();
         std::lock_guard<std::mutex> lk(S->mu);
-        S->st.class_max_launch_ns[L->cls] = std::max(S->st.class_max_launch_ns[L->cls], dt);
+        L->launch_rc = GCL_OK;
+        L->go = true;
       }
-      if (rc != GCL_OK) {
-        cudaStreamSynchronize(L->s);
-        fail_batch(S, L, rc);
-      }
+      L->cv_go.notify_one();
       progress = true;
     }
     std::unique_lock<std::mutex> lk(S->mu);
@@ -769,9 +810,18 @@ bool copy_graph(Graph& g, const int32_t* rp, const int32_t* col, const int32_t* 
 }
 
 // Frees the lanes (each on its own stream, before its context goes), the
-// device table and the server itself.  The dispatcher must not be running.
+// device table and the server itself.  The dispatcher must not be running;
+// the lanes' launch threads are stopped here.
 void teardown(gcl_server* S) {
   cudaSetDevice(S->device);
+  for (Lane* L : S->lanes) {
+    {
+      std::lock_guard<std::mutex> lk(S->mu);
+      L->quit = true;
+    }
+    L->cv_go.notify_all();
+    if (L->worker.joinable()) L->worker.join();
+  }
   for (Lane* L : S->lanes) {
     if (L->s) cudaStreamSynchronize(L->s);
     L->release();
@@ -883,6 +933,10 @@ int gcl_serve_create(int device, const gcl_serve_config* cfg, gcl_server** out) 
     return rc;
   }
   try {
+    for (Lane* L : S->lanes) {
+      L->cbarg = {S, L};
+      L->worker = std::thread(lane_worker, S, L);
+    }
     S->th = std::thread(dispatcher, S);
   } catch (...) {
     teardown(S);
