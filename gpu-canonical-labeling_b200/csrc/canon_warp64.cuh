@@ -808,34 +808,58 @@ struct W64Result {
   int64_t nodes;
 };
 
-static __device__ __noinline__ W64Result w64_search(const BatchArgs& A, int n, int64_t vo, int64_t eo,
-                                             int64_t m, const int32_t* rp, uint8_t* slot) {
+// The root node (sequential.cpp:626-630): adjacency and the colour
+// partition into shared memory, then the refinement with every cell active.
+// The root's code is the first path's first code.
+struct W64Root {
+  uint64_t starts;
+  int code;
+  int32_t status;
+};
+
+static __device__ __noinline__ W64Root w64_root(const BatchArgs& A, int n, int64_t vo, int64_t eo,
+                                                int64_t m, const int32_t* rp) {
+  W64Smem& S = w64_smem();
+  W64Root out{0ull, 0, kOk};
+  const uint64_t starts = w64_load(n, rp, A.col + eo, A.color ? A.color + vo : nullptr, m);
+  if (!starts) {
+    out.status = kBadInput;
+    return out;
+  }
+  const W64Refined r = w64_refine(n, starts, 0, starts);
+  if (!r.ok) {
+    out.status = kInternal;
+    return out;
+  }
+  __syncwarp();
+  if (lane_id() == 0) S.firstcode[0] = (uint16_t)r.code;
+  __syncwarp();
+  out.starts = r.starts;
+  out.code = r.code;
+  return out;
+}
+
+// The search below the root, with the root's partition in shared memory
+// (`starts`, its refinement code `code`; level 1).
+static __device__ __noinline__ W64Result w64_search_tree(const BatchArgs& A, int n, uint64_t starts,
+                                                         int code, uint8_t* slot,
+                                                         uint64_t deadline) {
   W64Smem& S = w64_smem();
   const uint32_t lane = lane_id();
   uint8_t* reps = slot;
   uint8_t* auts = slot + (uint64_t)kW64Levels * 64u;
   W64Result res{kOk, 0, 1};
-  if (n == 0) return res;  // the reference visits the (discrete) root only
-  uint64_t deadline = 0;
-  if (A.budget_ns)
-    deadline = __shfl_sync(GCL_FULL, lane == 0 ? global_ns() : 0ull, 0) + A.budget_ns;
-
-  uint64_t starts = w64_load(n, rp, A.col + eo, A.color ? A.color + vo : nullptr, m);
-  if (!starts) {
-    res.status = kBadInput;
-    return res;
-  }
   const uint64_t full = low_mask((uint32_t)n);
-  // Nauty_Sequential state (sequential.h:24-45)
-  uint32_t level = 0, seqlen = 0, eqlevfirst = 0, first_seqlen = 0, best_seqlen = 0;
-  int code = 0, canon_level = 0, eqlevcanon = 0, comp_canon = 0, tcl = 0, num_aut = 0;
+  // Nauty_Sequential state (sequential.h:24-45), after the root node
+  uint32_t level = 1, seqlen = 0, eqlevfirst = 0, first_seqlen = 0, best_seqlen = 0;
+  int canon_level = 0, eqlevcanon = 0, comp_canon = 0, tcl = 0, num_aut = 0;
   bool first_found = false;
   int64_t nodes = 1;
   int32_t status = kOk;
 
-  // the next refinement to run, given by its initially active cells; the
-  // root refinement starts with every cell active (sequential.cpp:628)
-  uint64_t pending = starts;
+  // the next refinement to run on the first path, given by its initially
+  // active cells
+  uint64_t pending = 0;
   uint64_t iter = 0;
   while (true) {
     if (pending) {
@@ -1063,6 +1087,80 @@ static __device__ __noinline__ W64Result w64_search(const BatchArgs& A, int n, i
   res.num_aut = num_aut;
   res.nodes = nodes;
   return res;
+}
+
+__device__ __forceinline__ uint64_t w64_deadline(const BatchArgs& A) {
+  if (!A.budget_ns) return 0;
+  return __shfl_sync(GCL_FULL, lane_id() == 0 ? global_ns() : 0ull, 0) + A.budget_ns;
+}
+
+// The partition after the root refinement, kept in device memory between
+// the root pass and the search pass of a batch: a header (starts, singleton
+// vertices, code), then per vertex or position the adjacency mask, the cell
+// member mask (at cell starts), the cell start, in_level and the singleton
+// cell's vertex -- what the search reads of the root node.
+__host__ __device__ constexpr uint64_t w64_root_slot_bytes() {
+  return 32u + (uint64_t)kW64MaxN * (8u + 8u + 3u);
+}
+
+static __device__ __noinline__ void w64_save_root(uint8_t* dst, int n, uint64_t starts, int code) {
+  W64Smem& S = w64_smem();
+  const uint32_t lane = lane_id();
+  uint64_t* h = reinterpret_cast<uint64_t*>(dst);
+  uint64_t* adj = h + 4;
+  uint64_t* cm = adj + kW64MaxN;
+  uint8_t* b = reinterpret_cast<uint8_t*>(cm + kW64MaxN);
+  if (lane == 0) {
+    h[0] = starts;
+    h[1] = S.sing;
+    h[2] = (uint64_t)(uint32_t)code;
+  }
+  for (uint32_t v = lane; v < (uint32_t)n; v += 32) {
+    adj[v] = S.adj[v];
+    cm[v] = S.cmask[v];
+    b[v] = S.cs[v];
+    b[kW64MaxN + v] = S.inlev[v];
+    b[2 * kW64MaxN + v] = S.pv[v];
+  }
+}
+
+static __device__ __noinline__ uint64_t w64_restore_root(const uint8_t* src, int n, int* code) {
+  W64Smem& S = w64_smem();
+  const uint32_t lane = lane_id();
+  const uint64_t* h = reinterpret_cast<const uint64_t*>(src);
+  const uint64_t* adj = h + 4;
+  const uint64_t* cm = adj + kW64MaxN;
+  const uint8_t* b = reinterpret_cast<const uint8_t*>(cm + kW64MaxN);
+  for (uint32_t v = lane; v < (uint32_t)n; v += 32) {
+    S.adj[v] = adj[v];
+    S.cmask[v] = cm[v];
+    S.cs[v] = b[v];
+    S.inlev[v] = b[kW64MaxN + v];
+    S.pv[v] = b[2 * kW64MaxN + v];
+  }
+  const uint64_t starts = h[0];
+  *code = (int)(uint32_t)h[2];
+  if (lane == 0) {
+    S.sing = h[1];
+    S.firstcode[0] = (uint16_t)*code;
+  }
+  __syncwarp();
+  return starts;
+}
+
+// The whole search of one graph: root node, then the tree below it.
+static __device__ __forceinline__ W64Result w64_search(const BatchArgs& A, int n, int64_t vo,
+                                                       int64_t eo, int64_t m, const int32_t* rp,
+                                                       uint8_t* slot) {
+  W64Result res{kOk, 0, 1};
+  if (n == 0) return res;  // the reference visits the (discrete) root only
+  const uint64_t deadline = w64_deadline(A);
+  const W64Root root = w64_root(A, n, vo, eo, m, rp);
+  if (root.status != kOk) {
+    res.status = root.status;
+    return res;
+  }
+  return w64_search_tree(A, n, root.starts, root.code, slot, deadline);
 }
 
 static __device__ __noinline__ void w64_write_outputs(const BatchArgs& A, int g, int n, int64_t vo) {

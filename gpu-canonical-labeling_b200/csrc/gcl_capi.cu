@@ -53,6 +53,8 @@ struct Deferred {
   int next_sp_fail2;
   int large_count[kSpBuckets];  // n > 64 graphs per size bucket
   int next_large[kSpBuckets];
+  int search_count;    // n <= 64 graphs whose root partition is not discrete
+  int next_search;
 };
 
 // Largest graphs first: a counting sort of the graph ids by descending n
@@ -176,6 +178,99 @@ __global__ void __launch_bounds__(kW64Threads, 8)
   }
 }
 
+// The batch's graphs of up to 64 vertices in two passes.  The root pass
+// loads each graph and refines its root partition -- the largest share of
+// the work on small sparse graphs -- and finishes the graphs whose root
+// partition is discrete (their canonical form is the root's); the others
+// leave the root's partition in `roots` and their id in `search_list`.  The
+// search pass runs their trees.  Each pass keeps the warps of an SM in the
+// same few functions, and only the graphs that search take part in the
+// second.  Results equal w64_batch_kernel's.
+__global__ void __launch_bounds__(kW64Threads, 8)
+    w64_root_kernel(BatchArgs A, Deferred* D, int* large_list, uint8_t* roots, int* search_list) {
+  const uint32_t lane = lane_id();
+  while (true) {
+    int i = 0;
+    if (lane == 0) i = atomicAdd(&D->next, 1);
+    i = __shfl_sync(GCL_FULL, i, 0);
+    if (i >= A.count) break;
+    const int g = A.order ? A.order[i] : i;
+    const int64_t vo = A.voff[g];
+    const int n = (int)(A.voff[g + 1] - vo);
+    if (n > kW64MaxN) {
+      if (lane == 0) {
+        A.status[g] = kTooLarge;
+        const int bk = sp_bucket(n);
+        large_list[(int64_t)bk * A.count + atomicAdd(&D->large_count[bk], 1)] = g;
+      }
+      continue;
+    }
+    W64Root root{0ull, 0, kOk};
+    bool search = false;
+    if (n > 0) {
+      const int64_t eo = A.eoff[g];
+      root = w64_root(A, n, vo, eo, A.eoff[g + 1] - eo, A.rowptr + vo + g);
+      search = root.status == kOk && root.starts != low_mask((uint32_t)n);
+    }
+    if (search) {
+      int j = 0;
+      if (lane == 0) j = atomicAdd(&D->search_count, 1);
+      j = __shfl_sync(GCL_FULL, j, 0);
+      w64_save_root(roots + (uint64_t)j * w64_root_slot_bytes(), n, root.starts, root.code);
+      __syncwarp();
+      if (lane == 0) search_list[j] = g;
+      continue;
+    }
+    // finished at the root: the discrete root is the first and best leaf
+    // (first_terminal, sequential.cpp:259-303), one node, no automorphism
+    if (root.status == kOk && n > 0) {
+      W64Smem& S = w64_smem();
+      const Rows2 R = w64_leaf_rows(n);
+      w64_store_leaf(n, R, S.best_cert, S.bpos);
+    }
+    if (lane == 0) {
+      A.status[g] = root.status;
+      if (A.out_stats) {
+        A.out_stats[2 * (int64_t)g] = 0;
+        A.out_stats[2 * (int64_t)g + 1] = 1;
+      }
+    }
+    if (root.status == kOk) w64_write_outputs(A, g, n, vo);
+    __syncwarp();
+  }
+}
+
+__global__ void __launch_bounds__(kW64Threads, 8)
+    w64_search_kernel(BatchArgs A, Deferred* D, int* overflow_list, const uint8_t* roots,
+                      const int* search_list) {
+  const int warp = (int)(threadIdx.x >> 5);
+  const uint32_t lane = lane_id();
+  uint8_t* slot = A.work + ((uint64_t)blockIdx.x * kW64Warps + (uint64_t)warp) * A.slot_bytes;
+  const int total = *(volatile int*)&D->search_count;
+  while (true) {
+    int i = 0;
+    if (lane == 0) i = atomicAdd(&D->next_search, 1);
+    i = __shfl_sync(GCL_FULL, i, 0);
+    if (i >= total) break;
+    const int g = search_list[i];
+    const int64_t vo = A.voff[g];
+    const int n = (int)(A.voff[g + 1] - vo);
+    int code = 0;
+    const uint64_t starts = w64_restore_root(roots + (uint64_t)i * w64_root_slot_bytes(), n, &code);
+    const W64Result r = w64_search_tree(A, n, starts, code, slot, w64_deadline(A));
+    if (lane == 0) {
+      A.status[g] = r.status;
+      if (A.out_stats) {
+        A.out_stats[2 * (int64_t)g] = r.num_aut;
+        A.out_stats[2 * (int64_t)g + 1] = r.nodes;
+      }
+      if (r.status == kAutOverflow) overflow_list[atomicAdd(&D->overflow_count, 1)] = g;
+    }
+    if (r.status == kOk) w64_write_outputs(A, g, n, vo);
+    __syncwarp();
+  }
+}
+
 }  // namespace gcl
 
 using namespace gcl;
@@ -244,6 +339,7 @@ struct gcl_context {
     DevBuf* bufs[] = {&work, &work_big, &sp_work_mid, &sp_work_big, &deferred, &wide_sh,
                       &wide_slots,
                       &overflow_list, &large_list, &sp_fail_list, &sp_fail_list2, &order,
+                      &roots, &search_list,
                       &voff, &eoff,
                       &rowptr, &col, &color, &ooff, &dense, &roff, &rows, &label, &stats,
                       &status};
@@ -276,6 +372,8 @@ struct gcl_context {
   cudaEvent_t tev[2][1 + kSpBuckets] = {};
   bool tev_used[1 + kSpBuckets] = {};
   DevBuf deferred, overflow_list, large_list, sp_fail_list, sp_fail_list2, order;
+  // the warp kernel's root pass -> search pass hand-over
+  DevBuf roots, search_list;
   // staging for host-pointer calls
   DevBuf voff, eoff, rowptr, col, color, ooff, dense, roff, rows, label, stats, status;
 };
@@ -458,6 +556,10 @@ int gcl_canon_batch_device_async(gcl_context* c, int count, const int64_t* d_vof
   GCL_TRY(c->overflow_list.ensure((size_t)count * sizeof(int)));
   GCL_TRY(c->large_list.ensure((size_t)count * kSpBuckets * sizeof(int)));
   GCL_TRY(c->order.ensure((size_t)count * sizeof(int)));
+  if (max_n > 0) {
+    GCL_TRY(c->roots.ensure((size_t)count * w64_root_slot_bytes()));
+    GCL_TRY(c->search_list.ensure((size_t)count * sizeof(int)));
+  }
   GCL_TRY(cudaMemsetAsync(c->deferred.p, 0, sizeof(Deferred), c->stream));
   order_by_size_kernel<<<1, kOrderThreads, 0, c->stream>>>(count, d_voff, (int*)c->order.p);
   GCL_TRY(cudaGetLastError());
@@ -492,8 +594,21 @@ int gcl_canon_batch_device_async(gcl_context* c, int count, const int64_t* d_vof
     for (int k = 0; k <= kSpBuckets; ++k) c->tev_used[k] = false;
     GCL_TRY(cudaEventRecord(c->tev[0][0], c->stream));
   }
-  w64_batch_kernel<<<grid1, kW64Threads, 0, c->stream>>>(A, D, (int*)c->overflow_list.p,
-                                                         (int*)c->large_list.p, 0);
+  if (max_n > 0) {
+    // root pass, then the search pass over the graphs whose root is not
+    // discrete
+    w64_root_kernel<<<grid1, kW64Threads, 0, c->stream>>>(A, D, (int*)c->large_list.p,
+                                                          (uint8_t*)c->roots.p,
+                                                          (int*)c->search_list.p);
+    GCL_TRY(cudaGetLastError());
+    w64_search_kernel<<<grid1, kW64Threads, 0, c->stream>>>(A, D, (int*)c->overflow_list.p,
+                                                            (const uint8_t*)c->roots.p,
+                                                            (const int*)c->search_list.p);
+  } else {
+    // a batch of empty graphs (max_n 0): one pass, no hand-over buffers
+    w64_batch_kernel<<<grid1, kW64Threads, 0, c->stream>>>(A, D, (int*)c->overflow_list.p,
+                                                           (int*)c->large_list.p, 0);
+  }
   GCL_TRY(cudaGetLastError());
   if (c->timing) {
     GCL_TRY(cudaEventRecord(c->tev[1][0], c->stream));
