@@ -518,7 +518,7 @@ class ServeStats(ctypes.Structure):
                                               "large_graphs")] + [
         ("class_batches", ctypes.c_int64 * 4), ("class_batch_ns", ctypes.c_int64 * 4),
         ("class_queue_ns", ctypes.c_int64 * 4), ("class_max_launch_ns", ctypes.c_int64 * 4),
-        ("class_max_complete_ns", ctypes.c_int64 * 4)]
+        ("class_max_complete_ns", ctypes.c_int64 * 4), ("enqueue_part_max_ns", ctypes.c_int64 * 6)]
 
 
 def _serve_sigs(lib):

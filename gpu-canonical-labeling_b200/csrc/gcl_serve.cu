@@ -456,9 +456,22 @@ int launch(gcl_server* S, Lane* L) {
   }
   L->count = count;
   cudaError_t e = cudaSuccess;
+  int64_t part[6] = {0, 0, 0, 0, 0, 0};
+  auto since = [](Clock::time_point t) {
+    return std::chrono::duration_cast<std::chrono::nanoseconds>(Clock::now() - t).count();
+  };
   auto ens = [&](HostBuf& h, DevMem& d, size_t bytes) {
+    Clock::time_point t = Clock::now();
     if (e == cudaSuccess) e = h.ensure(bytes);
+    part[0] += since(t);
+    t = Clock::now();
     if (e == cudaSuccess) e = d.ensure(bytes);
+    part[1] += since(t);
+  };
+  auto report = [&] {
+    std::lock_guard<std::mutex> lk(S->mu);
+    for (int k = 0; k < 6; ++k)
+      S->st.enqueue_part_max_ns[k] = std::max(S->st.enqueue_part_max_ns[k], part[k]);
   };
   ens(L->h_voff, L->d_voff, (count + 1) * 8);
   ens(L->h_eoff, L->d_eoff, (count + 1) * 8);
@@ -473,6 +486,7 @@ int launch(gcl_server* S, Lane* L) {
   ens(L->h_class, L->d_class, (size_t)count * 8);
   ens(L->h_seen, L->d_seen, (size_t)count * 4);
   if (e != cudaSuccess) return rc_of(e);
+  Clock::time_point tp = Clock::now();
   int64_t* voff = L->h_voff.as<int64_t>();
   int64_t* eoff = L->h_eoff.as<int64_t>();
   int64_t* roff = L->h_roff.as<int64_t>();
@@ -497,6 +511,8 @@ int launch(gcl_server* S, Lane* L) {
       eoff[gi + 1] = eoff[gi] + m;
       roff[gi + 1] = roff[gi] + (int64_t)g.n * ((g.n + 63) / 64);
     }
+  part[2] = since(tp);
+  tp = Clock::now();
   cudaStream_t s = L->s;
   auto h2d = [&](DevMem& d, const HostBuf& h, size_t bytes) {
     if (e == cudaSuccess && bytes) e = cudaMemcpyAsync(d.p, h.p, bytes, cudaMemcpyHostToDevice, s);
@@ -508,6 +524,8 @@ int launch(gcl_server* S, Lane* L) {
   if (colored) h2d(L->d_color, L->h_color, (size_t)nv * 4);
   h2d(L->d_roff, L->h_roff, (count + 1) * 8);
   if (e != cudaSuccess) return rc_of(e);
+  part[3] = since(tp);
+  tp = Clock::now();
   int rc = GCL_OK;
   const int32_t* d_color = colored ? L->d_color.as<int32_t>() : nullptr;
   if (L->large) {
@@ -532,6 +550,8 @@ int launch(gcl_server* S, Lane* L) {
                                       L->d_roff.as<int64_t>(), L->d_label.as<int32_t>(), nullptr,
                                       L->d_status.as<int32_t>());
   }
+  part[4] = since(tp);
+  tp = Clock::now();
   if (rc != GCL_OK) return rc;
   if (e != cudaSuccess) return rc_of(e);
   TableArgs T;
@@ -561,6 +581,8 @@ int launch(gcl_server* S, Lane* L) {
   d2h(L->h_hash, L->d_hash, (size_t)count * 8);
   d2h(L->h_class, L->d_class, (size_t)count * 8);
   d2h(L->h_seen, L->d_seen, (size_t)count * 4);
+  part[5] = since(tp);
+  report();
   if (e != cudaSuccess) return rc_of(e);
   return GCL_OK;
 }

@@ -452,6 +452,11 @@ typedef struct {
      (results handed out), ns -- the dispatcher serves every lane, so this is
      time no other lane could be launched or finished */
   int64_t class_max_launch_ns[4], class_max_complete_ns[4];
+  /* the longest host time of each part of enqueuing one batch, over all
+     batches (ns): pinned host buffers grown, device buffers grown, requests
+     packed, copies in issued, the search launched, the table kernel and the
+     copies out issued */
+  int64_t enqueue_part_max_ns[6];
 } gcl_serve_stats;
 
 /* cfg may be NULL (all defaults); zero fields take their default. */

@@ -27,10 +27,12 @@ def test_group_order_large_vertex_transitive(pkg, G):
     assert order == (1 << d) * math.factorial(d) and checked in (0, 1)
 
 
-@pytest.mark.gpu_staged
+@pytest.mark.gpu
 def test_group_order_long_base(pkg, G):
-    # S_600: both Schreier-Sims checks run out of budget; the first path's
-    # basic orbits give the order
+    # S_200 (about 8 s on a B200; S_300 takes 35 s, S_600 minutes: the wide
+    # search of an empty graph visits O(n^2) nodes per level): both
+    # Schreier-Sims checks run out of budget, and the first path's basic
+    # orbits give the order, reported as unchecked
     ctx = pkg.Context(0)
-    order, checked = pkg.group_order(G.from_edges(600, []), ctx=ctx, return_checked=True)
-    assert order == math.factorial(600) and checked in (0, 1)
+    order, checked = pkg.group_order(G.from_edges(200, []), ctx=ctx, return_checked=True)
+    assert order == math.factorial(200) and checked == 0
