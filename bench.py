@@ -903,9 +903,10 @@ def mixed_block(args, pkg, local):
             ctx = pkg.Context(local)
             if tune and quick:
                 out["tuning"] = ctx.autotune([gs[i] for i in quick[:200]], repeats=1)
-            pkg.canon_batch(G.pack(gs[:64]), ctx=ctx, dense=False, rows=True)  # workspace warm-up
+            warm = [gs[i] for i in quick[:64]] or gs[:1]
+            pkg.canon_batch(warm, ctx=ctx, dense=False, rows=True)  # workspace warm-up
             t = time.perf_counter()
-            r = pkg.canon_batch(arena, ctx=ctx, dense=False, rows=True)
+            r = pkg.canon_batch(arena, ctx=ctx, dense=False, rows=True, per_graph_errors=True)
             dt = time.perf_counter() - t
             ctx.close()
             ok = r.status == 0

@@ -409,8 +409,12 @@ class BatchResult:
 
 def canon_batch(graphs: Union[Arena, Sequence[Graph]], max_aut: int = 10000,
                 ctx: Optional[Context] = None, dense: bool = True,
-                label: bool = True, rows: bool = False) -> BatchResult:
-    """Canonize every graph of a ragged arena in one batched call."""
+                label: bool = True, rows: bool = False,
+                per_graph_errors: bool = False) -> BatchResult:
+    """Canonize every graph of a ragged arena in one batched call.  The call
+    fails (GclError) when a graph has no result; with per_graph_errors the
+    result comes back anyway and `status` says which graphs have none
+    (1 ring outgrown, 2 too large, 3 bad input, 4 internal, 5 time budget)."""
     ctx = ctx or default_context()
     arena = graphs if isinstance(graphs, Arena) else pack(graphs)
     ooff = arena.out_offsets()
@@ -426,7 +430,9 @@ def canon_batch(graphs: Union[Arena, Sequence[Graph]], max_aut: int = 10000,
                                  _ptr(arena.rowptr), _ptr(col), _ptr(color), max_aut, _ptr(out),
                                  _ptr(ooff), _ptr(prow), _ptr(roff), _ptr(lab), _ptr(stats),
                                  _ptr(status))
-    _check(rc, "gcl_canon_batch")
+    per_graph = rc in (-4, -5, -6, -7) and (status[:arena.count] != 0).any()
+    if not (per_graph_errors and per_graph):
+        _check(rc, "gcl_canon_batch")
     return BatchResult(out, ooff, lab, stats[:arena.count], status[:arena.count], arena,
                        prow, roff)
 

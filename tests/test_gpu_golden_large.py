@@ -30,8 +30,10 @@ sys.path.insert(0, os.path.join(HERE, "golden"))
 import make_golden_large as GL  # noqa: E402  (recipes and hashing of the fixture)
 
 # one warp runs the batched search: keep to the records whose reference run
-# (one CPU core) is short
+# (one CPU core) is short, or whose search has few nodes (the reference spends
+# its time on n^2 certificates there, the GPU kernel's are O(m))
 BATCH_REF_SECONDS = 1.0
+BATCH_NODES = 100
 
 
 @pytest.fixture(scope="module")
@@ -51,11 +53,15 @@ def built(records):
 
 
 def test_wide_search_equals_reference_at_scale(pkg, records, built):
+    # every named configuration graph and every fourth mixed-size graph (the
+    # whole fixture takes about three minutes)
     ctx = pkg.Context(0)
     bad = []
     for rec in records:
+        if rec["name"].startswith("mixed_") and rec["recipe"]["index"] % 4:
+            continue
         g = built[rec["name"]]
-        rows, _, _ = pkg.canon_rows(g, max_aut=rec["max_aut"], ctx=ctx)
+        rows, _, _ = pkg.api.canon_rows(g, max_aut=rec["max_aut"], ctx=ctx)
         if GL.rows_sha256(rows) != rec["rows_sha256"]:
             bad.append(rec["name"])
     ctx.close()
@@ -64,7 +70,8 @@ def test_wide_search_equals_reference_at_scale(pkg, records, built):
 
 def test_batched_search_equals_reference_at_scale(pkg, records, built):
     ctx = pkg.Context(0)
-    recs = [r for r in records if r["ref_seconds"] <= BATCH_REF_SECONDS]
+    recs = [r for r in records
+            if r["ref_seconds"] <= BATCH_REF_SECONDS or r["nodes"] <= BATCH_NODES]
     assert any(r["n"] > 4096 for r in recs)  # the large tier is covered
     recs.sort(key=lambda r: r["n"])
     bad = []
@@ -86,8 +93,8 @@ def test_relabel_invariance_beyond_the_reference(pkg, G):
     rng = np.random.default_rng(20000)
     g = G.random_regular(20000, 4, rng)
     ctx = pkg.Context(0)
-    a, _, _ = pkg.canon_rows(g, ctx=ctx)
-    b, _, _ = pkg.canon_rows(G.random_relabel(g, rng), ctx=ctx)
+    a, _, _ = pkg.api.canon_rows(g, ctx=ctx)
+    b, _, _ = pkg.api.canon_rows(G.random_relabel(g, rng), ctx=ctx)
     ctx.close()
     assert np.array_equal(a, b)
     # the rows describe a 4-regular graph (degree of each canonical vertex)
