@@ -90,6 +90,9 @@ def parse():
                    help="largest request size (the 1%% tail is log-uniform on (2048, nmax])")
     p.add_argument("--serve-large-n", type=int, default=0,
                    help="server large_n (0 = the library default)")
+    p.add_argument("--serve-large-sizes", type=int, nargs="*", default=[8192, 20000],
+                   help="sizes of single requests timed alone on a server (the 1%% tail)")
+    p.add_argument("--serve-large-budget-s", type=float, default=60.0)
     p.add_argument("--serve-big-wide", action="store_true",
                    help="server big_wide: big requests through the wide search")
     p.add_argument("--single-gate", type=int, default=1, choices=(0, 1, 2),
@@ -106,6 +109,8 @@ def parse():
                    help="also time the mixed-size batch (n log-uniform [64,4096]); off by default: "
                         "its union graphs take the reference's search minutes each")
     p.add_argument("--mixed-graphs", type=int, default=2000)
+    p.add_argument("--union-budget-s", type=float, default=30.0,
+                   help="time budget of the 16-copy union in the single-graph block")
     p.add_argument("--mixed-budget-s", type=float, default=10.0,
                    help="per-graph time budget of the mixed-size batch")
     p.add_argument("--mixed-plain", type=int, default=200,
@@ -736,9 +741,9 @@ def serving_block(args, pkg, local):
     if args.serve_big_wide:
         scfg["big_wide"] = 1
     srv = pkg.Server(local, **scfg)
-    # warm-up on the same server (its lanes size their buffers): a short
-    # replay of the first requests
-    Ww = G.serving_workload(300, args.serve_rate, seed=5001, n_max=min(args.serve_nmax, 2048))
+    # warm-up on the same server (its lanes size their workspaces): a short
+    # replay of another stream with the same size range
+    Ww = G.serving_workload(600, args.serve_rate, seed=5001, n_max=args.serve_nmax)
     srv.replay(G.pack(Ww.graphs), Ww.kind, Ww.g1, Ww.g2, Ww.arrival, timeout_s=600)
     st0 = srv.stats()
     t0 = time.perf_counter()
@@ -788,6 +793,33 @@ def serving_block(args, pkg, local):
                                          "copies_in", "search_launch", "table_and_copies_out"),
                                         (x / 1e6 for x in st["enqueue_part_max_ns"]))),
     }
+    # the size tail beyond the stream's n_max (config: 1% up to 20,000):
+    # single requests of the stream's family, each alone on the server, with
+    # a time budget; what bounds them is the reference's search on trees
+    # (its node count grows about quadratically with n), each node a
+    # refinement of the whole graph
+    big = {}
+    old = os.environ.get("GCL_GRAPH_BUDGET_S")
+    os.environ["GCL_GRAPH_BUDGET_S"] = str(args.serve_large_budget_s)
+    try:
+        rng = np.random.default_rng(5002)
+        for n in args.serve_large_sizes:
+            g = G.tree_plus_edges(n, rng)
+            srv = pkg.Server(local)
+            t = time.perf_counter()
+            r = srv.replay(G.pack([g]), np.zeros(1, np.int32), np.zeros(1, np.int32),
+                           np.zeros(1, np.int32), np.zeros(1), timeout_s=args.serve_large_budget_s + 60)
+            dt = time.perf_counter() - t
+            srv.close()
+            big[str(n)] = {"status": int(r[0].status), "latency_ms": r[0].latency_s * 1e3,
+                           "gpu_ms": (r[0].gpu_done_s - r[0].launch_s) * 1e3, "wall_ms": dt * 1e3}
+    finally:
+        if old is None:
+            os.environ.pop("GCL_GRAPH_BUDGET_S", None)
+        else:
+            os.environ["GCL_GRAPH_BUDGET_S"] = old
+    block["size_tail_alone"] = {"budget_s": args.serve_large_budget_s,
+                                "family": "tree (max deg 4) + 0-6 edges", "requests": big}
     # the plain form under the same arrivals: the first requests served one
     # at a time in arrival order, each graph through its own gcl_canon_one
     # call; service times are measured, queueing (FIFO, one server) follows
@@ -861,6 +893,52 @@ def single_graph_block(args, pkg, local, with_cpu):
             row["equal_to_cpu_ref"] = bool(np.array_equal(m, a.matrix))
         out[name] = row
     ctx.close()
+    out["union_reg4_64"] = union_block(args, pkg, local)
+    return out
+
+
+def union_block(args, pkg, local):
+    """Disjoint unions of k copies of one random 4-regular graph on 64
+    vertices (seed 66, the fixture's union family) through the wide search
+    with work sharing: k = 2..6 against the reference's canonical forms in
+    the fixture, and k = 16 (beyond the reference: 8 copies take it minutes)
+    under a time budget, relabeling-checked when it finishes."""
+    G = pkg.graphs
+    gold = _golden_large()
+    comp = G.random_regular(64, 4, np.random.default_rng(66))
+    ctx = pkg.Context(local)
+    ctx.set_option(pkg.api.GCL_OPT_WIDE_SHARE, 1)
+    out = {"copies_vs_reference": {}}
+    old = os.environ.get("GCL_GRAPH_BUDGET_S")
+    try:
+        for k in (2, 3, 4, 5, 6):
+            g = G.disjoint_union(comp, k)
+            t = time.perf_counter()
+            rows, nodes, _ = pkg.api.canon_rows(g, ctx=ctx)
+            rec = gold.get(f"union_reg4_64_x{k}")
+            out["copies_vs_reference"][k] = {
+                "gpu_ms": (time.perf_counter() - t) * 1e3, "nodes": nodes,
+                "reference_nodes": rec["nodes"] if rec else None,
+                "reference_single_core_s": rec["ref_seconds"] if rec else None,
+                "equal_to_reference": bool(rec and _rows_sha256(rows) == rec["rows_sha256"])}
+        os.environ["GCL_GRAPH_BUDGET_S"] = str(args.union_budget_s)
+        g = G.disjoint_union(comp, 16)
+        row = {"n": g.n, "budget_s": args.union_budget_s}
+        t = time.perf_counter()
+        try:
+            a, nodes, _ = pkg.api.canon_rows(g, ctx=ctx)
+            row.update(gpu_ms=(time.perf_counter() - t) * 1e3, nodes=nodes, finished=True)
+            b, _, _ = pkg.api.canon_rows(G.random_relabel(g, np.random.default_rng(16)), ctx=ctx)
+            row["relabel_invariant"] = bool(np.array_equal(a, b))
+        except pkg.GclError as e:
+            row.update(gpu_ms=(time.perf_counter() - t) * 1e3, finished=False, status=int(e.rc))
+        out["copies_16"] = row
+    finally:
+        if old is None:
+            os.environ.pop("GCL_GRAPH_BUDGET_S", None)
+        else:
+            os.environ["GCL_GRAPH_BUDGET_S"] = old
+        ctx.close()
     return out
 
 

@@ -332,6 +332,214 @@ __device__ __noinline__ uint32_t sp_list_nonsingleton() {
 }
 
 // ---------------------------------------------------------------------------
+// One refinement step with a non-singleton splitter of at most 32 members
+// whose members have at most 32 neighbours in all (partition_refinement.cpp:
+// 244-465), warp-synchronously: lane i takes the i-th edge out of the
+// splitter; lanes holding the same neighbour are grouped (its count is the
+// group's size), the neighbours' leaders are grouped by cell, and each
+// touched cell ranks its touched vertices by count with a radix pass over
+// ballots.  A cell that splits is rearranged in place: its untouched
+// vertices first, then its touched ones in ascending count (the reference's
+// fragment order; order inside a fragment is immaterial).  The hash then
+// folds every non-singleton cell in position order -- an untouched one
+// contributes its start, a touched one its fragments -- and lane 0 does the
+// bookkeeping of the splits (starts, in_level, active set, hint) in the same
+// order.  Nothing goes through the per-step scratch arrays of the general
+// path.  Returns false, having changed nothing, when the splitter is too
+// large; `lc` and `hint` are the refinement's running hash and hint.
+// ---------------------------------------------------------------------------
+__device__ __noinline__ bool sp_refine_small(uint32_t s, uint32_t len, uint32_t lvl1,
+                                             uint32_t* lc_io, uint32_t* hint_io) {
+  SpWarp& W = sp_w();
+  const uint32_t lane = lane_id();
+  if (len > 32) return false;
+  // the splitter's edges, lane by lane
+  uint32_t d = 0;
+  int32_t b = 0;
+  if (lane < len) {
+    const uint32_t w = W.elem[s + lane];
+    b = W.rp[w];
+    d = (uint32_t)(W.rp[w + 1] - b);
+  }
+  uint32_t incl = d;
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(GCL_FULL, incl, o);
+    if (lane >= (uint32_t)o) incl += y;
+  }
+  const uint32_t D = __shfl_sync(GCL_FULL, incl, 31);
+  if (D > 32) return false;
+  const uint32_t excl = incl - d;
+  const uint32_t nonempty = __ballot_sync(GCL_FULL, d > 0);
+  const uint32_t firsts = __reduce_or_sync(GCL_FULL, d > 0 ? (1u << excl) : 0u);
+  uint32_t u = kNone;
+  {
+    // lane i < D: member = the k-th non-empty one, k = firsts up to lane i
+    const uint32_t k = (uint32_t)__popc(firsts & (lanemask_lt() | (1u << lane)));
+    const int src = lane < D ? __fns(nonempty, 0, (int)k) : 0;
+    const int32_t bs = __shfl_sync(GCL_FULL, b, src);
+    const uint32_t es = __shfl_sync(GCL_FULL, excl, src);
+    if (lane < D) u = (uint32_t)W.col[bs + (int32_t)(lane - es)];
+  }
+  // the neighbour's cell; singleton cells never split (:257-259)
+  uint32_t p = 0, c = kNone, L = 0;
+  if (u != kNone) {
+    p = W.pos[u];
+    c = sp_cell_of(W, p);
+    L = sp_cell_end(W, c) - c;
+    if (L <= 1) u = kNone;
+  }
+  const uint32_t gu = __match_any_sync(GCL_FULL, u);
+  const uint32_t cnt = (uint32_t)__popc(gu);  // u's neighbours in the splitter
+  const bool lead = u != kNone && lane == (uint32_t)(__ffs(gu) - 1);
+  const uint32_t gc = __match_any_sync(GCL_FULL, lead ? c : kNone);
+  const uint32_t k = lead ? (uint32_t)__popc(gc) : 0u;  // touched vertices of the cell
+  // rank by count within the cell (radix pass, counts <= 32: 6 bits)
+  uint32_t peers = lead ? gc : 0u, less = 0;
+  for (int bit = 5; bit >= 0; --bit) {
+    const bool one = (cnt >> bit) & 1u;
+    const uint32_t m1 = __ballot_sync(GCL_FULL, lead && one);
+    if (lead) {
+      if (one) {
+        less += (uint32_t)__popc(peers & ~m1);
+        peers &= m1;
+      } else {
+        peers &= ~m1;
+      }
+    }
+  }
+  const uint32_t eqidx = (uint32_t)__popc(peers & lanemask_lt());
+  const uint32_t fsize = (uint32_t)__popc(peers);
+  const bool uniform = lead && k == L && fsize == k;  // one common count: no split
+  const bool split = lead && !uniform;
+  const uint32_t R0 = c + (L - k);
+  const uint32_t f = R0 + less;  // this vertex's fragment start
+  const bool cell_lead = lead && lane == (uint32_t)(__ffs(gc) - 1);
+  // rearrange the split cells: touched vertices to R0 + rank, the untouched
+  // vertices found in [R0, c + L) to the positions the touched ones leave
+  uint32_t x = 0, h = 0;
+  bool out = false;
+  if (split) {
+    const bool in = p >= R0;
+    const uint32_t inner = __reduce_or_sync(gc, in ? (1u << (p - R0)) : 0u);
+    const uint32_t outs = __ballot_sync(gc, !in);
+    if (!in) {
+      const uint32_t j = (uint32_t)__popc(outs & lanemask_lt());
+      const uint32_t holes = ~inner & (k >= 32 ? 0xffffffffu : ((1u << k) - 1u));
+      h = R0 + (uint32_t)__fns(holes, 0, (int)j + 1);
+      x = W.elem[h];
+      out = true;
+    }
+  }
+  __syncwarp();
+  if (out) {
+    W.elem[p] = x;
+    W.pos[x] = p;
+  }
+  if (split) {
+    const uint32_t t = f + eqidx;
+    W.elem[t] = u;
+    W.pos[u] = t;
+  }
+  if (cell_lead) bm_set_atomic(W.tcb, W.tcbs, c);
+  __syncwarp();
+  // the fold over the non-singleton cells in position order (:253-465)
+  uint32_t lc = *lc_io, hint = *hint_io;
+  const uint32_t K = sp_list_nonsingleton();
+  uint32_t pend = 0;  // lanes whose fragment is a new cell start
+  for (uint32_t i0 = 0; i0 < K; i0 += 32) {
+    const uint32_t il = i0 + lane;
+    const uint32_t cl = il < K ? W.nsl[il] : 0u;
+    const uint32_t tmask = __ballot_sync(GCL_FULL, il < K && bm_test(W.tcb, cl));
+    const uint32_t cnt32 = min(32u, K - i0);
+    if (!tmask) {  // 32 untouched cells: each member has count 0, item = start
+      lc = mash_fold32(lc, cl, cnt32);
+      continue;
+    }
+    for (uint32_t jj = 0; jj < cnt32; ++jj) {
+      const uint32_t cc = __shfl_sync(GCL_FULL, cl, (int)jj);
+      if (!((tmask >> jj) & 1u)) {
+        lc = mash(lc, cc);  // untouched: every member has count 0
+        continue;
+      }
+      const uint32_t src = (uint32_t)__ffs(__ballot_sync(GCL_FULL, cell_lead && c == cc)) - 1;
+      const bool uni = __shfl_sync(GCL_FULL, uniform, (int)src);
+      if (uni) {
+        lc = mash(lc, __shfl_sync(GCL_FULL, cnt, (int)src) + cc);
+        continue;
+      }
+      const uint32_t Lc = __shfl_sync(GCL_FULL, L, (int)src);
+      const uint32_t kc = __shfl_sync(GCL_FULL, k, (int)src);
+      const bool was = bm_test(W.act, cc);
+      const uint32_t oldlev = W.inlev[cc];
+      __syncwarp();
+      uint32_t maxsz = 0, maxf = cc, lastf = cc;
+      if (Lc > kc) {  // the untouched fragment first
+        lc = mash(lc, 0u + cc);
+        if (lane == 0) set_inlev(W, cc, lvl1);
+        maxsz = Lc - kc;
+      }
+      // the touched fragments in ascending count (= ascending start)
+      uint32_t F = __ballot_sync(GCL_FULL, split && c == cc && eqidx == 0);
+      while (F) {
+        const uint32_t fm = __reduce_min_sync(GCL_FULL, ((F >> lane) & 1u) ? f : kNone);
+        const uint32_t s2 = (uint32_t)__ffs(__ballot_sync(GCL_FULL, ((F >> lane) & 1u) && f == fm)) - 1;
+        F &= ~(1u << s2);
+        const uint32_t sz = __shfl_sync(GCL_FULL, fsize, (int)s2);
+        lc = mash(lc, __shfl_sync(GCL_FULL, cnt, (int)s2) + fm);
+        if (fm != cc) {
+          pend |= 1u << s2;
+          if (sz == 1) hint = fm;
+        }
+        if (lane == 0) {
+          set_inlev(W, fm, lvl1);
+          if (fm != cc) {
+            W.ncells += 1;
+            if (!bm_test(W.act, fm)) {
+              bm_set1(W.act, W.acts, fm);
+              W.nact += 1;
+            }
+          }
+        }
+        if (sz > maxsz) {
+          maxsz = sz;
+          maxf = fm;
+        }
+        lastf = fm;
+      }
+      if (lane == 0) {
+        if (!was) {
+          if (!bm_test(W.act, cc)) {
+            bm_set1(W.act, W.acts, cc);
+            W.nact += 1;
+          }
+          if (bm_test(W.act, maxf)) {
+            bm_clear1(W.act, W.acts, maxf);
+            W.nact -= 1;
+          }
+        }
+        set_inlev(W, lastf, oldlev);
+      }
+      __syncwarp();
+    }
+  }
+  // the new starts, set after the fold (which walked the old ones)
+  while (pend) {
+    const uint32_t s2 = (uint32_t)__ffs(pend) - 1;
+    pend &= pend - 1;
+    const uint32_t fs = __shfl_sync(GCL_FULL, f, (int)s2);
+    if (lane == 0) add_start(W, fs);
+  }
+  if (cell_lead) {  // the touched-cell marks go
+    W.tcb[c >> 6] = 0;
+    W.tcbs[c >> 12] = 0;
+  }
+  __syncwarp();
+  *lc_io = lc;
+  *hint_io = hint;
+  return true;
+}
+
+// ---------------------------------------------------------------------------
 // Partition_s_refinement (partition_refinement.cpp:150-485).  The active
 // bitmap holds the initially active cells; returns the code (-1 on a failed
 // consistency check).  The caller increments the level.
@@ -344,17 +552,27 @@ __device__ __noinline__ int sp_refine(uint32_t level) {
   uint32_t lc = W.ncells, hint = 0;
   uint64_t iters = 0;
   int ok = 1;
+  // the arrays a step touches, in registers for the whole refinement (the
+  // warp record's pointers would otherwise be reloaded after every store)
+  uint32_t* const elem = W.elem;
+  uint32_t* const pos = W.pos;
+  uint64_t* const stb = W.stb;
+  uint64_t* const sts = W.sts;
+  uint64_t* const act = W.act;
+  uint64_t* const acts = W.acts;
+  const int32_t* const rp = W.rp;
+  const int32_t* const col = W.col;
   while (W.ncells < n && W.nact > 0) {
     if (++iters > 4ull * n + 64) {  // every step removes an active cell or splits one
       ok = 0;
       break;
     }
     uint32_t s;
-    if (bm_test(W.act, hint)) {
+    if (bm_test(act, hint)) {
       s = hint;
     } else {
-      s = bm_next(W.act, W.acts, hint + 1, n, nw, nsw);
-      if (s >= n) s = bm_next(W.act, W.acts, 0, n, nw, nsw);
+      s = bm_next(act, acts, hint + 1, n, nw, nsw);
+      if (s >= n) s = bm_next(act, acts, 0, n, nw, nsw);
     }
     if (s >= n) {
       ok = 0;
@@ -362,12 +580,12 @@ __device__ __noinline__ int sp_refine(uint32_t level) {
     }
     __syncwarp();
     if (lane == 0) {
-      bm_clear1(W.act, W.acts, s);
+      bm_clear1(act, acts, s);
       W.nact -= 1;
       W.ntouched = 0;
     }
-    __syncwarp();
-    const uint32_t e = sp_cell_end(W, s);
+    const uint32_t e = bm_test(stb, s + 1) || s + 1 >= n ? s + 1
+                                                          : bm_next(stb, sts, s + 1, n, nw, nsw);
     const uint32_t len = e - s;
     lc = mash(lc, s + e - 1);
     if (len > 1) lc = mash(lc, len);
@@ -378,16 +596,20 @@ __device__ __noinline__ int sp_refine(uint32_t level) {
     // [neighbours, non-neighbours]: its misplaced neighbours swap with the
     // non-neighbours inside its first k positions, then the split cells are
     // folded in position order (:296-309, 399-435).
-    if (len == 1 && W.rp[W.elem[s] + 1] - W.rp[W.elem[s]] <= 32) {
-      const uint32_t w = W.elem[s];
-      const int32_t b = W.rp[w], d = W.rp[w + 1] - b;
-      const bool have = (int32_t)lane < d;
+    int32_t sb = 0, sd = 0;
+    if (len == 1) {
+      const uint32_t w = elem[s];
+      sb = rp[w];
+      sd = rp[w + 1] - sb;
+    }
+    if (len == 1 && sd <= 32) {
+      const bool have = (int32_t)lane < sd;
       uint32_t u = 0, p = 0, c = kNone, L = 0;
       if (have) {
-        u = (uint32_t)W.col[b + (int32_t)lane];
-        p = W.pos[u];
-        c = sp_cell_of(W, p);
-        L = sp_cell_end(W, c) - c;
+        u = (uint32_t)col[sb + (int32_t)lane];
+        p = pos[u];
+        c = bm_prev(stb, sts, p);
+        L = bm_next(stb, sts, c + 1, n, nw, nsw) - c;
       }
       const bool act_l = have && L > 1;
       const uint32_t grp = __match_any_sync(GCL_FULL, act_l ? c : kNone);
@@ -403,51 +625,57 @@ __device__ __noinline__ int sp_refine(uint32_t level) {
           const uint32_t j = (uint32_t)__popc(outs & lanemask_lt());
           const uint32_t holes = ~inner & (k >= 32 ? 0xffffffffu : ((1u << k) - 1u));
           h = c + (uint32_t)__fns(holes, 0, (int)j + 1);
-          x = W.elem[h];
+          x = elem[h];
           mv = true;
         }
       }
+      // whether each split cell was active, read before any of this step's
+      // active-set writes (they only touch the split cells' own starts)
+      const bool lead = spl_l && lane == (uint32_t)(__ffs(grp) - 1);
+      const bool was_l = lead && bm_test(act, c);
       __syncwarp();
       if (mv) {
-        W.elem[h] = u;
-        W.pos[u] = h;
-        W.elem[p] = x;
-        W.pos[x] = p;
+        elem[h] = u;
+        pos[u] = h;
+        elem[p] = x;
+        pos[x] = p;
       }
-      __syncwarp();
-      uint32_t leaders = __ballot_sync(GCL_FULL, spl_l && lane == (uint32_t)(__ffs(grp) - 1));
+      // split cells in position order: hash, in_level, starts, active set;
+      // hint and hash are the same on every lane, lane 0 writes
+      uint32_t leaders = __ballot_sync(GCL_FULL, lead);
       while (leaders) {
         const bool mine = (leaders >> lane) & 1u;
         const uint32_t cmin = __reduce_min_sync(GCL_FULL, mine ? c : kNone);
         const uint32_t src = (uint32_t)__ffs(__ballot_sync(GCL_FULL, mine && c == cmin)) - 1;
-        const uint32_t kk = __shfl_sync(GCL_FULL, k, (int)src), LL = __shfl_sync(GCL_FULL, L, (int)src);
+        const uint32_t kk = __shfl_sync(GCL_FULL, k, (int)src);
+        const uint32_t LL = __shfl_sync(GCL_FULL, L, (int)src);
+        const bool was = __shfl_sync(GCL_FULL, was_l, (int)src);
         leaders &= ~(1u << src);
         const uint32_t pp = cmin + kk;
         lc = mash(lc, pp - 1);  // cell.first + neighbors_size - 1
-        const bool was = bm_test(W.act, cmin);
-        __syncwarp();
+        const uint32_t nb = kk, nn = LL - kk;
+        const bool to_rest = was || nb >= nn;
+        if (to_rest) {
+          if (nn == 1) hint = pp;
+        } else {
+          if (nb == 1) hint = cmin;
+        }
         if (lane == 0) {
           set_inlev(W, pp, W.inlev[cmin]);
           set_inlev(W, cmin, lvl1);
           add_start(W, pp);
           W.ncells += 1;
-          const uint32_t nb = kk, nn = LL - kk;
-          if (was || nb >= nn) {
-            bm_set1(W.act, W.acts, pp);
-            W.nact += 1;
-            if (nn == 1) hint = pp;
-          } else {
-            bm_set1(W.act, W.acts, cmin);
-            W.nact += 1;
-            if (nb == 1) hint = cmin;
-          }
-          W.hint = hint;
+          bm_set1(act, acts, to_rest ? pp : cmin);
+          W.nact += 1;
         }
-        __syncwarp();
-        hint = W.hint;
       }
+      __syncwarp();
       continue;
     }
+
+    // a small non-singleton splitter: warp-synchronous, no scratch arrays
+    if (len > 1 && sp_refine_small(s, len, lvl1, &lc, &hint)) continue;
+    __syncwarp();  // lane 0's reset of the touched count is seen by all
 
     // count neighbours in the splitter, record touched vertices and cells
     // (cells that are singletons never split and are skipped, :257-259)
@@ -548,6 +776,10 @@ __device__ __noinline__ int sp_refine(uint32_t level) {
         const uint32_t cl = il < K ? W.nsl[il] : 0u;
         const uint32_t tmask = __ballot_sync(GCL_FULL, il < K && bm_test(W.tcb, cl));
         const uint32_t cnt32 = min(32u, K - i0);
+        if (!tmask) {  // 32 untouched cells: item = start
+          lc = mash_fold32(lc, cl, cnt32);
+          continue;
+        }
         for (uint32_t jj = 0; jj < cnt32; ++jj) {
           const uint32_t c = __shfl_sync(GCL_FULL, cl, (int)jj);
           if (!((tmask >> jj) & 1u)) {

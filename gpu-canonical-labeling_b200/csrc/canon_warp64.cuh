@@ -183,14 +183,22 @@ static __device__ __noinline__ W64Refined w64_refine(int n, uint64_t starts, uin
       // when N(w) meets it partially.  Only neighbours outside singleton
       // cells can be in such a cell, so most steps end here.
       const uint64_t N = S.adj[S.pv[s]];
-      uint64_t X = N & ~sing;
+      const uint64_t X = N & ~sing;
       if (!X) continue;
-      uint64_t splitc = 0;
-      while (X) {
-        const uint32_t c = S.cs[ctz64(X)];
-        const uint64_t C = S.cmask[c];
-        X &= ~C;
-        if (C & ~N) splitc |= bit64(c);
+      // lane i looks at the i-th such neighbour's cell: split when the cell
+      // is not all neighbours
+      uint64_t splitc;
+      {
+        const uint32_t xl = (uint32_t)X, xh = (uint32_t)(X >> 32);
+        const uint32_t nl = (uint32_t)__popc(xl), nx = nl + (uint32_t)__popc(xh);
+        uint64_t mine = 0;
+        if (lane < nx) {
+          const uint32_t v = lane < nl ? (uint32_t)__fns(xl, 0, (int)lane + 1)
+                                       : 32u + (uint32_t)__fns(xh, 0, (int)(lane - nl) + 1);
+          const uint32_t c = S.cs[v];
+          if (S.cmask[c] & ~N) mine = bit64(c);
+        }
+        splitc = warp_or64(mine);
       }
       // split cells in position order: hash, active set, in_level (:296-465)
       while (splitc) {
@@ -302,29 +310,37 @@ static __device__ __noinline__ W64Refined w64_refine(int n, uint64_t starts, uin
         const uint64_t single_all = all & ((all >> 1) | lastbit);
         const uint64_t hs = NS & single_all;
         if (hs) hint = msb64(hs);
-        const uint64_t was = active;
-        active |= NS;
-        t = NS;
-        while (t) {
-          const uint32_t c = msb64(starts & low_mask(ctz64(t)));
-          const uint64_t nc = starts & ge_mask(c + 1);
+        // each fragment start of a split cell that was not active offers
+        // (size, -position) for its cell's first largest fragment, one
+        // shared-memory max per cell (S.dsu is free outside the orbits)
+        uint32_t key0 = 0, key1 = 0, cell0 = 0, cell1 = 0;
+        bool fr0 = false, fr1 = false;
+        if ((all >> v0) & 1ull) {
+          cell0 = msb64(starts & low_mask(v0 + 1));
+          const uint64_t nc = starts & ge_mask(cell0 + 1);
           const uint32_t end = nc ? ctz64(nc) : (uint32_t)n;
-          t &= ~low_mask(end);
-          if ((was >> c) & 1ull) continue;
-          uint64_t fr = all & ge_mask(c) & low_mask(end);
-          uint32_t maxsz = 0, maxp = c;
-          while (fr) {
-            const uint32_t f = ctz64(fr);
-            fr &= fr - 1;
-            const uint32_t sz = (fr ? ctz64(fr) : end) - f;
-            if (sz > maxsz) {
-              maxsz = sz;
-              maxp = f;
-            }
-          }
-          active |= bit64(c);
-          active &= ~bit64(maxp);
+          const uint64_t nf = all & ge_mask(v0 + 1);
+          fr0 = !((active >> cell0) & 1ull) && (NS & low_mask(end) & ge_mask(cell0 + 1)) != 0;
+          key0 = ((min(nf ? ctz64(nf) : (uint32_t)n, end) - v0) << 6) | (63u - v0);
         }
+        if ((all >> v1) & 1ull) {
+          cell1 = msb64(starts & low_mask(v1 + 1));
+          const uint64_t nc = starts & ge_mask(cell1 + 1);
+          const uint32_t end = nc ? ctz64(nc) : (uint32_t)n;
+          const uint64_t nf = all & ge_mask(v1 + 1);
+          fr1 = !((active >> cell1) & 1ull) && (NS & low_mask(end) & ge_mask(cell1 + 1)) != 0;
+          key1 = ((min(nf ? ctz64(nf) : (uint32_t)n, end) - v1) << 6) | (63u - v1);
+        }
+        __syncwarp();
+        if (fr0 && cell0 == v0) S.dsu[cell0] = 0;
+        if (fr1 && cell1 == v1) S.dsu[cell1] = 0;
+        __syncwarp();
+        if (fr0) atomicMax(&S.dsu[cell0], key0);
+        if (fr1) atomicMax(&S.dsu[cell1], key1);
+        __syncwarp();
+        const uint64_t out = ballot2(fr0 && S.dsu[cell0] == key0, fr1 && S.dsu[cell1] == key1);
+        const uint64_t in = ballot2(fr0 && cell0 == v0, fr1 && cell1 == v1);
+        active = (active | NS | in) & ~out;
         __syncwarp();
         if (w0 != 0xffu) S.inlev[v0] = (uint8_t)w0;
         if (w1 != 0xffu) S.inlev[v1] = (uint8_t)w1;

@@ -112,7 +112,7 @@ constexpr uint32_t kSpPool = 32, kSpPoolHuge = 8;
 constexpr uint32_t kSpAutCap = 256, kSpAutCapHuge = 64;
 constexpr uint32_t kSpPoolMid = 256, kSpAutCapMid = 2048;
 
-__global__ void __launch_bounds__(kSpThreads)
+__global__ void __launch_bounds__(kSpThreads, 5)
     sp_batch_kernel(BatchArgs A, const int* list, const int* count, int* next, int* fail_list,
                     int* fail_count, uint32_t n_max, uint64_t m2_max, uint32_t pool, uint32_t cap,
                     uint64_t slot_bytes, uint64_t smem_per_warp) {

@@ -434,6 +434,32 @@ std::vector<Req*> take_batch(gcl_server* S, Lane* L) {
   return out;
 }
 
+// Sizes a lane's host and device buffers up front for batches of `graphs`
+// graphs with `verts` vertices, `edges` CSR entries and `words` packed-row
+// words in all, so that serving does not allocate pinned memory: pinning
+// pages takes the driver's lock, and every other lane's CUDA calls waited
+// behind it (hundreds of ms under load).  Larger batches still grow them.
+cudaError_t lane_reserve(Lane* L, int64_t graphs, int64_t verts, int64_t edges, int64_t words) {
+  cudaError_t e = cudaSuccess;
+  auto ens = [&](HostBuf& h, DevMem& d, size_t bytes) {
+    if (e == cudaSuccess) e = h.ensure(bytes);
+    if (e == cudaSuccess) e = d.ensure(bytes);
+  };
+  ens(L->h_voff, L->d_voff, (size_t)(graphs + 1) * 8);
+  ens(L->h_eoff, L->d_eoff, (size_t)(graphs + 1) * 8);
+  ens(L->h_rp, L->d_rp, (size_t)(verts + graphs) * 4);
+  ens(L->h_col, L->d_col, (size_t)edges * 4);
+  ens(L->h_color, L->d_color, (size_t)verts * 4);
+  ens(L->h_roff, L->d_roff, (size_t)(graphs + 1) * 8);
+  ens(L->h_rows, L->d_rows, (size_t)words * 8);
+  ens(L->h_label, L->d_label, (size_t)verts * 4);
+  ens(L->h_status, L->d_status, (size_t)graphs * 4);
+  ens(L->h_hash, L->d_hash, (size_t)graphs * 8);
+  ens(L->h_class, L->d_class, (size_t)graphs * 8);
+  ens(L->h_seen, L->d_seen, (size_t)graphs * 4);
+  return e;
+}
+
 int launch(gcl_server* S, Lane* L) {
   int count = 0;
   int64_t nv = 0, ne = 0, words = 0;
@@ -941,6 +967,20 @@ int gcl_serve_create(int device, const gcl_serve_config* cfg, gcl_server** out) 
       if (rc == GCL_OK && (L->cls == kBig || L->large))
         rc = gcl_set_option(L->ctx, GCL_OPT_SMEM_STAGE, 0);
     }
+  }
+  // each lane's buffers for a full batch of its class (mean degree 8; the
+  // large lanes for a pair of 8,192-vertex graphs)
+  for (Lane* L : S->lanes) {
+    if (rc != GCL_OK) break;
+    int64_t g = 0, nmax = 0;
+    switch (L->cls) {
+      case kSmall: g = c.max_batch, nmax = 64; break;
+      case kMid: g = c.mid_batch, nmax = 256; break;
+      case kBig: g = S->max_batch[kBig], nmax = 2048; break;
+      default: g = 2, nmax = 8192; break;
+    }
+    const int64_t v = g * nmax;
+    rc = rc_of(lane_reserve(L, g, v, v * 8, v * ((nmax + 63) / 64)));
   }
   if (rc == GCL_OK) rc = rc_of(S->keys.ensure((size_t)c.table_slots * 8));
   if (rc == GCL_OK) rc = rc_of(S->vals.ensure((size_t)c.table_slots * 4));
