@@ -329,12 +329,13 @@ class Clocks:
 
 
 def read_traffic():
-    """dram bytes per launch of the batch kernel from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "w64_batch_kernel_small10k.txt")
+    """DRAM bytes of one step's warp-kernel launches (root pass + search pass)
+    from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "w64_root_search_kernels_small10k.txt")
     if not os.path.exists(p):
         return None
     for ln in open(p):
-        if ln.strip().startswith("dram_bytes_per_launch:"):
+        if ln.strip().startswith("dram_bytes_per_step:"):
             return float(ln.split(":")[1].split()[0])
     return None
 
@@ -609,7 +610,10 @@ def gpu_arm(args):
                           "h2d_bytes_per_step": int(h2d_dense),
                           "d2h_bytes_per_step": int(d2h_dense),
                           "output": "n*n byte matrices (the reference's Nauty_Parallel form)"},
-            "gpu_launches": 2 * args.steps,
+            # per step: order_by_size, the root pass, the search pass and the
+            # full-ring rerun pass (which exits at once when no graph outgrew
+            # the first ring)
+            "gpu_launches": 4 * args.steps,
             **({"e2e_overlap": {"value": job_rate(count, world, args.steps, e2e_ov_s),
                                 "unit": UNIT, "contexts": args.e2e_contexts,
                                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),

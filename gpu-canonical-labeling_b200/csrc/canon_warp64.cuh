@@ -185,18 +185,18 @@ static __device__ __noinline__ W64Refined w64_refine(int n, uint64_t starts, uin
       const uint64_t N = S.adj[S.pv[s]];
       const uint64_t X = N & ~sing;
       if (!X) continue;
-      // lane i looks at the i-th such neighbour's cell: split when the cell
-      // is not all neighbours
+      // lane i looks at the cells of the i-th and (i+32)-th such
+      // neighbours: a cell splits when it is not all neighbours
       uint64_t splitc;
       {
         const uint32_t xl = (uint32_t)X, xh = (uint32_t)(X >> 32);
         const uint32_t nl = (uint32_t)__popc(xl), nx = nl + (uint32_t)__popc(xh);
         uint64_t mine = 0;
-        if (lane < nx) {
-          const uint32_t v = lane < nl ? (uint32_t)__fns(xl, 0, (int)lane + 1)
-                                       : 32u + (uint32_t)__fns(xh, 0, (int)(lane - nl) + 1);
+        for (uint32_t i = lane; i < nx; i += 32) {
+          const uint32_t v = i < nl ? (uint32_t)__fns(xl, 0, (int)i + 1)
+                                    : 32u + (uint32_t)__fns(xh, 0, (int)(i - nl) + 1);
           const uint32_t c = S.cs[v];
-          if (S.cmask[c] & ~N) mine = bit64(c);
+          if (S.cmask[c] & ~N) mine |= bit64(c);
         }
         splitc = warp_or64(mine);
       }
