@@ -562,7 +562,14 @@ __device__ __noinline__ int sp_refine(uint32_t level) {
   uint64_t* const acts = W.acts;
   const int32_t* const rp = W.rp;
   const int32_t* const col = W.col;
-  while (W.ncells < n && W.nact > 0) {
+  uint32_t* const inlev = W.inlev;
+  uint2* const ulog = W.ulog;
+  const uint32_t ucap = W.ulog_cap;
+  // the cell and active counts and the undo log's top, kept by every lane
+  // alike during the singleton steps; the warp record holds them while the
+  // other paths run (they update them there) and after the refinement
+  uint32_t ncells = W.ncells, nact = W.nact, utop = W.utop;
+  while (ncells < n && nact > 0) {
     if (++iters > 4ull * n + 64) {  // every step removes an active cell or splits one
       ok = 0;
       break;
@@ -579,11 +586,8 @@ __device__ __noinline__ int sp_refine(uint32_t level) {
       break;
     }
     __syncwarp();
-    if (lane == 0) {
-      bm_clear1(act, acts, s);
-      W.nact -= 1;
-      W.ntouched = 0;
-    }
+    if (lane == 0) bm_clear1(act, acts, s);
+    nact -= 1;
     const uint32_t e = bm_test(stb, s + 1) || s + 1 >= n ? s + 1
                                                           : bm_next(stb, sts, s + 1, n, nw, nsw);
     const uint32_t len = e - s;
@@ -661,21 +665,44 @@ __device__ __noinline__ int sp_refine(uint32_t level) {
           if (nb == 1) hint = cmin;
         }
         if (lane == 0) {
-          set_inlev(W, pp, W.inlev[cmin]);
-          set_inlev(W, cmin, lvl1);
-          add_start(W, pp);
-          W.ncells += 1;
+          // in_level of both fragments and the new start, logged in the
+          // order set_inlev / add_start would log them
+          const uint32_t oldc = inlev[cmin], oldp = inlev[pp];
+          if (utop + 3 <= ucap) {
+            ulog[utop] = make_uint2(pp, oldp);
+            ulog[utop + 1] = make_uint2(cmin, oldc);
+            ulog[utop + 2] = make_uint2(pp | kStartFlag, 0u);
+          } else {
+            W.ulog_bad = 1;  // full: backtracks rescan the partition
+          }
+          inlev[pp] = oldc;
+          inlev[cmin] = lvl1;
+          bm_set1(stb, sts, pp);
           bm_set1(act, acts, to_rest ? pp : cmin);
-          W.nact += 1;
         }
+        if (utop + 3 <= ucap) utop += 3;
+        ncells += 1;
+        nact += 1;
       }
       __syncwarp();
       continue;
     }
+    // the other paths keep the counts in the warp record
+    if (lane == 0) {
+      W.ncells = ncells;
+      W.nact = nact;
+      W.utop = utop;
+      W.ntouched = 0;
+    }
+    __syncwarp();
 
     // a small non-singleton splitter: warp-synchronous, no scratch arrays
-    if (len > 1 && sp_refine_small(s, len, lvl1, &lc, &hint)) continue;
-    __syncwarp();  // lane 0's reset of the touched count is seen by all
+    if (len > 1 && sp_refine_small(s, len, lvl1, &lc, &hint)) {
+      ncells = W.ncells;
+      nact = W.nact;
+      utop = W.utop;
+      continue;
+    }
 
     // count neighbours in the splitter, record touched vertices and cells
     // (cells that are singletons never split and are skipped, :257-259)
@@ -895,6 +922,13 @@ __device__ __noinline__ int sp_refine(uint32_t level) {
       W.tcbs[c >> 12] = 0;
     }
     __syncwarp();
+    ncells = W.ncells;
+    nact = W.nact;
+    utop = W.utop;
+  }
+  if (lane == 0) {
+    W.ncells = ncells;
+    W.utop = utop;
   }
   // clear what is left of the active set
   __syncwarp();

@@ -1112,14 +1112,15 @@ __device__ __forceinline__ uint64_t w64_deadline(const BatchArgs& A) {
 
 // The partition after the root refinement, kept in device memory between
 // the root pass and the search pass of a batch: a header (starts, singleton
-// vertices, code), then per vertex or position the adjacency mask, the cell
+// vertices, code, graph id), then per vertex or position the adjacency mask, the cell
 // member mask (at cell starts), the cell start, in_level and the singleton
 // cell's vertex -- what the search reads of the root node.
 __host__ __device__ constexpr uint64_t w64_root_slot_bytes() {
   return 32u + (uint64_t)kW64MaxN * (8u + 8u + 3u);
 }
 
-static __device__ __noinline__ void w64_save_root(uint8_t* dst, int n, uint64_t starts, int code) {
+static __device__ __noinline__ void w64_save_root(uint8_t* dst, int g, int n, uint64_t starts,
+                                                  int code) {
   W64Smem& S = w64_smem();
   const uint32_t lane = lane_id();
   uint64_t* h = reinterpret_cast<uint64_t*>(dst);
@@ -1130,6 +1131,7 @@ static __device__ __noinline__ void w64_save_root(uint8_t* dst, int n, uint64_t 
     h[0] = starts;
     h[1] = S.sing;
     h[2] = (uint64_t)(uint32_t)code;
+    h[3] = (uint64_t)(uint32_t)g;
   }
   for (uint32_t v = lane; v < (uint32_t)n; v += 32) {
     adj[v] = S.adj[v];
@@ -1138,6 +1140,20 @@ static __device__ __noinline__ void w64_save_root(uint8_t* dst, int n, uint64_t 
     b[kW64MaxN + v] = S.inlev[v];
     b[2 * kW64MaxN + v] = S.pv[v];
   }
+}
+
+__device__ __forceinline__ int w64_root_graph(const uint8_t* src) {
+  return (int)(uint32_t)reinterpret_cast<const uint64_t*>(src)[3];
+}
+
+// Search-cost class of a graph from its root partition: log2 of n times the
+// vertices beyond one per cell (on the batched small-graph workload this
+// estimate correlates 0.92 with nodes x n); the search pass takes the
+// classes from the most expensive down, so long searches start first.
+constexpr int kW64CostClasses = 16;
+__device__ __forceinline__ int w64_cost_class(int n, uint64_t starts) {
+  const uint32_t est = (uint32_t)n * (uint32_t)(n - popc64(starts)) + 1u;
+  return min(kW64CostClasses - 1, 31 - __clz((int)est));
 }
 
 static __device__ __noinline__ uint64_t w64_restore_root(const uint8_t* src, int n, int* code) {

@@ -55,6 +55,7 @@ struct Deferred {
   int next_large[kSpBuckets];
   int search_count;    // n <= 64 graphs whose root partition is not discrete
   int next_search;
+  int cost_count[kW64CostClasses];  // ... per search-cost class
 };
 
 // Largest graphs first: a counting sort of the graph ids by descending n
@@ -182,10 +183,12 @@ __global__ void __launch_bounds__(kW64Threads, 8)
 // loads each graph and refines its root partition -- the largest share of
 // the work on small sparse graphs -- and finishes the graphs whose root
 // partition is discrete (their canonical form is the root's); the others
-// leave the root's partition in `roots` and their id in `search_list`.  The
-// search pass runs their trees.  Each pass keeps the warps of an SM in the
-// same few functions, and only the graphs that search take part in the
-// second.  Results equal w64_batch_kernel's.
+// leave the root's partition in a slot of `roots` and the slot's index in
+// the list of their search-cost class (`search_list`, count entries per
+// class).  The search pass runs their trees, the most expensive class
+// first.  Each pass keeps the warps of an SM in the same few functions, and
+// only the graphs that search take part in the second.  Results equal
+// w64_batch_kernel's.
 __global__ void __launch_bounds__(kW64Threads, 8)
     w64_root_kernel(BatchArgs A, Deferred* D, int* large_list, uint8_t* roots, int* search_list) {
   const uint32_t lane = lane_id();
@@ -216,9 +219,12 @@ __global__ void __launch_bounds__(kW64Threads, 8)
       int j = 0;
       if (lane == 0) j = atomicAdd(&D->search_count, 1);
       j = __shfl_sync(GCL_FULL, j, 0);
-      w64_save_root(roots + (uint64_t)j * w64_root_slot_bytes(), n, root.starts, root.code);
+      w64_save_root(roots + (uint64_t)j * w64_root_slot_bytes(), g, n, root.starts, root.code);
       __syncwarp();
-      if (lane == 0) search_list[j] = g;
+      if (lane == 0) {
+        const int k = w64_cost_class(n, root.starts);
+        search_list[(int64_t)k * A.count + atomicAdd(&D->cost_count[k], 1)] = j;
+      }
       continue;
     }
     // finished at the root: the discrete root is the first and best leaf
@@ -246,17 +252,31 @@ __global__ void __launch_bounds__(kW64Threads, 8)
   const int warp = (int)(threadIdx.x >> 5);
   const uint32_t lane = lane_id();
   uint8_t* slot = A.work + ((uint64_t)blockIdx.x * kW64Warps + (uint64_t)warp) * A.slot_bytes;
-  const int total = *(volatile int*)&D->search_count;
+  // the classes from the most expensive down: lane q holds class 15 - q
+  const int cq = lane < (uint32_t)kW64CostClasses
+                     ? *(volatile int*)&D->cost_count[kW64CostClasses - 1 - (int)lane]
+                     : 0;
+  int incl = cq;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(GCL_FULL, incl, o);
+    if (lane >= (uint32_t)o) incl += y;
+  }
+  const int total = __shfl_sync(GCL_FULL, incl, 31);
   while (true) {
     int i = 0;
     if (lane == 0) i = atomicAdd(&D->next_search, 1);
     i = __shfl_sync(GCL_FULL, i, 0);
     if (i >= total) break;
-    const int g = search_list[i];
+    // the class of entry i: the first lane whose inclusive count passes i
+    const int q = __ffs(__ballot_sync(GCL_FULL, incl > i)) - 1;
+    const int first = __shfl_sync(GCL_FULL, incl - cq, q);
+    const int slot_i = search_list[(int64_t)(kW64CostClasses - 1 - q) * A.count + (i - first)];
+    const uint8_t* root = roots + (uint64_t)slot_i * w64_root_slot_bytes();
+    const int g = w64_root_graph(root);
     const int64_t vo = A.voff[g];
     const int n = (int)(A.voff[g + 1] - vo);
     int code = 0;
-    const uint64_t starts = w64_restore_root(roots + (uint64_t)i * w64_root_slot_bytes(), n, &code);
+    const uint64_t starts = w64_restore_root(root, n, &code);
     const W64Result r = w64_search_tree(A, n, starts, code, slot, w64_deadline(A));
     if (lane == 0) {
       A.status[g] = r.status;
@@ -558,7 +578,7 @@ int gcl_canon_batch_device_async(gcl_context* c, int count, const int64_t* d_vof
   GCL_TRY(c->order.ensure((size_t)count * sizeof(int)));
   if (max_n > 0) {
     GCL_TRY(c->roots.ensure((size_t)count * w64_root_slot_bytes()));
-    GCL_TRY(c->search_list.ensure((size_t)count * sizeof(int)));
+    GCL_TRY(c->search_list.ensure((size_t)count * kW64CostClasses * sizeof(int)));
   }
   GCL_TRY(cudaMemsetAsync(c->deferred.p, 0, sizeof(Deferred), c->stream));
   order_by_size_kernel<<<1, kOrderThreads, 0, c->stream>>>(count, d_voff, (int*)c->order.p);
