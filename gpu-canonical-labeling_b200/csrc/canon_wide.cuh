@@ -1021,20 +1021,26 @@ __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
     W.ntouched = 0;
   }
   __syncwarp();
-  for (uint32_t i = lane; i < n; i += 32) {
-    W.cnt[i] = 0;
-    W.cellcnt[i] = 0;
-    W.fill[i] = 0;
-  }
-  for (uint32_t w = lane; w < W.nw; w += 32) {
-    W.act[w] = 0;
-    W.tcb[w] = 0;
-  }
-  for (uint32_t w = lane; w < W.nsw; w += 32) {
-    W.acts[w] = 0;
-    W.tcbs[w] = 0;
-  }
-  __syncwarp();
+  // the per-step scratch starts clear; set up once the warp has work (a
+  // grid has more warps than most searches have items)
+  bool ready = false;
+  auto setup = [&] {
+    for (uint32_t i = lane; i < n; i += 32) {
+      W.cnt[i] = 0;
+      W.cellcnt[i] = 0;
+      W.fill[i] = 0;
+    }
+    for (uint32_t w = lane; w < W.nw; w += 32) {
+      W.act[w] = 0;
+      W.tcb[w] = 0;
+    }
+    for (uint32_t w = lane; w < W.nsw; w += 32) {
+      W.acts[w] = 0;
+      W.tcbs[w] = 0;
+    }
+    __syncwarp();
+    ready = true;
+  };
   const uint64_t deadline = A.budget_ns ? H->t0 + A.budget_ns : 0;
   WideBest best{0, 0, 0xffffffffu};
   uint32_t known = 0, fix_init = 0, prev_k = 0;
@@ -1065,6 +1071,7 @@ __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
         gift = true;
         cnt.add(kCntGiftsTaken, 1);
         tc = cnt.now();
+        if (!ready) setup();
         const int32_t ns = wide_gift_node(P, A, slot, D, &k, &tf, &tl, &v, &gift_eq);
         cnt.add(kCntRefineCycles, cnt.now() - tc);
         if (ns != kOk) {
@@ -1086,6 +1093,7 @@ __global__ void __launch_bounds__(kSpThreads) wide_items_kernel(WideArgs A) {
       }
     }
     if (*(volatile int32_t*)&H->status != kOk) break;
+    if (!ready) setup();
     if (!gift) {
       if constexpr (kShare) {
         if (lane == 0) atomicAdd(&H->busy, 1u);
