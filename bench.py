@@ -113,6 +113,8 @@ def parse():
                    help="time budget of the 16-copy union in the single-graph block")
     p.add_argument("--mixed-budget-s", type=float, default=10.0,
                    help="per-graph time budget of the mixed-size batch")
+    p.add_argument("--mixed-handoff-ms", type=int, default=1000,
+                   help="hand-off budget of the third mixed-batch run (GCL_OPT_BATCH_HANDOFF_MS)")
     p.add_argument("--mixed-plain", type=int, default=200,
                    help="graphs of the mixed batch timed one launch each")
     return p.parse_args()
@@ -981,10 +983,18 @@ def mixed_block(args, pkg, local):
                            f"d-regular d in {{3,4,6}} / tori / 2-4 copies of a regular component "
                            f"(seed 4000)",
                "graph_budget_s": args.mixed_budget_s}
-        for label, tune in (("default_shapes", False), ("autotuned", True)):
+        tuning = None
+        for label, tune, handoff in (("default_shapes", False, 0), ("autotuned", True, 0),
+                                     ("autotuned_handoff", True, args.mixed_handoff_ms)):
             ctx = pkg.Context(local)
             if tune and quick:
-                out["tuning"] = ctx.autotune([gs[i] for i in quick[:200]], repeats=1)
+                if tuning is None:
+                    tuning = ctx.autotune([gs[i] for i in quick[:200]], repeats=1)
+                    out["tuning"] = tuning
+                else:
+                    ctx.set_tuning(tuning)
+            if handoff:
+                ctx.set_option(pkg.api.GCL_OPT_BATCH_HANDOFF_MS, handoff)
             warm = [gs[i] for i in quick[:64]] or gs[:1]
             pkg.canon_batch(warm, ctx=ctx, dense=False, rows=True)  # workspace warm-up
             t = time.perf_counter()
@@ -999,6 +1009,7 @@ def mixed_block(args, pkg, local):
                     checked += 1
                     same += _rows_sha256(r.packed(int(i))) == rec["rows_sha256"]
             out[label] = {"seconds": dt, "graphs_finished": int(ok.sum()),
+                          "handoff_ms": handoff,
                           "graphs_timed_out": int((r.status == 5).sum()),
                           "other_status": int(((~ok) & (r.status != 5)).sum()),
                           "graphs_per_s": float(ok.sum()) / dt,

@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cstddef>
 #include <cstdint>
 #include <cstdio>
@@ -374,6 +375,8 @@ struct gcl_context {
   bool wide_count = false;       // wide search: the items kernel's counters (GCL_OPT_COUNTERS)
   uint32_t wide_pool = kWidePool;  // wide search: per-level orbit arrays of a warp
   bool wide_probe = true;          // wide search: a level's first item runs before the rest
+  uint64_t handoff_ns = 0;         // gcl_canon_batch: batch-warp budget before the wide search
+  uint64_t budget_override_ns = 0; // per-graph budget of the next batched launch (0 = default)
   // mapped host buffers (gcl_host_alloc): host address, size, device address
   struct Mapped {
     uint8_t* p;
@@ -604,7 +607,7 @@ int gcl_canon_batch_device_async(gcl_context* c, int count, const int64_t* d_vof
   A.status = d_out_status;
   A.work = (uint8_t*)c->work.p;
   A.slot_bytes = slot_bytes;
-  A.budget_ns = graph_budget_ns();
+  A.budget_ns = c->budget_override_ns ? c->budget_override_ns : graph_budget_ns();
   Deferred* D = (Deferred*)c->deferred.p;
   const int64_t w64_grid = c->tune_w64_bps > 0
                                ? (int64_t)c->sms * std::min(c->tune_w64_bps, c->w64_per_sm)
@@ -766,6 +769,10 @@ int gcl_set_option(gcl_context* c, int option, int64_t value) {
     case GCL_OPT_WIDE_PROBE:
       if (value != 0 && value != 1) return GCL_ERR_ARG;
       c->wide_probe = value != 0;
+      return GCL_OK;
+    case GCL_OPT_BATCH_HANDOFF_MS:
+      if (value < 0) return GCL_ERR_ARG;
+      c->handoff_ns = (uint64_t)value * 1000000ull;
       return GCL_OK;
     case GCL_OPT_STREAM_PRIORITY: {
       if (value != 0 && value != 1) return GCL_ERR_ARG;
@@ -1017,6 +1024,64 @@ int canon_one(gcl_context* c, const int32_t* rowptr, const int32_t* col, const i
   return GCL_OK;
 }
 
+
+// The graphs (n > 64) of a host batch that ran past the hand-off budget in
+// their batch warp (gcl_canon_batch with GCL_OPT_BATCH_HANDOFF_MS): the wide
+// search, one graph at a time on the context (the smallest first), each
+// within the per-graph budget and all within `hard_ns` (0 = no limit).  A
+// graph it finishes gets
+// the wide search's results in place of the timeout: the same canonical
+// form, a labeling that is one of the equivalent best leaves, and the wide
+// search's own statistics; one it does not finish keeps its timeout.
+int batch_handoff(gcl_context* c, int count, const int64_t* voff, const int64_t* eoff,
+                  const int32_t* d_color, int max_aut, const int64_t* ooff, const int64_t* roff,
+                  uint8_t* out_dense, uint64_t* out_rows, int32_t* out_label,
+                  int64_t* out_stats, int32_t* out_status, uint8_t* d_dense, uint64_t* d_rows,
+                  int32_t* d_label, int64_t* d_stats, uint64_t hard_ns) {
+  cudaStream_t s = c->stream;
+  const auto t0 = std::chrono::steady_clock::now();
+  const int32_t* d_rp = (const int32_t*)c->rowptr.p;
+  const int32_t* d_col = (const int32_t*)c->col.p;
+  int32_t* d_status = (int32_t*)c->status.p;
+  std::vector<int> todo;
+  for (int g = 0; g < count; ++g)
+    if (out_status[g] == kTimeout && voff[g + 1] - voff[g] > kW64MaxN) todo.push_back(g);
+  std::stable_sort(todo.begin(), todo.end(),
+                   [&](int a, int b) { return voff[a + 1] - voff[a] < voff[b + 1] - voff[b]; });
+  for (const int g : todo) {
+    const int64_t n = voff[g + 1] - voff[g];
+    if (hard_ns && (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(
+                       std::chrono::steady_clock::now() - t0).count() > hard_ns)
+      break;
+    const int64_t vo = voff[g], eo = eoff[g];
+    const int rc = gcl_canon_wide_device_async(
+        c, d_rp + vo + g, d_col + eo, d_color ? d_color + vo : nullptr, (int)n, eoff[g + 1] - eo,
+        max_aut, d_dense ? d_dense + ooff[g] : nullptr, d_rows ? d_rows + roff[g] : nullptr,
+        d_label ? d_label + vo : nullptr, d_stats ? d_stats + 2 * g : nullptr, d_status + g);
+    if (rc != GCL_OK) return rc;
+    int32_t st = 0;
+    GCL_TRY(cudaMemcpyAsync(&st, d_status + g, sizeof st, cudaMemcpyDeviceToHost, s));
+    GCL_TRY(cudaStreamSynchronize(s));
+    if (st != kOk) continue;  // keeps the batch's timeout
+    if (out_dense && n)
+      GCL_TRY(cudaMemcpyAsync(out_dense + ooff[g], d_dense + ooff[g], (size_t)(n * n),
+                              cudaMemcpyDeviceToHost, s));
+    if (out_rows && n)
+      GCL_TRY(cudaMemcpyAsync(out_rows + roff[g], d_rows + roff[g],
+                              (size_t)(roff[g + 1] - roff[g]) * sizeof(uint64_t),
+                              cudaMemcpyDeviceToHost, s));
+    if (d_label)
+      GCL_TRY(cudaMemcpyAsync(out_label + vo, d_label + vo, (size_t)n * sizeof(int32_t),
+                              cudaMemcpyDeviceToHost, s));
+    if (d_stats)
+      GCL_TRY(cudaMemcpyAsync(out_stats + 2 * g, d_stats + 2 * g, 2 * sizeof(int64_t),
+                              cudaMemcpyDeviceToHost, s));
+    GCL_TRY(cudaStreamSynchronize(s));
+    out_status[g] = kOk;
+  }
+  return GCL_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1089,11 +1154,17 @@ int gcl_canon_batch(gcl_context* c, int count, const int64_t* voff, const int64_
     GCL_TRY(c->stats.ensure(2 * cnt * sizeof(int64_t)));
     d_stats = (int64_t*)c->stats.p;
   }
+  // with a hand-off budget, graphs above 64 vertices whose batch warp runs
+  // past it are searched again by the wide search below
+  const uint64_t hard_ns = graph_budget_ns();
+  const bool handoff = c->handoff_ns > 0 && max_n > kW64MaxN && (hard_ns == 0 || c->handoff_ns < hard_ns);
+  if (handoff) c->budget_override_ns = c->handoff_ns;
   int rc = gcl_canon_batch_device_async(c, count, (int64_t*)c->voff.p, (int64_t*)c->eoff.p,
                                         (int32_t*)c->rowptr.p, (int32_t*)c->col.p, d_color,
                                         max_aut, max_n, max_m2, d_dense, d_ooff, d_rows, d_roff,
                                         d_label, d_stats,
                                         (int32_t*)c->status.p);
+  c->budget_override_ns = 0;
   if (rc != GCL_OK) return rc;
   if (out_dense && dense_bytes)
     GCL_TRY(cudaMemcpyAsync(out_dense, d_dense, dense_bytes, cudaMemcpyDeviceToHost, s));
@@ -1104,6 +1175,12 @@ int gcl_canon_batch(gcl_context* c, int count, const int64_t* voff, const int64_
     GCL_TRY(cudaMemcpyAsync(out_stats, d_stats, 2 * cnt * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
   GCL_TRY(cudaMemcpyAsync(out_status, c->status.p, cnt * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
   GCL_TRY(cudaStreamSynchronize(s));
+  if (handoff) {
+    const int rh = batch_handoff(c, count, voff, eoff, d_color, max_aut, ooff, roff, out_dense,
+                                 out_rows, out_label, out_stats, out_status, d_dense, d_rows,
+                                 d_label, d_stats, hard_ns);
+    if (rh != GCL_OK) return rh;
+  }
   drain.done = true;
   for (int g = 0; g < count; ++g)
     if (out_status[g] != kOk) return graph_status_to_rc(out_status[g]);

@@ -122,6 +122,14 @@ void* gcl_stream(gcl_context* ctx);
  *   sequential order (on vertex-transitive graphs such as tori one sibling
  *   per level covers the whole cell); 0 starts a level's items together.
  *   Same canonical form either way.
+ * GCL_OPT_BATCH_HANDOFF_MS: t > 0 makes gcl_canon_batch give each graph of
+ *   more than 64 vertices t ms in its batch warp; the graphs still searching
+ *   then are searched again, one at a time, by the wide search (within the
+ *   per-graph budget each and that budget in all).  Their canonical forms are
+ *   the same; their labelings may be other equivalent best leaves and their
+ *   statistics are the wide search's.  For mixed batches where a few graphs
+ *   of large, symmetric or rigid families would hold the batch for minutes
+ *   on one warp.  0 (default) off.
  * GCL_OPT_COUNTERS: 1 makes the wide searches of the context count events
  *   and clock cycles per part of the work (gcl_wide_counters), in a
  *   separately compiled items kernel; 0 (default) runs the kernel without
@@ -137,6 +145,7 @@ void* gcl_stream(gcl_context* ctx);
 #define GCL_OPT_WIDE_SHARE 7
 #define GCL_OPT_COUNTERS 8
 #define GCL_OPT_WIDE_PROBE 9
+#define GCL_OPT_BATCH_HANDOFF_MS 10
 int gcl_set_option(gcl_context* ctx, int option, int64_t value);
 
 /* Counters of the context's last wide search (gcl_canon_one on a graph of

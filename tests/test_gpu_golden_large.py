@@ -100,3 +100,25 @@ def test_relabel_invariance_beyond_the_reference(pkg, G):
     # the rows describe a 4-regular graph (degree of each canonical vertex)
     words = a.reshape(g.n, (g.n + 63) // 64)
     assert (np.bitwise_count(words).sum(axis=1) == 4).all()
+
+
+def test_batch_handoff_to_wide_search(pkg, G, records, built):
+    """GCL_OPT_BATCH_HANDOFF_MS: a graph whose batch warp runs past the
+    hand-off budget (a random 3-regular graph of 1,024 vertices searches
+    about 4 s on one warp) is finished by the wide search, with the
+    reference's canonical form; the small graphs of the batch are untouched."""
+    by = {r["name"]: r for r in records}
+    rec = by["reg3_1024"]
+    small = G.small_batch(40, seed=71)
+    graphs = small[:20] + [built["reg3_1024"]] + small[20:]
+    ctx = pkg.Context(0)
+    plain = pkg.canon_batch(small, ctx=ctx, dense=False, rows=True)
+    ctx.set_option(pkg.api.GCL_OPT_BATCH_HANDOFF_MS, 100)
+    res = pkg.canon_batch(graphs, ctx=ctx, dense=False, rows=True)
+    ctx.close()
+    assert (res.status == 0).all()
+    assert GL.rows_sha256(res.packed(20)) == rec["rows_sha256"]
+    for i in range(40):
+        j = i if i < 20 else i + 1
+        assert np.array_equal(res.packed(j), plain.packed(i))
+        assert np.array_equal(res.stats[j], plain.stats[i])
