@@ -498,6 +498,10 @@ def gpu_arm(args):
 
     e2e_s = e2e_run(False)
     e2e_dense_s = e2e_run(True)
+    # the same call with the batch in two halves on two streams
+    ctx.set_option(api.GCL_OPT_BATCH_SPLIT, 1)
+    e2e_split_s = e2e_run(False)
+    ctx.set_option(api.GCL_OPT_BATCH_SPLIT, 0)
 
     def e2e_overlap(k):
         # k contexts (k streams) on k host threads, each with its own output
@@ -607,7 +611,13 @@ def gpu_arm(args):
             "config": bench_config(args, count, world),
             "e2e": {"value": job_rate(count, world, args.steps, e2e_s), "unit": UNIT,
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-                    "output": "bit-packed canonical rows (n x ceil(n/64) words per graph)"},
+                    "output": "bit-packed canonical rows (n x ceil(n/64) words per graph)",
+                    "call": "gcl_canon_batch, the batch in one piece on the context's stream"},
+            "e2e_split": {"value": job_rate(count, world, args.steps, e2e_split_s),
+                          "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                          "d2h_bytes_per_step": int(d2h),
+                          "call": "gcl_canon_batch with GCL_OPT_BATCH_SPLIT 1 (two halves on two "
+                                  "streams)"},
             "e2e_dense": {"value": job_rate(count, world, args.steps, e2e_dense_s), "unit": UNIT,
                           "h2d_bytes_per_step": int(h2d_dense),
                           "d2h_bytes_per_step": int(d2h_dense),

@@ -55,6 +55,7 @@ GCL_OPT_WIDE_SHARE = 7
 GCL_OPT_COUNTERS = 8
 GCL_OPT_WIDE_PROBE = 9
 GCL_OPT_BATCH_HANDOFF_MS = 10
+GCL_OPT_BATCH_SPLIT = 11
 
 # gcl_wide_counters, in index order (include/gcl.h)
 WIDE_COUNTERS = ("items", "items_pruned", "gifts_taken", "gifts_given", "nodes", "leaves",

@@ -93,7 +93,6 @@ struct __align__(16) W64Smem {
   // live in the slot workspace
   uint8_t aut_head[kW64AutHead][kW64MaxN];
   uint64_t fix_head[kW64AutHead];
-  uint64_t cls[kW64MaxN];  // orbit computation: previous orbit -> member mask
 };
 
 // One W64Smem per warp of the block, at namespace scope so every phase
@@ -161,6 +160,11 @@ static __device__ __noinline__ W64Refined w64_refine(int n, uint64_t starts, uin
   uint64_t sing = S.sing;
   uint32_t lc = popc64(starts), hint = 0, iters = 0;
   int ok = 1;
+  // registers: the member masks of the cells starting at positions lane and
+  // lane + 32 (valid where `starts` has the bit), and the cells of vertices
+  // lane and lane + 32
+  uint64_t cmr0 = S.cmask[v0], cmr1 = S.cmask[v1];
+  uint32_t csr0 = ok0 ? S.cs[v0] : 0u, csr1 = ok1 ? S.cs[v1] : 0u;
   while (starts != full && active) {
     if (++iters > 64u * 64u + 64u) {  // every step removes an active cell or splits one
       ok = 0;
@@ -185,57 +189,90 @@ static __device__ __noinline__ W64Refined w64_refine(int n, uint64_t starts, uin
       const uint64_t N = S.adj[S.pv[s]];
       const uint64_t X = N & ~sing;
       if (!X) continue;
-      // lane i looks at the cells of the i-th and (i+32)-th such
-      // neighbours: a cell splits when it is not all neighbours
-      uint64_t splitc;
-      {
-        const uint32_t xl = (uint32_t)X, xh = (uint32_t)(X >> 32);
-        const uint32_t nl = (uint32_t)__popc(xl), nx = nl + (uint32_t)__popc(xh);
-        uint64_t mine = 0;
-        for (uint32_t i = lane; i < nx; i += 32) {
-          const uint32_t v = i < nl ? (uint32_t)__fns(xl, 0, (int)i + 1)
-                                    : 32u + (uint32_t)__fns(xh, 0, (int)(i - nl) + 1);
-          const uint32_t c = S.cs[v];
-          if (S.cmask[c] & ~N) mine |= bit64(c);
-        }
-        splitc = warp_or64(mine);
-      }
-      // split cells in position order: hash, active set, in_level (:296-465)
-      while (splitc) {
-        const uint32_t c = ctz64(splitc);
-        splitc &= splitc - 1;
-        const uint64_t C = S.cmask[c], CN = C & N, CR = C & ~N;
+      // a cell splits when N meets it partially: the lanes test the cells
+      // starting at their two positions
+      const bool sp0 = ((starts >> v0) & 1ull) && (cmr0 & N) && (cmr0 & ~N);
+      const bool sp1 = ((starts >> v1) & 1ull) && (cmr1 & N) && (cmr1 & ~N);
+      const uint64_t splitc = ballot2(sp0, sp1);
+      if (!splitc) continue;
+      // The split cells, each by the lane owning its start (:296-465): the
+      // neighbours keep the start c, the rest start at p = c + |C & N|.
+      // Cells are disjoint ranges, and whether c was active does not depend
+      // on the cells before it, so they split independently; only the hash
+      // and the hint follow position order (below).
+      uint64_t addA = 0, addS = 0, addG = 0;  // active, starts, singleton additions
+      uint32_t hv0 = 0xffu, hv1 = 0xffu, nbp = 0;
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        if (!(k ? sp1 : sp0)) continue;
+        const uint32_t c = k ? v1 : v0;
+        const uint64_t C = k ? cmr1 : cmr0, CN = C & N, CR = C & ~N;
         const uint32_t nb = popc64(CN), nn = popc64(CR), p = c + nb;
-        const uint32_t old = S.inlev[c];
-        lc = mash(lc, p - 1);  // cell.first + neighbors_size - 1
+        uint32_t hv = 0xffu;
         if (((active >> c) & 1ull) || nb >= nn) {
-          active |= bit64(p);
-          if (nn == 1) hint = p;
+          addA |= bit64(p);
+          if (nn == 1) hv = p;
         } else {
-          active |= bit64(c);
-          if (nb == 1) hint = c;
+          addA |= bit64(c);
+          if (nb == 1) hv = c;
         }
-        starts |= bit64(p);
-        if (nb == 1) sing |= CN;
-        if (nn == 1) sing |= CR;
-        __syncwarp();
-        if (lane == 0) {
-          S.cmask[c] = CN;
-          S.cmask[p] = CR;
-          S.inlev[c] = (uint8_t)lvl1;
-          S.inlev[p] = (uint8_t)old;
-          if (nb == 1) S.pv[c] = (uint8_t)ctz64(CN);
-          if (nn == 1) S.pv[p] = (uint8_t)ctz64(CR);
+        addS |= bit64(p);
+        if (nb == 1) addG |= CN;
+        if (nn == 1) addG |= CR;
+        S.cmask[c] = CN;
+        S.cmask[p] = CR;
+        S.inlev[p] = S.inlev[c];
+        S.inlev[c] = (uint8_t)lvl1;
+        if (nb == 1) S.pv[c] = (uint8_t)ctz64(CN);
+        if (nn == 1) S.pv[p] = (uint8_t)ctz64(CR);
+        if (k) {
+          cmr1 = CN;
+          hv1 = hv;
+          nbp |= nb << 8;
+        } else {
+          cmr0 = CN;
+          hv0 = hv;
+          nbp |= nb;
         }
-        if ((CR >> v0) & 1ull) S.cs[v0] = (uint8_t)p;
-        if ((CR >> v1) & 1ull) S.cs[v1] = (uint8_t)p;
-        __syncwarp();
       }
+      // hash: cell.first + neighbors_size - 1 per split cell, in position order
+      for (uint64_t t = splitc; t; t &= t - 1) {
+        const uint32_t c = ctz64(t);
+        const uint32_t w = __shfl_sync(GCL_FULL, nbp, (int)(c & 31u));
+        lc = mash(lc, c + ((c >= 32u ? w >> 8 : w) & 0xffu) - 1u);
+      }
+      // hint: the last split cell in position order that sets one
+      const uint64_t hc = ballot2(hv0 != 0xffu, hv1 != 0xffu);
+      if (hc) {
+        const uint32_t cl = msb64(hc);
+        hint = __shfl_sync(GCL_FULL, cl >= 32u ? hv1 : hv0, (int)(cl & 31u));
+      }
+      active |= warp_or64(addA);
+      const uint64_t NSt = warp_or64(addS);
+      starts |= NSt;
+      sing |= warp_or64(addG);
+      // vertices of split cells outside N move to the second fragment
+      {
+        const uint32_t w0 = __shfl_sync(GCL_FULL, nbp, (int)(csr0 & 31u));
+        const uint32_t w1 = __shfl_sync(GCL_FULL, nbp, (int)(csr1 & 31u));
+        if (ok0 && ((splitc >> csr0) & 1ull) && !((N >> v0) & 1ull)) {
+          csr0 += (csr0 >= 32u ? w0 >> 8 : w0) & 0xffu;
+          S.cs[v0] = (uint8_t)csr0;
+        }
+        if (ok1 && ((splitc >> csr1) & 1ull) && !((N >> v1) & 1ull)) {
+          csr1 += (csr1 >= 32u ? w1 >> 8 : w1) & 0xffu;
+          S.cs[v1] = (uint8_t)csr1;
+        }
+      }
+      __syncwarp();
+      // the new fragments' member masks, written by their cells' owners
+      if ((NSt >> v0) & 1ull) cmr0 = S.cmask[v0];
+      if ((NSt >> v1) & 1ull) cmr1 = S.cmask[v1];
     } else {
       // Non-singleton splitter: fragments in ascending neighbour count.
       lc = mash(lc, e - s);
       const uint64_t spl = S.cmask[s];
-      uint32_t cs0 = ok0 ? S.cs[v0] : 0u, cs1 = ok1 ? S.cs[v1] : 0u;
+      uint32_t cs0 = csr0, cs1 = csr1;
       uint64_t cm0 = ok0 ? S.cmask[cs0] : 0ull, cm1 = ok1 ? S.cmask[cs1] : 0ull;
       const uint32_t k0 = ok0 ? popc64(adj0 & spl) : 0u, k1 = ok1 ? popc64(adj1 & spl) : 0u;
       const uint32_t mx = __reduce_max_sync(GCL_FULL, max(k0, k1));
@@ -347,6 +384,10 @@ static __device__ __noinline__ W64Refined w64_refine(int n, uint64_t starts, uin
         starts = all;
       }
       __syncwarp();
+      csr0 = cs0;
+      csr1 = cs1;
+      cmr0 = S.cmask[v0];
+      cmr1 = S.cmask[v1];
     }
   }
   __syncwarp();
@@ -645,68 +686,65 @@ static __device__ __noinline__ bool w64_orbits(int n, int idx, int num_aut, uint
   const bool ok0 = v0 < (uint32_t)n, ok1 = v1 < (uint32_t)n;
   uint32_t L0 = ok0 && ((mem >> v0) & 1ull) && rv ? (uint32_t)rp[v0] : v0;
   uint32_t L1 = ok1 && ((mem >> v1) & 1ull) && rv ? (uint32_t)rp[v1] : v1;
-  // previous orbits as cycles: next larger member, wrapping to the least
-  __syncwarp();
-  S.cls[v0] = 0;
-  S.cls[v1] = 0;
-  __syncwarp();
-  if (ok0) atomicOr((unsigned long long*)&S.cls[L0], (unsigned long long)bit64(v0));
-  if (ok1) atomicOr((unsigned long long*)&S.cls[L1], (unsigned long long)bit64(v1));
-  __syncwarp();
-  uint32_t sg0 = v0, sg1 = v1;
-  if (ok0) {
-    const uint64_t c = S.cls[L0], up = c & ge_mask(v0 + 1);
-    sg0 = ctz64(up ? up : c);
-  }
-  if (ok1) {
-    const uint64_t c = S.cls[L1], up = c & ge_mask(v1 + 1);
-    sg1 = ctz64(up ? up : c);
-  }
-  uint32_t* lab = S.dsu;
-  lab[v0] = L0;
-  lab[v1] = L1;
-  for (int round = 0;; ++round) {
-    if (round > 2 * kW64MaxN) return false;
-    __syncwarp();
-    L0 = lab[v0];
-    L1 = lab[v1];
-    uint32_t n0 = min(L0, lab[sg0]), n1 = min(L1, lab[sg1]);
-#pragma unroll
-    for (int k = 0; k < kW64AutHead; ++k) {
-      if (!((selh >> k) & 1u)) continue;
-      if (ok0) n0 = min(n0, lab[S.aut_head[k][v0]]);
-      if (ok1) n1 = min(n1, lab[S.aut_head[k][v1]]);
+  // The orbits are the components of the graph whose edges join every
+  // vertex v to its previous orbit's label L(v) and to its image under each
+  // selected automorphism; a component is labelled by its least vertex.
+  // Union-find with parent(v) = L(v) to start (L(v) <= v): lane l holds the
+  // parents of vertices l and l + 32 packed in one word, so a lookup is one
+  // shuffle; a hook (larger root under the smaller) is an atomicMin in
+  // shared memory.  Parents never exceed their vertex, so every root is the
+  // least vertex of its tree.
+  uint32_t fp = (L0 & 0xffu) | ((L1 & 0xffu) << 8);
+  uint32_t* par = S.dsu;
+  // parent := grandparent until every vertex points at a root (a tree of
+  // depth d needs ceil(log2 d) passes)
+  auto compress = [&]() -> bool {
+    for (int it = 0; it < 10; ++it) {
+      const uint32_t f0 = fp & 0xffu, f1 = (fp >> 8) & 0xffu;
+      const uint32_t g0 = __shfl_sync(GCL_FULL, fp, (int)(f0 & 31u));
+      const uint32_t g1 = __shfl_sync(GCL_FULL, fp, (int)(f1 & 31u));
+      const uint32_t h0 = (f0 >= 32u ? g0 >> 8 : g0) & 0xffu;
+      const uint32_t h1 = (f1 >= 32u ? g1 >> 8 : g1) & 0xffu;
+      const bool c = h0 != f0 || h1 != f1;
+      fp = h0 | (h1 << 8);
+      if (!__any_sync(GCL_FULL, c)) return true;
     }
-    if (seltail)
-      for (int i = max(from, kW64AutHead); i < limit; ++i) {
-        const uint64_t fm = fixes[i];
-        if ((seqm & ~fm) || !(mem & ~fm)) continue;
-        const uint8_t* pm = auts + (uint64_t)i * 64u;
-        if (ok0) n0 = min(n0, lab[pm[v0]]);
-        if (ok1) n1 = min(n1, lab[pm[v1]]);
-      }
-    const bool changed = n0 < L0 || n1 < L1;
-    __syncwarp();
-    if (n0 < L0) {  // hook the old parent, then the vertex, under the smaller label
-      atomicMin(&lab[L0], n0);
-      atomicMin(&lab[v0], n0);
-    }
-    if (n1 < L1) {
-      atomicMin(&lab[L1], n1);
-      atomicMin(&lab[v1], n1);
-    }
-    for (int j = 0; j < 2; ++j) {  // shortcut: parent := grandparent
+    return false;
+  };
+  // the edges v -- pi(v) of one automorphism
+  auto apply = [&](const uint8_t* img) -> bool {
+    const uint32_t u0 = ok0 ? (uint32_t)img[v0] : v0, u1 = ok1 ? (uint32_t)img[v1] : v1;
+    for (int round = 0; round <= kW64MaxN; ++round) {  // a hook round removes a root
+      const uint32_t x0 = __shfl_sync(GCL_FULL, fp, (int)(u0 & 31u));
+      const uint32_t x1 = __shfl_sync(GCL_FULL, fp, (int)(u1 & 31u));
+      const uint32_t ra0 = fp & 0xffu, rb0 = (u0 >= 32u ? x0 >> 8 : x0) & 0xffu;
+      const uint32_t ra1 = (fp >> 8) & 0xffu, rb1 = (u1 >= 32u ? x1 >> 8 : x1) & 0xffu;
+      const bool d0 = ra0 != rb0, d1 = ra1 != rb1;
+      if (!__any_sync(GCL_FULL, d0 || d1)) return true;
+      par[v0] = ra0;
+      par[v1] = ra1;
       __syncwarp();
-      const uint32_t g0 = lab[lab[v0]], g1 = lab[lab[v1]];
+      if (d0) atomicMin(&par[max(ra0, rb0)], min(ra0, rb0));
+      if (d1) atomicMin(&par[max(ra1, rb1)], min(ra1, rb1));
       __syncwarp();
-      atomicMin(&lab[v0], g0);
-      atomicMin(&lab[v1], g1);
+      fp = par[v0] | (par[v1] << 8);
+      __syncwarp();  // read before the next round's stores
+      if (!compress()) return false;
     }
-    if (!__any_sync(GCL_FULL, changed)) break;
-  }
-  __syncwarp();
-  L0 = lab[v0];
-  L1 = lab[v1];
+    return false;
+  };
+  if (!compress()) return false;
+#pragma unroll 1
+  for (uint32_t k = 0; k < (uint32_t)kW64AutHead; ++k)
+    if (((selh >> k) & 1u) && !apply(S.aut_head[k])) return false;
+  if (seltail)
+    for (int i = max(from, kW64AutHead); i < limit; ++i) {
+      const uint64_t fm = fixes[i];
+      if ((seqm & ~fm) || !(mem & ~fm)) continue;
+      if (!apply(auts + (uint64_t)i * 64u)) return false;
+    }
+  L0 = fp & 0xffu;
+  L1 = (fp >> 8) & 0xffu;
   bool r0 = false, r1 = false;
   if (ok0 && ((mem >> v0) & 1ull)) {
     rp[v0] = (uint8_t)L0;

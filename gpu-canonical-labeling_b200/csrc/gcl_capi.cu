@@ -376,6 +376,9 @@ struct gcl_context {
   uint32_t wide_pool = kWidePool;  // wide search: per-level orbit arrays of a warp
   bool wide_probe = true;          // wide search: a level's first item runs before the rest
   uint64_t handoff_ns = 0;         // gcl_canon_batch: batch-warp budget before the wide search
+  bool batch_split = false;        // gcl_canon_batch: large small-graph batches in two halves
+  gcl_context* peer = nullptr;     // the second half's context (own stream and workspace)
+  cudaEvent_t split_ev = nullptr;  // orders the companion stream after this one
   uint64_t budget_override_ns = 0; // per-graph budget of the next batched launch (0 = default)
   // mapped host buffers (gcl_host_alloc): host address, size, device address
   struct Mapped {
@@ -523,6 +526,10 @@ int gcl_destroy(gcl_context* c) {
   if (!c) return GCL_ERR_ARG;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->peer) gcl_destroy(c->peer);
+  c->peer = nullptr;
+  cudaSetDevice(c->device);
+  if (c->split_ev) cudaEventDestroy(c->split_ev);
   for (auto& row : c->tev)
     for (cudaEvent_t& ev : row)
       if (ev) cudaEventDestroy(ev);
@@ -774,6 +781,10 @@ int gcl_set_option(gcl_context* c, int option, int64_t value) {
       if (value < 0) return GCL_ERR_ARG;
       c->handoff_ns = (uint64_t)value * 1000000ull;
       return GCL_OK;
+    case GCL_OPT_BATCH_SPLIT:
+      if (value != 0 && value != 1) return GCL_ERR_ARG;
+      c->batch_split = value != 0;
+      return GCL_OK;
     case GCL_OPT_STREAM_PRIORITY: {
       if (value != 0 && value != 1) return GCL_ERR_ARG;
       int lo = 0, hi = 0;
@@ -786,6 +797,7 @@ int gcl_set_option(gcl_context* c, int option, int64_t value) {
       cudaStreamDestroy(c->stream);
       c->stream = s2;
       c->each_buf([&](DevBuf& b) { b.stream = s2; });
+      if (c->peer) return gcl_set_option(c->peer, GCL_OPT_STREAM_PRIORITY, value);
       return GCL_OK;
     }
     default:
@@ -1086,6 +1098,133 @@ int batch_handoff(gcl_context* c, int count, const int64_t* voff, const int64_t*
 
 extern "C" {
 
+// Batches of at least this many graphs of up to 64 vertices run as two
+// halves on two streams (GCL_OPT_BATCH_SPLIT).
+constexpr int kSplitMinGraphs = 4096;
+
+// gcl_canon_batch in two halves: graphs [0, h) on the context's stream,
+// [h, count) on the companion context's.  The offsets of the arena are
+// absolute, so each half is the same arrays seen from its first graph: the
+// uploads, the kernels and the downloads of a half touch its own ranges only.
+// Returns GCL_OK or an error code; the caller maps per-graph statuses.
+static int canon_batch_halves(gcl_context* c, const BatchShape& B, int count,
+                              const int64_t* voff, const int64_t* eoff, const int32_t* rowptr,
+                              const int32_t* col, const int32_t* color, int max_aut,
+                              uint8_t* out_dense, const int64_t* ooff, uint64_t* out_rows,
+                              const int64_t* roff, int32_t* out_label, int64_t* out_stats,
+                              int32_t* out_status) {
+  if (!c->peer) {
+    gcl_context* q = nullptr;
+    const int rc = gcl_create(c->device, &q);
+    if (rc != GCL_OK) return rc;
+    c->peer = q;
+    GCL_TRY(cudaSetDevice(c->device));
+    // the same stream priority as the context's (GCL_OPT_STREAM_PRIORITY)
+    int pr = 0, lo = 0, hi = 0;
+    if (cudaStreamGetPriority(c->stream, &pr) == cudaSuccess &&
+        cudaDeviceGetStreamPriorityRange(&lo, &hi) == cudaSuccess && lo != hi && pr == hi) {
+      const int rp = gcl_set_option(q, GCL_OPT_STREAM_PRIORITY, 1);
+      if (rp != GCL_OK) return rp;
+    }
+    (void)cudaGetLastError();
+  }
+  gcl_context* q = c->peer;
+  q->tune_w64_bps = c->tune_w64_bps;
+  q->workspace_bytes = c->workspace_bytes;
+  if (!c->split_ev) GCL_TRY(cudaEventCreateWithFlags(&c->split_ev, cudaEventDisableTiming));
+  const size_t cnt = (size_t)count;
+  GCL_TRY(c->voff.ensure((cnt + 1) * sizeof(int64_t)));
+  GCL_TRY(c->eoff.ensure((cnt + 1) * sizeof(int64_t)));
+  GCL_TRY(c->rowptr.ensure(B.nrp * sizeof(int32_t)));
+  GCL_TRY(c->col.ensure(std::max<size_t>(B.ne, 1) * sizeof(int32_t)));
+  GCL_TRY(c->status.ensure(cnt * sizeof(int32_t)));
+  if (color && B.nv) GCL_TRY(c->color.ensure(B.nv * sizeof(int32_t)));
+  if (out_dense) {
+    GCL_TRY(c->ooff.ensure((cnt + 1) * sizeof(int64_t)));
+    GCL_TRY(c->dense.ensure(std::max<size_t>(B.dense_bytes, 1)));
+  }
+  if (out_rows) {
+    GCL_TRY(c->roff.ensure((cnt + 1) * sizeof(int64_t)));
+    GCL_TRY(c->rows.ensure(std::max<size_t>(B.rows_words, 1) * sizeof(uint64_t)));
+  }
+  if (out_label && B.nv) GCL_TRY(c->label.ensure(B.nv * sizeof(int32_t)));
+  if (out_stats) GCL_TRY(c->stats.ensure(2 * cnt * sizeof(int64_t)));
+  int64_t* d_voff = (int64_t*)c->voff.p;
+  int64_t* d_eoff = (int64_t*)c->eoff.p;
+  int32_t* d_rowptr = (int32_t*)c->rowptr.p;
+  int32_t* d_col = (int32_t*)c->col.p;
+  int32_t* d_color = color && B.nv ? (int32_t*)c->color.p : nullptr;
+  int64_t* d_ooff = out_dense ? (int64_t*)c->ooff.p : nullptr;
+  uint8_t* d_dense = out_dense ? (uint8_t*)c->dense.p : nullptr;
+  int64_t* d_roff = out_rows ? (int64_t*)c->roff.p : nullptr;
+  uint64_t* d_rows = out_rows ? (uint64_t*)c->rows.p : nullptr;
+  int32_t* d_label = out_label && B.nv ? (int32_t*)c->label.p : nullptr;
+  int64_t* d_stats = out_stats ? (int64_t*)c->stats.p : nullptr;
+  int32_t* d_status = (int32_t*)c->status.p;
+  cudaStream_t s0 = c->stream, s1 = q->stream;
+  DrainOnExit drain0(s0), drain1(s1);
+  // the buffers were (re)allocated in the context's stream order: the
+  // companion stream starts after that
+  GCL_TRY(cudaEventRecord(c->split_ev, s0));
+  GCL_TRY(cudaStreamWaitEvent(s1, c->split_ev, 0));
+  auto h2d = [](void* dst, const void* src, size_t bytes, cudaStream_t s) {
+    return bytes ? cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s) : cudaSuccess;
+  };
+  auto d2h = [](void* dst, const void* src, size_t bytes, cudaStream_t s) {
+    return bytes ? cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s) : cudaSuccess;
+  };
+  // graphs [g0, g1): their offsets, CSR rows (n + 1 entries per graph from
+  // voff[g] + g), neighbours, colours and output offsets
+  auto upload = [&](int g0, int g1, cudaStream_t s) -> cudaError_t {
+    const size_t k = (size_t)(g1 - g0) + 1;
+    const size_t r0 = (size_t)(voff[g0] + g0), r1 = (size_t)(voff[g1] + g1);
+    cudaError_t e = h2d(d_voff + g0, voff + g0, k * sizeof(int64_t), s);
+    if (e == cudaSuccess) e = h2d(d_eoff + g0, eoff + g0, k * sizeof(int64_t), s);
+    if (e == cudaSuccess) e = h2d(d_rowptr + r0, rowptr + r0, (r1 - r0) * sizeof(int32_t), s);
+    if (e == cudaSuccess)
+      e = h2d(d_col + eoff[g0], col + eoff[g0], (size_t)(eoff[g1] - eoff[g0]) * sizeof(int32_t), s);
+    if (e == cudaSuccess && d_color)
+      e = h2d(d_color + voff[g0], color + voff[g0], (size_t)(voff[g1] - voff[g0]) * sizeof(int32_t), s);
+    if (e == cudaSuccess && d_ooff) e = h2d(d_ooff + g0, ooff + g0, k * sizeof(int64_t), s);
+    if (e == cudaSuccess && d_roff) e = h2d(d_roff + g0, roff + g0, k * sizeof(int64_t), s);
+    return e;
+  };
+  auto download = [&](int g0, int g1, cudaStream_t s) -> cudaError_t {
+    cudaError_t e = cudaSuccess;
+    if (d_dense)
+      e = d2h(out_dense + ooff[g0], d_dense + ooff[g0], (size_t)(ooff[g1] - ooff[g0]), s);
+    if (e == cudaSuccess && d_rows)
+      e = d2h(out_rows + roff[g0], d_rows + roff[g0], (size_t)(roff[g1] - roff[g0]) * sizeof(uint64_t), s);
+    if (e == cudaSuccess && d_label)
+      e = d2h(out_label + voff[g0], d_label + voff[g0], (size_t)(voff[g1] - voff[g0]) * sizeof(int32_t), s);
+    if (e == cudaSuccess && d_stats)
+      e = d2h(out_stats + 2 * (size_t)g0, d_stats + 2 * (size_t)g0, 2 * (size_t)(g1 - g0) * sizeof(int64_t), s);
+    if (e == cudaSuccess)
+      e = d2h(out_status + g0, d_status + g0, (size_t)(g1 - g0) * sizeof(int32_t), s);
+    return e;
+  };
+  const int h = count / 2;
+  GCL_TRY(upload(0, h, s0));
+  int rc = gcl_canon_batch_device_async(c, h, d_voff, d_eoff, d_rowptr, d_col, d_color, max_aut,
+                                        B.max_n, B.max_m2, d_dense, d_ooff, d_rows, d_roff, d_label,
+                                        d_stats, d_status);
+  if (rc != GCL_OK) return rc;
+  GCL_TRY(upload(h, count, s1));
+  rc = gcl_canon_batch_device_async(q, count - h, d_voff + h, d_eoff + h, d_rowptr + h, d_col,
+                                    d_color, max_aut, B.max_n, B.max_m2, d_dense,
+                                    d_ooff ? d_ooff + h : nullptr, d_rows,
+                                    d_roff ? d_roff + h : nullptr, d_label,
+                                    d_stats ? d_stats + 2 * (size_t)h : nullptr, d_status + h);
+  GCL_TRY(cudaSetDevice(c->device));
+  if (rc != GCL_OK) return rc;
+  GCL_TRY(download(0, h, s0));
+  GCL_TRY(download(h, count, s1));
+  GCL_TRY(cudaStreamSynchronize(s0));
+  GCL_TRY(cudaStreamSynchronize(s1));
+  drain0.done = drain1.done = true;
+  return GCL_OK;
+}
+
 int gcl_canon_batch(gcl_context* c, int count, const int64_t* voff, const int64_t* eoff,
                     const int32_t* rowptr, const int32_t* col, const int32_t* color, int max_aut,
                     uint8_t* out_dense, const int64_t* ooff, uint64_t* out_rows,
@@ -1102,6 +1241,15 @@ int gcl_canon_batch(gcl_context* c, int count, const int64_t* voff, const int64_
   const int max_n = B.max_n;
   const int64_t max_m2 = B.max_m2;
   GCL_TRY(cudaSetDevice(c->device));
+  if (c->batch_split && count >= kSplitMinGraphs && max_n <= kW64MaxN && !c->timing) {
+    const int rs = canon_batch_halves(c, B, count, voff, eoff, rowptr, col, color, max_aut,
+                                      out_dense, ooff, out_rows, roff, out_label, out_stats,
+                                      out_status);
+    if (rs != GCL_OK) return rs;
+    for (int g = 0; g < count; ++g)
+      if (out_status[g] != kOk) return graph_status_to_rc(out_status[g]);
+    return GCL_OK;
+  }
   const size_t nv = B.nv, ne = B.ne;
   const size_t cnt = (size_t)count;  // byte counts in size_t, not int
   const size_t nrp = B.nrp;
