@@ -1148,13 +1148,15 @@ __device__ __forceinline__ uint64_t w64_deadline(const BatchArgs& A) {
   return __shfl_sync(GCL_FULL, lane_id() == 0 ? global_ns() : 0ull, 0) + A.budget_ns;
 }
 
-// The partition after the root refinement, kept in device memory between
-// the root pass and the search pass of a batch: a header (starts, singleton
+// The partition after the root refinement, handed from the warp that refined
+// the root to the warp that searches below it: a header (starts, singleton
 // vertices, code, graph id), then per vertex or position the adjacency mask, the cell
 // member mask (at cell starts), the cell start, in_level and the singleton
-// cell's vertex -- what the search reads of the root node.
+// cell's vertex -- what the search reads of the root node.  Slots are whole
+// 128-byte lines apart, so a warp never holds a line of a neighbouring slot
+// in its L1 from before that slot was written.
 __host__ __device__ constexpr uint64_t w64_root_slot_bytes() {
-  return 32u + (uint64_t)kW64MaxN * (8u + 8u + 3u);
+  return (32u + (uint64_t)kW64MaxN * (8u + 8u + 3u) + 127u) & ~127ull;
 }
 
 static __device__ __noinline__ void w64_save_root(uint8_t* dst, int g, int n, uint64_t starts,
@@ -1186,9 +1188,11 @@ __device__ __forceinline__ int w64_root_graph(const uint8_t* src) {
 
 // Search-cost class of a graph from its root partition: log2 of n times the
 // vertices beyond one per cell (on the batched small-graph workload this
-// estimate correlates 0.92 with nodes x n); the search pass takes the
-// classes from the most expensive down, so long searches start first.
+// estimate correlates 0.92 with nodes x n).  Graphs of class kW64InlineClass
+// and above are searched at once by the warp that refined their root, so the
+// longest searches of a batch start first.
 constexpr int kW64CostClasses = 16;
+constexpr int kW64InlineClass = 9;
 __device__ __forceinline__ int w64_cost_class(int n, uint64_t starts) {
   const uint32_t est = (uint32_t)n * (uint32_t)(n - popc64(starts)) + 1u;
   return min(kW64CostClasses - 1, 31 - __clz((int)est));

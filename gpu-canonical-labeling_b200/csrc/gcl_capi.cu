@@ -54,9 +54,10 @@ struct Deferred {
   int next_sp_fail2;
   int large_count[kSpBuckets];  // n > 64 graphs per size bucket
   int next_large[kSpBuckets];
-  int search_count;    // n <= 64 graphs whose root partition is not discrete
-  int next_search;
-  int cost_count[kW64CostClasses];  // ... per search-cost class
+  int search_count;    // root slots handed to the search queue
+  int next_search;     // tickets of the search queue
+  int roots_done;      // graphs whose root step is over
+  int queue_error;     // a wait of the search queue ran out
 };
 
 // Largest graphs first: a counting sort of the graph ids by descending n
@@ -180,19 +181,48 @@ __global__ void __launch_bounds__(kW64Threads, 8)
   }
 }
 
-// The batch's graphs of up to 64 vertices in two passes.  The root pass
-// loads each graph and refines its root partition -- the largest share of
-// the work on small sparse graphs -- and finishes the graphs whose root
-// partition is discrete (their canonical form is the root's); the others
-// leave the root's partition in a slot of `roots` and the slot's index in
-// the list of their search-cost class (`search_list`, count entries per
-// class).  The search pass runs their trees, the most expensive class
-// first.  Each pass keeps the warps of an SM in the same few functions, and
-// only the graphs that search take part in the second.  Results equal
-// w64_batch_kernel's.
+// A searched graph's results: status, counters, a ring that outgrew the
+// first pass's store goes to the full-ring rerun, and the outputs.
+__device__ __forceinline__ void w64_finish_search(const BatchArgs& A, Deferred* D,
+                                                  int* overflow_list, int g, int n, int64_t vo,
+                                                  const W64Result& r) {
+  if (lane_id() == 0) {
+    A.status[g] = r.status;
+    if (A.out_stats) {
+      A.out_stats[2 * (int64_t)g] = r.num_aut;
+      A.out_stats[2 * (int64_t)g + 1] = r.nodes;
+    }
+    if (r.status == kAutOverflow) overflow_list[atomicAdd(&D->overflow_count, 1)] = g;
+  }
+  if (r.status == kOk) w64_write_outputs(A, g, n, vo);
+  __syncwarp();
+}
+
+// Bounded waits of the search queue (iterations of a sleep of at most 1 us):
+// every wait is for a root refinement that a running warp has claimed and
+// finishes without waiting itself.
+constexpr int kW64QueueWait = 1 << 22;
+
+// The batch's graphs of up to 64 vertices in one pipelined launch.
+//
+// Roots: every warp takes graphs in the order given (largest first), loads
+// each and refines its root partition -- the largest share of the work on
+// small sparse graphs.  A graph whose root partition is discrete is finished
+// there (its canonical form is the root's).  A graph of search-cost class
+// kW64InlineClass or more is searched at once by the same warp, so the
+// longest searches of the batch start in its first microseconds; any other
+// graph leaves its root partition in a slot of `roots` and flags it ready.
+// Searches: a warp that finds no root left takes a ticket, waits until the
+// ticket's slot is flagged (or every root is done and the ticket is past the
+// last slot) and searches below it.  A warp never waits on a search, only on
+// a root refinement a running warp has claimed, so the launch needs no
+// co-residency.  Results equal w64_batch_kernel's.
 __global__ void __launch_bounds__(kW64Threads, 8)
-    w64_root_kernel(BatchArgs A, Deferred* D, int* large_list, uint8_t* roots, int* search_list) {
+    w64_pipe_kernel(BatchArgs A, Deferred* D, int* large_list, int* overflow_list,
+                    uint8_t* roots, int* ready) {
+  const int warp = (int)(threadIdx.x >> 5);
   const uint32_t lane = lane_id();
+  uint8_t* slot = A.work + ((uint64_t)blockIdx.x * kW64Warps + (uint64_t)warp) * A.slot_bytes;
   while (true) {
     int i = 0;
     if (lane == 0) i = atomicAdd(&D->next, 1);
@@ -206,6 +236,8 @@ __global__ void __launch_bounds__(kW64Threads, 8)
         A.status[g] = kTooLarge;
         const int bk = sp_bucket(n);
         large_list[(int64_t)bk * A.count + atomicAdd(&D->large_count[bk], 1)] = g;
+        __threadfence();
+        atomicAdd(&D->roots_done, 1);
       }
       continue;
     }
@@ -216,79 +248,92 @@ __global__ void __launch_bounds__(kW64Threads, 8)
       root = w64_root(A, n, vo, eo, A.eoff[g + 1] - eo, A.rowptr + vo + g);
       search = root.status == kOk && root.starts != low_mask((uint32_t)n);
     }
+    if (search && w64_cost_class(n, root.starts) >= kW64InlineClass) {
+      if (lane == 0) {
+        __threadfence();
+        atomicAdd(&D->roots_done, 1);
+      }
+      const W64Result r = w64_search_tree(A, n, root.starts, root.code, slot, w64_deadline(A));
+      w64_finish_search(A, D, overflow_list, g, n, vo, r);
+      continue;
+    }
     if (search) {
       int j = 0;
       if (lane == 0) j = atomicAdd(&D->search_count, 1);
       j = __shfl_sync(GCL_FULL, j, 0);
       w64_save_root(roots + (uint64_t)j * w64_root_slot_bytes(), g, n, root.starts, root.code);
+      if (lane == 0) A.status[g] = kInternal;  // until its search ends
+      __threadfence();
       __syncwarp();
-      if (lane == 0) {
-        const int k = w64_cost_class(n, root.starts);
-        search_list[(int64_t)k * A.count + atomicAdd(&D->cost_count[k], 1)] = j;
+      if (lane == 0) atomicExch(&ready[j], 1);
+    } else {
+      // finished at the root: the discrete root is the first and best leaf
+      // (first_terminal, sequential.cpp:259-303), one node, no automorphism
+      if (root.status == kOk && n > 0) {
+        W64Smem& S = w64_smem();
+        const Rows2 R = w64_leaf_rows(n);
+        w64_store_leaf(n, R, S.best_cert, S.bpos);
       }
-      continue;
-    }
-    // finished at the root: the discrete root is the first and best leaf
-    // (first_terminal, sequential.cpp:259-303), one node, no automorphism
-    if (root.status == kOk && n > 0) {
-      W64Smem& S = w64_smem();
-      const Rows2 R = w64_leaf_rows(n);
-      w64_store_leaf(n, R, S.best_cert, S.bpos);
+      if (lane == 0) {
+        A.status[g] = root.status;
+        if (A.out_stats) {
+          A.out_stats[2 * (int64_t)g] = 0;
+          A.out_stats[2 * (int64_t)g + 1] = 1;
+        }
+      }
+      if (root.status == kOk) w64_write_outputs(A, g, n, vo);
+      __syncwarp();
     }
     if (lane == 0) {
-      A.status[g] = root.status;
-      if (A.out_stats) {
-        A.out_stats[2 * (int64_t)g] = 0;
-        A.out_stats[2 * (int64_t)g + 1] = 1;
+      __threadfence();
+      atomicAdd(&D->roots_done, 1);
+    }
+  }
+  while (true) {
+    int t = 0;
+    if (lane == 0) t = atomicAdd(&D->next_search, 1);
+    t = __shfl_sync(GCL_FULL, t, 0);
+    int ok = 0;
+    if (lane == 0) {
+      uint32_t nap = 32;
+      int it = 0;
+      for (; it < kW64QueueWait; ++it) {
+        if (*(volatile int*)&D->search_count > t) {
+          ok = 1;
+          break;
+        }
+        if (*(volatile int*)&D->roots_done >= A.count) {
+          __threadfence();  // every slot taken before the last root is seen
+          ok = *(volatile int*)&D->search_count > t ? 1 : 0;
+          break;
+        }
+        __nanosleep(nap);
+        if (nap < 1024) nap <<= 1;
+      }
+      if (it == kW64QueueWait) atomicExch(&D->queue_error, 1);
+      if (ok) {
+        int k = 0;
+        while (!*(volatile int*)&ready[t] && k < kW64QueueWait) {
+          __nanosleep(64);
+          ++k;
+        }
+        if (k == kW64QueueWait) {
+          atomicExch(&D->queue_error, 1);
+          ok = 0;
+        }
+        __threadfence();
       }
     }
-    if (root.status == kOk) w64_write_outputs(A, g, n, vo);
-    __syncwarp();
-  }
-}
-
-__global__ void __launch_bounds__(kW64Threads, 8)
-    w64_search_kernel(BatchArgs A, Deferred* D, int* overflow_list, const uint8_t* roots,
-                      const int* search_list) {
-  const int warp = (int)(threadIdx.x >> 5);
-  const uint32_t lane = lane_id();
-  uint8_t* slot = A.work + ((uint64_t)blockIdx.x * kW64Warps + (uint64_t)warp) * A.slot_bytes;
-  // the classes from the most expensive down: lane q holds class 15 - q
-  const int cq = lane < (uint32_t)kW64CostClasses
-                     ? *(volatile int*)&D->cost_count[kW64CostClasses - 1 - (int)lane]
-                     : 0;
-  int incl = cq;
-  for (int o = 1; o < 32; o <<= 1) {
-    const int y = __shfl_up_sync(GCL_FULL, incl, o);
-    if (lane >= (uint32_t)o) incl += y;
-  }
-  const int total = __shfl_sync(GCL_FULL, incl, 31);
-  while (true) {
-    int i = 0;
-    if (lane == 0) i = atomicAdd(&D->next_search, 1);
-    i = __shfl_sync(GCL_FULL, i, 0);
-    if (i >= total) break;
-    // the class of entry i: the first lane whose inclusive count passes i
-    const int q = __ffs(__ballot_sync(GCL_FULL, incl > i)) - 1;
-    const int first = __shfl_sync(GCL_FULL, incl - cq, q);
-    const int slot_i = search_list[(int64_t)(kW64CostClasses - 1 - q) * A.count + (i - first)];
-    const uint8_t* root = roots + (uint64_t)slot_i * w64_root_slot_bytes();
+    ok = __shfl_sync(GCL_FULL, ok, 0);
+    if (!ok) break;
+    const uint8_t* root = roots + (uint64_t)t * w64_root_slot_bytes();
     const int g = w64_root_graph(root);
     const int64_t vo = A.voff[g];
     const int n = (int)(A.voff[g + 1] - vo);
     int code = 0;
     const uint64_t starts = w64_restore_root(root, n, &code);
     const W64Result r = w64_search_tree(A, n, starts, code, slot, w64_deadline(A));
-    if (lane == 0) {
-      A.status[g] = r.status;
-      if (A.out_stats) {
-        A.out_stats[2 * (int64_t)g] = r.num_aut;
-        A.out_stats[2 * (int64_t)g + 1] = r.nodes;
-      }
-      if (r.status == kAutOverflow) overflow_list[atomicAdd(&D->overflow_count, 1)] = g;
-    }
-    if (r.status == kOk) w64_write_outputs(A, g, n, vo);
-    __syncwarp();
+    w64_finish_search(A, D, overflow_list, g, n, vo, r);
   }
 }
 
@@ -360,7 +405,7 @@ struct gcl_context {
     DevBuf* bufs[] = {&work, &work_big, &sp_work_mid, &sp_work_big, &deferred, &wide_sh,
                       &wide_slots,
                       &overflow_list, &large_list, &sp_fail_list, &sp_fail_list2, &order,
-                      &roots, &search_list,
+                      &roots, &ready,
                       &voff, &eoff,
                       &rowptr, &col, &color, &ooff, &dense, &roff, &rows, &label, &stats,
                       &status};
@@ -398,8 +443,8 @@ struct gcl_context {
   cudaEvent_t tev[2][1 + kSpBuckets] = {};
   bool tev_used[1 + kSpBuckets] = {};
   DevBuf deferred, overflow_list, large_list, sp_fail_list, sp_fail_list2, order;
-  // the warp kernel's root pass -> search pass hand-over
-  DevBuf roots, search_list;
+  // the warp kernel's root slots and their ready flags (root -> search hand-over)
+  DevBuf roots, ready;
   // staging for host-pointer calls
   DevBuf voff, eoff, rowptr, col, color, ooff, dense, roff, rows, label, stats, status;
 };
@@ -588,7 +633,8 @@ int gcl_canon_batch_device_async(gcl_context* c, int count, const int64_t* d_vof
   GCL_TRY(c->order.ensure((size_t)count * sizeof(int)));
   if (max_n > 0) {
     GCL_TRY(c->roots.ensure((size_t)count * w64_root_slot_bytes()));
-    GCL_TRY(c->search_list.ensure((size_t)count * kW64CostClasses * sizeof(int)));
+    GCL_TRY(c->ready.ensure((size_t)count * sizeof(int)));
+    GCL_TRY(cudaMemsetAsync(c->ready.p, 0, (size_t)count * sizeof(int), c->stream));
   }
   GCL_TRY(cudaMemsetAsync(c->deferred.p, 0, sizeof(Deferred), c->stream));
   order_by_size_kernel<<<1, kOrderThreads, 0, c->stream>>>(count, d_voff, (int*)c->order.p);
@@ -625,15 +671,12 @@ int gcl_canon_batch_device_async(gcl_context* c, int count, const int64_t* d_vof
     GCL_TRY(cudaEventRecord(c->tev[0][0], c->stream));
   }
   if (max_n > 0) {
-    // root pass, then the search pass over the graphs whose root is not
-    // discrete
-    w64_root_kernel<<<grid1, kW64Threads, 0, c->stream>>>(A, D, (int*)c->large_list.p,
+    // root refinements, then the searches below the roots that are not
+    // discrete, in one launch
+    w64_pipe_kernel<<<grid1, kW64Threads, 0, c->stream>>>(A, D, (int*)c->large_list.p,
+                                                          (int*)c->overflow_list.p,
                                                           (uint8_t*)c->roots.p,
-                                                          (int*)c->search_list.p);
-    GCL_TRY(cudaGetLastError());
-    w64_search_kernel<<<grid1, kW64Threads, 0, c->stream>>>(A, D, (int*)c->overflow_list.p,
-                                                            (const uint8_t*)c->roots.p,
-                                                            (const int*)c->search_list.p);
+                                                          (int*)c->ready.p);
   } else {
     // a batch of empty graphs (max_n 0): one pass, no hand-over buffers
     w64_batch_kernel<<<grid1, kW64Threads, 0, c->stream>>>(A, D, (int*)c->overflow_list.p,
