@@ -24,10 +24,15 @@
 //     against the first leaf (sequential.cpp:127-167) becomes certificate
 //     equality, which is the same predicate for a bijection.
 //
-// Code layout: the warp's state lives in shared memory between phases and
-// each phase (refine, individualize, backtrack, orbits, leaf work) is one
-// non-inlined function, so the hot instruction footprint stays small enough
-// for the instruction caches when many warps per SM sit in different phases.
+// Code layout: the warp's state lives in shared memory between phases.  The
+// root step (load and root refinement), the search below the root, the root
+// hand-over and the output writer are non-inlined functions, so an SM's warps
+// share a small instruction footprint across those stages; the per-node
+// phases (refine, individualize, backtrack, orbits, leaf work) are inlined
+// into them.  Timed on the batched small-graph workload: inlining the
+// per-node phases cut the pipelined launch by 13% (calls cost register
+// saves and restores through local memory on every node), while inlining the
+// root step or the whole search as well made it slower again.
 #pragma once
 #include <cstdint>
 
@@ -147,7 +152,7 @@ struct W64Refined {
   int ok;
 };
 
-static __device__ __noinline__ W64Refined w64_refine(int n, uint64_t starts, uint32_t level,
+static __device__ __forceinline__ W64Refined w64_refine(int n, uint64_t starts, uint32_t level,
                                                      uint64_t active) {
   W64Smem& S = w64_smem();
   const uint32_t lane = lane_id();
@@ -399,7 +404,7 @@ static __device__ __noinline__ W64Refined w64_refine(int n, uint64_t starts, uin
 // split_by_and_refine's split (partition_refinement.cpp:486-528): vertex v
 // moves to a singleton cell at t, the rest of the cell starts at t+1.
 // Returns false when the cell is already a singleton (nothing to refine).
-static __device__ __noinline__ bool w64_individualize(int n, uint32_t level, uint32_t v, uint32_t t) {
+static __device__ __forceinline__ bool w64_individualize(int n, uint32_t level, uint32_t v, uint32_t t) {
   W64Smem& S = w64_smem();
   const uint32_t lane = lane_id();
   const uint64_t mem = S.cmask[t];
@@ -430,7 +435,7 @@ static __device__ __noinline__ bool w64_individualize(int n, uint32_t level, uin
 // of cells created after level Lv merges with the cell that follows it, and
 // the merged cell takes that cell's in_level.  Returns the new starts mask
 // (0 if the partition is inconsistent).
-static __device__ __noinline__ uint64_t w64_backtrack(int n, uint64_t starts, uint32_t Lv) {
+static __device__ __forceinline__ uint64_t w64_backtrack(int n, uint64_t starts, uint32_t Lv) {
   W64Smem& S = w64_smem();
   const uint32_t lane = lane_id();
   const uint32_t q0 = lane, q1 = lane + 32;
@@ -507,7 +512,7 @@ struct Rows2 {
   uint64_t r0, r1;
 };
 
-static __device__ __noinline__ Rows2 w64_leaf_rows(int n) {
+static __device__ __forceinline__ Rows2 w64_leaf_rows(int n) {
   W64Smem& S = w64_smem();
   const uint32_t lane = lane_id();
   Rows2 R{0ull, 0ull};
@@ -529,7 +534,7 @@ static __device__ __noinline__ Rows2 w64_leaf_rows(int n) {
 }
 
 // compare_adj_upper(current, stored) (sequential.cpp:114-124)
-static __device__ __noinline__ int w64_cmp_upper(int n, Rows2 R, const uint64_t* B) {
+static __device__ __forceinline__ int w64_cmp_upper(int n, Rows2 R, const uint64_t* B) {
   W64Smem& S = w64_smem();
   const uint32_t lane = lane_id();
   uint32_t row = 64u;
@@ -565,7 +570,7 @@ __device__ __forceinline__ bool w64_rows_equal(int n, Rows2 R, const uint64_t* B
 }
 
 // Rows into a stored certificate and the vertex positions into `pos`.
-static __device__ __noinline__ void w64_store_leaf(int n, Rows2 R, uint64_t* B, uint8_t* pos) {
+static __device__ __forceinline__ void w64_store_leaf(int n, Rows2 R, uint64_t* B, uint8_t* pos) {
   W64Smem& S = w64_smem();
   const uint32_t lane = lane_id();
   __syncwarp();
@@ -583,7 +588,7 @@ static __device__ __noinline__ void w64_store_leaf(int n, Rows2 R, uint64_t* B, 
 // aut[label[j]] = elem[j] with the stored leaf given by its vertex positions
 // (sequential.cpp:505-520, 544-555), written to one ring slot; its mask of
 // fixed points goes to *fix.
-static __device__ __noinline__ void w64_store_aut(int n, const uint8_t* pos, uint8_t* dst,
+static __device__ __forceinline__ void w64_store_aut(int n, const uint8_t* pos, uint8_t* dst,
                                                   uint64_t* fix) {
   W64Smem& S = w64_smem();
   const uint32_t lane = lane_id();
@@ -656,7 +661,7 @@ __device__ __forceinline__ void w64_select_tc(int n, uint64_t starts, int tcl) {
 // vertex's old parent under it (atomicMin), and shortcuts parents twice; a
 // round that improves no label ends it, and then every vertex points at the
 // least vertex of its component.  Returns false when the round bound was hit.
-static __device__ __noinline__ bool w64_orbits(int n, int idx, int num_aut, uint32_t max_aut,
+static __device__ __forceinline__ bool w64_orbits(int n, int idx, int num_aut, uint32_t max_aut,
                                                uint32_t seqlen, uint8_t* reps, const uint8_t* auts,
                                                const uint64_t* fixes) {
   W64Smem& S = w64_smem();
