@@ -67,56 +67,50 @@ constexpr int kOrderThreads = 1024;
 __global__ void __launch_bounds__(kOrderThreads)
     order_by_size_kernel(int count, const int64_t* voff, int* order) {
   constexpr int kBins = kW64MaxN + 2;  // n = 0..64, and every n > 64 in the last bin
+  constexpr int kPer = 8;              // graphs per thread and chunk, loaded before use
   __shared__ int hist[kBins];
   __shared__ int start[kBins];
-  const uint32_t lane = lane_id();
   for (int b = threadIdx.x; b < kBins; b += blockDim.x) hist[b] = 0;
   __syncthreads();
-  // the lanes of a warp with the same bin add to it once (match_any groups)
-  const int rounds = (count + (int)blockDim.x - 1) / (int)blockDim.x;
-  auto bin_of = [&](int g) {
-    if (g >= count) return -1;
-    const int64_t n = voff[g + 1] - voff[g];
-    return n > kW64MaxN ? kW64MaxN + 1 : (int)n;
+  const int chunk = (int)blockDim.x * kPer;
+  // a thread's graphs of a chunk: every size is read before the first is
+  // counted, so the reads overlap instead of waiting on each other
+  auto bins = [&](int base, int (&bn)[kPer]) {
+    int64_t a[kPer], b[kPer];
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+      const int g = base + k * (int)blockDim.x + (int)threadIdx.x;
+      a[k] = g < count ? voff[g] : 0;
+      b[k] = g < count ? voff[g + 1] : -1;
+    }
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+      const int64_t n = b[k] - a[k];
+      bn[k] = n < 0 ? -1 : (n > kW64MaxN ? kW64MaxN + 1 : (int)n);
+    }
   };
-  for (int r = 0; r < rounds; ++r) {
-    const int b = bin_of(r * (int)blockDim.x + (int)threadIdx.x);
-    const uint32_t grp = __match_any_sync(GCL_FULL, b);
-    if (b >= 0 && lane == (uint32_t)(__ffs(grp) - 1)) atomicAdd(&hist[b], __popc(grp));
+  for (int base = 0; base < count; base += chunk) {
+    int bn[kPer];
+    bins(base, bn);
+#pragma unroll
+    for (int k = 0; k < kPer; ++k)
+      if (bn[k] >= 0) atomicAdd(&hist[bn[k]], 1);
   }
   __syncthreads();
-  // starts, largest bin first: warp 0, lane l sums bins 65 - 3l .. 63 - 3l
-  if (threadIdx.x < 32) {
-    int h[3], sum = 0;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      const int b = kBins - 1 - (3 * (int)lane + k);
-      h[k] = b >= 0 ? hist[b] : 0;
-      sum += h[k];
-    }
-    int incl = sum;
-    for (int o = 1; o < 32; o <<= 1) {
-      const int y = __shfl_up_sync(GCL_FULL, incl, o);
-      if (lane >= (uint32_t)o) incl += y;
-    }
-    int run = incl - sum;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      const int b = kBins - 1 - (3 * (int)lane + k);
-      if (b >= 0) start[b] = run;
-      run += h[k];
+  if (threadIdx.x == 0) {  // starts, largest bin first
+    int run = 0;
+    for (int b = kBins - 1; b >= 0; --b) {
+      start[b] = run;
+      run += hist[b];
     }
   }
   __syncthreads();
-  for (int r = 0; r < rounds; ++r) {
-    const int g = r * (int)blockDim.x + (int)threadIdx.x;
-    const int b = bin_of(g);
-    const uint32_t grp = __match_any_sync(GCL_FULL, b);
-    const int leader = __ffs(grp) - 1;
-    int base = 0;
-    if (b >= 0 && lane == (uint32_t)leader) base = atomicAdd(&start[b], __popc(grp));
-    base = __shfl_sync(GCL_FULL, base, leader);
-    if (b >= 0) order[base + __popc(grp & ((1u << lane) - 1u))] = g;
+  for (int base = 0; base < count; base += chunk) {
+    int bn[kPer];
+    bins(base, bn);
+#pragma unroll
+    for (int k = 0; k < kPer; ++k)
+      if (bn[k] >= 0) order[atomicAdd(&start[bn[k]], 1)] = base + k * (int)blockDim.x + (int)threadIdx.x;
   }
 }
 
