@@ -941,7 +941,7 @@ __device__ __noinline__ int sp_refine(uint32_t level) {
 }
 
 // split_by_and_refine's split (partition_refinement.cpp:486-528)
-__device__ __noinline__ bool sp_individualize(uint32_t level, uint32_t v, uint32_t t) {
+__device__ __forceinline__ bool sp_individualize(uint32_t level, uint32_t v, uint32_t t) {
   SpWarp& W = sp_w();
   const uint32_t lane = lane_id();
   const uint32_t e = sp_cell_end(W, t);
@@ -1104,7 +1104,7 @@ __device__ __noinline__ bool sp_backtrack(uint32_t Lv) {
 // start created below Lv is cleared, and every in_level changed below Lv
 // returns to the value before its first change (entries are processed in
 // parallel: per position the earliest entry wins).
-__device__ __noinline__ bool sp_backtrack_log(uint32_t Lv) {
+__device__ __forceinline__ bool sp_backtrack_log(uint32_t Lv) {
   SpWarp& W = sp_w();
   const uint32_t lane = lane_id();
   if (W.ulog_bad) {
@@ -1157,7 +1157,7 @@ __device__ __noinline__ bool sp_backtrack_log(uint32_t Lv) {
 // ---- leaves ----------------------------------------------------------------
 // Certificate of a discrete partition: for every vertex, the canonical
 // positions of its neighbours in ascending order, stored at its CSR offset.
-__device__ __noinline__ void sp_leaf_cert(uint32_t* cert) {
+__device__ __forceinline__ void sp_leaf_cert(uint32_t* cert) {
   SpWarp& W = sp_w();
   const uint32_t lane = lane_id();
   for (uint32_t v = lane; v < W.n; v += 32) {
@@ -1180,7 +1180,7 @@ __device__ __noinline__ void sp_leaf_cert(uint32_t* cert) {
 // row order.  upper: compare_adj_upper (entries right of the diagonal,
 // sequential.cpp:114-124); otherwise full-row equality.  Returns -1/0/+1.
 template <bool kCg = false>
-__device__ __noinline__ int sp_cmp_leaf(const uint32_t* cur, const uint32_t* label,
+__device__ __forceinline__ int sp_cmp_leaf(const uint32_t* cur, const uint32_t* label,
                                         const uint32_t* cert2, bool upper) {
   SpWarp& W = sp_w();
   const uint32_t lane = lane_id();
@@ -1224,14 +1224,14 @@ __device__ __noinline__ int sp_cmp_leaf(const uint32_t* cur, const uint32_t* lab
   return 0;
 }
 
-__device__ __noinline__ void sp_copy_u32(uint32_t* dst, const uint32_t* src, uint32_t k) {
+__device__ __forceinline__ void sp_copy_u32(uint32_t* dst, const uint32_t* src, uint32_t k) {
   const uint32_t lane = lane_id();
   for (uint32_t i = lane; i < k; i += 32) dst[i] = src[i];
   __syncwarp();
 }
 
 // get_gca_level (sequential.cpp:183-213)
-__device__ __noinline__ int sp_gca(const uint32_t* a, uint32_t na, uint32_t seqlen) {
+__device__ __forceinline__ int sp_gca(const uint32_t* a, uint32_t na, uint32_t seqlen) {
   SpWarp& W = sp_w();
   const uint32_t lane = lane_id();
   const uint32_t m = min(na, seqlen);
@@ -1244,7 +1244,7 @@ __device__ __noinline__ int sp_gca(const uint32_t* a, uint32_t na, uint32_t seql
 }
 
 // first non-singleton cell (target_cell_selector, partition_refinement.cpp:607-655)
-__device__ __noinline__ uint32_t sp_first_nonsingleton() {
+__device__ __forceinline__ uint32_t sp_first_nonsingleton() {
   SpWarp& W = sp_w();
   const uint32_t lane = lane_id();
   const uint32_t n = W.n, nw = (n + 63) / 64;
@@ -1272,7 +1272,7 @@ __device__ __noinline__ uint32_t sp_first_nonsingleton() {
 
 // next representative of target cell idx: smallest vertex >= counter among
 // its members whose representative is itself (sequential.cpp:359-361)
-__device__ __noinline__ uint32_t sp_next_rep(const SpTc& t) {
+__device__ __forceinline__ uint32_t sp_next_rep(const SpTc& t) {
   SpWarp& W = sp_w();
   const uint32_t lane = lane_id();
   const uint32_t* reps = t.rslot >= 0 ? W.reps + (uint64_t)t.rslot * W.stride : nullptr;
@@ -1299,7 +1299,7 @@ __device__ __forceinline__ uint32_t sp_find(volatile uint32_t* d, uint32_t x, ui
 // nothing (compute_orbits_fast's DSU, perm_group.cpp:60-116).  pm must map
 // the member set onto itself.  False if the rounds do not converge.
 template <bool kCg>
-__device__ __noinline__ bool sp_dsu_apply(const uint16_t* pm, const uint32_t* members,
+__device__ __forceinline__ bool sp_dsu_apply(const uint16_t* pm, const uint32_t* members,
                                           uint32_t count, uint32_t n) {
   SpWarp& W = sp_w();
   const uint32_t lane = lane_id();
@@ -1334,7 +1334,7 @@ __device__ __noinline__ bool sp_dsu_apply(const uint16_t* pm, const uint32_t* me
 // uniting over the cell's members alone (O(cell) per automorphism instead of
 // O(n)); the least vertex of each orbit -- the representative -- is the same.
 template <bool kCg = false>
-__device__ __noinline__ bool sp_orbits(int idx, int num_aut, uint32_t seqlen) {
+__device__ __forceinline__ bool sp_orbits(int idx, int num_aut, uint32_t seqlen) {
   SpWarp& W = sp_w();
   const uint32_t lane = lane_id();
   const uint32_t n = W.n;
@@ -1436,7 +1436,7 @@ __device__ __noinline__ bool sp_orbits(int idx, int num_aut, uint32_t seqlen) {
 
 // After a backtrack to sequence length s: positions >= s of the sequence
 // change, so what entries [0, count) knew about them is dropped.
-__device__ __noinline__ void sp_fix_clamp(uint32_t s, uint32_t count) {
+__device__ __forceinline__ void sp_fix_clamp(uint32_t s, uint32_t count) {
   SpWarp& W = sp_w();
   count = min(count, W.fixcap);
   for (uint32_t a = lane_id(); a < count; a += 32) {
@@ -1451,7 +1451,7 @@ __device__ __noinline__ void sp_fix_clamp(uint32_t s, uint32_t count) {
 }
 
 // aut[label[j]] = elem[j] (sequential.cpp:505-520, 544-555)
-__device__ __noinline__ void sp_store_aut(const uint32_t* label, uint16_t* dst) {
+__device__ __forceinline__ void sp_store_aut(const uint32_t* label, uint16_t* dst) {
   SpWarp& W = sp_w();
   const uint32_t lane = lane_id();
   for (uint32_t j = lane; j < W.n; j += 32) dst[label[j]] = (uint16_t)W.elem[j];
