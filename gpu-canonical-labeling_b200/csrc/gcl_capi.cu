@@ -57,7 +57,6 @@ struct Deferred {
   int search_count;    // root slots handed to the search queue
   int next_search;     // tickets of the search queue
   int roots_done;      // graphs whose root step is over
-  int queue_error;     // a wait of the search queue ran out
 };
 
 // Largest graphs first: a counting sort of the graph ids by descending n
@@ -339,17 +338,13 @@ __global__ void __launch_bounds__(kW64Threads, 6)
         __nanosleep(nap);
         if (nap < 1024) nap <<= 1;
       }
-      if (it == kW64QueueWait) atomicExch(&D->queue_error, 1);
       if (ok) {
         int k = 0;
         while (!*(volatile int*)&ready[t] && k < kW64QueueWait) {
           __nanosleep(64);
           ++k;
         }
-        if (k == kW64QueueWait) {
-          atomicExch(&D->queue_error, 1);
-          ok = 0;
-        }
+        if (k == kW64QueueWait) ok = 0;  // the slot's graph keeps its internal-error status
         __threadfence();
       }
     }
