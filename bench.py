@@ -76,7 +76,7 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-sustained", action="store_true",
                    help="skip the one-second repeat of the step that samples clocks")
-    p.add_argument("--e2e-contexts", type=int, default=2,
+    p.add_argument("--e2e-contexts", type=int, default=4,
                    help="e2e with this many contexts on host threads, so one call's copies "
                         "and search tail run under another call's kernels (1 = one call "
                         "at a time)")
